@@ -1,0 +1,176 @@
+/*
+ * qmtools_b200.h -- C ABI of libqmtools_b200.so, the sm_100a implementation of the
+ * QMTools grid hot path (electron density, Hartree potential, nuclear terms).
+ *
+ * The reference (fullmetalfelix/QMTools-pycuda) has no native ABI: its Python facade
+ * `QMTools` (qmtools/qmtools.py:2320-2831) JIT-compiles CUDA C with PyCUDA and launches
+ * kernels with `prepared_call`.  Each entry point below replaces one of those facade
+ * methods (or the kernel it launches); the citation on each line names it.
+ *
+ * Conventions
+ *   - Plain pointers and sizes only.  Pointers named *_dev are device pointers; every
+ *     other pointer is host memory and is copied in before the call returns.
+ *   - Grids are float32, x-fastest (idx = x + y*nx + z*nx*ny), the reference layout
+ *     (qmtools/cuda/kernel_density.cu:151-154).  Lengths in bohr unless stated.
+ *   - `stream` is a cudaStream_t passed as void* (NULL = legacy default stream).
+ *     Calls are asynchronous on that stream unless they return a host scalar.
+ *   - Every function returns a qmt_status; qmt_last_error() gives a message for the
+ *     last failure on the calling thread.  Nothing exits or aborts.
+ *   - A qmt_mol handle owns its device memory; qmt_mol_destroy frees it.  Handles may be
+ *     used from different host threads as long as one handle is not used concurrently.
+ */
+#ifndef QMTOOLS_B200_H
+#define QMTOOLS_B200_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+typedef int qmt_status;
+enum {
+  QMT_OK = 0,
+  QMT_BAD_ARG = 1,        /* invalid argument or shape                         */
+  QMT_OOM = 2,            /* device allocation failed                          */
+  QMT_NOT_CONVERGED = 3,  /* iterative solver stopped at its sweep cap         */
+  QMT_NAN = 4,            /* non-finite value in an input or a result          */
+  QMT_UNSUPPORTED_L = 5,  /* basis shell with angular momentum > 2             */
+  QMT_CUDA_ERR = 6,       /* CUDA runtime error                                */
+  QMT_NO_DEVICE = 7       /* no usable sm_100 device                           */
+};
+
+/* Precision of the density contraction T = Phi * P (row-dot and sums stay FP32/FP64). */
+enum {
+  QMT_PREC_FP64 = 0,      /* SIMT FP64                                                  */
+  QMT_PREC_FP32 = 1,      /* SIMT FP32 (the plain path)                                 */
+  QMT_PREC_TF32 = 2,      /* tcgen05 kind::tf32, one product                            */
+  QMT_PREC_TF32X3 = 3,    /* tcgen05 kind::tf32, hi/lo split, 3 products                */
+  QMT_PREC_BF16 = 4,      /* tcgen05 kind::f16 (bf16), one product                      */
+  QMT_PREC_BF16X3 = 5,    /* tcgen05 kind::f16 (bf16), hi/lo split, 3 products          */
+  QMT_PREC_FP16X3 = 6     /* tcgen05 kind::f16 (fp16), power-of-two scaled hi/lo split, */
+                          /* 3 products                                                 */
+};
+
+typedef struct qmt_mol qmt_mol;
+
+/* ---- library ------------------------------------------------------------------------ */
+const char* qmt_last_error(void);
+int qmt_abi_version(void);
+/* Selects the device for this host thread and checks it is sm_100. */
+qmt_status qmt_init(int device);
+
+/* ---- molecule (BasisSet + Molecule device upload) ------------------------------------ */
+/* Replaces the uploads of BasisSet.__init__ (qmtools/qmtools.py:97-103) and
+ * Molecule.__init__ (qmtools/qmtools.py:174-178).  Inputs are the reference's own host
+ * arrays: types[natoms] int32, coords[natoms*3] float32 bohr, almos[norbs*4] int16
+ * (atom, L, m, shellOffset), alphas/coeffs[nparams] float32 padded to 20 per shell,
+ * dm[norbs*norbs] float32 row-major.  Only the lower triangle p >= q of dm is read,
+ * as the reference kernels do (kernel_density.cu:87, kernel_hartree.cu:353). */
+qmt_status qmt_mol_create(int natoms, const int32_t* types, const float* coords,
+                          int norbs, const int16_t* almos,
+                          int nparams, const float* alphas, const float* coeffs,
+                          const float* dm, void* stream, qmt_mol** out);
+/* Molecule.Translate upload (qmtools/qmtools.py:182-188): new coords[natoms*3] bohr. */
+qmt_status qmt_mol_set_coords(qmt_mol* mol, const float* coords, void* stream);
+/* New density matrix (same norbs). */
+qmt_status qmt_mol_set_dm(qmt_mol* mol, const float* dm, void* stream);
+qmt_status qmt_mol_destroy(qmt_mol* mol);
+/* FP64 Tr(P S) with the analytic overlap S, computed on the device (new; no reference
+ * counterpart -- the electron count the density grid must integrate to, before x2). */
+qmt_status qmt_mol_trace_ps(qmt_mol* mol, double* trace_out, void* stream);
+
+/* ---- density -------------------------------------------------------------------------- */
+/* QMTools.Compute_density (qmtools/qmtools.py:2381-2430) with gpu_densityqube_shmem_subgrid
+ * (kernel_density.cu:34-155): q_v = 2 h^3 s^-3 sum_sub sum_pq P_pq phi_p phi_q at voxel-centre
+ * sub-points, into qube_dev[nx*ny*nz].  If rescale != 0 the grid is then scaled so that its
+ * sum equals the total nuclear charge (qmtools/qmtools.py:2419-2424).  sum_out (host, may be
+ * NULL) receives the FP64 sum before rescaling.  Blocks until sum_out is written. */
+qmt_status qmt_density(qmt_mol* mol, int nx, int ny, int nz, float step,
+                       float ox, float oy, float oz, int subgrid, int precision,
+                       int rescale, float* qube_dev, double* sum_out, void* stream);
+
+/* ---- analytic GTO potential --------------------------------------------------------- */
+/* QMTools.Compute_hartree (qmtools/qmtools.py:2436-2489) with gpu_hartree_GTO
+ * (kernel_hartree.cu:288-869): V(C) = -2 sum_pq P_pq (phi_p phi_q | 1/|r-C|) + sum_A Z_A/|C-R_A|
+ * at voxel corners C = origin + i h, written into v_dev[nx*ny*nz] (a.u.). */
+qmt_status qmt_hartree_gto(qmt_mol* mol, int nx, int ny, int nz, float step,
+                           float ox, float oy, float oz, float* v_dev, void* stream);
+/* Same potential at npts arbitrary points pts_dev[npts*3] (bohr); used for Dirichlet
+ * boundaries.  New entry point. */
+qmt_status qmt_hartree_gto_points(qmt_mol* mol, int npts, const float* pts_dev,
+                                  float* v_dev, void* stream);
+/* Same potential on the outer shell of an nx*ny*nz grid at voxel centres
+ * origin + (i + 1/2) h, written into those voxels of v_dev (interior untouched); the
+ * Dirichlet boundary of qmt_jacobi_dirichlet.  New entry point. */
+qmt_status qmt_hartree_gto_boundary(qmt_mol* mol, int nx, int ny, int nz, float step,
+                                    float ox, float oy, float oz, float* v_dev, void* stream);
+
+/* ---- Jacobi relaxation ---------------------------------------------------------------- */
+/* QMTools.Compute_hartree_iter (qmtools/qmtools.py:2497-2573) with gpu_hartree_iteration
+ * (kernel_hartree.cu:85-171): sweeps V' = (sum of 6 neighbours - Q/h)/6 with a zero outer
+ * shell, Q = rho_dev.  v_dev holds the start value and receives the result; t_dev is a
+ * scratch grid of the same size.  Every check_every sweep pairs the FP64 sum |V - T| is
+ * compared with tol (the reference checks every 100 pairs); the solve stops there or at
+ * max_sweeps (returning QMT_NOT_CONVERGED).  sweeps_out/delta_out are host, may be NULL. */
+qmt_status qmt_jacobi(int nx, int ny, int nz, float step, const float* rho_dev,
+                      float* v_dev, float* t_dev, int max_sweeps, int check_every,
+                      double tol, int* sweeps_out, double* delta_out, void* stream);
+/* Physical-unit Jacobi (new): lap V = -4 pi rho (a.u.), Dirichlet values taken from the
+ * outer shell of v_dev (e.g. from qmt_hartree_gto_points), interior start value from v_dev.
+ * Same stopping rule; FP64 residual norm. */
+qmt_status qmt_jacobi_dirichlet(int nx, int ny, int nz, float step, const float* rho_dev,
+                                float* v_dev, float* t_dev, int max_sweeps, int check_every,
+                                double tol, int* sweeps_out, double* delta_out, void* stream);
+
+/* ---- FFT Poisson ---------------------------------------------------------------------- */
+/* QMTools.Compute_hartree_fft (qmtools/qmtools.py:2578-2639) with gpu_add_nuclear_charge
+ * (kernel_fft.cu:23-79) and gpu_poisson_frequency_solve (kernel_fft.cu:82-107).
+ * q_dev: electron grid (x-fastest).  out_dev receives the potential in volts, C-order
+ * (i*ny*nz + j*nz + k) like the reference's returned array.
+ * padded = 0: the reference's periodic solve; padded = 1: free-space solve on a zero-padded
+ * grid of at least 2n per axis with the Hockney Green's function (new). */
+qmt_status qmt_fft_poisson(qmt_mol* mol, int nx, int ny, int nz, float step,
+                           float ox, float oy, float oz, float sigma, float cutoff,
+                           int padded, const float* q_dev, float* out_dev, void* stream);
+
+/* ---- grid utilities and nuclear fields ----------------------------------------------- */
+/* QMTools.Compute_qtot / gpu_total (qmtools/qmtools.py:2796-2803, kernel_utils.cu:68-98),
+ * deterministic FP64 sum of n floats. */
+qmt_status qmt_grid_total(const float* q_dev, int64_t n, double* out, void* stream);
+/* QMTools.Compute_qscale / gpu_rescale (qmtools/qmtools.py:2808-2813, kernel_utils.cu:54-65). */
+qmt_status qmt_grid_scale(float* q_dev, int64_t n, float factor, void* stream);
+/* QMTools.Compute_qdiff / gpu_qdiff(_rel) (qmtools/qmtools.py:2818-2831,
+ * kernel_utils.cu:101-167): sum |a-b|, or 100*sum |a-b|/b when rel != 0. */
+qmt_status qmt_grid_diff(const float* a_dev, const float* b_dev, int64_t n, int rel,
+                         double* out, void* stream);
+/* Error report (new): max |a-b|, ||a-b||_2/||b||_2, sum a, sum b, all FP64; out[4]. */
+qmt_status qmt_grid_errors(const float* a_dev, const float* b_dev, int64_t n,
+                           double* out4, void* stream);
+/* QMTools.Compute_qseed / gpu_density_seed (qmtools/qmtools.py:2645-2672,
+ * kernel_utils.cu:5-50) into q_dev (not cleared first, like the reference). */
+qmt_status qmt_density_seed(qmt_mol* mol, int nx, int ny, int nz, float step,
+                            float ox, float oy, float oz, float* q_dev, void* stream);
+/* sum_A Z_A/|r - R_A| at voxel centres (gpu_hartree_add_nuclei, kernel_hartree.cu:209-251),
+ * added into v_dev when accumulate != 0, else stored. */
+qmt_status qmt_vne_point(qmt_mol* mol, int nx, int ny, int nz, float step,
+                         float ox, float oy, float oz, int accumulate, float* v_dev,
+                         void* stream);
+/* QMTools.Compute_VNe_classic / gpu_vne_classic (qmtools/qmtools.py:2750-2790,
+ * kernel_vne_classic.cu:13-84). */
+qmt_status qmt_vne_classic(qmt_mol* mol, int nx, int ny, int nz, float step,
+                           float ox, float oy, float oz, int divisions, float* v_dev,
+                           void* stream);
+/* QMTools.Compute_VNe / gpu_vne (qmtools/qmtools.py:2677-2745, kernel_vne.cu:13-128):
+ * ping-pong pseudo-field; res_dev receives the field, out_dev is scratch; both are cleared
+ * first.  Stops when the mean |delta| of a pair falls to tol or after maxiters pairs. */
+qmt_status qmt_vne_pseudo(qmt_mol* mol, int nx, int ny, int nz, float step,
+                          float ox, float oy, float oz, float ads, float dif, double tol,
+                          int maxiters, float* res_dev, float* out_dev, int* iters_out,
+                          void* stream);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* QMTOOLS_B200_H */

@@ -1,0 +1,623 @@
+// Tensor-core density path (sm_100a, tcgen05 + TMA).
+//
+//   stage:  basis_stage_kernel evaluates Phi' = Phi * 2^s_j (power-of-two column scales)
+//           for 128-row tiles of sample points and writes it as operand pieces
+//           hi = fmt(Phi'), lo = fmt(Phi' - hi) to HBM, row-major [row][kpad].
+//   mma:    density_mma_kernel, one CTA per SM, warp-specialised:
+//             warp 0      TMA producer: A (Phi' pieces, 128 x 64B..128B K-chunks) and
+//                         B (scaled density-matrix pieces) into a shared-memory ring;
+//             warp 1      tcgen05.mma issuer (one thread); T' = Phi' * Ptilde accumulated
+//                         in TMEM, two 256-column accumulator buffers;
+//             warps 2..5  epilogue: tcgen05.ld of T' rows, row-dot with Phi' (FP64
+//                         accumulation), sub-point average, grid write, FP64 tile sums.
+//   With Ptilde_jk = P_jk 2^(g - s_j - s_k):  rho_i = 2^-g sum_j Phi'_ij T'_ij.
+//   Split products (3 terms) hi*hi + hi*lo + lo*hi recover ~22 significant bits for fp16
+//   pieces (scaled to stay in the normal range) and tf32, ~16 bits for bf16.
+//
+// Replaces the per-voxel pair loop of gpu_densityqube_shmem_subgrid (kernel_density.cu:74-140).
+#include <cuda.h>
+#include <cuda_bf16.h>
+#include <cuda_fp16.h>
+#include <cudaTypedefs.h>
+
+#include <algorithm>
+#include <cstring>
+
+#include "density.cuh"
+#include "reduce.cuh"
+#include "sm100.cuh"
+
+namespace qmt {
+using namespace sm100;
+
+enum { FMT_F16 = 0, FMT_BF16 = 1, FMT_TF32 = 2 };
+
+struct TcShape {
+  int fmt, nsplit, esize, ke, kpad, npanels, pw, nrows_b;
+};
+
+static TcShape tc_shape(int prec, int norbs) {
+  TcShape t{};
+  switch (prec) {
+    case QMT_PREC_TF32: t.fmt = FMT_TF32; t.nsplit = 1; break;
+    case QMT_PREC_TF32X3: t.fmt = FMT_TF32; t.nsplit = 2; break;
+    case QMT_PREC_BF16: t.fmt = FMT_BF16; t.nsplit = 1; break;
+    case QMT_PREC_BF16X3: t.fmt = FMT_BF16; t.nsplit = 2; break;
+    default: t.fmt = FMT_F16; t.nsplit = 2; break;
+  }
+  t.esize = t.fmt == FMT_TF32 ? 4 : 2;
+  t.ke = 128 / t.esize;
+  t.kpad = (norbs + 63) / 64 * 64;
+  t.npanels = (t.kpad + 255) / 256;
+  t.pw = ((t.kpad + t.npanels - 1) / t.npanels + 15) / 16 * 16;
+  t.nrows_b = t.npanels * t.pw;
+  return t;
+}
+
+// ---- element conversions (host and device) ------------------------------------------
+__host__ __device__ inline uint32_t tf32_round_bits(float x) {
+  uint32_t u;
+#ifdef __CUDA_ARCH__
+  u = __float_as_uint(x);
+#else
+  std::memcpy(&u, &x, 4);
+#endif
+  if ((u & 0x7f800000u) == 0x7f800000u) return u;
+  u += 0xfffu + ((u >> 13) & 1u);
+  return u & 0xffffe000u;
+}
+__host__ __device__ inline float bits_f32(uint32_t u) {
+#ifdef __CUDA_ARCH__
+  return __uint_as_float(u);
+#else
+  float f;
+  std::memcpy(&f, &u, 4);
+  return f;
+#endif
+}
+
+template <int FMT>
+__device__ __forceinline__ void split_store(float x, void* hi, void* lo, int64_t idx, bool two) {
+  if constexpr (FMT == FMT_TF32) {
+    const uint32_t h = tf32_round_bits(x);
+    reinterpret_cast<uint32_t*>(hi)[idx] = h;
+    if (two) reinterpret_cast<uint32_t*>(lo)[idx] = tf32_round_bits(x - bits_f32(h));
+  } else if constexpr (FMT == FMT_F16) {
+    const __half h = __float2half_rn(x);
+    reinterpret_cast<__half*>(hi)[idx] = h;
+    if (two) reinterpret_cast<__half*>(lo)[idx] = __float2half_rn(x - __half2float(h));
+  } else {
+    const __nv_bfloat16 h = __float2bfloat16_rn(x);
+    reinterpret_cast<__nv_bfloat16*>(hi)[idx] = h;
+    if (two) reinterpret_cast<__nv_bfloat16*>(lo)[idx] = __float2bfloat16_rn(x - __bfloat162float(h));
+  }
+}
+
+// ---------------------------------------------------------------------------------------
+// Stage 1: basis functions of 128-row tiles into operand pieces.
+// ---------------------------------------------------------------------------------------
+template <int FMT>
+__global__ void __launch_bounds__(256) basis_stage_kernel(MolView mol, PointMap pm, int64_t tile0,
+                                                          int ntiles, int kpad,
+                                                          const float* __restrict__ fscale,
+                                                          void* __restrict__ out_hi,
+                                                          void* __restrict__ out_lo, int two) {
+  constexpr int ROWS = 128, CW = 64;
+  __shared__ float buf[ROWS][CW + 1];
+  __shared__ double pts[ROWS][3];
+  __shared__ int srange[2];
+  for (int t = blockIdx.x; t < ntiles; t += gridDim.x) {
+    const int64_t tile = tile0 + t;
+    __syncthreads();
+    if (threadIdx.x < ROWS) {
+      double x, y, z;
+      int64_t vox;
+      if (!tile_point<double>(pm, tile, threadIdx.x, x, y, z, vox)) x = y = z = 1e30;
+      pts[threadIdx.x][0] = x;
+      pts[threadIdx.x][1] = y;
+      pts[threadIdx.x][2] = z;
+    }
+    for (int w0 = 0; w0 < kpad; w0 += CW) {
+      for (int i = threadIdx.x; i < ROWS * CW; i += blockDim.x) buf[i / CW][i % CW] = 0.f;
+      if (threadIdx.x == 0) {
+        int s0 = mol.nshells, s1 = 0;
+        for (int s = 0; s < mol.nshells; ++s) {
+          const Shell& sh = mol.shells[s];
+          if (sh.func < w0 + CW && sh.func + 2 * sh.L + 1 > w0) {
+            s0 = min(s0, s);
+            s1 = max(s1, s + 1);
+          }
+        }
+        srange[0] = s0;
+        srange[1] = s1;
+      }
+      __syncthreads();
+      const int s0 = srange[0], ns = max(0, srange[1] - s0);
+      for (int it = threadIdx.x; it < ROWS * ns; it += blockDim.x) {
+        const int r = it % ROWS;
+        const double px = pts[r][0];
+        if (px > 1e29) continue;
+        const Shell sh = mol.shells[s0 + it / ROWS];
+        float v[5];
+        // FP64 displacement from the nucleus, rounded once (accuracy of steep exponents)
+        const int n = shell_values<float>(sh, mol.alpha, mol.coeff, (float)(px - (double)mol.coords[3 * sh.atom]),
+                                          (float)(pts[r][1] - (double)mol.coords[3 * sh.atom + 1]),
+                                          (float)(pts[r][2] - (double)mol.coords[3 * sh.atom + 2]), v);
+        for (int k = 0; k < n; ++k) {
+          const int j = sh.func + k;
+          if (j >= w0 && j < w0 + CW) buf[r][j - w0] = v[k] * fscale[j];
+        }
+      }
+      __syncthreads();
+      for (int i = threadIdx.x; i < ROWS * CW; i += blockDim.x) {
+        const int r = i / CW, c = i % CW;
+        if (w0 + c < kpad)
+          split_store<FMT>(buf[r][c], out_hi, out_lo, ((int64_t)t * ROWS + r) * kpad + w0 + c, two != 0);
+      }
+      __syncthreads();
+    }
+  }
+}
+
+// ---------------------------------------------------------------------------------------
+// Stage 2: tcgen05 contraction with the fused row-dot epilogue.
+// ---------------------------------------------------------------------------------------
+struct TcParams {
+  PointMap pm;
+  int64_t tile0;
+  int ntiles;
+  int kpad, kchunks, npanels, pw, stages, nsplit, esize;
+  uint32_t a_bytes, b_bytes, stage_bytes, tx_bytes;
+  uint32_t idesc;
+  const void* phi_hi;
+  const void* phi_lo;
+  float* qube;
+  double* partials;
+  double outscale;
+  double inv_g;
+  int* err;
+};
+
+constexpr int MAX_STAGES = 8;
+
+__device__ __forceinline__ void load_phi32(const TcParams& p, int64_t row, int col, float* out) {
+  if (p.esize == 4) {
+    const float4* h = reinterpret_cast<const float4*>(reinterpret_cast<const float*>(p.phi_hi) + row * p.kpad + col);
+#pragma unroll
+    for (int i = 0; i < 8; ++i) {
+      const float4 a = h[i];
+      out[4 * i] = a.x;
+      out[4 * i + 1] = a.y;
+      out[4 * i + 2] = a.z;
+      out[4 * i + 3] = a.w;
+    }
+    if (p.nsplit == 2) {
+      const float4* l = reinterpret_cast<const float4*>(reinterpret_cast<const float*>(p.phi_lo) + row * p.kpad + col);
+#pragma unroll
+      for (int i = 0; i < 8; ++i) {
+        const float4 a = l[i];
+        out[4 * i] += a.x;
+        out[4 * i + 1] += a.y;
+        out[4 * i + 2] += a.z;
+        out[4 * i + 3] += a.w;
+      }
+    }
+  }
+}
+
+template <int FMT>
+__device__ __forceinline__ void load_phi16(const TcParams& p, int64_t row, int col, float* out) {
+  const uint4* h = reinterpret_cast<const uint4*>(reinterpret_cast<const uint16_t*>(p.phi_hi) + row * p.kpad + col);
+#pragma unroll
+  for (int i = 0; i < 4; ++i) {
+    const uint4 a = h[i];
+    const uint32_t w[4] = {a.x, a.y, a.z, a.w};
+#pragma unroll
+    for (int j = 0; j < 4; ++j) {
+      if constexpr (FMT == FMT_F16) {
+        const float2 f = __half22float2(*reinterpret_cast<const __half2*>(&w[j]));
+        out[8 * i + 2 * j] = f.x;
+        out[8 * i + 2 * j + 1] = f.y;
+      } else {
+        out[8 * i + 2 * j] = __uint_as_float(w[j] << 16);
+        out[8 * i + 2 * j + 1] = __uint_as_float(w[j] & 0xffff0000u);
+      }
+    }
+  }
+  if (p.nsplit == 2) {
+    const uint4* l = reinterpret_cast<const uint4*>(reinterpret_cast<const uint16_t*>(p.phi_lo) + row * p.kpad + col);
+#pragma unroll
+    for (int i = 0; i < 4; ++i) {
+      const uint4 a = l[i];
+      const uint32_t w[4] = {a.x, a.y, a.z, a.w};
+#pragma unroll
+      for (int j = 0; j < 4; ++j) {
+        if constexpr (FMT == FMT_F16) {
+          const float2 f = __half22float2(*reinterpret_cast<const __half2*>(&w[j]));
+          out[8 * i + 2 * j] += f.x;
+          out[8 * i + 2 * j + 1] += f.y;
+        } else {
+          out[8 * i + 2 * j] += __uint_as_float(w[j] << 16);
+          out[8 * i + 2 * j + 1] += __uint_as_float(w[j] & 0xffff0000u);
+        }
+      }
+    }
+  }
+}
+
+template <int FMT>
+__global__ void __launch_bounds__(192, 1)
+    density_mma_kernel(const __grid_constant__ CUtensorMap tmA_hi, const __grid_constant__ CUtensorMap tmA_lo,
+                       const __grid_constant__ CUtensorMap tmB_hi, const __grid_constant__ CUtensorMap tmB_lo,
+                       const TcParams p) {
+  extern __shared__ uint8_t smem_dyn[];
+  __shared__ __align__(8) uint64_t full_bar[MAX_STAGES], empty_bar[MAX_STAGES];
+  __shared__ __align__(8) uint64_t tfull[2], tempty[2], drain_bar;
+  __shared__ uint32_t tmem_slot;
+  __shared__ double rho_s[128];
+  __shared__ double red[4];
+  __shared__ volatile int abort_flag;
+
+  uint8_t* smem = reinterpret_cast<uint8_t*>((reinterpret_cast<uintptr_t>(smem_dyn) + 1023) & ~uintptr_t(1023));
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+
+  if (threadIdx.x == 0) {
+    abort_flag = 0;
+    for (int s = 0; s < p.stages; ++s) {
+      mbar_init(&full_bar[s], 1);
+      mbar_init(&empty_bar[s], 1);
+    }
+    for (int b = 0; b < 2; ++b) {
+      mbar_init(&tfull[b], 1);
+      mbar_init(&tempty[b], 128);
+    }
+    mbar_init(&drain_bar, 1);
+    fence_mbar_init();
+  }
+  if (warp == 0 && lane == 0) {
+    prefetch_tmap(&tmA_hi);
+    prefetch_tmap(&tmB_hi);
+    if (p.nsplit == 2) {
+      prefetch_tmap(&tmA_lo);
+      prefetch_tmap(&tmB_lo);
+    }
+  }
+  if (warp == 1) {
+    tmem_alloc(&tmem_slot, 512);
+    tmem_relinquish();
+  }
+  tc_fence_before();
+  __syncthreads();
+  tc_fence_after();
+  const uint32_t tmem = tmem_slot;
+
+  auto stage_ptr = [&](int s) { return smem + (size_t)s * p.stage_bytes; };
+
+  if (warp == 0) {
+    if (lane == 0) {
+      uint32_t it = 0;
+      int last_par[MAX_STAGES];
+      for (int s = 0; s < MAX_STAGES; ++s) last_par[s] = -1;
+      bool ok = true;
+      for (int t = blockIdx.x; t < p.ntiles && ok; t += gridDim.x) {
+        for (int pn = 0; pn < p.npanels && ok; ++pn) {
+          for (int kc = 0; kc < p.kchunks; ++kc, ++it) {
+            const int s = it % p.stages;
+            const uint32_t ph = (it / p.stages) & 1u;
+            if (!mbar_wait(&empty_bar[s], ph ^ 1u, &abort_flag)) {
+              ok = false;
+              break;
+            }
+            uint8_t* st = stage_ptr(s);
+            mbar_expect_tx(&full_bar[s], p.tx_bytes);
+            const int x = kc * (128 / p.esize);
+            tma_load_2d(st, &tmA_hi, &full_bar[s], x, t * 128);
+            if (p.nsplit == 2) tma_load_2d(st + p.a_bytes, &tmA_lo, &full_bar[s], x, t * 128);
+            uint8_t* bst = st + p.nsplit * p.a_bytes;
+            tma_load_2d(bst, &tmB_hi, &full_bar[s], x, pn * p.pw);
+            if (p.nsplit == 2) tma_load_2d(bst + p.b_bytes, &tmB_lo, &full_bar[s], x, pn * p.pw);
+            last_par[s] = (int)ph;
+          }
+        }
+      }
+      if (!ok) {  // drain copies still in flight before the CTA exits
+        for (int s = 0; s < p.stages; ++s)
+          if (last_par[s] >= 0) mbar_wait(&full_bar[s], (uint32_t)last_par[s], &abort_flag, 1u << 20);
+      }
+    }
+  } else if (warp == 1) {
+    if (lane == 0) {
+      uint32_t it = 0, acc_it = 0;
+      bool ok = true;
+      const int ksteps = 128 / (p.esize * (p.esize == 4 ? 8 : 16));  // 4 steps of 32 bytes
+      for (int t = blockIdx.x; t < p.ntiles && ok; t += gridDim.x) {
+        for (int pn = 0; pn < p.npanels && ok; ++pn, ++acc_it) {
+          const uint32_t buf = acc_it & 1u, aph = (acc_it >> 1) & 1u;
+          if (!mbar_wait(&tempty[buf], aph ^ 1u, &abort_flag)) {
+            ok = false;
+            break;
+          }
+          tc_fence_after();
+          const uint32_t d = tmem + buf * 256u;
+          for (int kc = 0; kc < p.kchunks; ++kc, ++it) {
+            const int s = it % p.stages;
+            const uint32_t ph = (it / p.stages) & 1u;
+            if (!mbar_wait(&full_bar[s], ph, &abort_flag)) {
+              ok = false;
+              break;
+            }
+            tc_fence_after();
+            const uint32_t a0 = smem_u32(stage_ptr(s));
+            const uint32_t a1 = a0 + p.a_bytes;
+            const uint32_t b0 = a0 + p.nsplit * p.a_bytes;
+            const uint32_t b1 = b0 + p.b_bytes;
+            for (int ks = 0; ks < ksteps; ++ks) {
+              const uint32_t off = ks * 32u;
+              const uint32_t acc = (kc | ks) != 0;
+              if constexpr (FMT == FMT_TF32) {
+                mma_tf32(d, sw128_kmajor_desc(a0 + off), sw128_kmajor_desc(b0 + off), p.idesc, acc);
+                if (p.nsplit == 2) {
+                  mma_tf32(d, sw128_kmajor_desc(a0 + off), sw128_kmajor_desc(b1 + off), p.idesc, 1u);
+                  mma_tf32(d, sw128_kmajor_desc(a1 + off), sw128_kmajor_desc(b0 + off), p.idesc, 1u);
+                }
+              } else {
+                mma_f16(d, sw128_kmajor_desc(a0 + off), sw128_kmajor_desc(b0 + off), p.idesc, acc);
+                if (p.nsplit == 2) {
+                  mma_f16(d, sw128_kmajor_desc(a0 + off), sw128_kmajor_desc(b1 + off), p.idesc, 1u);
+                  mma_f16(d, sw128_kmajor_desc(a1 + off), sw128_kmajor_desc(b0 + off), p.idesc, 1u);
+                }
+              }
+            }
+            tc_commit(&empty_bar[s]);
+          }
+          if (ok) tc_commit(&tfull[buf]);
+        }
+      }
+      // every MMA issued by this thread has completed once drain_bar flips
+      tc_commit(&drain_bar);
+      mbar_wait(&drain_bar, 0u, &abort_flag, 1u << 22);
+    }
+  } else {
+    // epilogue: warps 2..5 -> TMEM lane quadrants 2,3,0,1
+    const int q = warp & 3;
+    const int row = q * 32 + lane;
+    const int et = threadIdx.x - 64;
+    uint32_t acc_it = 0;
+    bool ok = true;
+    for (int t = blockIdx.x; t < p.ntiles && ok; t += gridDim.x) {
+      double acc = 0.0;
+      const int64_t grow = (int64_t)t * 128 + row;
+      for (int pn = 0; pn < p.npanels; ++pn, ++acc_it) {
+        const uint32_t buf = acc_it & 1u, aph = (acc_it >> 1) & 1u;
+        if (!mbar_wait(&tfull[buf], aph, &abort_flag)) {
+          ok = false;
+          break;
+        }
+        tc_fence_after();
+        for (int c = 0; c < p.pw / 32; ++c) {
+          const int col = pn * p.pw + 32 * c;
+          if (col >= p.kpad) break;
+          float v[32], ph[32];
+          tmem_ld32(tmem + ((uint32_t)(q * 32) << 16) + buf * 256u + 32u * c, v);
+          if constexpr (FMT == FMT_TF32) load_phi32(p, grow, col, ph);
+          else load_phi16<FMT>(p, grow, col, ph);
+#pragma unroll
+          for (int k = 0; k < 32; ++k) acc = fma((double)ph[k], (double)v[k], acc);
+        }
+        tc_fence_before();
+        mbar_arrive(&tempty[buf]);
+      }
+      if (!ok) break;
+      rho_s[row] = acc * p.inv_g;
+      named_barrier(1, 128);
+      double mysum = 0.0;
+      if (et < p.pm.vpt) {
+        double r = 0.0;
+        for (int s = 0; s < p.pm.s3; ++s) r += rho_s[et * p.pm.s3 + s];
+        const int64_t vox = (p.tile0 + t) * p.pm.vpt + et;
+        if (vox < p.pm.nvox) {
+          const float qv = (float)(r * p.outscale);
+          p.qube[vox] = qv;
+          mysum = qv;
+        }
+      }
+      for (int o = 16; o > 0; o >>= 1) mysum += __shfl_xor_sync(0xffffffffu, mysum, o);
+      if (lane == 0) red[q] = mysum;
+      named_barrier(1, 128);
+      if (et == 0) p.partials[p.tile0 + t] = red[0] + red[1] + red[2] + red[3];
+    }
+  }
+
+  tc_fence_before();
+  __syncthreads();
+  if (abort_flag && threadIdx.x == 0) atomicExch(p.err, 1);
+  if (warp == 1) {
+    tc_fence_after();
+    tmem_dealloc(tmem, 512);
+  }
+}
+
+// ---------------------------------------------------------------------------------------
+// Host side
+// ---------------------------------------------------------------------------------------
+static PFN_cuTensorMapEncodeTiled_v12000 encode_fn() {
+  static PFN_cuTensorMapEncodeTiled_v12000 fn = nullptr;
+  if (!fn) {
+    void* ptr = nullptr;
+    cudaDriverEntryPointQueryResult q;
+    if (cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &ptr, cudaEnableDefault, &q) == cudaSuccess &&
+        q == cudaDriverEntryPointSuccess)
+      fn = reinterpret_cast<PFN_cuTensorMapEncodeTiled_v12000>(ptr);
+  }
+  return fn;
+}
+
+static qmt_status make_map(CUtensorMap* m, const void* base, int esize, uint64_t inner, uint64_t outer,
+                           uint32_t box_inner, uint32_t box_outer) {
+  auto fn = encode_fn();
+  if (!fn) return fail(QMT_CUDA_ERR, "cuTensorMapEncodeTiled unavailable");
+  cuuint64_t dims[2] = {inner, outer};
+  cuuint64_t strides[1] = {inner * (uint64_t)esize};
+  cuuint32_t box[2] = {box_inner, box_outer};
+  cuuint32_t estr[2] = {1, 1};
+  const CUtensorMapDataType dt = esize == 4 ? CU_TENSOR_MAP_DATA_TYPE_FLOAT32 : CU_TENSOR_MAP_DATA_TYPE_UINT16;
+  CUresult r = fn(m, dt, 2, const_cast<void*>(base), dims, strides, box, estr, CU_TENSOR_MAP_INTERLEAVE_NONE,
+                  CU_TENSOR_MAP_SWIZZLE_128B, CU_TENSOR_MAP_L2_PROMOTION_L2_256B,
+                  CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+  if (r != CUDA_SUCCESS) return fail(QMT_CUDA_ERR, "cuTensorMapEncodeTiled failed");
+  return QMT_OK;
+}
+
+static void split_host(double x, int fmt, void* hi, void* lo, size_t idx) {
+  if (fmt == FMT_TF32) {
+    const uint32_t h = tf32_round_bits((float)x);
+    const uint32_t l = tf32_round_bits((float)(x - (double)bits_f32(h)));
+    reinterpret_cast<uint32_t*>(hi)[idx] = h;
+    reinterpret_cast<uint32_t*>(lo)[idx] = l;
+  } else if (fmt == FMT_F16) {
+    const __half h = __float2half_rn((float)x);
+    const __half l = __float2half_rn((float)(x - (double)__half2float(h)));
+    reinterpret_cast<__half*>(hi)[idx] = h;
+    reinterpret_cast<__half*>(lo)[idx] = l;
+  } else {
+    const __nv_bfloat16 h = __float2bfloat16_rn((float)x);
+    const __nv_bfloat16 l = __float2bfloat16_rn((float)(x - (double)__bfloat162float(h)));
+    reinterpret_cast<__nv_bfloat16*>(hi)[idx] = h;
+    reinterpret_cast<__nv_bfloat16*>(lo)[idx] = l;
+  }
+}
+
+// Builds the scaled, split density matrix and the Phi column scales for `prec`.
+static qmt_status ensure_tc_operands(qmt_mol* m, int prec, const TcShape& sh, cudaStream_t s) {
+  if (m->tc_prec == prec) return QMT_OK;
+  const int n = m->norbs, np = m->npad, K = sh.kpad;
+  std::vector<int> sj(K, 0);
+  std::vector<float> fs(K, 0.f);
+  for (int j = 0; j < n; ++j) {
+    const double b = std::max(m->fbound[j], 1e-30);
+    sj[j] = (int)std::floor(std::log2(16000.0 / b));
+    sj[j] = std::max(-60, std::min(60, sj[j]));
+    fs[j] = (float)std::ldexp(1.0, sj[j]);
+  }
+  double mx = 0;
+  for (int j = 0; j < n; ++j)
+    for (int k = 0; k < n; ++k)
+      mx = std::max(mx, std::fabs(std::ldexp(m->P64[(size_t)j * np + k], -sj[j] - sj[k])));
+  int g = mx > 0 ? (int)std::floor(std::log2(16000.0 / mx)) : 0;
+  g = std::max(-100, std::min(100, g));
+  const size_t piece = (size_t)sh.nrows_b * K * sh.esize;
+  std::vector<uint8_t> host(2 * piece, 0);
+  for (int j = 0; j < n; ++j)
+    for (int k = 0; k < n; ++k) {
+      const double v = std::ldexp(m->P64[(size_t)j * np + k], g - sj[j] - sj[k]);
+      split_host(v, sh.fmt, host.data(), host.data() + piece, (size_t)j * K + k);
+    }
+  qmt_status st;
+  if ((st = m->d_tc_P.reserve(2 * piece))) return st;
+  if ((st = m->d_fscale.reserve(K * sizeof(float)))) return st;
+  QMT_CUDA(cudaMemcpyAsync(m->d_tc_P.ptr, host.data(), 2 * piece, cudaMemcpyHostToDevice, s));
+  QMT_CUDA(cudaMemcpyAsync(m->d_fscale.ptr, fs.data(), K * sizeof(float), cudaMemcpyHostToDevice, s));
+  QMT_CUDA(cudaStreamSynchronize(s));
+  m->tc_g = g;
+  m->tc_prec = prec;
+  return QMT_OK;
+}
+
+template <int FMT>
+static qmt_status run_tc(qmt_mol* m, const TcShape& sh, const PointMap& pm, int64_t ntiles, int prec,
+                         float* qube, double outscale, cudaStream_t s) {
+  qmt_status st;
+  const size_t tile_bytes = (size_t)128 * sh.kpad * sh.esize;
+  const int nsm = sm_count();
+  // staging chunk: bounded to ~2 GiB, a multiple of the SM count when larger than one wave
+  int64_t chunk = std::max<int64_t>(1, ((size_t)2 << 30) / (tile_bytes * sh.nsplit));
+  if (chunk > nsm) chunk = chunk / nsm * nsm;
+  chunk = std::min<int64_t>(chunk, ntiles);
+  if ((st = m->d_Phi_hi.reserve(chunk * tile_bytes))) return st;
+  if (sh.nsplit == 2 && (st = m->d_Phi_lo.reserve(chunk * tile_bytes))) return st;
+  void* lo_ptr = sh.nsplit == 2 ? m->d_Phi_lo.ptr : m->d_Phi_hi.ptr;
+
+  CUtensorMap tA_hi, tA_lo, tB_hi, tB_lo;
+  const uint8_t* Pb = m->d_tc_P.as<uint8_t>();
+  const size_t piece = (size_t)sh.nrows_b * sh.kpad * sh.esize;
+  if ((st = make_map(&tA_hi, m->d_Phi_hi.ptr, sh.esize, sh.kpad, (uint64_t)chunk * 128, sh.ke, 128)) ||
+      (st = make_map(&tA_lo, lo_ptr, sh.esize, sh.kpad, (uint64_t)chunk * 128, sh.ke, 128)) ||
+      (st = make_map(&tB_hi, Pb, sh.esize, sh.kpad, sh.nrows_b, sh.ke, sh.pw)) ||
+      (st = make_map(&tB_lo, Pb + piece, sh.esize, sh.kpad, sh.nrows_b, sh.ke, sh.pw)))
+    return st;
+
+  TcParams p{};
+  p.pm = pm;
+  p.kpad = sh.kpad;
+  p.kchunks = sh.kpad / sh.ke;
+  p.npanels = sh.npanels;
+  p.pw = sh.pw;
+  p.nsplit = sh.nsplit;
+  p.esize = sh.esize;
+  p.a_bytes = 128u * 128u;
+  p.b_bytes = (uint32_t)sh.pw * 128u;
+  p.stage_bytes = sh.nsplit * (p.a_bytes + p.b_bytes);
+  p.tx_bytes = p.stage_bytes;
+  p.idesc = make_idesc((uint32_t)sh.fmt, 128, (uint32_t)sh.pw);
+  p.phi_hi = m->d_Phi_hi.ptr;
+  p.phi_lo = lo_ptr;
+  p.qube = qube;
+  p.partials = m->d_partials.as<double>();
+  p.outscale = outscale;
+  p.inv_g = std::ldexp(1.0, -m->tc_g);
+  p.err = reinterpret_cast<int*>(m->d_scalars.as<double>() + 8);
+
+  int maxsm = 0, dev = 0;
+  cudaGetDevice(&dev);
+  cudaDeviceGetAttribute(&maxsm, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev);
+  const int static_bytes = 4096;
+  int stages = (int)((maxsm - static_bytes - 1024) / p.stage_bytes);
+  stages = std::min(stages, MAX_STAGES);
+  if (stages < 2) return fail(QMT_BAD_ARG, "tensor-core stage does not fit in shared memory");
+  p.stages = stages;
+  const size_t dyn = (size_t)stages * p.stage_bytes + 1024;
+  auto kern = density_mma_kernel<FMT>;
+  QMT_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)dyn));
+  QMT_CUDA(cudaMemsetAsync(p.err, 0, sizeof(int), s));
+
+  for (int64_t t0 = 0; t0 < ntiles; t0 += chunk) {
+    const int nt = (int)std::min<int64_t>(chunk, ntiles - t0);
+    const int gb = (int)std::min<int64_t>(nt, (int64_t)nsm * 4);
+    basis_stage_kernel<FMT><<<gb, 256, 0, s>>>(m->view(), pm, t0, nt, sh.kpad, m->d_fscale.as<float>(),
+                                               m->d_Phi_hi.ptr, lo_ptr, sh.nsplit == 2);
+    QMT_CHECK_LAUNCH("basis_stage_kernel");
+    p.tile0 = t0;
+    p.ntiles = nt;
+    const int gm = (int)std::min<int64_t>(nt, nsm);
+    kern<<<gm, 192, dyn, s>>>(tA_hi, tA_lo, tB_hi, tB_lo, p);
+    QMT_CHECK_LAUNCH("density_mma_kernel");
+  }
+  (void)prec;
+  return QMT_OK;
+}
+
+qmt_status density_tc(qmt_mol* mol, int nx, int ny, int nz, float step, float ox, float oy, float oz,
+                      int subgrid, int precision, int rescale, float* qube, double* sum_out,
+                      cudaStream_t s) {
+  const TcShape sh = tc_shape(precision, mol->norbs);
+  qmt_status st;
+  PointMap pm;
+  int64_t ntiles;
+  if ((st = make_point_map(nx, ny, nz, step, ox, oy, oz, subgrid, 128, pm, ntiles))) return st;
+  if ((st = ensure_tc_operands(mol, precision, sh, s))) return st;
+  if ((st = mol->d_partials.reserve(ntiles * sizeof(double)))) return st;
+  const double outscale = 2.0 * (double)step * step * step / pm.s3;
+  if (sh.fmt == FMT_TF32) st = run_tc<FMT_TF32>(mol, sh, pm, ntiles, precision, qube, outscale, s);
+  else if (sh.fmt == FMT_F16) st = run_tc<FMT_F16>(mol, sh, pm, ntiles, precision, qube, outscale, s);
+  else st = run_tc<FMT_BF16>(mol, sh, pm, ntiles, precision, qube, outscale, s);
+  if (st) return st;
+  st = finish_density(mol, pm.nvox, ntiles, rescale, qube, sum_out, s);
+  if (st) return st;
+  int err = 0;
+  QMT_CUDA(cudaMemcpyAsync(&err, mol->d_scalars.as<double>() + 8, sizeof(int), cudaMemcpyDeviceToHost, s));
+  QMT_CUDA(cudaStreamSynchronize(s));
+  if (err) return fail(QMT_CUDA_ERR, "tensor-core density kernel gave up waiting on a barrier");
+  return QMT_OK;
+}
+
+}  // namespace qmt

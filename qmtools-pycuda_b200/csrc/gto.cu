@@ -1,0 +1,499 @@
+// Analytic electrostatic potential of the GTO density plus the nuclei.
+//
+// Replaces gpu_hartree_GTO (kernel_hartree.cu:288-869), which loops over DM pairs p >= q and
+// then primitive pairs with per-(L,m) closed forms, serialising the block on thread 0.
+// Here the density is first written as a sum over merged primitive pairs of Hermite
+// Gaussians (McMurchie-Davidson):
+//     rho(r) = 2 sum_pq P_pq phi_p phi_q = sum_pairs sum_tuv D_tuv Lambda_tuv(r; p, P)
+// with D_tuv already contracted with the density matrix (host, FP64).  The potential at a
+// point C is then
+//     V(C) = -sum_pairs (2 pi / p) sum_tuv D_tuv R_tuv(p, P - C) + sum_A Z_A / |C - R_A|,
+// with R_tuv from Boys functions F_0..F_L (table + Taylor, downward recursion).  All device
+// arithmetic is FP64.
+#include <algorithm>
+#include <cstdio>
+#include <string>
+#include <unordered_map>
+
+#include "mol.cuh"
+
+namespace qmt {
+
+__host__ __device__ constexpr int ncoef(int L) { return (L + 1) * (L + 2) * (L + 3) / 6; }
+constexpr int BOYS_NT = 401;     // T = 0, 0.1, ..., 40
+constexpr int BOYS_NM = 11;      // m = 0..10
+constexpr double BOYS_DT = 0.1;
+
+struct GPair {
+  double px, py, pz, p;
+  double pref;   // -(2 pi / p) * spin/triangle factors * K * ca * cb (D carries P)
+  int L;
+  int doff;      // offset of the D coefficients
+};
+
+// (t,u,v) triples ordered by t+u+v; recursion parents for R^{(j)}_{tuv} from R^{(j+1)}.
+struct HermIdx {
+  int t, u, v, dir, p1, p2, mult;
+};
+
+__host__ __device__ constexpr int herm_index(int t, int u, int v) {
+  // position in the list ordered by total order, then t descending, then u descending
+  int s = t + u + v, base = 0;
+  for (int k = 0; k < s; ++k) base += (k + 1) * (k + 2) / 2;
+  int pos = 0;
+  for (int tt = s; tt > t; --tt) pos += s - tt + 1;
+  pos += (s - t) - u;
+  return base + pos;
+}
+
+struct HermTable {
+  HermIdx e[35];
+};
+
+__host__ __device__ constexpr HermTable make_herm_table() {
+  HermTable h{};
+  int k = 0;
+  for (int s = 0; s <= 4; ++s)
+    for (int t = s; t >= 0; --t)
+      for (int u = s - t; u >= 0; --u) {
+        const int v = s - t - u;
+        HermIdx x{t, u, v, -1, -1, -1, 0};
+        if (t > 0) {
+          x.dir = 0;
+          x.p1 = herm_index(t - 1, u, v);
+          x.mult = t - 1;
+          x.p2 = t > 1 ? herm_index(t - 2, u, v) : 0;
+        } else if (u > 0) {
+          x.dir = 1;
+          x.p1 = herm_index(t, u - 1, v);
+          x.mult = u - 1;
+          x.p2 = u > 1 ? herm_index(t, u - 2, v) : 0;
+        } else if (v > 0) {
+          x.dir = 2;
+          x.p1 = herm_index(t, u, v - 1);
+          x.mult = v - 1;
+          x.p2 = v > 1 ? herm_index(t, u, v - 2) : 0;
+        }
+        h.e[k++] = x;
+      }
+  return h;
+}
+
+// F_m(T) for m = 0..L into F[], FP64.
+template <int L>
+__device__ __forceinline__ void boys_fn(double T, const double* __restrict__ tab, double* F) {
+  if (T < 40.0) {
+    const int i = (int)(T * (1.0 / BOYS_DT) + 0.5);
+    const double d = T - i * BOYS_DT;
+    const double* row = tab + (size_t)i * BOYS_NM;
+    // Taylor: F_L(T) = sum_k F_{L+k}(T_i) (-d)^k / k!
+    double f = 0.0, c = 1.0;
+#pragma unroll
+    for (int k = 0; k <= 6; ++k) {
+      f += row[L + k] * c;
+      c *= -d / (k + 1);
+    }
+    F[L] = f;
+    const double et = exp(-T);
+#pragma unroll
+    for (int m = L - 1; m >= 0; --m) F[m] = (2.0 * T * F[m + 1] + et) / (2 * m + 1);
+  } else {
+    const double it = 1.0 / T;
+    F[0] = 0.88622692545275801365 * sqrt(it);  // sqrt(pi)/2 / sqrt(T)
+#pragma unroll
+    for (int m = 0; m < L; ++m) F[m + 1] = F[m] * (2 * m + 1) * 0.5 * it;
+  }
+}
+
+template <int L>
+__device__ __forceinline__ double pair_potential(const GPair& g, const double* __restrict__ D, double cx, double cy,
+                                                 double cz, const double* __restrict__ tab) {
+  const double X = g.px - cx, Y = g.py - cy, Z = g.pz - cz;
+  const double T = g.p * (X * X + Y * Y + Z * Z);
+  double F[L + 1];
+  boys_fn<L>(T, tab, F);
+  constexpr int NC = ncoef(L);
+  constexpr HermTable H = make_herm_table();
+  double cur[NC], nxt[NC];
+  const double m2p = -2.0 * g.p;
+  double pw = 1.0;
+#pragma unroll
+  for (int j = 0; j < L; ++j) pw *= m2p;
+  cur[0] = pw * F[L];
+#pragma unroll
+  for (int j = L - 1; j >= 0; --j) {
+    pw = 1.0;
+#pragma unroll
+    for (int q = 0; q < j; ++q) pw *= m2p;
+    nxt[0] = pw * F[j];
+    const int n = ncoef(L - j);
+#pragma unroll
+    for (int k = 1; k < NC; ++k) {
+      if (k < n) {
+        const HermIdx h = H.e[k];
+        const double c = h.dir == 0 ? X : (h.dir == 1 ? Y : Z);
+        double r = c * cur[h.p1];
+        if (h.mult > 0) r += h.mult * cur[h.p2];
+        nxt[k] = r;
+      }
+    }
+#pragma unroll
+    for (int k = 0; k < NC; ++k) cur[k] = nxt[k];
+  }
+  double acc = 0.0;
+#pragma unroll
+  for (int k = 0; k < NC; ++k) acc += D[k] * cur[k];
+  return g.pref * acc;
+}
+
+constexpr int GTO_THREADS = 128;
+constexpr int GTO_CHUNK = 64;
+
+// mode 0: grid corners origin + i h (x-fastest);  mode 1: grid centres;  mode 2: point list;
+// mode 3: outer shell of the grid at centres (boundary), written into the full grid.
+struct GtoPoints {
+  int mode;
+  int nx, ny, nz;
+  double h, ox, oy, oz;
+  const float* pts;
+  int64_t npts;
+};
+
+__device__ __forceinline__ bool gto_point(const GtoPoints& gp, int64_t i, double& x, double& y, double& z,
+                                          int64_t& out) {
+  if (gp.mode == 2) {
+    x = gp.pts[3 * i];
+    y = gp.pts[3 * i + 1];
+    z = gp.pts[3 * i + 2];
+    out = i;
+    return true;
+  }
+  int64_t ix, iy, iz;
+  if (gp.mode == 3) {
+    // enumerate the outer shell: z = 0 and z = nz-1 planes, then the y faces, then x faces
+    const int64_t nx = gp.nx, ny = gp.ny, nz = gp.nz;
+    const int64_t pl = nx * ny;
+    if (i < 2 * pl) {
+      iz = i < pl ? 0 : nz - 1;
+      const int64_t r = i % pl;
+      ix = r % nx;
+      iy = r / nx;
+    } else {
+      int64_t r = i - 2 * pl;
+      const int64_t inner = nz - 2;
+      const int64_t yf = nx * inner;
+      if (r < 2 * yf) {
+        iy = r < yf ? 0 : ny - 1;
+        r %= yf;
+        ix = r % nx;
+        iz = 1 + r / nx;
+      } else {
+        r -= 2 * yf;
+        const int64_t xf = (ny - 2) * inner;
+        ix = r < xf ? 0 : nx - 1;
+        r %= xf;
+        iy = 1 + r % (ny - 2);
+        iz = 1 + r / (ny - 2);
+      }
+    }
+  } else {
+    ix = i % gp.nx;
+    iy = (i / gp.nx) % gp.ny;
+    iz = i / ((int64_t)gp.nx * gp.ny);
+  }
+  const double off = gp.mode == 0 ? 0.0 : 0.5;
+  x = gp.ox + (ix + off) * gp.h;
+  y = gp.oy + (iy + off) * gp.h;
+  z = gp.oz + (iz + off) * gp.h;
+  out = ix + iy * (int64_t)gp.nx + iz * (int64_t)gp.nx * gp.ny;
+  return true;
+}
+
+__global__ void __launch_bounds__(GTO_THREADS) gto_kernel(const GPair* __restrict__ pairs, int npairs,
+                                                          const double* __restrict__ dco,
+                                                          const double* __restrict__ tab, MolView mol,
+                                                          GtoPoints gp, float* __restrict__ out) {
+  __shared__ GPair sp[GTO_CHUNK];
+  __shared__ double sd[GTO_CHUNK * 35];
+  __shared__ int soff[GTO_CHUNK];
+  const int64_t i = blockIdx.x * (int64_t)GTO_THREADS + threadIdx.x;
+  double cx = 0, cy = 0, cz = 0;
+  int64_t o = -1;
+  const bool valid = i < gp.npts && gto_point(gp, i, cx, cy, cz, o);
+  double V = 0.0;
+  for (int c0 = 0; c0 < npairs; c0 += GTO_CHUNK) {
+    const int nc = min(GTO_CHUNK, npairs - c0);
+    __syncthreads();
+    if (threadIdx.x < nc) sp[threadIdx.x] = pairs[c0 + threadIdx.x];
+    __syncthreads();
+    if (threadIdx.x == 0) {
+      int acc = 0;
+      for (int k = 0; k < nc; ++k) {
+        soff[k] = acc;
+        acc += ncoef(sp[k].L);
+      }
+    }
+    __syncthreads();
+    for (int k = threadIdx.x; k < nc * 35; k += GTO_THREADS) {
+      const int pk = k / 35, j = k % 35;
+      if (j < ncoef(sp[pk].L)) sd[soff[pk] + j] = dco[sp[pk].doff + j];
+    }
+    __syncthreads();
+    if (valid) {
+      for (int k = 0; k < nc; ++k) {
+        const GPair g = sp[k];
+        const double* D = sd + soff[k];
+        switch (g.L) {
+          case 0: V += pair_potential<0>(g, D, cx, cy, cz, tab); break;
+          case 1: V += pair_potential<1>(g, D, cx, cy, cz, tab); break;
+          case 2: V += pair_potential<2>(g, D, cx, cy, cz, tab); break;
+          case 3: V += pair_potential<3>(g, D, cx, cy, cz, tab); break;
+          default: V += pair_potential<4>(g, D, cx, cy, cz, tab); break;
+        }
+      }
+    }
+  }
+  if (!valid) return;
+  for (int a = 0; a < mol.natoms; ++a) {
+    const double dx = cx - mol.coords[3 * a], dy = cy - mol.coords[3 * a + 1], dz = cz - mol.coords[3 * a + 2];
+    const double r = sqrt(dx * dx + dy * dy + dz * dz);
+    if (r > 1e-8) V += mol.types[a] / r;
+  }
+  out[o] = (float)V;
+}
+
+// ---- host: Boys table ------------------------------------------------------------------------
+static qmt_status boys_table(const double** out) {
+  static thread_local DevBuf tab;  // one copy per host thread (per device in practice)
+  static thread_local bool ready = false;
+  if (!ready) {
+    std::vector<double> h((size_t)BOYS_NT * BOYS_NM);
+    for (int i = 0; i < BOYS_NT; ++i) {
+      const double T = i * BOYS_DT;
+      for (int m = 0; m < BOYS_NM; ++m) {
+        double term = 1.0 / (2 * m + 1), acc = term;
+        for (int k = 1; k < 400; ++k) {
+          term *= 2 * T / (2 * m + 2 * k + 1);
+          acc += term;
+          if (term < 1e-18 * acc) break;
+        }
+        h[(size_t)i * BOYS_NM + m] = std::exp(-T) * acc;
+      }
+    }
+    qmt_status st = tab.reserve(h.size() * sizeof(double));
+    if (st) return st;
+    QMT_CUDA(cudaMemcpy(tab.ptr, h.data(), h.size() * sizeof(double), cudaMemcpyHostToDevice));
+    ready = true;
+  }
+  *out = tab.as<double>();
+  return QMT_OK;
+}
+
+// ---- host: pair table --------------------------------------------------------------------------
+static void hermite_e_host(int la, int lb, double a, double b, double xa, double xb, double E[3][3][5]) {
+  const double p = a + b, xp = (a * xa + b * xb) / p, pa = xp - xa, pb = xp - xb, i2p = 0.5 / p;
+  for (int i = 0; i < 3; ++i)
+    for (int j = 0; j < 3; ++j)
+      for (int t = 0; t < 5; ++t) E[i][j][t] = 0.0;
+  E[0][0][0] = 1.0;
+  for (int i = 0; i <= la; ++i)
+    for (int j = 0; j <= lb; ++j) {
+      if (i == 0 && j == 0) continue;
+      for (int t = 0; t <= i + j; ++t) {
+        double v;
+        if (i > 0) {
+          v = pa * E[i - 1][j][t] + (t + 1 < 5 ? (t + 1) * E[i - 1][j][t + 1] : 0.0);
+          if (t > 0) v += i2p * E[i - 1][j][t - 1];
+        } else {
+          v = pb * E[i][j - 1][t] + (t + 1 < 5 ? (t + 1) * E[i][j - 1][t + 1] : 0.0);
+          if (t > 0) v += i2p * E[i][j - 1][t - 1];
+        }
+        E[i][j][t] = v;
+      }
+    }
+}
+
+static int cart_host(int L, int k, double* c, int (*e)[3]) {
+  for (int q = 0; q < 3; ++q) e[q][0] = e[q][1] = e[q][2] = 0;
+  if (L == 0) { c[0] = YS; return 1; }
+  if (L == 1) { c[0] = YP; e[0][k == 0 ? 2 : (k == 1 ? 0 : 1)] = 1; return 1; }
+  switch (k) {
+    case 0: c[0] = 2 * YD0; e[0][2] = 2; c[1] = -YD0; e[1][0] = 2; c[2] = -YD0; e[2][1] = 2; return 3;
+    case 1: c[0] = YD1; e[0][0] = 1; e[0][2] = 1; return 1;
+    case 2: c[0] = YD1; e[0][1] = 1; e[0][2] = 1; return 1;
+    case 3: c[0] = YD2; e[0][0] = 2; c[1] = -YD2; e[1][1] = 2; return 2;
+    default: c[0] = YD1; e[0][0] = 1; e[0][1] = 1; return 1;
+  }
+}
+
+static qmt_status build_pairs(qmt_mol* m, cudaStream_t s) {
+  if (m->gto_ready) return QMT_OK;
+  struct Acc {
+    double px, py, pz, p, pref;
+    int L;
+    double D[35];
+  };
+  std::vector<Acc> acc;
+  std::unordered_map<std::string, int> index;
+  const int ns = m->nshells, np = m->npad;
+  for (int iA = 0; iA < ns; ++iA) {
+    const Shell& A = m->shells[iA];
+    const double Ax = m->coords[3 * A.atom], Ay = m->coords[3 * A.atom + 1], Az = m->coords[3 * A.atom + 2];
+    for (int iB = iA; iB < ns; ++iB) {
+      const Shell& B = m->shells[iB];
+      const double Bx = m->coords[3 * B.atom], By = m->coords[3 * B.atom + 1], Bz = m->coords[3 * B.atom + 2];
+      const double AB2 = (Ax - Bx) * (Ax - Bx) + (Ay - By) * (Ay - By) + (Az - Bz) * (Az - Bz);
+      const double fac = iA == iB ? 1.0 : 2.0;
+      double pmax = 0;
+      for (int k1 = 0; k1 < 2 * A.L + 1; ++k1)
+        for (int k2 = 0; k2 < 2 * B.L + 1; ++k2)
+          pmax = std::max(pmax, std::fabs(m->P64[(size_t)(A.func + k1) * np + B.func + k2]));
+      if (pmax == 0) continue;
+      for (int ia = 0; ia < A.nprim; ++ia)
+        for (int ib = 0; ib < B.nprim; ++ib) {
+          const double a = m->alpha64[A.prim + ia], ca = m->coeff64[A.prim + ia];
+          const double b = m->alpha64[B.prim + ib], cb = m->coeff64[B.prim + ib];
+          const double p = a + b;
+          const double K = std::exp(-a * b / p * AB2);
+          // -2 (electron charge x spin) * triangle factor * (2 pi / p) * K * ca * cb
+          const double pref = -2.0 * fac * 2.0 * 3.14159265358979323846 / p * K * ca * cb;
+          const double chg = std::fabs(pref) * pmax * std::pow(std::max(1.0, 2 * p), 0.5 * (A.L + B.L));
+          if (chg < 1e-15) continue;
+          double Ex[3][3][5], Ey[3][3][5], Ez[3][3][5];
+          hermite_e_host(A.L, B.L, a, b, Ax, Bx, Ex);
+          hermite_e_host(A.L, B.L, a, b, Ay, By, Ey);
+          hermite_e_host(A.L, B.L, a, b, Az, Bz, Ez);
+          double D[35] = {0};
+          const int L = A.L + B.L;
+          for (int k1 = 0; k1 < 2 * A.L + 1; ++k1) {
+            double c1[3];
+            int e1[3][3];
+            const int n1 = cart_host(A.L, k1, c1, e1);
+            for (int k2 = 0; k2 < 2 * B.L + 1; ++k2) {
+              const double w = m->P64[(size_t)(A.func + k1) * np + B.func + k2];
+              if (w == 0) continue;
+              double c2[3];
+              int e2[3][3];
+              const int n2 = cart_host(B.L, k2, c2, e2);
+              for (int u1 = 0; u1 < n1; ++u1)
+                for (int u2 = 0; u2 < n2; ++u2) {
+                  const int i = e1[u1][0], k = e1[u1][1], mm = e1[u1][2];
+                  const int j = e2[u2][0], l = e2[u2][1], n = e2[u2][2];
+                  const double cc = w * c1[u1] * c2[u2];
+                  for (int t = 0; t <= i + j; ++t)
+                    for (int u = 0; u <= k + l; ++u)
+                      for (int v = 0; v <= mm + n; ++v)
+                        D[herm_index(t, u, v)] += cc * Ex[i][j][t] * Ey[k][l][u] * Ez[mm][n][v];
+                }
+            }
+          }
+          // merge products with the same centres and exponents (general contractions)
+          int ka = A.atom, kb = B.atom;
+          double xa = a, xb = b;
+          if (ka > kb || (ka == kb && xa > xb)) {
+            std::swap(ka, kb);
+            std::swap(xa, xb);
+          }
+          char key[64];
+          std::snprintf(key, sizeof(key), "%d:%a:%d:%a", ka, xa, kb, xb);
+          auto it = index.find(key);
+          if (it == index.end()) {
+            Acc g{};
+            g.px = (a * Ax + b * Bx) / p;
+            g.py = (a * Ay + b * By) / p;
+            g.pz = (a * Az + b * Bz) / p;
+            g.p = p;
+            g.pref = pref;
+            g.L = L;
+            for (int q = 0; q < ncoef(L); ++q) g.D[q] = D[q];
+            index.emplace(key, (int)acc.size());
+            acc.push_back(g);
+          } else {
+            Acc& g = acc[it->second];
+            const double r = pref / g.pref;
+            g.L = std::max(g.L, L);
+            for (int q = 0; q < ncoef(L); ++q) g.D[q] += r * D[q];
+          }
+        }
+    }
+  }
+  // sort by L so that warps see uniform work, pack D
+  std::vector<int> order(acc.size());
+  for (size_t i = 0; i < order.size(); ++i) order[i] = (int)i;
+  std::stable_sort(order.begin(), order.end(), [&](int x, int y) { return acc[x].L < acc[y].L; });
+  std::vector<GPair> pairs;
+  std::vector<double> dco;
+  for (int idx : order) {
+    const Acc& g = acc[idx];
+    GPair q;
+    q.px = g.px;
+    q.py = g.py;
+    q.pz = g.pz;
+    q.p = g.p;
+    q.pref = g.pref;
+    q.L = g.L;
+    q.doff = (int)dco.size();
+    for (int k = 0; k < ncoef(g.L); ++k) dco.push_back(g.D[k]);
+    pairs.push_back(q);
+  }
+  if (pairs.empty()) {
+    GPair z{};
+    pairs.push_back(z);
+    dco.push_back(0.0);
+  }
+  const size_t pb = pairs.size() * sizeof(GPair), db = dco.size() * sizeof(double);
+  qmt_status st = m->d_pairs.reserve(pb + db + 256);
+  if (st) return st;
+  QMT_CUDA(cudaMemcpyAsync(m->d_pairs.ptr, pairs.data(), pb, cudaMemcpyHostToDevice, s));
+  QMT_CUDA(cudaMemcpyAsync(m->d_pairs.as<uint8_t>() + ((pb + 255) / 256) * 256, dco.data(), db,
+                           cudaMemcpyHostToDevice, s));
+  QMT_CUDA(cudaStreamSynchronize(s));
+  m->gto_npairs = (int)pairs.size();
+  m->gto_doff_bytes = ((pb + 255) / 256) * 256;
+  m->gto_ready = true;
+  return QMT_OK;
+}
+
+static qmt_status run_gto(qmt_mol* m, const GtoPoints& gp, float* out, cudaStream_t s) {
+  qmt_status st;
+  const double* tab = nullptr;
+  if ((st = boys_table(&tab))) return st;
+  if ((st = build_pairs(m, s))) return st;
+  if (gp.npts <= 0) return QMT_OK;
+  const GPair* pairs = m->d_pairs.as<GPair>();
+  const double* dco = reinterpret_cast<const double*>(m->d_pairs.as<uint8_t>() + m->gto_doff_bytes);
+  const int64_t blocks = (gp.npts + GTO_THREADS - 1) / GTO_THREADS;
+  gto_kernel<<<(unsigned)blocks, GTO_THREADS, 0, s>>>(pairs, m->gto_npairs, dco, tab, m->view(), gp, out);
+  QMT_CHECK_LAUNCH("gto_kernel");
+  return QMT_OK;
+}
+
+}  // namespace qmt
+
+using namespace qmt;
+
+extern "C" {
+
+qmt_status qmt_hartree_gto(qmt_mol* mol, int nx, int ny, int nz, float step, float ox, float oy, float oz,
+                           float* v_dev, void* stream) {
+  if (!mol || !v_dev || nx < 1 || ny < 1 || nz < 1 || !(step > 0.f)) return fail(QMT_BAD_ARG, "bad GTO arguments");
+  GtoPoints gp{0, nx, ny, nz, step, ox, oy, oz, nullptr, (int64_t)nx * ny * nz};
+  return run_gto(mol, gp, v_dev, as_stream(stream));
+}
+
+qmt_status qmt_hartree_gto_points(qmt_mol* mol, int npts, const float* pts_dev, float* v_dev, void* stream) {
+  if (!mol || npts < 0 || (npts > 0 && (!pts_dev || !v_dev))) return fail(QMT_BAD_ARG, "bad GTO arguments");
+  GtoPoints gp{2, 0, 0, 0, 0, 0, 0, 0, pts_dev, npts};
+  return run_gto(mol, gp, v_dev, as_stream(stream));
+}
+
+qmt_status qmt_hartree_gto_boundary(qmt_mol* mol, int nx, int ny, int nz, float step, float ox, float oy,
+                                    float oz, float* v_dev, void* stream) {
+  if (!mol || !v_dev || nx < 3 || ny < 3 || nz < 3 || !(step > 0.f))
+    return fail(QMT_BAD_ARG, "bad GTO boundary arguments");
+  const int64_t n = 2 * (int64_t)nx * ny + 2 * (int64_t)nx * (nz - 2) + 2 * (int64_t)(ny - 2) * (nz - 2);
+  GtoPoints gp{3, nx, ny, nz, step, ox, oy, oz, nullptr, n};
+  return run_gto(mol, gp, v_dev, as_stream(stream));
+}
+
+}  // extern "C"

@@ -1,0 +1,261 @@
+// Library state, status strings and the molecule handle (device-resident basis,
+// coordinates and density matrix).
+#include <cuda_bf16.h>
+#include <cuda_fp16.h>
+
+#include <algorithm>
+#include <cstring>
+#include <mutex>
+
+#include "mol.cuh"
+
+namespace qmt {
+
+static thread_local std::string g_last_error;
+
+void set_error(const std::string& msg) { g_last_error = msg; }
+
+qmt_status fail(qmt_status code, const std::string& msg) {
+  set_error(msg);
+  return code;
+}
+
+qmt_status cuda_fail(cudaError_t e, const char* what) {
+  set_error(std::string(what) + ": " + cudaGetErrorString(e));
+  if (e == cudaErrorMemoryAllocation) return QMT_OOM;
+  if (e == cudaErrorNoDevice || e == cudaErrorInsufficientDriver) return QMT_NO_DEVICE;
+  return QMT_CUDA_ERR;
+}
+
+qmt_status DevBuf::reserve(size_t n) {
+  if (n <= bytes) return QMT_OK;
+  if (ptr) cudaFree(ptr);
+  ptr = nullptr;
+  bytes = 0;
+  cudaError_t e = cudaMalloc(&ptr, n);
+  if (e != cudaSuccess) {
+    ptr = nullptr;
+    return cuda_fail(e, "cudaMalloc");
+  }
+  bytes = n;
+  return QMT_OK;
+}
+
+void DevBuf::release() {
+  if (ptr) cudaFree(ptr);
+  ptr = nullptr;
+  bytes = 0;
+}
+
+int sm_count() {
+  static int n = 0;
+  if (n == 0) {
+    int dev = 0;
+    cudaGetDevice(&dev);
+    cudaDeviceGetAttribute(&n, cudaDevAttrMultiProcessorCount, dev);
+    if (n <= 0) n = 148;
+  }
+  return n;
+}
+
+// Bound on max_r |phi| for a shell: s: sum|c|; p: sum|c| max_r r e^{-a r^2}; d: sum|c| max r^2 e^{-a r^2},
+// times the largest angular constant.  Used only to pick power-of-two operand scales.
+static double shell_bound(int L, const float* al, const float* co, int n) {
+  double b = 0;
+  for (int k = 0; k < n; ++k) {
+    const double a = al[k], c = std::fabs((double)co[k]);
+    if (L == 0) b += c;
+    else if (L == 1) b += c / std::sqrt(2.0 * std::exp(1.0) * a);
+    else b += c / (std::exp(1.0) * a);
+  }
+  const double ang = L == 0 ? YS : (L == 1 ? YP : 2 * YD0 + YD1);
+  return b * ang;
+}
+
+}  // namespace qmt
+
+using namespace qmt;
+
+qmt_mol::~qmt_mol() {
+  for (DevBuf* b : {&d_coords, &d_types, &d_shells, &d_alpha, &d_coeff, &d_alpha64, &d_coeff64,
+                    &d_P32, &d_P64, &d_Phi_hi, &d_Phi_lo, &d_tc_P, &d_fscale, &d_partials,
+                    &d_scalars, &d_pairs, &d_work})
+    b->release();
+}
+
+static qmt_status upload(DevBuf& b, const void* src, size_t n, cudaStream_t s) {
+  qmt_status st = b.reserve(n);
+  if (st) return st;
+  QMT_CUDA(cudaMemcpyAsync(b.ptr, src, n, cudaMemcpyHostToDevice, s));
+  return QMT_OK;
+}
+
+qmt_status qmt_mol::upload_coords(const float* c, cudaStream_t s) {
+  coords.assign(c, c + 3 * natoms);
+  for (float v : coords)
+    if (!std::isfinite(v)) return fail(QMT_NAN, "non-finite coordinate");
+  return upload(d_coords, coords.data(), coords.size() * sizeof(float), s);
+}
+
+qmt_status qmt_mol::upload_dm(const float* dm, cudaStream_t s) {
+  const int n = norbs, np = npad;
+  P64.assign((size_t)np * np, 0.0);
+  for (int p = 0; p < n; ++p)
+    for (int q = 0; q <= p; ++q) {
+      const float v = dm[(size_t)p * n + q];
+      if (!std::isfinite(v)) return fail(QMT_NAN, "non-finite density matrix entry");
+      P64[(size_t)p * np + q] = v;
+      P64[(size_t)q * np + p] = v;
+    }
+  std::vector<float> P32(P64.begin(), P64.end());
+  qmt_status st = upload(d_P64, P64.data(), P64.size() * sizeof(double), s);
+  if (st) return st;
+  st = upload(d_P32, P32.data(), P32.size() * sizeof(float), s);
+  if (st) return st;
+  // host copies must outlive the async copies: synchronise before the vectors go away
+  QMT_CUDA(cudaStreamSynchronize(s));
+  tc_prec = -1;
+  gto_ready = false;
+  return QMT_OK;
+}
+
+extern "C" {
+
+const char* qmt_last_error(void) { return g_last_error.c_str(); }
+
+int qmt_abi_version(void) { return 1; }
+
+qmt_status qmt_init(int device) {
+  int n = 0;
+  cudaError_t e = cudaGetDeviceCount(&n);
+  if (e != cudaSuccess || n == 0) return fail(QMT_NO_DEVICE, "no CUDA device");
+  if (device < 0 || device >= n) return fail(QMT_BAD_ARG, "device index out of range");
+  QMT_CUDA(cudaSetDevice(device));
+  int major = 0;
+  QMT_CUDA(cudaDeviceGetAttribute(&major, cudaDevAttrComputeCapabilityMajor, device));
+  if (major != 10) return fail(QMT_NO_DEVICE, "libqmtools_b200 needs an sm_100 device");
+  return QMT_OK;
+}
+
+qmt_status qmt_mol_create(int natoms, const int32_t* types, const float* coords, int norbs,
+                          const int16_t* almos, int nparams, const float* alphas,
+                          const float* coeffs, const float* dm, void* stream, qmt_mol** out) {
+  if (!out || !types || !coords || !almos || !alphas || !coeffs || !dm)
+    return fail(QMT_BAD_ARG, "null argument");
+  *out = nullptr;
+  if (natoms <= 0 || norbs <= 0 || nparams <= 0) return fail(QMT_BAD_ARG, "empty molecule");
+  cudaStream_t s = as_stream(stream);
+  auto* m = new qmt_mol();
+  m->natoms = natoms;
+  m->norbs = norbs;
+  m->npad = (norbs + 31) / 32 * 32;
+  m->types.assign(types, types + natoms);
+  m->qtot = 0;
+  for (int a = 0; a < natoms; ++a) m->qtot += types[a];
+  // group the per-function ALMO rows into shells (qmtools/qmtools.py:163-171)
+  static const int mord[3][5] = {{0}, {0, 1, -1}, {0, 1, -1, 2, -2}};
+  int f = 0;
+  m->fbound.assign(m->npad, 0.0);
+  while (f < norbs) {
+    const int a = almos[4 * f + 0], L = almos[4 * f + 1], so = almos[4 * f + 3];
+    if (a < 0 || a >= natoms) {
+      delete m;
+      return fail(QMT_BAD_ARG, "ALMO atom index out of range");
+    }
+    if (L < 0 || L > MAX_L) {
+      delete m;
+      return fail(QMT_UNSUPPORTED_L, "basis shell with L > 2");
+    }
+    if (f + 2 * L + 1 > norbs || so < 0 || so + MAXAOC > nparams) {
+      delete m;
+      return fail(QMT_BAD_ARG, "truncated shell in ALMO table");
+    }
+    for (int k = 0; k < 2 * L + 1; ++k) {
+      const int16_t* r = almos + 4 * (f + k);
+      if (r[0] != a || r[1] != L || r[3] != so || r[2] != mord[L][k]) {
+        delete m;
+        return fail(QMT_BAD_ARG, "ALMO rows of a shell must follow the m order of the basis");
+      }
+    }
+    Shell sh{};
+    sh.atom = a;
+    sh.L = L;
+    sh.func = f;
+    sh.prim = (int)m->alpha.size();
+    int np = 0;
+    for (int k = 0; k < MAXAOC; ++k) {
+      if (coeffs[so + k] == 0.0f) continue;  // padded slots contribute exactly zero
+      m->alpha.push_back(alphas[so + k]);
+      m->coeff.push_back(coeffs[so + k]);
+      ++np;
+    }
+    sh.nprim = np;
+    const double bnd = shell_bound(L, m->alpha.data() + sh.prim, m->coeff.data() + sh.prim, np);
+    for (int k = 0; k < 2 * L + 1; ++k) m->fbound[f + k] = bnd;
+    m->shells.push_back(sh);
+    f += 2 * L + 1;
+  }
+  m->nshells = (int)m->shells.size();
+  m->alpha64.assign(m->alpha.begin(), m->alpha.end());
+  m->coeff64.assign(m->coeff.begin(), m->coeff.end());
+  if (m->alpha.empty()) {
+    m->alpha.push_back(0.f);
+    m->coeff.push_back(0.f);
+    m->alpha64.push_back(0.);
+    m->coeff64.push_back(0.);
+  }
+  qmt_status st;
+  if ((st = m->upload_coords(coords, s)) ||
+      (st = upload(m->d_types, m->types.data(), natoms * sizeof(int), s)) ||
+      (st = upload(m->d_shells, m->shells.data(), m->shells.size() * sizeof(Shell), s)) ||
+      (st = upload(m->d_alpha, m->alpha.data(), m->alpha.size() * sizeof(float), s)) ||
+      (st = upload(m->d_coeff, m->coeff.data(), m->coeff.size() * sizeof(float), s)) ||
+      (st = upload(m->d_alpha64, m->alpha64.data(), m->alpha64.size() * sizeof(double), s)) ||
+      (st = upload(m->d_coeff64, m->coeff64.data(), m->coeff64.size() * sizeof(double), s)) ||
+      (st = m->upload_dm(dm, s))) {
+    delete m;
+    return st;
+  }
+  *out = m;
+  return QMT_OK;
+}
+
+qmt_status qmt_mol_set_coords(qmt_mol* mol, const float* coords, void* stream) {
+  if (!mol || !coords) return fail(QMT_BAD_ARG, "null argument");
+  cudaStream_t s = as_stream(stream);
+  qmt_status st = mol->upload_coords(coords, s);
+  if (st) return st;
+  QMT_CUDA(cudaStreamSynchronize(s));
+  mol->gto_ready = false;
+  return QMT_OK;
+}
+
+qmt_status qmt_mol_set_dm(qmt_mol* mol, const float* dm, void* stream) {
+  if (!mol || !dm) return fail(QMT_BAD_ARG, "null argument");
+  return mol->upload_dm(dm, as_stream(stream));
+}
+
+qmt_status qmt_mol_destroy(qmt_mol* mol) {
+  if (!mol) return QMT_OK;
+  cudaDeviceSynchronize();
+  delete mol;
+  return QMT_OK;
+}
+
+}  // extern "C"
+
+MolView qmt_mol::view() const {
+  MolView v;
+  v.natoms = natoms;
+  v.nshells = nshells;
+  v.norbs = norbs;
+  v.npad = npad;
+  v.coords = (const float*)d_coords.ptr;
+  v.types = (const int*)d_types.ptr;
+  v.shells = (const Shell*)d_shells.ptr;
+  v.alpha = (const float*)d_alpha.ptr;
+  v.coeff = (const float*)d_coeff.ptr;
+  v.alpha64 = (const double*)d_alpha64.ptr;
+  v.coeff64 = (const double*)d_coeff64.ptr;
+  return v;
+}

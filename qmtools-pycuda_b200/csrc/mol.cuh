@@ -1,0 +1,55 @@
+// Host-side molecule handle and device buffers.
+#pragma once
+
+#include <vector>
+
+#include "qmt_common.cuh"
+
+namespace qmt {
+
+// Owned device allocation that only grows.
+struct DevBuf {
+  void* ptr = nullptr;
+  size_t bytes = 0;
+  qmt_status reserve(size_t n);
+  void release();
+  template <typename T>
+  T* as() const { return reinterpret_cast<T*>(ptr); }
+};
+
+int sm_count();
+
+}  // namespace qmt
+
+struct qmt_mol {
+  int natoms = 0, norbs = 0, npad = 0, nshells = 0;
+  double qtot = 0;
+  std::vector<int> types;
+  std::vector<float> coords;
+  std::vector<qmt::Shell> shells;
+  std::vector<float> alpha, coeff;
+  std::vector<double> alpha64, coeff64;
+  std::vector<double> P64;      // symmetric (from the lower triangle), npad x npad
+  std::vector<double> fbound;   // per-function bound on |phi|
+
+  qmt::DevBuf d_coords, d_types, d_shells, d_alpha, d_coeff, d_alpha64, d_coeff64;
+  qmt::DevBuf d_P32, d_P64;
+  // tensor-core operands
+  int tc_prec = -1;             // precision the operands below were built for
+  int tc_g = 0;                 // global exponent of the scaled density matrix
+  qmt::DevBuf d_tc_P;           // split, scaled density matrix (hi then lo)
+  qmt::DevBuf d_fscale;         // per-function power-of-two scale of Phi
+  qmt::DevBuf d_Phi_hi, d_Phi_lo;
+  // scratch
+  qmt::DevBuf d_partials, d_scalars, d_work;
+  // analytic potential: primitive-pair table
+  bool gto_ready = false;
+  int gto_npairs = 0;
+  size_t gto_doff_bytes = 0;
+  qmt::DevBuf d_pairs;
+
+  ~qmt_mol();
+  qmt_status upload_coords(const float* c, cudaStream_t s);
+  qmt_status upload_dm(const float* dm, cudaStream_t s);
+  qmt::MolView view() const;
+};

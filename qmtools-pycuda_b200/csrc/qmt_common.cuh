@@ -1,0 +1,140 @@
+// Shared definitions for libqmtools_b200: status handling, molecule layout on the
+// device, and the basis-function evaluation used by every density kernel.
+#pragma once
+
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+#include <cmath>
+#include <string>
+#include <vector>
+
+#include "qmtools_b200.h"
+
+namespace qmt {
+
+// ---- status ------------------------------------------------------------------------
+void set_error(const std::string& msg);
+qmt_status fail(qmt_status code, const std::string& msg);
+qmt_status cuda_fail(cudaError_t e, const char* what);
+
+#define QMT_CUDA(call)                                              \
+  do {                                                              \
+    cudaError_t e_ = (call);                                        \
+    if (e_ != cudaSuccess) return ::qmt::cuda_fail(e_, #call);      \
+  } while (0)
+
+#define QMT_CHECK_LAUNCH(what)                                      \
+  do {                                                              \
+    cudaError_t e_ = cudaGetLastError();                            \
+    if (e_ != cudaSuccess) return ::qmt::cuda_fail(e_, what);       \
+  } while (0)
+
+inline cudaStream_t as_stream(void* s) { return reinterpret_cast<cudaStream_t>(s); }
+
+constexpr double ANG2BOR = 1.8897259886;   // kernel_common.h:1
+constexpr int MAXAOC = 20;                 // kernel_common.h:10
+constexpr int MAX_L = 2;
+
+// Real solid harmonics times r^l (the reference's constants, kernel_density.cu:17-28).
+constexpr double YS = 0.28209479177387814;
+constexpr double YP = 0.4886025119029199;
+constexpr double YD1 = 1.0925484305920792;
+constexpr double YD0 = 0.31539156525252005;
+constexpr double YD2 = 0.5462742152960396;
+
+// One contracted shell.  Functions of a shell are contiguous in the basis order and
+// follow the reference's m order (qmtools/qmtools.py:52): p = (z, x, y),
+// d = (2zz-xx-yy, xz, yz, xx-yy, xy).
+struct Shell {
+  int atom;
+  int L;
+  int nprim;
+  int prim;    // offset into the primitive arrays
+  int func;    // first basis function
+  int pad[3];
+};
+
+// ---- device-side molecule view --------------------------------------------------------
+struct MolView {
+  int natoms;
+  int nshells;
+  int norbs;
+  int npad;                  // norbs rounded up for GEMM operands
+  const float* coords;       // [natoms*3] bohr
+  const int* types;          // [natoms]
+  const Shell* shells;       // [nshells]
+  const float* alpha;        // [nprim_total]
+  const float* coeff;        // [nprim_total]
+  const double* alpha64;
+  const double* coeff64;
+};
+
+// Writes the values of the shell's functions at displacement (dx,dy,dz) from its atom
+// into out[0..2L].  T = float or double.  Primitives with alpha*r^2 > cut contribute
+// below exp(-cut) relative and are skipped.
+template <typename T>
+__device__ __forceinline__ int shell_values(const Shell& sh, const T* __restrict__ al,
+                                            const T* __restrict__ co, T dx, T dy, T dz,
+                                            T* out) {
+  const T r2 = dx * dx + dy * dy + dz * dz;
+  T rad = T(0);
+  for (int k = 0; k < sh.nprim; ++k) {
+    const T e = al[sh.prim + k] * r2;
+    if (e < T(60)) rad += co[sh.prim + k] * exp(-e);
+  }
+  if (sh.L == 0) {
+    out[0] = T(YS) * rad;
+    return 1;
+  }
+  if (sh.L == 1) {
+    const T c = T(YP) * rad;
+    out[0] = c * dz;
+    out[1] = c * dx;
+    out[2] = c * dy;
+    return 3;
+  }
+  const T c1 = T(YD1) * rad;
+  out[0] = T(YD0) * rad * (T(2) * dz * dz - dx * dx - dy * dy);
+  out[1] = c1 * dx * dz;
+  out[2] = c1 * dz * dy;
+  out[3] = T(YD2) * rad * (dx * dx - dy * dy);
+  out[4] = c1 * dx * dy;
+  return 5;
+}
+
+// Point of row `row` of a density tile: voxels are taken in flat x-fastest order,
+// `vpt` voxels per tile, s^3 sub-points per voxel (sub-point index fastest).
+struct PointMap {
+  int nx, ny, nz;
+  int s;          // subgrid
+  int s3;
+  int vpt;        // voxels per tile
+  int64_t nvox;
+  float h;
+  float ox, oy, oz;
+};
+
+template <typename T>
+__device__ __forceinline__ bool tile_point(const PointMap& pm, int64_t tile, int row,
+                                           T& x, T& y, T& z, int64_t& vox) {
+  const int v = row / pm.s3;
+  const int sub = row - v * pm.s3;
+  if (v >= pm.vpt) return false;
+  vox = tile * pm.vpt + v;
+  if (vox >= pm.nvox) return false;
+  const int64_t ix = vox % pm.nx;
+  const int64_t iy = (vox / pm.nx) % pm.ny;
+  const int64_t iz = vox / ((int64_t)pm.nx * pm.ny);
+  const int sx = sub % pm.s;
+  const int sy = (sub / pm.s) % pm.s;
+  const int sz = sub / (pm.s * pm.s);
+  const T inv = T(1) / T(pm.s);
+  const T h = T(pm.h);
+  x = T(pm.ox) + (T(ix) + (T(sx) + T(0.5)) * inv) * h;
+  y = T(pm.oy) + (T(iy) + (T(sy) + T(0.5)) * inv) * h;
+  z = T(pm.oz) + (T(iz) + (T(sz) + T(0.5)) * inv) * h;
+  return true;
+}
+
+}  // namespace qmt
