@@ -91,6 +91,11 @@ qmt_status qmt_density(qmt_mol* mol, int nx, int ny, int nz, float step,
                        float ox, float oy, float oz, int subgrid, int precision,
                        int rescale, float* qube_dev, double* sum_out, void* stream);
 
+/* Selects the tensor-core density implementation (new; process-wide): 0 = automatic (fused
+ * when the contraction is fp16/bf16 and N <= 320, staged otherwise), 1 = staged (basis values
+ * through HBM), 2 = fused (basis values stay in shared memory). */
+qmt_status qmt_set_density_path(int mode);
+
 /* ---- analytic GTO potential --------------------------------------------------------- */
 /* QMTools.Compute_hartree (qmtools/qmtools.py:2436-2489) with gpu_hartree_GTO
  * (kernel_hartree.cu:288-869): V(C) = -2 sum_pq P_pq (phi_p phi_q | 1/|r-C|) + sum_A Z_A/|C-R_A|

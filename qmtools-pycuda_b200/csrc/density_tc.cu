@@ -520,6 +520,7 @@ static qmt_status ensure_tc_operands(qmt_mol* m, int prec, const TcShape& sh, cu
   QMT_CUDA(cudaStreamSynchronize(s));
   m->tc_g = g;
   m->tc_prec = prec;
+  m->fused_prec = -1;   // d_fscale now holds the staged path's scales
   return QMT_OK;
 }
 
@@ -596,6 +597,412 @@ static qmt_status run_tc(qmt_mol* m, const TcShape& sh, const PointMap& pm, int6
   return QMT_OK;
 }
 
+// ---------------------------------------------------------------------------------------
+// Fused path (kind::f16 formats, K <= 320): Phi' never leaves shared memory.
+//
+//   rho = sum_jk Phi_j P_jk Phi_k = 2 sum_k Phi_k (Phi U)_k,  U = triu(P, 1) + diag(P)/2,
+// so only the upper triangle of the scaled density matrix is streamed and multiplied: the
+// K-step covering rows j in [j0, j0+16) of U only touches output columns k >= j0.
+//
+// CTA layout (one per SM, persistent over 128-row tiles), 10 warps:
+//   warp 0     TMA producer of U (32-byte swizzled, one 16-element K-step per stage);
+//              U is the same for every tile, so it streams ahead across tiles;
+//   warp 1     TMEM allocation and the single MMA-issuing thread;
+//   warps 2-9  evaluate Phi' for the tile straight into the 128-byte swizzled K-major
+//              A layout (hi and lo pieces), then run the epilogue: T' rows from TMEM
+//              (warp w reads lane quadrant w%4, column chunks of parity (w-2)/4), Phi'
+//              from shared memory, FP64 row-dot, sub-point average, grid write, FP64 sums.
+// Per tile the phases are serial (A is resident and single-buffered); the U stream and
+// the MMA run asynchronously to the compute warps' work.
+// ---------------------------------------------------------------------------------------
+struct FusedParams {
+  MolView mol;
+  PointMap pm;
+  int64_t ntiles;
+  int kpad, ksteps, nsplit, stages;
+  uint32_t a_bytes;        // one A piece: 128 rows x kpad x 2 B
+  uint32_t b_slot;         // one U piece slot in a stage: kpad rows x 32 B
+  uint32_t stage_bytes;
+  uint32_t fmt;
+  const float* fscale;
+  float* qube;
+  double* partials;
+  double outscale;
+  double inv_g2;           // 2 * 2^-g
+  int* err;
+};
+
+// Byte offset of element (row, j) in the 128-byte swizzled K-major A tile.
+__device__ __forceinline__ uint32_t a_offset(int row, int j) {
+  const int kc = j >> 6, e = j & 63;
+  const int u = (e >> 3) ^ (row & 7);
+  return (uint32_t)(kc * 16384 + (row >> 3) * 1024 + (row & 7) * 128 + u * 16 + (e & 7) * 2);
+}
+
+__device__ __forceinline__ uint64_t sw32_kmajor_desc(uint32_t saddr) {
+  uint64_t d = 0;
+  d |= (uint64_t)((saddr >> 4) & 0x3FFFu);
+  d |= (uint64_t)1u << 16;             // leading byte offset (unused for swizzled K-major)
+  d |= (uint64_t)(256u >> 4) << 32;    // stride byte offset: 8 rows x 32 B
+  d |= (uint64_t)1u << 46;             // descriptor version for sm_100
+  d |= (uint64_t)6u << 61;             // 32-byte swizzle
+  return d;
+}
+
+template <int FMT>
+__device__ __forceinline__ void store_split16(uint8_t* hi, uint8_t* lo, uint32_t off, float x, bool two) {
+  if constexpr (FMT == FMT_F16) {
+    const __half h = __float2half_rn(x);
+    *reinterpret_cast<__half*>(hi + off) = h;
+    if (two) *reinterpret_cast<__half*>(lo + off) = __float2half_rn(x - __half2float(h));
+  } else {
+    const __nv_bfloat16 h = __float2bfloat16_rn(x);
+    *reinterpret_cast<__nv_bfloat16*>(hi + off) = h;
+    if (two) *reinterpret_cast<__nv_bfloat16*>(lo + off) = __float2bfloat16_rn(x - __bfloat162float(h));
+  }
+}
+
+template <int FMT>
+__device__ __forceinline__ void unpack8(uint4 a, float* out) {
+  const uint32_t w[4] = {a.x, a.y, a.z, a.w};
+#pragma unroll
+  for (int j = 0; j < 4; ++j) {
+    if constexpr (FMT == FMT_F16) {
+      const float2 f = __half22float2(*reinterpret_cast<const __half2*>(&w[j]));
+      out[2 * j] = f.x;
+      out[2 * j + 1] = f.y;
+    } else {
+      out[2 * j] = __uint_as_float(w[j] << 16);
+      out[2 * j + 1] = __uint_as_float(w[j] & 0xffff0000u);
+    }
+  }
+}
+
+template <int FMT>
+__global__ void __launch_bounds__(320, 1)
+    density_fused_kernel(const __grid_constant__ CUtensorMap tmU_hi, const __grid_constant__ CUtensorMap tmU_lo,
+                         const FusedParams p) {
+  extern __shared__ uint8_t smem_dyn[];
+  __shared__ __align__(8) uint64_t full_bar[MAX_STAGES], empty_bar[MAX_STAGES];
+  __shared__ __align__(8) uint64_t a_full, t_full, drain_bar;
+  __shared__ uint32_t tmem_slot;
+  __shared__ double pos[128][3];
+  __shared__ double rho_part[2][128];
+  __shared__ double red[8];
+  __shared__ volatile int abort_flag;
+
+  uint8_t* smem = reinterpret_cast<uint8_t*>((reinterpret_cast<uintptr_t>(smem_dyn) + 1023) & ~uintptr_t(1023));
+  uint8_t* A_hi = smem;
+  uint8_t* A_lo = smem + p.a_bytes;
+  uint8_t* stages = smem + p.nsplit * p.a_bytes;
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  const bool two = p.nsplit == 2;
+  const MolView& mol = p.mol;
+
+  if (threadIdx.x == 0) {
+    abort_flag = 0;
+    for (int s = 0; s < p.stages; ++s) {
+      mbar_init(&full_bar[s], 1);
+      mbar_init(&empty_bar[s], 1);
+    }
+    mbar_init(&a_full, 1);
+    mbar_init(&t_full, 1);
+    mbar_init(&drain_bar, 1);
+    fence_mbar_init();
+  }
+  // zero A once: padding columns and rows never written later stay zero
+  for (uint32_t i = threadIdx.x; i < p.nsplit * p.a_bytes / 16; i += blockDim.x)
+    reinterpret_cast<uint4*>(smem)[i] = make_uint4(0, 0, 0, 0);
+  if (warp == 0 && lane == 0) {
+    prefetch_tmap(&tmU_hi);
+    if (two) prefetch_tmap(&tmU_lo);
+  }
+  if (warp == 1) {
+    tmem_alloc(&tmem_slot, 512);
+    tmem_relinquish();
+  }
+  tc_fence_before();
+  __syncthreads();
+  tc_fence_after();
+  const uint32_t tmem = tmem_slot;
+
+  if (warp == 0) {
+    if (lane == 0) {
+      uint32_t it = 0;
+      int last_par[MAX_STAGES];
+      for (int s = 0; s < MAX_STAGES; ++s) last_par[s] = -1;
+      bool ok = true;
+      for (int64_t t = blockIdx.x; t < p.ntiles && ok; t += gridDim.x) {
+        for (int ks = 0; ks < p.ksteps; ++ks, ++it) {
+          const int s = it % p.stages;
+          const uint32_t ph = (it / p.stages) & 1u;
+          if (!mbar_wait(&empty_bar[s], ph ^ 1u, &abort_flag)) {
+            ok = false;
+            break;
+          }
+          const int j0 = ks * 16;
+          const int npc = (p.kpad - j0 + 63) / 64;  // 64-row pieces
+          uint8_t* st = stages + (size_t)s * p.stage_bytes;
+          mbar_expect_tx(&full_bar[s], (uint32_t)(npc * 64 * 32 * p.nsplit));
+          for (int c = 0; c < npc; ++c) {
+            tma_load_2d(st + c * 2048, &tmU_hi, &full_bar[s], j0, j0 + 64 * c);
+            if (two) tma_load_2d(st + p.b_slot + c * 2048, &tmU_lo, &full_bar[s], j0, j0 + 64 * c);
+          }
+          last_par[s] = (int)ph;
+        }
+      }
+      if (!ok)
+        for (int s = 0; s < p.stages; ++s)
+          if (last_par[s] >= 0) mbar_wait(&full_bar[s], (uint32_t)last_par[s], &abort_flag, 1u << 20);
+    }
+  } else if (warp == 1) {
+    if (lane == 0) {
+      uint32_t it = 0, tile_it = 0;
+      bool ok = true;
+      const uint32_t abase = smem_u32(A_hi), lbase = smem_u32(A_lo);
+      for (int64_t t = blockIdx.x; t < p.ntiles && ok; t += gridDim.x, ++tile_it) {
+        if (!mbar_wait(&a_full, tile_it & 1u, &abort_flag)) break;
+        tc_fence_after();
+        for (int ks = 0; ks < p.ksteps; ++ks, ++it) {
+          const int s = it % p.stages;
+          const uint32_t ph = (it / p.stages) & 1u;
+          if (!mbar_wait(&full_bar[s], ph, &abort_flag)) {
+            ok = false;
+            break;
+          }
+          tc_fence_after();
+          const int j0 = ks * 16;
+          const uint32_t aoff = (uint32_t)((j0 >> 6) * 16384 + ((j0 & 63) >> 4) * 32);
+          const uint32_t bst = smem_u32(stages + (size_t)s * p.stage_bytes);
+          for (int c0 = j0; c0 < p.kpad; c0 += 256) {
+            const int n = min(256, p.kpad - c0);
+            const uint32_t idesc = make_idesc(p.fmt, 128, (uint32_t)n);
+            const uint32_t boff = (uint32_t)(c0 - j0) * 32u;
+            const uint32_t d = tmem + (uint32_t)c0;
+            mma_f16(d, sw128_kmajor_desc(abase + aoff), sw32_kmajor_desc(bst + boff), idesc, ks > 0 ? 1u : 0u);
+            if (two) {
+              mma_f16(d, sw128_kmajor_desc(abase + aoff), sw32_kmajor_desc(bst + p.b_slot + boff), idesc, 1u);
+              mma_f16(d, sw128_kmajor_desc(lbase + aoff), sw32_kmajor_desc(bst + boff), idesc, 1u);
+            }
+          }
+          tc_commit(&empty_bar[s]);
+        }
+        if (ok) tc_commit(&t_full);
+      }
+      tc_commit(&drain_bar);
+      mbar_wait(&drain_bar, 0u, &abort_flag, 1u << 22);
+    }
+  } else {
+    const int ct = threadIdx.x - 64;    // 0..255 compute thread
+    const int q = warp & 3;             // TMEM lane quadrant
+    const int hh = (warp - 2) >> 2;     // column-chunk parity handled in the epilogue
+    const int row = q * 32 + lane;
+    uint32_t tile_it = 0;
+    for (int64_t t = blockIdx.x; t < p.ntiles; t += gridDim.x, ++tile_it) {
+      // ---- Phi' for the tile into A -------------------------------------------------------
+      if (ct < 128) {
+        double x, y, z;
+        int64_t vox;
+        if (!tile_point<double>(p.pm, t, ct, x, y, z, vox)) x = y = z = 1e30;
+        pos[ct][0] = x;
+        pos[ct][1] = y;
+        pos[ct][2] = z;
+      }
+      named_barrier(1, 256);
+      for (int itm = ct; itm < 128 * mol.natoms; itm += 256) {
+        const int r = itm & 127, a = itm >> 7;
+        const double px = pos[r][0];
+        const int s0 = mol.atom_shell[a], s1 = mol.atom_shell[a + 1];
+        if (px > 1e29) {
+          for (int sidx = s0; sidx < s1; ++sidx) {
+            const Shell sh = mol.shells[sidx];
+            for (int k = 0; k < 2 * sh.L + 1; ++k) store_split16<FMT>(A_hi, A_lo, a_offset(r, sh.func + k), 0.f, two);
+          }
+          continue;
+        }
+        // FP64 displacement from the nucleus, rounded once (accuracy of steep exponents)
+        const float dx = (float)(px - (double)mol.coords[3 * a]);
+        const float dy = (float)(pos[r][1] - (double)mol.coords[3 * a + 1]);
+        const float dz = (float)(pos[r][2] - (double)mol.coords[3 * a + 2]);
+        for (int sidx = s0; sidx < s1; ++sidx) {
+          const Shell sh = mol.shells[sidx];
+          float v[5];
+          const int n = shell_values<float>(sh, mol.alpha, mol.coeff, dx, dy, dz, v);
+          for (int k = 0; k < n; ++k) {
+            const int j = sh.func + k;
+            store_split16<FMT>(A_hi, A_lo, a_offset(r, j), v[k] * p.fscale[j], two);
+          }
+        }
+      }
+      // generic-proxy writes of A must be visible to the tensor core
+      asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+      tc_fence_before();
+      named_barrier(1, 256);
+      if (ct == 0) mbar_arrive(&a_full);
+      // ---- epilogue -----------------------------------------------------------------------
+      if (!mbar_wait(&t_full, tile_it & 1u, &abort_flag)) break;
+      tc_fence_after();
+      double acc = 0.0;
+      for (int c = hh; c * 32 < p.kpad; c += 2) {
+        const int col = c * 32;
+        float v[32], ph[32];
+        tmem_ld32(tmem + ((uint32_t)(q * 32) << 16) + (uint32_t)col, v);
+        const int kc = col >> 6, u0 = (col & 63) >> 3;
+        const uint8_t* rb = A_hi + kc * 16384 + (row >> 3) * 1024 + (row & 7) * 128;
+#pragma unroll
+        for (int u = 0; u < 4; ++u) unpack8<FMT>(*reinterpret_cast<const uint4*>(rb + (((u0 + u) ^ (row & 7)) * 16)), ph + 8 * u);
+        if (two) {
+          const uint8_t* rl = A_lo + kc * 16384 + (row >> 3) * 1024 + (row & 7) * 128;
+#pragma unroll
+          for (int u = 0; u < 4; ++u) {
+            float lo8[8];
+            unpack8<FMT>(*reinterpret_cast<const uint4*>(rl + (((u0 + u) ^ (row & 7)) * 16)), lo8);
+#pragma unroll
+            for (int e = 0; e < 8; ++e) ph[8 * u + e] += lo8[e];
+          }
+        }
+#pragma unroll
+        for (int k = 0; k < 32; ++k) acc = fma((double)ph[k], (double)v[k], acc);
+      }
+      tc_fence_before();
+      rho_part[hh][row] = acc;
+      named_barrier(1, 256);
+      double mysum = 0.0;
+      if (ct < p.pm.vpt) {
+        double r = 0.0;
+        for (int sub = 0; sub < p.pm.s3; ++sub) {
+          const int rr = ct * p.pm.s3 + sub;
+          r += rho_part[0][rr] + rho_part[1][rr];
+        }
+        const int64_t vox = t * p.pm.vpt + ct;
+        if (vox < p.pm.nvox) {
+          const float qv = (float)(r * p.inv_g2 * p.outscale);
+          p.qube[vox] = qv;
+          mysum = qv;
+        }
+      }
+      for (int o = 16; o > 0; o >>= 1) mysum += __shfl_xor_sync(0xffffffffu, mysum, o);
+      if (lane == 0) red[warp - 2] = mysum;
+      named_barrier(1, 256);
+      if (ct == 0) {
+        double tot = 0;
+        for (int w = 0; w < 8; ++w) tot += red[w];
+        p.partials[t] = tot;
+      }
+      named_barrier(1, 256);
+    }
+  }
+
+  tc_fence_before();
+  __syncthreads();
+  if (abort_flag && threadIdx.x == 0) atomicExch(p.err, 1);
+  if (warp == 1) {
+    tc_fence_after();
+    tmem_dealloc(tmem, 512);
+  }
+}
+
+static qmt_status make_map_sw32(CUtensorMap* m, const void* base, uint64_t inner, uint64_t outer) {
+  auto fn = encode_fn();
+  if (!fn) return fail(QMT_CUDA_ERR, "cuTensorMapEncodeTiled unavailable");
+  cuuint64_t dims[2] = {inner, outer};
+  cuuint64_t strides[1] = {inner * 2};
+  cuuint32_t box[2] = {16, 64};
+  cuuint32_t estr[2] = {1, 1};
+  CUresult r = fn(m, CU_TENSOR_MAP_DATA_TYPE_UINT16, 2, const_cast<void*>(base), dims, strides, box, estr,
+                  CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_32B, CU_TENSOR_MAP_L2_PROMOTION_L2_256B,
+                  CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+  if (r != CUDA_SUCCESS) return fail(QMT_CUDA_ERR, "cuTensorMapEncodeTiled failed");
+  return QMT_OK;
+}
+
+// Upper-triangular scaled density matrix for the fused path: row n (output column) holds
+// U_jn for j <= n, i.e. Ptilde_jn for j < n and Ptilde_nn / 2 on the diagonal.  Rows are
+// padded to kpad + 64 so every 64-row TMA box stays inside the tensor.
+static qmt_status ensure_fused_operands(qmt_mol* m, int prec, const TcShape& sh, cudaStream_t s) {
+  if (m->fused_prec == prec) return QMT_OK;
+  const int n = m->norbs, np = m->npad, K = sh.kpad;
+  std::vector<int> sj(K, 0);
+  std::vector<float> fs(K, 0.f);
+  for (int j = 0; j < n; ++j) {
+    const double b = std::max(m->fbound[j], 1e-30);
+    sj[j] = std::max(-60, std::min(60, (int)std::floor(std::log2(16000.0 / b))));
+    fs[j] = (float)std::ldexp(1.0, sj[j]);
+  }
+  double mx = 0;
+  for (int j = 0; j < n; ++j)
+    for (int k = j; k < n; ++k)
+      mx = std::max(mx, std::fabs(std::ldexp(m->P64[(size_t)j * np + k], -sj[j] - sj[k])));
+  int g = mx > 0 ? (int)std::floor(std::log2(16000.0 / mx)) : 0;
+  g = std::max(-100, std::min(100, g));
+  const int rows = K + 64;
+  const size_t piece = (size_t)rows * K * 2;
+  std::vector<uint8_t> host(2 * piece, 0);
+  for (int nn = 0; nn < n; ++nn)
+    for (int j = 0; j <= nn; ++j) {
+      double v = std::ldexp(m->P64[(size_t)j * np + nn], g - sj[j] - sj[nn]);
+      if (j == nn) v *= 0.5;
+      split_host(v, sh.fmt, host.data(), host.data() + piece, (size_t)nn * K + j);
+    }
+  qmt_status st;
+  if ((st = m->d_fused_B.reserve(2 * piece))) return st;
+  if ((st = m->d_fscale.reserve(K * sizeof(float)))) return st;
+  QMT_CUDA(cudaMemcpyAsync(m->d_fused_B.ptr, host.data(), 2 * piece, cudaMemcpyHostToDevice, s));
+  QMT_CUDA(cudaMemcpyAsync(m->d_fscale.ptr, fs.data(), K * sizeof(float), cudaMemcpyHostToDevice, s));
+  QMT_CUDA(cudaStreamSynchronize(s));
+  m->fused_g = g;
+  m->fused_prec = prec;
+  m->tc_prec = -1;   // d_fscale now holds the fused path's scales
+  return QMT_OK;
+}
+
+template <int FMT>
+static qmt_status run_fused(qmt_mol* m, const TcShape& sh, const PointMap& pm, int64_t ntiles, float* qube,
+                            double outscale, cudaStream_t s) {
+  qmt_status st;
+  const int K = sh.kpad;
+  const size_t piece = (size_t)(K + 64) * K * 2;
+  CUtensorMap tU_hi, tU_lo;
+  const uint8_t* B = m->d_fused_B.as<uint8_t>();
+  if ((st = make_map_sw32(&tU_hi, B, K, K + 64)) || (st = make_map_sw32(&tU_lo, B + piece, K, K + 64)))
+    return st;
+  FusedParams p{};
+  p.mol = m->view();
+  p.pm = pm;
+  p.ntiles = ntiles;
+  p.kpad = K;
+  p.ksteps = K / 16;
+  p.nsplit = sh.nsplit;
+  p.a_bytes = 128u * K * 2u;
+  p.b_slot = (uint32_t)K * 32u;
+  p.stage_bytes = p.nsplit * p.b_slot;
+  p.fmt = (uint32_t)sh.fmt;
+  p.fscale = m->d_fscale.as<float>();
+  p.qube = qube;
+  p.partials = m->d_partials.as<double>();
+  p.outscale = outscale;
+  p.inv_g2 = 2.0 * std::ldexp(1.0, -m->fused_g);
+  p.err = reinterpret_cast<int*>(m->d_scalars.as<double>() + 8);
+  int maxsm = 0, dev = 0;
+  cudaGetDevice(&dev);
+  cudaDeviceGetAttribute(&maxsm, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev);
+  const int static_bytes = 6144;
+  const long avail = (long)maxsm - static_bytes - 1024 - (long)p.nsplit * p.a_bytes;
+  int stages = (int)std::min<long>(MAX_STAGES, avail / (long)p.stage_bytes);
+  if (stages < 2) return fail(QMT_BAD_ARG, "fused density tile does not fit in shared memory");
+  p.stages = stages;
+  const size_t dyn = (size_t)p.nsplit * p.a_bytes + (size_t)stages * p.stage_bytes + 1024;
+  auto kern = density_fused_kernel<FMT>;
+  QMT_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)dyn));
+  QMT_CUDA(cudaMemsetAsync(p.err, 0, sizeof(int), s));
+  const int grid = (int)std::min<int64_t>(ntiles, sm_count());
+  kern<<<grid, 320, dyn, s>>>(tU_hi, tU_lo, p);
+  QMT_CHECK_LAUNCH("density_fused_kernel");
+  return QMT_OK;
+}
+
+static int g_density_path = 0;   // 0 auto, 1 staged, 2 fused
+
 qmt_status density_tc(qmt_mol* mol, int nx, int ny, int nz, float step, float ox, float oy, float oz,
                       int subgrid, int precision, int rescale, float* qube, double* sum_out,
                       cudaStream_t s) {
@@ -604,12 +1011,21 @@ qmt_status density_tc(qmt_mol* mol, int nx, int ny, int nz, float step, float ox
   PointMap pm;
   int64_t ntiles;
   if ((st = make_point_map(nx, ny, nz, step, ox, oy, oz, subgrid, 128, pm, ntiles))) return st;
-  if ((st = ensure_tc_operands(mol, precision, sh, s))) return st;
   if ((st = mol->d_partials.reserve(ntiles * sizeof(double)))) return st;
   const double outscale = 2.0 * (double)step * step * step / pm.s3;
-  if (sh.fmt == FMT_TF32) st = run_tc<FMT_TF32>(mol, sh, pm, ntiles, precision, qube, outscale, s);
-  else if (sh.fmt == FMT_F16) st = run_tc<FMT_F16>(mol, sh, pm, ntiles, precision, qube, outscale, s);
-  else st = run_tc<FMT_BF16>(mol, sh, pm, ntiles, precision, qube, outscale, s);
+  const bool fusable = sh.fmt != FMT_TF32 && sh.kpad <= 320;
+  const bool fused = g_density_path == 2 ? fusable : (g_density_path == 1 ? false : fusable);
+  if (g_density_path == 2 && !fusable) return fail(QMT_BAD_ARG, "fused density path needs fp16/bf16 and N <= 320");
+  if (fused) {
+    if ((st = ensure_fused_operands(mol, precision, sh, s))) return st;
+    if (sh.fmt == FMT_F16) st = run_fused<FMT_F16>(mol, sh, pm, ntiles, qube, outscale, s);
+    else st = run_fused<FMT_BF16>(mol, sh, pm, ntiles, qube, outscale, s);
+  } else {
+    if ((st = ensure_tc_operands(mol, precision, sh, s))) return st;
+    if (sh.fmt == FMT_TF32) st = run_tc<FMT_TF32>(mol, sh, pm, ntiles, precision, qube, outscale, s);
+    else if (sh.fmt == FMT_F16) st = run_tc<FMT_F16>(mol, sh, pm, ntiles, precision, qube, outscale, s);
+    else st = run_tc<FMT_BF16>(mol, sh, pm, ntiles, precision, qube, outscale, s);
+  }
   if (st) return st;
   st = finish_density(mol, pm.nvox, ntiles, rescale, qube, sum_out, s);
   if (st) return st;
@@ -621,3 +1037,9 @@ qmt_status density_tc(qmt_mol* mol, int nx, int ny, int nz, float step, float ox
 }
 
 }  // namespace qmt
+
+extern "C" qmt_status qmt_set_density_path(int mode) {
+  if (mode < 0 || mode > 2) return qmt::fail(QMT_BAD_ARG, "density path must be 0 (auto), 1 (staged) or 2 (fused)");
+  qmt::g_density_path = mode;
+  return QMT_OK;
+}

@@ -79,7 +79,7 @@ using namespace qmt;
 qmt_mol::~qmt_mol() {
   for (DevBuf* b : {&d_coords, &d_types, &d_shells, &d_alpha, &d_coeff, &d_alpha64, &d_coeff64,
                     &d_P32, &d_P64, &d_Phi_hi, &d_Phi_lo, &d_tc_P, &d_fscale, &d_partials,
-                    &d_scalars, &d_pairs, &d_work})
+                    &d_scalars, &d_pairs, &d_work, &d_atom_shell, &d_fused_B})
     b->release();
 }
 
@@ -115,6 +115,7 @@ qmt_status qmt_mol::upload_dm(const float* dm, cudaStream_t s) {
   // host copies must outlive the async copies: synchronise before the vectors go away
   QMT_CUDA(cudaStreamSynchronize(s));
   tc_prec = -1;
+  fused_prec = -1;
   gto_ready = false;
   return QMT_OK;
 }
@@ -196,6 +197,16 @@ qmt_status qmt_mol_create(int natoms, const int32_t* types, const float* coords,
     f += 2 * L + 1;
   }
   m->nshells = (int)m->shells.size();
+  m->atom_shell.assign(natoms + 1, 0);
+  for (int a = 0, sidx = 0; a <= natoms; ++a) {
+    while (sidx < m->nshells && m->shells[sidx].atom < a) ++sidx;
+    m->atom_shell[a] = sidx;
+  }
+  for (int sidx = 1; sidx < m->nshells; ++sidx)
+    if (m->shells[sidx].atom < m->shells[sidx - 1].atom) {
+      delete m;
+      return fail(QMT_BAD_ARG, "basis functions must be grouped by atom in atom order");
+    }
   m->alpha64.assign(m->alpha.begin(), m->alpha.end());
   m->coeff64.assign(m->coeff.begin(), m->coeff.end());
   if (m->alpha.empty()) {
@@ -208,6 +219,7 @@ qmt_status qmt_mol_create(int natoms, const int32_t* types, const float* coords,
   if ((st = m->upload_coords(coords, s)) ||
       (st = upload(m->d_types, m->types.data(), natoms * sizeof(int), s)) ||
       (st = upload(m->d_shells, m->shells.data(), m->shells.size() * sizeof(Shell), s)) ||
+      (st = upload(m->d_atom_shell, m->atom_shell.data(), m->atom_shell.size() * sizeof(int), s)) ||
       (st = upload(m->d_alpha, m->alpha.data(), m->alpha.size() * sizeof(float), s)) ||
       (st = upload(m->d_coeff, m->coeff.data(), m->coeff.size() * sizeof(float), s)) ||
       (st = upload(m->d_alpha64, m->alpha64.data(), m->alpha64.size() * sizeof(double), s)) ||
@@ -253,6 +265,7 @@ MolView qmt_mol::view() const {
   v.coords = (const float*)d_coords.ptr;
   v.types = (const int*)d_types.ptr;
   v.shells = (const Shell*)d_shells.ptr;
+  v.atom_shell = (const int*)d_atom_shell.ptr;
   v.alpha = (const float*)d_alpha.ptr;
   v.coeff = (const float*)d_coeff.ptr;
   v.alpha64 = (const double*)d_alpha64.ptr;

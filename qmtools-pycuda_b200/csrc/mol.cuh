@@ -27,11 +27,16 @@ struct qmt_mol {
   std::vector<int> types;
   std::vector<float> coords;
   std::vector<qmt::Shell> shells;
+  std::vector<int> atom_shell;  // shells of atom a are [atom_shell[a], atom_shell[a+1])
   std::vector<float> alpha, coeff;
   std::vector<double> alpha64, coeff64;
   std::vector<double> P64;      // symmetric (from the lower triangle), npad x npad
   std::vector<double> fbound;   // per-function bound on |phi|
 
+  qmt::DevBuf d_atom_shell;
+  int fused_prec = -1;          // precision of the fused-path operands below
+  int fused_g = 0;
+  qmt::DevBuf d_fused_B;        // upper-triangular scaled density matrix pieces (hi then lo)
   qmt::DevBuf d_coords, d_types, d_shells, d_alpha, d_coeff, d_alpha64, d_coeff64;
   qmt::DevBuf d_P32, d_P64;
   // tensor-core operands

@@ -64,6 +64,7 @@ struct MolView {
   const float* coords;       // [natoms*3] bohr
   const int* types;          // [natoms]
   const Shell* shells;       // [nshells]
+  const int* atom_shell;     // [natoms+1]
   const float* alpha;        // [nprim_total]
   const float* coeff;        // [nprim_total]
   const double* alpha64;

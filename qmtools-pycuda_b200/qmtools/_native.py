@@ -34,6 +34,7 @@ SIGNATURES = {
     "qmt_mol_destroy": [_vp],
     "qmt_mol_trace_ps": [_vp, _pd, _vp],
     "qmt_density": [_vp, _i, _i, _i, _f, _f, _f, _f, _i, _i, _i, _vp, _pd, _vp],
+    "qmt_set_density_path": [_i],
     "qmt_hartree_gto": [_vp, _i, _i, _i, _f, _f, _f, _f, _vp, _vp],
     "qmt_hartree_gto_points": [_vp, _i, _vp, _vp, _vp],
     "qmt_hartree_gto_boundary": [_vp, _i, _i, _i, _f, _f, _f, _f, _vp, _vp],

@@ -15,7 +15,7 @@ pytestmark = pytest.mark.gpu
 
 # rel-L2 tolerance of the unscaled grid against the FP64 oracle, per precision (the grid is
 # stored in float32, so even the FP64 path carries ~3e-8 of output rounding)
-TOL = {"fp64": 1e-7, "fp32": 1e-6, "fp16x3": 1e-6, "tf32x3": 1e-6, "bf16x3": 1e-4,
+TOL = {"fp64": 1e-7, "fp32": 1e-6, "fp16x3": 1e-6, "tf32x3": 2e-6, "bf16x3": 1e-4,
        "tf32": 5e-3, "bf16": 5e-2}
 
 
@@ -110,3 +110,32 @@ def test_density_deterministic(c1):
     b = qmtools.QMTools.Compute_density(g, mol, precision="fp16x3")
     assert np.array_equal(a.qube, b.qube)
     assert a.qsum == b.qsum
+
+
+@pytest.fixture(params=[1, 2], ids=["staged", "fused"])
+def density_path(request):
+    """Run a test once through each tensor-core implementation, then restore automatic choice."""
+    from qmtools import _native as N
+    N.call("qmt_set_density_path", request.param)
+    yield request.param
+    N.call("qmt_set_density_path", 0)
+
+
+@pytest.mark.parametrize("prec", ["fp16x3", "bf16x3", "bf16"])
+def test_density_paths_agree_with_oracle(c1, density_path, prec):
+    """Staged (HBM) and fused (shared-memory, upper-triangular) tensor-core paths, N = 294."""
+    sm, mol = c1
+    g = _small_grid(sm, 24, 0.8)
+    ref = _oracle(g, mol)
+    out = qmtools.QMTools.Compute_density(g, mol, precision=prec, rescale=False)
+    assert rel_l2(out.qube.ravel(), ref) <= TOL[prec]
+
+
+@pytest.mark.parametrize("sub", [1, 2, 3])
+def test_fused_path_subgrids_and_small_basis(c0, density_path, sub):
+    """N = 58 (one 64-wide K block), partial last tile, sub-point averaging."""
+    sm, mol = c0
+    g = _small_grid(sm, 16 if sub > 1 else 24, 0.6)
+    ref = _oracle(g, mol, subgrid=sub)
+    out = qmtools.QMTools.Compute_density(g, mol, subgrid=sub, precision="fp16x3", rescale=False)
+    assert rel_l2(out.qube.ravel(), ref) <= TOL["fp16x3"]
