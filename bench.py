@@ -102,7 +102,8 @@ class ClockSampler:
                 "samples": len(sm)}
 
 
-def dist_setup(n_gpus):
+def dist_setup(backend="nccl"):
+    """One process per GPU (replicas): torchrun environment, short process-group timeout."""
     world = int(os.environ.get("WORLD_SIZE", "1"))
     rank = int(os.environ.get("RANK", "0"))
     local = int(os.environ.get("LOCAL_RANK", "0"))
@@ -111,25 +112,35 @@ def dist_setup(n_gpus):
         import torch
         import torch.distributed as dist
         from datetime import timedelta
-        torch.cuda.set_device(local)
-        dist.init_process_group("nccl", timeout=timedelta(seconds=300),
-                                device_id=torch.device("cuda", local))
+        if backend == "nccl":
+            torch.cuda.set_device(local)
+            dist.init_process_group("nccl", timeout=timedelta(seconds=300),
+                                    device_id=torch.device("cuda", local))
+        else:
+            dist.init_process_group(backend, timeout=timedelta(seconds=60))
         pg = dist
     return world, rank, local, pg
+
+
+def _dev(pg):
+    import torch
+    return "cuda" if pg.get_backend() == "nccl" else "cpu"
 
 
 def barrier(pg):
     if pg is not None:
         import torch
         pg.barrier()
-        torch.cuda.synchronize()
+        if _dev(pg) == "cuda":
+            torch.cuda.synchronize()
 
 
 def max_over_ranks(pg, v):
+    """Timed regions are reported as the max over ranks."""
     if pg is None:
         return v
     import torch
-    t = torch.tensor([v], dtype=torch.float64, device="cuda")
+    t = torch.tensor([v], dtype=torch.float64, device=_dev(pg))
     pg.all_reduce(t, op=pg.ReduceOp.MAX)
     return float(t.item())
 
@@ -324,7 +335,7 @@ def main():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     args = ap.parse_args()
     args.warmup = max(args.warmup, 3)
-    world, rank, local, pg = dist_setup(args.gpus)
+    world, rank, local, pg = dist_setup()
     try:
         if args.impl == "reference":
             out = run_reference(args, world, rank, local, pg)

@@ -93,7 +93,8 @@ qmt_status qmt_density(qmt_mol* mol, int nx, int ny, int nz, float step,
 
 /* Selects the tensor-core density implementation (new; process-wide): 0 = automatic (fused
  * when the contraction is fp16/bf16 and N <= 320, staged otherwise), 1 = staged (basis values
- * through HBM), 2 = fused (basis values stay in shared memory). */
+ * through HBM), 2 = fused (basis values stay in shared memory), 3 = fused over the upper
+ * triangle of P only (half the tensor work, about 2x the FP32 accumulation error). */
 qmt_status qmt_set_density_path(int mode);
 
 /* ---- analytic GTO potential --------------------------------------------------------- */

@@ -16,7 +16,8 @@ def density_seed(shape, step, origin, coords, types):
 
     Node i0 = floor(x/h) + t (t in {0,1}) gets Z * prod |x - i0 h| / h; the last
     atom to write a node wins (plain stores, one block per atom).  Index and
-    weights follow the kernel's FP32 arithmetic.
+    weights follow the kernel's FP32 arithmetic, including nvcc's default contraction
+    of `x - i0*h` into one fused multiply-add (exact product and sum, one rounding).
     """
     nx, ny, nz = shape
     h = np.float32(step)
@@ -31,7 +32,8 @@ def density_seed(shape, step, origin, coords, types):
                     i0 = base + np.array([tx, ty, tz])
                     p = np.float32(Z)
                     for d in range(3):
-                        p = np.float32(p * np.float32(np.abs(np.float32(rel[d] - np.float32(i0[d]) * h)) / h))
+                        diff = np.float32(np.float64(rel[d]) - np.float64(np.float32(i0[d])) * np.float64(h))
+                        p = np.float32(p * np.float32(np.abs(diff) / h))
                     q[i0[0] + i0[1] * nx + i0[2] * nx * ny] = p
     return q
 

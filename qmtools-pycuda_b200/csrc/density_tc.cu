@@ -322,7 +322,7 @@ __global__ void __launch_bounds__(192, 1)
       }
       if (!ok) {  // drain copies still in flight before the CTA exits
         for (int s = 0; s < p.stages; ++s)
-          if (last_par[s] >= 0) mbar_wait(&full_bar[s], (uint32_t)last_par[s], &abort_flag, 1u << 20);
+          if (last_par[s] >= 0) mbar_wait(&full_bar[s], (uint32_t)last_par[s], &abort_flag, 100000000ull);
       }
     }
   } else if (warp == 1) {
@@ -375,7 +375,7 @@ __global__ void __launch_bounds__(192, 1)
       }
       // every MMA issued by this thread has completed once drain_bar flips
       tc_commit(&drain_bar);
-      mbar_wait(&drain_bar, 0u, &abort_flag, 1u << 22);
+      mbar_wait(&drain_bar, 0u, &abort_flag, 500000000ull);
     }
   } else {
     // epilogue: warps 2..5 -> TMEM lane quadrants 2,3,0,1
@@ -520,7 +520,6 @@ static qmt_status ensure_tc_operands(qmt_mol* m, int prec, const TcShape& sh, cu
   QMT_CUDA(cudaStreamSynchronize(s));
   m->tc_g = g;
   m->tc_prec = prec;
-  m->fused_prec = -1;   // d_fscale now holds the staged path's scales
   return QMT_OK;
 }
 
@@ -600,9 +599,11 @@ static qmt_status run_tc(qmt_mol* m, const TcShape& sh, const PointMap& pm, int6
 // ---------------------------------------------------------------------------------------
 // Fused path (kind::f16 formats, K <= 320): Phi' never leaves shared memory.
 //
-//   rho = sum_jk Phi_j P_jk Phi_k = 2 sum_k Phi_k (Phi U)_k,  U = triu(P, 1) + diag(P)/2,
-// so only the upper triangle of the scaled density matrix is streamed and multiplied: the
-// K-step covering rows j in [j0, j0+16) of U only touches output columns k >= j0.
+//   rho = sum_k Phi_k (Phi P)_k over the full symmetric P (default), or, in the triangular
+//   variant, rho = 2 sum_k Phi_k (Phi U)_k with U = triu(P, 1) + diag(P)/2: only the upper
+//   triangle is streamed and multiplied (the K-step covering rows j in [j0, j0+16) touches
+//   output columns k >= j0), half the work, but the partial sums of Phi U are larger than
+//   those of Phi P, so the FP32 tensor-core accumulation loses about a factor 2 in accuracy.
 //
 // CTA layout (one per SM, persistent over 128-row tiles), 10 warps:
 //   warp 0     TMA producer of U (32-byte swizzled, one 16-element K-step per stage);
@@ -620,11 +621,12 @@ struct FusedParams {
   PointMap pm;
   int64_t ntiles;
   int kpad, ksteps, nsplit, stages;
+  int tri;                 // 1: upper-triangular U (half the work); 0: full symmetric P
   uint32_t a_bytes;        // one A piece: 128 rows x kpad x 2 B
   uint32_t b_slot;         // one U piece slot in a stage: kpad rows x 32 B
   uint32_t stage_bytes;
   uint32_t fmt;
-  const float* fscale;
+  const float* coeff_scaled;   // contraction coefficients times the shell's power-of-two scale
   float* qube;
   double* partials;
   double outscale;
@@ -659,6 +661,25 @@ __device__ __forceinline__ void store_split16(uint8_t* hi, uint8_t* lo, uint32_t
     const __nv_bfloat16 h = __float2bfloat16_rn(x);
     *reinterpret_cast<__nv_bfloat16*>(hi + off) = h;
     if (two) *reinterpret_cast<__nv_bfloat16*>(lo + off) = __float2bfloat16_rn(x - __bfloat162float(h));
+  }
+}
+
+template <int FMT>
+__device__ __forceinline__ void store_pair16(uint8_t* hi, uint8_t* lo, uint32_t off, float x0, float x1, bool two) {
+  if constexpr (FMT == FMT_F16) {
+    const __half2 h = __floats2half2_rn(x0, x1);
+    *reinterpret_cast<__half2*>(hi + off) = h;
+    if (two) {
+      const float2 hf = __half22float2(h);
+      *reinterpret_cast<__half2*>(lo + off) = __floats2half2_rn(x0 - hf.x, x1 - hf.y);
+    }
+  } else {
+    const __nv_bfloat162 h = __floats2bfloat162_rn(x0, x1);
+    *reinterpret_cast<__nv_bfloat162*>(hi + off) = h;
+    if (two) {
+      const float2 hf = __bfloat1622float2(h);
+      *reinterpret_cast<__nv_bfloat162*>(lo + off) = __floats2bfloat162_rn(x0 - hf.x, x1 - hf.y);
+    }
   }
 }
 
@@ -713,6 +734,7 @@ __global__ void __launch_bounds__(320, 1)
   // zero A once: padding columns and rows never written later stay zero
   for (uint32_t i = threadIdx.x; i < p.nsplit * p.a_bytes / 16; i += blockDim.x)
     reinterpret_cast<uint4*>(smem)[i] = make_uint4(0, 0, 0, 0);
+  asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
   if (warp == 0 && lane == 0) {
     prefetch_tmap(&tmU_hi);
     if (two) prefetch_tmap(&tmU_lo);
@@ -741,19 +763,20 @@ __global__ void __launch_bounds__(320, 1)
             break;
           }
           const int j0 = ks * 16;
-          const int npc = (p.kpad - j0 + 63) / 64;  // 64-row pieces
+          const int r0 = p.tri ? j0 : 0;            // first output column touched by this K-step
+          const int npc = (p.kpad - r0 + 63) / 64;  // 64-row pieces
           uint8_t* st = stages + (size_t)s * p.stage_bytes;
           mbar_expect_tx(&full_bar[s], (uint32_t)(npc * 64 * 32 * p.nsplit));
           for (int c = 0; c < npc; ++c) {
-            tma_load_2d(st + c * 2048, &tmU_hi, &full_bar[s], j0, j0 + 64 * c);
-            if (two) tma_load_2d(st + p.b_slot + c * 2048, &tmU_lo, &full_bar[s], j0, j0 + 64 * c);
+            tma_load_2d(st + c * 2048, &tmU_hi, &full_bar[s], j0, r0 + 64 * c);
+            if (two) tma_load_2d(st + p.b_slot + c * 2048, &tmU_lo, &full_bar[s], j0, r0 + 64 * c);
           }
           last_par[s] = (int)ph;
         }
       }
       if (!ok)
         for (int s = 0; s < p.stages; ++s)
-          if (last_par[s] >= 0) mbar_wait(&full_bar[s], (uint32_t)last_par[s], &abort_flag, 1u << 20);
+          if (last_par[s] >= 0) mbar_wait(&full_bar[s], (uint32_t)last_par[s], &abort_flag, 100000000ull);
     }
   } else if (warp == 1) {
     if (lane == 0) {
@@ -772,12 +795,13 @@ __global__ void __launch_bounds__(320, 1)
           }
           tc_fence_after();
           const int j0 = ks * 16;
+          const int r0 = p.tri ? j0 : 0;
           const uint32_t aoff = (uint32_t)((j0 >> 6) * 16384 + ((j0 & 63) >> 4) * 32);
           const uint32_t bst = smem_u32(stages + (size_t)s * p.stage_bytes);
-          for (int c0 = j0; c0 < p.kpad; c0 += 256) {
+          for (int c0 = r0; c0 < p.kpad; c0 += 256) {
             const int n = min(256, p.kpad - c0);
             const uint32_t idesc = make_idesc(p.fmt, 128, (uint32_t)n);
-            const uint32_t boff = (uint32_t)(c0 - j0) * 32u;
+            const uint32_t boff = (uint32_t)(c0 - r0) * 32u;
             const uint32_t d = tmem + (uint32_t)c0;
             mma_f16(d, sw128_kmajor_desc(abase + aoff), sw32_kmajor_desc(bst + boff), idesc, ks > 0 ? 1u : 0u);
             if (two) {
@@ -790,7 +814,7 @@ __global__ void __launch_bounds__(320, 1)
         if (ok) tc_commit(&t_full);
       }
       tc_commit(&drain_bar);
-      mbar_wait(&drain_bar, 0u, &abort_flag, 1u << 22);
+      mbar_wait(&drain_bar, 0u, &abort_flag, 500000000ull);
     }
   } else {
     const int ct = threadIdx.x - 64;    // 0..255 compute thread
@@ -809,28 +833,63 @@ __global__ void __launch_bounds__(320, 1)
         pos[ct][2] = z;
       }
       named_barrier(1, 256);
-      for (int itm = ct; itm < 128 * mol.natoms; itm += 256) {
-        const int r = itm & 127, a = itm >> 7;
-        const double px = pos[r][0];
-        const int s0 = mol.atom_shell[a], s1 = mol.atom_shell[a + 1];
-        if (px > 1e29) {
+      // work item = (atom, half of the rows): warp-uniform atom data, two rows per thread
+      // (lane and lane + 64 of its half) for independent exponential chains
+      {
+        const int wi = ct >> 5;
+        for (int itm = wi; itm < 2 * mol.natoms; itm += 8) {
+          const int a = itm >> 1;
+          const int r0 = (itm & 1) * 32 + lane, r1 = r0 + 64;
+          const double ax = __ldg(mol.coords + 3 * a), ay = __ldg(mol.coords + 3 * a + 1),
+                       az = __ldg(mol.coords + 3 * a + 2);
+          const bool ok0 = pos[r0][0] < 1e29, ok1 = pos[r1][0] < 1e29;
+          // FP64 displacement from the nucleus, rounded once (accuracy of steep exponents)
+          const float x0 = (float)(pos[r0][0] - ax), y0 = (float)(pos[r0][1] - ay), z0 = (float)(pos[r0][2] - az);
+          const float x1 = (float)(pos[r1][0] - ax), y1 = (float)(pos[r1][1] - ay), z1 = (float)(pos[r1][2] - az);
+          const float q0 = x0 * x0 + y0 * y0 + z0 * z0, q1 = x1 * x1 + y1 * y1 + z1 * z1;
+          const int s0 = __ldg(mol.atom_shell + a), s1 = __ldg(mol.atom_shell + a + 1);
           for (int sidx = s0; sidx < s1; ++sidx) {
-            const Shell sh = mol.shells[sidx];
-            for (int k = 0; k < 2 * sh.L + 1; ++k) store_split16<FMT>(A_hi, A_lo, a_offset(r, sh.func + k), 0.f, two);
-          }
-          continue;
-        }
-        // FP64 displacement from the nucleus, rounded once (accuracy of steep exponents)
-        const float dx = (float)(px - (double)mol.coords[3 * a]);
-        const float dy = (float)(pos[r][1] - (double)mol.coords[3 * a + 1]);
-        const float dz = (float)(pos[r][2] - (double)mol.coords[3 * a + 2]);
-        for (int sidx = s0; sidx < s1; ++sidx) {
-          const Shell sh = mol.shells[sidx];
-          float v[5];
-          const int n = shell_values<float>(sh, mol.alpha, mol.coeff, dx, dy, dz, v);
-          for (int k = 0; k < n; ++k) {
-            const int j = sh.func + k;
-            store_split16<FMT>(A_hi, A_lo, a_offset(r, j), v[k] * p.fscale[j], two);
+            const int L = __ldg(&mol.shells[sidx].L), np_ = __ldg(&mol.shells[sidx].nprim);
+            const int pr = __ldg(&mol.shells[sidx].prim), f0 = __ldg(&mol.shells[sidx].func);
+            float rad0 = 0.f, rad1 = 0.f;
+            for (int k = 0; k < np_; ++k) {
+              const float al = __ldg(mol.alpha + pr + k), co = __ldg(p.coeff_scaled + pr + k);
+              const float e0 = al * q0, e1 = al * q1;
+              if (e0 < 60.f) rad0 += co * expf(-e0);
+              if (e1 < 60.f) rad1 += co * expf(-e1);
+            }
+            if (!ok0) rad0 = 0.f;
+            if (!ok1) rad1 = 0.f;
+            float v0[5], v1[5];
+            if (L == 0) {
+              v0[0] = (float)YS * rad0;
+              v1[0] = (float)YS * rad1;
+            } else if (L == 1) {
+              const float c0 = (float)YP * rad0, c1 = (float)YP * rad1;
+              v0[0] = c0 * z0; v0[1] = c0 * x0; v0[2] = c0 * y0;
+              v1[0] = c1 * z1; v1[1] = c1 * x1; v1[2] = c1 * y1;
+            } else {
+              const float c0 = (float)YD1 * rad0, c1 = (float)YD1 * rad1;
+              v0[0] = (float)YD0 * rad0 * (2.f * z0 * z0 - x0 * x0 - y0 * y0);
+              v0[1] = c0 * x0 * z0; v0[2] = c0 * z0 * y0;
+              v0[3] = (float)YD2 * rad0 * (x0 * x0 - y0 * y0); v0[4] = c0 * x0 * y0;
+              v1[0] = (float)YD0 * rad1 * (2.f * z1 * z1 - x1 * x1 - y1 * y1);
+              v1[1] = c1 * x1 * z1; v1[2] = c1 * z1 * y1;
+              v1[3] = (float)YD2 * rad1 * (x1 * x1 - y1 * y1); v1[4] = c1 * x1 * y1;
+            }
+            const int nf = 2 * L + 1;
+            for (int k = 0; k < nf; ++k) {
+              const int j = f0 + k;
+              // two consecutive functions in the same 16-byte unit: one 4-byte store per piece
+              if (k + 1 < nf && (j & 1) == 0) {
+                store_pair16<FMT>(A_hi, A_lo, a_offset(r0, j), v0[k], v0[k + 1], two);
+                store_pair16<FMT>(A_hi, A_lo, a_offset(r1, j), v1[k], v1[k + 1], two);
+                ++k;
+              } else {
+                store_split16<FMT>(A_hi, A_lo, a_offset(r0, j), v0[k], two);
+                store_split16<FMT>(A_hi, A_lo, a_offset(r1, j), v1[k], two);
+              }
+            }
           }
         }
       }
@@ -919,8 +978,11 @@ static qmt_status make_map_sw32(CUtensorMap* m, const void* base, uint64_t inner
 // Upper-triangular scaled density matrix for the fused path: row n (output column) holds
 // U_jn for j <= n, i.e. Ptilde_jn for j < n and Ptilde_nn / 2 on the diagonal.  Rows are
 // padded to kpad + 64 so every 64-row TMA box stays inside the tensor.
+static int g_fused_tri = 0;   // upper-triangular variant of the fused path (off by default)
+
 static qmt_status ensure_fused_operands(qmt_mol* m, int prec, const TcShape& sh, cudaStream_t s) {
-  if (m->fused_prec == prec) return QMT_OK;
+  const int key = prec * 2 + g_fused_tri;
+  if (m->fused_prec == key) return QMT_OK;
   const int n = m->norbs, np = m->npad, K = sh.kpad;
   std::vector<int> sj(K, 0);
   std::vector<float> fs(K, 0.f);
@@ -939,20 +1001,26 @@ static qmt_status ensure_fused_operands(qmt_mol* m, int prec, const TcShape& sh,
   const size_t piece = (size_t)rows * K * 2;
   std::vector<uint8_t> host(2 * piece, 0);
   for (int nn = 0; nn < n; ++nn)
-    for (int j = 0; j <= nn; ++j) {
+    for (int j = 0; j < n; ++j) {
+      if (g_fused_tri && j > nn) continue;
       double v = std::ldexp(m->P64[(size_t)j * np + nn], g - sj[j] - sj[nn]);
-      if (j == nn) v *= 0.5;
+      if (g_fused_tri && j == nn) v *= 0.5;
       split_host(v, sh.fmt, host.data(), host.data() + piece, (size_t)nn * K + j);
     }
+  // every function of a shell shares the shell's bound, hence its scale: fold it into the
+  // contraction coefficients (exact, powers of two)
+  std::vector<float> cs(m->coeff.size());
+  for (const Shell& shl : m->shells)
+    for (int k = 0; k < shl.nprim; ++k) cs[shl.prim + k] = m->coeff[shl.prim + k] * fs[shl.func];
   qmt_status st;
   if ((st = m->d_fused_B.reserve(2 * piece))) return st;
-  if ((st = m->d_fscale.reserve(K * sizeof(float)))) return st;
+  if ((st = m->d_coeff_scaled.reserve(std::max<size_t>(1, cs.size()) * sizeof(float)))) return st;
   QMT_CUDA(cudaMemcpyAsync(m->d_fused_B.ptr, host.data(), 2 * piece, cudaMemcpyHostToDevice, s));
-  QMT_CUDA(cudaMemcpyAsync(m->d_fscale.ptr, fs.data(), K * sizeof(float), cudaMemcpyHostToDevice, s));
+  if (!cs.empty())
+    QMT_CUDA(cudaMemcpyAsync(m->d_coeff_scaled.ptr, cs.data(), cs.size() * sizeof(float), cudaMemcpyHostToDevice, s));
   QMT_CUDA(cudaStreamSynchronize(s));
   m->fused_g = g;
-  m->fused_prec = prec;
-  m->tc_prec = -1;   // d_fscale now holds the fused path's scales
+  m->fused_prec = key;
   return QMT_OK;
 }
 
@@ -972,16 +1040,17 @@ static qmt_status run_fused(qmt_mol* m, const TcShape& sh, const PointMap& pm, i
   p.ntiles = ntiles;
   p.kpad = K;
   p.ksteps = K / 16;
+  p.tri = g_fused_tri;
   p.nsplit = sh.nsplit;
   p.a_bytes = 128u * K * 2u;
   p.b_slot = (uint32_t)K * 32u;
   p.stage_bytes = p.nsplit * p.b_slot;
   p.fmt = (uint32_t)sh.fmt;
-  p.fscale = m->d_fscale.as<float>();
+  p.coeff_scaled = m->d_coeff_scaled.as<float>();
   p.qube = qube;
   p.partials = m->d_partials.as<double>();
   p.outscale = outscale;
-  p.inv_g2 = 2.0 * std::ldexp(1.0, -m->fused_g);
+  p.inv_g2 = (g_fused_tri ? 2.0 : 1.0) * std::ldexp(1.0, -m->fused_g);
   p.err = reinterpret_cast<int*>(m->d_scalars.as<double>() + 8);
   int maxsm = 0, dev = 0;
   cudaGetDevice(&dev);
@@ -1039,7 +1108,9 @@ qmt_status density_tc(qmt_mol* mol, int nx, int ny, int nz, float step, float ox
 }  // namespace qmt
 
 extern "C" qmt_status qmt_set_density_path(int mode) {
-  if (mode < 0 || mode > 2) return qmt::fail(QMT_BAD_ARG, "density path must be 0 (auto), 1 (staged) or 2 (fused)");
-  qmt::g_density_path = mode;
+  if (mode < 0 || mode > 3)
+    return qmt::fail(QMT_BAD_ARG, "density path must be 0 (auto), 1 (staged), 2 (fused) or 3 (fused, triangular)");
+  qmt::g_density_path = mode == 3 ? 2 : mode;
+  qmt::g_fused_tri = mode == 3 ? 1 : 0;
   return QMT_OK;
 }

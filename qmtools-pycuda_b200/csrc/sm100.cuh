@@ -1,7 +1,7 @@
 // Thin inline-PTX wrappers for the sm_100a features used by the tensor-core kernels:
 // mbarriers, TMA tiled loads, tcgen05 (TMEM allocation, MMA, commit, loads).
-// Every wait is bounded: after `limit` polls it raises `abort_flag` and returns false so
-// that no kernel can spin forever.
+// Every wait is bounded in wall time: it raises `abort_flag` and returns false so that no
+// kernel can spin forever.
 #pragma once
 
 #include <cuda.h>
@@ -43,14 +43,24 @@ __device__ __forceinline__ bool mbar_try_wait(uint64_t* bar, uint32_t parity) {
   return ok != 0;
 }
 
-// Bounded wait for the phase of `parity` to complete.
+__device__ __forceinline__ uint64_t globaltimer_ns() {
+  uint64_t t;
+  asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
+  return t;
+}
+
+// Bounded wait for the phase of `parity` to complete: gives up after `limit_ns` of wall
+// time (or as soon as another role raised `abort_flag`), raises the flag and returns false.
 __device__ __forceinline__ bool mbar_wait(uint64_t* bar, uint32_t parity, volatile int* abort_flag,
-                                          uint32_t limit = (1u << 24)) {
-  for (uint32_t i = 0; i < limit; ++i) {
+                                          uint64_t limit_ns = 2000000000ull) {
+  if (mbar_try_wait(bar, parity)) return true;
+  const uint64_t t0 = globaltimer_ns();
+  for (uint32_t i = 1;; ++i) {
     if (mbar_try_wait(bar, parity)) return true;
-    if ((i & 255u) == 255u) {
+    if ((i & 63u) == 0u) {
       if (*abort_flag) return false;
-      __nanosleep(128);
+      if (globaltimer_ns() - t0 > limit_ns) break;
+      __nanosleep(64);
     }
   }
   *abort_flag = 1;
