@@ -72,6 +72,12 @@ qmt_status qmt_mol_create(int natoms, const int32_t* types, const float* coords,
                           int norbs, const int16_t* almos,
                           int nparams, const float* alphas, const float* coeffs,
                           const float* dm, void* stream, qmt_mol** out);
+/* Re-initialises an existing handle for another molecule (same arguments as qmt_mol_create),
+ * reusing its device allocations: a serving loop keeps one handle per slot and never calls
+ * cudaMalloc/cudaFree in steady state.  New entry point. */
+qmt_status qmt_mol_reset(qmt_mol* mol, int natoms, const int32_t* types, const float* coords,
+                         int norbs, const int16_t* almos, int nparams, const float* alphas,
+                         const float* coeffs, const float* dm, void* stream);
 /* Molecule.Translate upload (qmtools/qmtools.py:182-188): new coords[natoms*3] bohr. */
 qmt_status qmt_mol_set_coords(qmt_mol* mol, const float* coords, void* stream);
 /* New density matrix (same norbs). */
@@ -85,8 +91,11 @@ qmt_status qmt_mol_trace_ps(qmt_mol* mol, double* trace_out, void* stream);
 /* QMTools.Compute_density (qmtools/qmtools.py:2381-2430) with gpu_densityqube_shmem_subgrid
  * (kernel_density.cu:34-155): q_v = 2 h^3 s^-3 sum_sub sum_pq P_pq phi_p phi_q at voxel-centre
  * sub-points, into qube_dev[nx*ny*nz].  If rescale != 0 the grid is then scaled so that its
- * sum equals the total nuclear charge (qmtools/qmtools.py:2419-2424).  sum_out (host, may be
- * NULL) receives the FP64 sum before rescaling.  Blocks until sum_out is written. */
+ * sum equals the total nuclear charge (qmtools/qmtools.py:2419-2424), on the device.
+ * sum_out (host, may be NULL) receives the FP64 sum before rescaling; with sum_out the call
+ * blocks and reports kernel failures, without it the call is fully asynchronous on `stream`
+ * (capturable in a CUDA graph once the molecule's operands exist) and failures are reported
+ * by the next call on this molecule that returns a sum. */
 qmt_status qmt_density(qmt_mol* mol, int nx, int ny, int nz, float step,
                        float ox, float oy, float oz, int subgrid, int precision,
                        int rescale, float* qube_dev, double* sum_out, void* stream);

@@ -578,7 +578,6 @@ static qmt_status run_tc(qmt_mol* m, const TcShape& sh, const PointMap& pm, int6
   const size_t dyn = (size_t)stages * p.stage_bytes + 1024;
   auto kern = density_mma_kernel<FMT>;
   QMT_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)dyn));
-  QMT_CUDA(cudaMemsetAsync(p.err, 0, sizeof(int), s));
 
   for (int64_t t0 = 0; t0 < ntiles; t0 += chunk) {
     const int nt = (int)std::min<int64_t>(chunk, ntiles - t0);
@@ -699,8 +698,12 @@ __device__ __forceinline__ void unpack8(uint4 a, float* out) {
   }
 }
 
+constexpr int FUSED_NCW = 12;                 // compute warps (Phi production and epilogue)
+constexpr int FUSED_NCT = FUSED_NCW * 32;
+constexpr int FUSED_THREADS = 64 + FUSED_NCT;  // + TMA warp + MMA warp
+
 template <int FMT>
-__global__ void __launch_bounds__(320, 1)
+__global__ void __launch_bounds__(FUSED_THREADS, 1)
     density_fused_kernel(const __grid_constant__ CUtensorMap tmU_hi, const __grid_constant__ CUtensorMap tmU_lo,
                          const FusedParams p) {
   extern __shared__ uint8_t smem_dyn[];
@@ -708,8 +711,8 @@ __global__ void __launch_bounds__(320, 1)
   __shared__ __align__(8) uint64_t a_full, t_full, drain_bar;
   __shared__ uint32_t tmem_slot;
   __shared__ double pos[128][3];
-  __shared__ double rho_part[2][128];
-  __shared__ double red[8];
+  __shared__ double rho_part[FUSED_NCW / 4][128];
+  __shared__ double red[FUSED_NCW];
   __shared__ volatile int abort_flag;
 
   uint8_t* smem = reinterpret_cast<uint8_t*>((reinterpret_cast<uintptr_t>(smem_dyn) + 1023) & ~uintptr_t(1023));
@@ -817,9 +820,10 @@ __global__ void __launch_bounds__(320, 1)
       mbar_wait(&drain_bar, 0u, &abort_flag, 500000000ull);
     }
   } else {
-    const int ct = threadIdx.x - 64;    // 0..255 compute thread
-    const int q = warp & 3;             // TMEM lane quadrant
-    const int hh = (warp - 2) >> 2;     // column-chunk parity handled in the epilogue
+    const int ct = threadIdx.x - 64;           // compute thread 0 .. FUSED_NCT-1
+    const int cw = ct >> 5;                    // compute warp 0 .. FUSED_NCW-1
+    const int q = warp & 3;                    // TMEM lane quadrant of this warp
+    const int hh = cw >> 2;                    // epilogue column-chunk class 0 .. FUSED_NCW/4-1
     const int row = q * 32 + lane;
     uint32_t tile_it = 0;
     for (int64_t t = blockIdx.x; t < p.ntiles; t += gridDim.x, ++tile_it) {
@@ -832,63 +836,82 @@ __global__ void __launch_bounds__(320, 1)
         pos[ct][1] = y;
         pos[ct][2] = z;
       }
-      named_barrier(1, 256);
+      named_barrier(1, FUSED_NCT);
       // work item = (atom, half of the rows): warp-uniform atom data, two rows per thread
       // (lane and lane + 64 of its half) for independent exponential chains
-      {
-        const int wi = ct >> 5;
-        for (int itm = wi; itm < 2 * mol.natoms; itm += 8) {
-          const int a = itm >> 1;
-          const int r0 = (itm & 1) * 32 + lane, r1 = r0 + 64;
-          const double ax = __ldg(mol.coords + 3 * a), ay = __ldg(mol.coords + 3 * a + 1),
-                       az = __ldg(mol.coords + 3 * a + 2);
-          const bool ok0 = pos[r0][0] < 1e29, ok1 = pos[r1][0] < 1e29;
-          // FP64 displacement from the nucleus, rounded once (accuracy of steep exponents)
-          const float x0 = (float)(pos[r0][0] - ax), y0 = (float)(pos[r0][1] - ay), z0 = (float)(pos[r0][2] - az);
-          const float x1 = (float)(pos[r1][0] - ax), y1 = (float)(pos[r1][1] - ay), z1 = (float)(pos[r1][2] - az);
-          const float q0 = x0 * x0 + y0 * y0 + z0 * z0, q1 = x1 * x1 + y1 * y1 + z1 * z1;
-          const int s0 = __ldg(mol.atom_shell + a), s1 = __ldg(mol.atom_shell + a + 1);
-          for (int sidx = s0; sidx < s1; ++sidx) {
-            const int L = __ldg(&mol.shells[sidx].L), np_ = __ldg(&mol.shells[sidx].nprim);
-            const int pr = __ldg(&mol.shells[sidx].prim), f0 = __ldg(&mol.shells[sidx].func);
-            float rad0 = 0.f, rad1 = 0.f;
-            for (int k = 0; k < np_; ++k) {
-              const float al = __ldg(mol.alpha + pr + k), co = __ldg(p.coeff_scaled + pr + k);
-              const float e0 = al * q0, e1 = al * q1;
-              if (e0 < 60.f) rad0 += co * expf(-e0);
-              if (e1 < 60.f) rad1 += co * expf(-e1);
+      for (int itm = cw; itm < 2 * mol.natoms; itm += FUSED_NCW) {
+        const int a = itm >> 1;
+        const int r0 = (itm & 1) * 32 + lane, r1 = r0 + 64;   // r1 sits 8192 B after r0 in A
+        const double ax = __ldg(mol.coords + 3 * a), ay = __ldg(mol.coords + 3 * a + 1),
+                     az = __ldg(mol.coords + 3 * a + 2);
+        const bool ok0 = pos[r0][0] < 1e29, ok1 = pos[r1][0] < 1e29;
+        // FP64 displacement from the nucleus, rounded once (accuracy of steep exponents)
+        const float x0 = (float)(pos[r0][0] - ax), y0 = (float)(pos[r0][1] - ay), z0 = (float)(pos[r0][2] - az);
+        const float x1 = (float)(pos[r1][0] - ax), y1 = (float)(pos[r1][1] - ay), z1 = (float)(pos[r1][2] - az);
+        const float q0 = x0 * x0 + y0 * y0 + z0 * z0, q1 = x1 * x1 + y1 * y1 + z1 * z1;
+        const int s0 = __ldg(mol.atom_shell + a), s1 = __ldg(mol.atom_shell + a + 1);
+        for (int sidx = s0; sidx < s1; ++sidx) {
+          const int4 sh = __ldg(reinterpret_cast<const int4*>(mol.shells + sidx));   // atom, L, nprim, prim
+          const int L = sh.y, np_ = sh.z, pr = sh.w;
+          const int f0 = __ldg(&mol.shells[sidx].func);
+          // up to 8 primitives fetched at once (independent loads), then 2 rows x 8 exponentials
+          float al[8], co[8];
+#pragma unroll
+          for (int k = 0; k < 8; ++k) {
+            al[k] = k < np_ ? __ldg(mol.alpha + pr + k) : 0.f;
+            co[k] = k < np_ ? __ldg(p.coeff_scaled + pr + k) : 0.f;
+          }
+          float rad0 = 0.f, rad1 = 0.f;
+#pragma unroll
+          for (int k = 0; k < 8; ++k) {
+            const float e0 = al[k] * q0, e1 = al[k] * q1;
+            if (k < np_ && e0 < kExpCut) rad0 = fmaf(co[k], expf(-e0), rad0);
+            if (k < np_ && e1 < kExpCut) rad1 = fmaf(co[k], expf(-e1), rad1);
+          }
+          for (int k = 8; k < np_; ++k) {
+            const float al2 = __ldg(mol.alpha + pr + k), co2 = __ldg(p.coeff_scaled + pr + k);
+            const float e0 = al2 * q0, e1 = al2 * q1;
+            if (e0 < kExpCut) rad0 = fmaf(co2, expf(-e0), rad0);
+            if (e1 < kExpCut) rad1 = fmaf(co2, expf(-e1), rad1);
+          }
+          if (!ok0) rad0 = 0.f;
+          if (!ok1) rad1 = 0.f;
+          float v0[5], v1[5];
+          if (L == 0) {
+            v0[0] = (float)YS * rad0;
+            v1[0] = (float)YS * rad1;
+          } else if (L == 1) {
+            const float c0 = (float)YP * rad0, c1 = (float)YP * rad1;
+            v0[0] = c0 * z0; v0[1] = c0 * x0; v0[2] = c0 * y0;
+            v1[0] = c1 * z1; v1[1] = c1 * x1; v1[2] = c1 * y1;
+          } else {
+            const float c0 = (float)YD1 * rad0, c1 = (float)YD1 * rad1;
+            v0[0] = (float)YD0 * rad0 * (2.f * z0 * z0 - x0 * x0 - y0 * y0);
+            v0[1] = c0 * x0 * z0; v0[2] = c0 * z0 * y0;
+            v0[3] = (float)YD2 * rad0 * (x0 * x0 - y0 * y0); v0[4] = c0 * x0 * y0;
+            v1[0] = (float)YD0 * rad1 * (2.f * z1 * z1 - x1 * x1 - y1 * y1);
+            v1[1] = c1 * x1 * z1; v1[2] = c1 * z1 * y1;
+            v1[3] = (float)YD2 * rad1 * (x1 * x1 - y1 * y1); v1[4] = c1 * x1 * y1;
+          }
+          const int nf = 2 * L + 1;
+          bool skip = false;   // the function was stored with its predecessor
+#pragma unroll
+          for (int k = 0; k < 5; ++k) {
+            if (k >= nf) break;
+            if (skip) {
+              skip = false;
+              continue;
             }
-            if (!ok0) rad0 = 0.f;
-            if (!ok1) rad1 = 0.f;
-            float v0[5], v1[5];
-            if (L == 0) {
-              v0[0] = (float)YS * rad0;
-              v1[0] = (float)YS * rad1;
-            } else if (L == 1) {
-              const float c0 = (float)YP * rad0, c1 = (float)YP * rad1;
-              v0[0] = c0 * z0; v0[1] = c0 * x0; v0[2] = c0 * y0;
-              v1[0] = c1 * z1; v1[1] = c1 * x1; v1[2] = c1 * y1;
+            const int j = f0 + k;
+            const uint32_t off = a_offset(r0, j);
+            // two consecutive functions in the same 16-byte unit: one 4-byte store per piece
+            if (k + 1 < nf && (j & 1) == 0) {
+              store_pair16<FMT>(A_hi, A_lo, off, v0[k], v0[k + 1], two);
+              store_pair16<FMT>(A_hi, A_lo, off + 8192u, v1[k], v1[k + 1], two);
+              skip = true;
             } else {
-              const float c0 = (float)YD1 * rad0, c1 = (float)YD1 * rad1;
-              v0[0] = (float)YD0 * rad0 * (2.f * z0 * z0 - x0 * x0 - y0 * y0);
-              v0[1] = c0 * x0 * z0; v0[2] = c0 * z0 * y0;
-              v0[3] = (float)YD2 * rad0 * (x0 * x0 - y0 * y0); v0[4] = c0 * x0 * y0;
-              v1[0] = (float)YD0 * rad1 * (2.f * z1 * z1 - x1 * x1 - y1 * y1);
-              v1[1] = c1 * x1 * z1; v1[2] = c1 * z1 * y1;
-              v1[3] = (float)YD2 * rad1 * (x1 * x1 - y1 * y1); v1[4] = c1 * x1 * y1;
-            }
-            const int nf = 2 * L + 1;
-            for (int k = 0; k < nf; ++k) {
-              const int j = f0 + k;
-              // two consecutive functions in the same 16-byte unit: one 4-byte store per piece
-              if (k + 1 < nf && (j & 1) == 0) {
-                store_pair16<FMT>(A_hi, A_lo, a_offset(r0, j), v0[k], v0[k + 1], two);
-                store_pair16<FMT>(A_hi, A_lo, a_offset(r1, j), v1[k], v1[k + 1], two);
-                ++k;
-              } else {
-                store_split16<FMT>(A_hi, A_lo, a_offset(r0, j), v0[k], two);
-                store_split16<FMT>(A_hi, A_lo, a_offset(r1, j), v1[k], two);
-              }
+              store_split16<FMT>(A_hi, A_lo, off, v0[k], two);
+              store_split16<FMT>(A_hi, A_lo, off + 8192u, v1[k], two);
             }
           }
         }
@@ -896,13 +919,13 @@ __global__ void __launch_bounds__(320, 1)
       // generic-proxy writes of A must be visible to the tensor core
       asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
       tc_fence_before();
-      named_barrier(1, 256);
+      named_barrier(1, FUSED_NCT);
       if (ct == 0) mbar_arrive(&a_full);
       // ---- epilogue -----------------------------------------------------------------------
       if (!mbar_wait(&t_full, tile_it & 1u, &abort_flag)) break;
       tc_fence_after();
-      double acc = 0.0;
-      for (int c = hh; c * 32 < p.kpad; c += 2) {
+      double acc[4] = {0.0, 0.0, 0.0, 0.0};
+      for (int c = hh; c * 32 < p.kpad; c += FUSED_NCW / 4) {
         const int col = c * 32;
         float v[32], ph[32];
         tmem_ld32(tmem + ((uint32_t)(q * 32) << 16) + (uint32_t)col, v);
@@ -921,17 +944,18 @@ __global__ void __launch_bounds__(320, 1)
           }
         }
 #pragma unroll
-        for (int k = 0; k < 32; ++k) acc = fma((double)ph[k], (double)v[k], acc);
+        for (int k = 0; k < 32; ++k) acc[k & 3] = fma((double)ph[k], (double)v[k], acc[k & 3]);
       }
       tc_fence_before();
-      rho_part[hh][row] = acc;
-      named_barrier(1, 256);
+      rho_part[hh][row] = (acc[0] + acc[1]) + (acc[2] + acc[3]);
+      named_barrier(1, FUSED_NCT);
       double mysum = 0.0;
       if (ct < p.pm.vpt) {
         double r = 0.0;
         for (int sub = 0; sub < p.pm.s3; ++sub) {
           const int rr = ct * p.pm.s3 + sub;
-          r += rho_part[0][rr] + rho_part[1][rr];
+#pragma unroll
+          for (int h3 = 0; h3 < FUSED_NCW / 4; ++h3) r += rho_part[h3][rr];
         }
         const int64_t vox = t * p.pm.vpt + ct;
         if (vox < p.pm.nvox) {
@@ -941,14 +965,14 @@ __global__ void __launch_bounds__(320, 1)
         }
       }
       for (int o = 16; o > 0; o >>= 1) mysum += __shfl_xor_sync(0xffffffffu, mysum, o);
-      if (lane == 0) red[warp - 2] = mysum;
-      named_barrier(1, 256);
+      if (lane == 0) red[cw] = mysum;
+      named_barrier(1, FUSED_NCT);
       if (ct == 0) {
         double tot = 0;
-        for (int w = 0; w < 8; ++w) tot += red[w];
+        for (int w = 0; w < FUSED_NCW; ++w) tot += red[w];
         p.partials[t] = tot;
       }
-      named_barrier(1, 256);
+      named_barrier(1, FUSED_NCT);
     }
   }
 
@@ -1055,17 +1079,17 @@ static qmt_status run_fused(qmt_mol* m, const TcShape& sh, const PointMap& pm, i
   int maxsm = 0, dev = 0;
   cudaGetDevice(&dev);
   cudaDeviceGetAttribute(&maxsm, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev);
-  const int static_bytes = 6144;
-  const long avail = (long)maxsm - static_bytes - 1024 - (long)p.nsplit * p.a_bytes;
+  auto kern = density_fused_kernel<FMT>;
+  cudaFuncAttributes fa;
+  QMT_CUDA(cudaFuncGetAttributes(&fa, kern));
+  const long avail = (long)maxsm - (long)fa.sharedSizeBytes - 1024 - (long)p.nsplit * p.a_bytes;
   int stages = (int)std::min<long>(MAX_STAGES, avail / (long)p.stage_bytes);
   if (stages < 2) return fail(QMT_BAD_ARG, "fused density tile does not fit in shared memory");
   p.stages = stages;
   const size_t dyn = (size_t)p.nsplit * p.a_bytes + (size_t)stages * p.stage_bytes + 1024;
-  auto kern = density_fused_kernel<FMT>;
   QMT_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)dyn));
-  QMT_CUDA(cudaMemsetAsync(p.err, 0, sizeof(int), s));
   const int grid = (int)std::min<int64_t>(ntiles, sm_count());
-  kern<<<grid, 320, dyn, s>>>(tU_hi, tU_lo, p);
+  kern<<<grid, FUSED_THREADS, dyn, s>>>(tU_hi, tU_lo, p);
   QMT_CHECK_LAUNCH("density_fused_kernel");
   return QMT_OK;
 }
@@ -1098,10 +1122,18 @@ qmt_status density_tc(qmt_mol* mol, int nx, int ny, int nz, float step, float ox
   if (st) return st;
   st = finish_density(mol, pm.nvox, ntiles, rescale, qube, sum_out, s);
   if (st) return st;
-  int err = 0;
-  QMT_CUDA(cudaMemcpyAsync(&err, mol->d_scalars.as<double>() + 8, sizeof(int), cudaMemcpyDeviceToHost, s));
-  QMT_CUDA(cudaStreamSynchronize(s));
-  if (err) return fail(QMT_CUDA_ERR, "tensor-core density kernel gave up waiting on a barrier");
+  // The kernels' barrier-timeout flag is sticky: a call that returns a host sum (and so
+  // synchronises anyway) reads and clears it; fully asynchronous calls leave it for the next
+  // synchronous call on this molecule.
+  if (sum_out) {
+    int err = 0;
+    QMT_CUDA(cudaMemcpyAsync(&err, mol->d_scalars.as<double>() + 8, sizeof(int), cudaMemcpyDeviceToHost, s));
+    QMT_CUDA(cudaStreamSynchronize(s));
+    if (err) {
+      QMT_CUDA(cudaMemsetAsync(mol->d_scalars.as<double>() + 8, 0, sizeof(int), s));
+      return fail(QMT_CUDA_ERR, "tensor-core density kernel gave up waiting on a barrier");
+    }
+  }
   return QMT_OK;
 }
 

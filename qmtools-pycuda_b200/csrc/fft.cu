@@ -9,12 +9,19 @@
 //   through scikit-cuda, whose import is commented out (qmtools/qmtools.py:16).
 // Free-space variant (new): the same charge density, convolved with the Hockney Green's
 //   function 1/(4 pi EPS0 |r|) on a zero-padded grid of at least 2n per axis (sizes with
-//   factors 2, 3, 5, 7), G(0) = voxel-cube average of 1/|r|; G_hat is cached per (M, h).
+//   factors 2, 3, 5, 7), G(0) = voxel-cube average of 1/|r|; G_hat is real and even, so only
+//   its octant [0, M/2]^3 is stored, cached per (M, h, device).
 //
-// The 1D transforms are mixed-radix Stockham (self-sorting) FFTs on batches of lines held
-// in shared memory; the 3D transform is three axis passes over an x-fastest complex grid,
-// each CTA reading whole lines (x pass) or B consecutive x-columns (y and z passes) so that
-// global accesses are contiguous.
+// 1D transforms are mixed-radix Stockham (self-sorting) FFTs of batches of lines in shared
+// memory, twiddles from a per-length table computed in FP64 on the host.  A solve is five
+// passes over an x-fastest complex work grid:
+//   1. x forward, with the RHS assembled on the fly from q and the nuclei (only lines and
+//      elements inside the physical box are non-zero: y < ny, z < nz, x < nx);
+//   2. y forward on the z < nz planes (elements y >= ny are zero and not read);
+//   3. z forward, multiply by G_hat (or the periodic k-space factor), z inverse, store z < nz;
+//   4. y inverse on the z < nz planes, store y < ny;
+//   5. x inverse, 1/M^3, real part written straight into the C-order output (x < nx).
+// Zero padding therefore costs about 2.5 full-grid passes instead of 6.
 #include <algorithm>
 #include <map>
 #include <tuple>
@@ -26,7 +33,9 @@ namespace qmt {
 constexpr double EPS0 = 0.0055263494;       // e/(V*Ang), kernel_fft.cu:18
 constexpr double R_BOHR = 0.529177211;      // kernel_fft.cu:17
 constexpr double CUBE_INV_R = 2.3800772417; // h * <1/|r|> over a voxel cube
+constexpr double PI = 3.14159265358979323846;
 constexpr int FFT_MAXFAC = 16;
+constexpr int FFT_MAXLEN = 2048;
 
 struct Plan1D {
   int L;
@@ -38,8 +47,7 @@ static bool factorize(int L, Plan1D& p) {
   p.L = L;
   p.nfac = 0;
   int n = L;
-  const int pref[] = {4, 2, 3, 5, 7};
-  for (int r : pref)
+  for (int r : {4, 2, 3, 5, 7})
     while (n % r == 0) {
       if (p.nfac >= FFT_MAXFAC) return false;
       p.fac[p.nfac++] = r;
@@ -65,100 +73,86 @@ static int nice_at_least(int n) {
   return n;
 }
 
-// Lines: line l has elements at base(l) + e*se, base(l) = (l % n1)*s1 + (l / n1)*s2.
-struct Lines {
-  int64_t n1, s1, s2, se;
-  int64_t nlines;
-};
-
 __device__ __forceinline__ float2 cmul(float2 a, float2 b) {
   return make_float2(a.x * b.x - a.y * b.y, a.x * b.y + a.y * b.x);
 }
+__device__ __forceinline__ float2 cadd(float2 a, float2 b) { return make_float2(a.x + b.x, a.y + b.y); }
+__device__ __forceinline__ float2 csub(float2 a, float2 b) { return make_float2(a.x - b.x, a.y - b.y); }
 
-// exp(sign * 2 pi i * num / den), num reduced mod den
-__device__ __forceinline__ float2 root(int64_t num, int den, float sign) {
-  const int64_t m = num % den;
-  float s, c;
-  sincospif(2.0f * (float)m / (float)den, &s, &c);
-  return make_float2(c, sign * s);
+// table entry m: exp(-2 pi i m / L); conjugated for the inverse direction
+__device__ __forceinline__ float2 twid(const float2* tw, int m, bool inv) {
+  const float2 t = tw[m];
+  return inv ? make_float2(t.x, -t.y) : t;
 }
 
-// One radix-R butterfly of a Stockham stage: twiddle by exp(sign 2 pi i k q/(Ns R)), DFT_R,
-// scatter to the self-sorted position.
+// One radix-R butterfly of a Stockham stage (twiddle, DFT_R, scatter to sorted position).
 template <int R>
 __device__ __forceinline__ void radix_stage(const float2* __restrict__ s, float2* __restrict__ d, int j, int k,
-                                            int idxD, int nbf, int Ns, float sign) {
-  float2 v[R], w[R];
+                                            int idxD, int nbf, int Ns, const float2* tw, int L, bool inv) {
+  const int step = L / (Ns * R);
+  float2 v[R];
+  v[0] = s[j];
 #pragma unroll
-  for (int m = 0; m < R; ++m) w[m] = root(m, R, sign);
-  const float2 t1 = root(k, Ns * R, sign);
-  float2 tw = make_float2(1.f, 0.f);
+  for (int q = 1; q < R; ++q) v[q] = cmul(s[j + q * nbf], twid(tw, k * q * step, inv));
+  if constexpr (R == 2) {
+    d[idxD] = cadd(v[0], v[1]);
+    d[idxD + Ns] = csub(v[0], v[1]);
+  } else if constexpr (R == 4) {
+    const float2 a0 = cadd(v[0], v[2]), a1 = csub(v[0], v[2]);
+    const float2 b0 = cadd(v[1], v[3]), b1 = csub(v[1], v[3]);
+    // b1 times exp(-+ i pi/2): forward -i, inverse +i
+    const float2 b1r = inv ? make_float2(-b1.y, b1.x) : make_float2(b1.y, -b1.x);
+    d[idxD] = cadd(a0, b0);
+    d[idxD + Ns] = cadd(a1, b1r);
+    d[idxD + 2 * Ns] = csub(a0, b0);
+    d[idxD + 3 * Ns] = csub(a1, b1r);
+  } else {
+    float2 w[R];
 #pragma unroll
-  for (int q = 0; q < R; ++q) {
-    v[q] = q ? cmul(s[j + q * nbf], tw) : s[j];
-    tw = cmul(tw, t1);
-  }
+    for (int m = 0; m < R; ++m) w[m] = twid(tw, m * (L / R), inv);
 #pragma unroll
-  for (int q = 0; q < R; ++q) {
-    float2 acc = v[0];
+    for (int q = 0; q < R; ++q) {
+      float2 acc = v[0];
 #pragma unroll
-    for (int p = 1; p < R; ++p) {
-      const float2 w2 = w[(p * q) % R];
-      acc.x += v[p].x * w2.x - v[p].y * w2.y;
-      acc.y += v[p].x * w2.y + v[p].y * w2.x;
+      for (int p = 1; p < R; ++p) acc = cadd(acc, cmul(v[p], w[(p * q) % R]));
+      d[idxD + q * Ns] = acc;
     }
-    d[idxD + q * Ns] = acc;
   }
 }
 
-__global__ void __launch_bounds__(256) fft_lines_kernel(float2* __restrict__ data, Plan1D plan, Lines ln, int B,
-                                                        float sign, float scale) {
-  extern __shared__ float2 fsm[];
+// Transforms nb lines of length plan.L held in `src` (ping-pong with `dst`); the pointer
+// holding the result is returned in *result.
+__device__ void fft_lines_smem(float2* src, float2* dst, const Plan1D& plan, int nb, const float2* tw, bool inv,
+                               float2** result) {
   const int L = plan.L;
-  float2* b0 = fsm;
-  float2* b1 = fsm + (size_t)B * L;
-  const int64_t l0 = (int64_t)blockIdx.x * B;
-  const int64_t rem = ln.nlines - l0;
-  const int nb = rem < B ? (int)rem : B;
-  const bool xfirst = ln.s1 == 1;   // consecutive lines are adjacent in memory
-  // load
-  for (int i = threadIdx.x; i < nb * L; i += blockDim.x) {
-    int b, e;
-    if (xfirst) { b = i % nb; e = i / nb; } else { e = i % L; b = i / L; }
-    const int64_t l = l0 + b;
-    b0[b * L + e] = data[(l % ln.n1) * ln.s1 + (l / ln.n1) * ln.s2 + e * ln.se];
-  }
-  __syncthreads();
-  float2* src = b0;
-  float2* dst = b1;
   int Ns = 1;
   for (int st = 0; st < plan.nfac; ++st) {
     const int R = plan.fac[st];
     const int nbf = L / R;
     for (int w = threadIdx.x; w < nb * nbf; w += blockDim.x) {
-      const int b = w / nbf, j = w % nbf;
+      const int b = w / nbf, j = w - b * nbf;
       const float2* s = src + b * L;
       float2* d = dst + b * L;
       const int k = j % Ns;
       const int idxD = (j / Ns) * Ns * R + k;
       switch (R) {
-        case 2: radix_stage<2>(s, d, j, k, idxD, nbf, Ns, sign); break;
-        case 3: radix_stage<3>(s, d, j, k, idxD, nbf, Ns, sign); break;
-        case 4: radix_stage<4>(s, d, j, k, idxD, nbf, Ns, sign); break;
-        case 5: radix_stage<5>(s, d, j, k, idxD, nbf, Ns, sign); break;
-        case 7: radix_stage<7>(s, d, j, k, idxD, nbf, Ns, sign); break;
-        default:
+        case 2: radix_stage<2>(s, d, j, k, idxD, nbf, Ns, tw, L, inv); break;
+        case 3: radix_stage<3>(s, d, j, k, idxD, nbf, Ns, tw, L, inv); break;
+        case 4: radix_stage<4>(s, d, j, k, idxD, nbf, Ns, tw, L, inv); break;
+        case 5: radix_stage<5>(s, d, j, k, idxD, nbf, Ns, tw, L, inv); break;
+        case 7: radix_stage<7>(s, d, j, k, idxD, nbf, Ns, tw, L, inv); break;
+        default: {
+          const int step = L / (Ns * R);
           for (int q = 0; q < R; ++q) {
             float2 acc = make_float2(0.f, 0.f);
             for (int p = 0; p < R; ++p) {
               float2 x = s[j + p * nbf];
-              if (p) x = cmul(x, root((int64_t)k * p, Ns * R, sign));
-              const float2 w2 = root((int64_t)p * q, R, sign);
-              acc.x += x.x * w2.x - x.y * w2.y;
-              acc.y += x.x * w2.y + x.y * w2.x;
+              if (p) x = cmul(x, twid(tw, k * p * step, inv));
+              acc = cadd(acc, cmul(x, twid(tw, ((p * q) % R) * (L / R), inv)));
             }
             d[idxD + q * Ns] = acc;
           }
+        }
       }
     }
     __syncthreads();
@@ -167,105 +161,125 @@ __global__ void __launch_bounds__(256) fft_lines_kernel(float2* __restrict__ dat
     dst = t;
     Ns *= R;
   }
-  for (int i = threadIdx.x; i < nb * L; i += blockDim.x) {
-    int b, e;
-    if (xfirst) { b = i % nb; e = i / nb; } else { e = i % L; b = i / L; }
-    const int64_t l = l0 + b;
-    float2 v = src[b * L + e];
-    v.x *= scale;
-    v.y *= scale;
-    data[(l % ln.n1) * ln.s1 + (l / ln.n1) * ln.s2 + e * ln.se] = v;
-  }
+  *result = src;
 }
 
-struct Fft3D {
+enum { PASS_PLAIN = 0, PASS_X_RHS = 1, PASS_Z_MUL = 2, PASS_X_OUT = 3 };
+
+struct PassArgs {
+  Plan1D plan;
+  int64_t n1, s1, s2, se, nlines;   // line l: base (l % n1)*s1 + (l / n1)*s2, element e at + e*se
+  int lload, lstore;                // elements >= lload are zero; only e < lstore are stored
+  int B;                            // lines per CTA
+  int inv;                          // direction of the (first) transform
+  float scale;
+  const float2* tw;
+  float2* data;
+  // RHS assembly (PASS_X_RHS): lines are (y, z) with n1 = ny
+  MolView mol;
+  const float* q;
   int nx, ny, nz;
-  Plan1D px, py, pz;
+  float h_ang, ox, oy, oz, norm, i2s2, cut2;
+  int periodic;
+  // multiply (PASS_Z_MUL): lines are (x, y) with n1 = Mx
+  const float* gsym;
+  int Mx, My, Mz;
+  // C-order real output (PASS_X_OUT): lines are (z, y) with n1 = nz
+  float* out;
 };
 
-static qmt_status fft_axis(float2* d, const Plan1D& p, const Lines& ln, float sign, float scale, cudaStream_t s) {
-  int B = std::max(1, std::min(16, 12288 / p.L));
-  const size_t smem = 2 * (size_t)B * p.L * sizeof(float2);
-  QMT_CUDA(cudaFuncSetAttribute(fft_lines_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
-  const int64_t blocks = (ln.nlines + B - 1) / B;
-  fft_lines_kernel<<<(unsigned)blocks, 256, smem, s>>>(d, p, ln, B, sign, scale);
-  QMT_CHECK_LAUNCH("fft_lines_kernel");
-  return QMT_OK;
-}
-
-// In-place 3D transform of an x-fastest nx*ny*nz complex grid; inverse includes 1/N.
-static qmt_status fft3d(float2* d, const Fft3D& f, bool inverse, cudaStream_t s) {
-  const float sign = inverse ? 1.f : -1.f;
-  const int64_t nx = f.nx, ny = f.ny, nz = f.nz;
-  const float sc = inverse ? (float)(1.0 / ((double)nx * ny * nz)) : 1.f;
-  Lines lx{ny, nx, nx * ny, 1, ny * nz};
-  Lines ly{nx, 1, nx * ny, nx, nx * nz};
-  Lines lz{nx, 1, nx, nx * ny, nx * ny};
-  qmt_status st;
-  if ((st = fft_axis(d, f.px, lx, sign, 1.f, s))) return st;
-  if ((st = fft_axis(d, f.py, ly, sign, 1.f, s))) return st;
-  return fft_axis(d, f.pz, lz, sign, sc, s);
-}
-
-// ---- RHS assembly (kernel_fft.cu:23-79, Angstrom units) ---------------------------------------
-// Writes the complex grid (x-fastest, dims M) with the value at voxel (x,y,z) < (nx,ny,nz);
-// mode 0: RHS = -rho_tot/EPS0 (periodic); mode 1: rho_tot * h^3 (charge per voxel, free space).
-__global__ void fft_rhs_kernel(MolView mol, const float* __restrict__ q, int nx, int ny, int nz, float h_ang,
-                               float ox, float oy, float oz, float sigma, float cut2, int mode, int Mx, int My,
-                               int Mz, float2* __restrict__ out) {
-  extern __shared__ float sat[];
-  for (int i = threadIdx.x; i < mol.natoms; i += blockDim.x) {
-    sat[4 * i] = mol.coords[3 * i] * (float)R_BOHR;
-    sat[4 * i + 1] = mol.coords[3 * i + 1] * (float)R_BOHR;
-    sat[4 * i + 2] = mol.coords[3 * i + 2] * (float)R_BOHR;
-    sat[4 * i + 3] = (float)mol.types[i];
+template <int MODE>
+__global__ void __launch_bounds__(256) fft_pass_kernel(const PassArgs a) {
+  extern __shared__ float2 fsm[];
+  const int L = a.plan.L;
+  float2* tw = fsm;
+  float2* b0 = fsm + L;
+  float2* b1 = b0 + (size_t)a.B * L;
+  float* sat = reinterpret_cast<float*>(b1 + (size_t)a.B * L);   // atoms (PASS_X_RHS)
+  for (int i = threadIdx.x; i < L; i += blockDim.x) tw[i] = a.tw[i];
+  if constexpr (MODE == PASS_X_RHS) {
+    for (int i = threadIdx.x; i < a.mol.natoms; i += blockDim.x) {
+      sat[4 * i] = a.mol.coords[3 * i] * (float)R_BOHR;
+      sat[4 * i + 1] = a.mol.coords[3 * i + 1] * (float)R_BOHR;
+      sat[4 * i + 2] = a.mol.coords[3 * i + 2] * (float)R_BOHR;
+      sat[4 * i + 3] = (float)a.mol.types[i];
+    }
+  }
+  const int64_t l0 = (int64_t)blockIdx.x * a.B;
+  const int64_t rem = a.nlines - l0;
+  const int nb = rem < a.B ? (int)rem : a.B;
+  const bool lines_adjacent = a.s1 == 1;
+  __syncthreads();
+  // ---- load ----
+  for (int i = threadIdx.x; i < nb * L; i += blockDim.x) {
+    int b, e;
+    if (lines_adjacent) { b = i % nb; e = i / nb; } else { e = i % L; b = i / L; }
+    const int64_t l = l0 + b;
+    float2 v = make_float2(0.f, 0.f);
+    if (e < a.lload) {
+      if constexpr (MODE == PASS_X_RHS) {
+        const int y = (int)(l % a.n1), z = (int)(l / a.n1), x = e;
+        const float px = a.ox + (x + 0.5f) * a.h_ang, py = a.oy + (y + 0.5f) * a.h_ang,
+                    pz = a.oz + (z + 0.5f) * a.h_ang;
+        float rho = a.q[x + (int64_t)y * a.nx + (int64_t)z * a.nx * a.ny] / (-a.h_ang * a.h_ang * a.h_ang);
+        for (int at = 0; at < a.mol.natoms; ++at) {
+          const float cx = px - sat[4 * at], cy = py - sat[4 * at + 1], cz = pz - sat[4 * at + 2];
+          const float r2 = cx * cx + cy * cy + cz * cz;
+          if (r2 <= a.cut2) rho += sat[4 * at + 3] * a.norm * expf(-r2 * a.i2s2);
+        }
+        v.x = a.periodic ? (float)(-(double)rho / EPS0) : rho * a.h_ang * a.h_ang * a.h_ang;
+      } else {
+        v = a.data[(l % a.n1) * a.s1 + (l / a.n1) * a.s2 + e * a.se];
+      }
+    }
+    b0[b * L + e] = v;
   }
   __syncthreads();
-  const int64_t n = (int64_t)Mx * My * Mz;
-  const float norm = 1.0f / (sigma * sigma * sigma * 2.0f * 3.14159265358979f * sqrtf(2.0f * 3.14159265358979f));
-  const float i2s2 = 1.0f / (2.0f * sigma * sigma);
-  for (int64_t idx = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; idx < n; idx += (int64_t)gridDim.x * blockDim.x) {
-    const int x = (int)(idx % Mx), y = (int)((idx / Mx) % My), z = (int)(idx / ((int64_t)Mx * My));
-    float v = 0.f;
-    if (x < nx && y < ny && z < nz) {
-      const float px = ox + (x + 0.5f) * h_ang, py = oy + (y + 0.5f) * h_ang, pz = oz + (z + 0.5f) * h_ang;
-      float rho = q[x + (int64_t)y * nx + (int64_t)z * nx * ny] / (-h_ang * h_ang * h_ang);
-      for (int a = 0; a < mol.natoms; ++a) {
-        const float cx = px - sat[4 * a], cy = py - sat[4 * a + 1], cz = pz - sat[4 * a + 2];
-        const float r2 = cx * cx + cy * cy + cz * cz;
-        if (r2 <= cut2) rho += sat[4 * a + 3] * norm * expf(-r2 * i2s2);
+  float2* res;
+  fft_lines_smem(b0, b1, a.plan, nb, tw, a.inv != 0, &res);
+  if constexpr (MODE == PASS_Z_MUL) {
+    for (int i = threadIdx.x; i < nb * L; i += blockDim.x) {
+      const int b = i / L, kz = i % L;
+      const int64_t l = l0 + b;
+      const int x = (int)(l % a.n1), y = (int)(l / a.n1);
+      float f;
+      if (a.periodic) {
+        // kernel_fft.cu:90-104: k in cycles/Ang, negative frequencies above N/2 - 1, k = 0 -> 0
+        const float kx = (x > a.Mx / 2 - 1 ? (float)(x - a.Mx) : (float)x) / (a.Mx * a.h_ang);
+        const float ky = (y > a.My / 2 - 1 ? (float)(y - a.My) : (float)y) / (a.My * a.h_ang);
+        const float kk = (kz > a.Mz / 2 - 1 ? (float)(kz - a.Mz) : (float)kz) / (a.Mz * a.h_ang);
+        const double k2 = (double)(kx * kx + ky * ky + kk * kk);
+        f = (x == 0 && y == 0 && kz == 0) ? 0.f : (float)(-1.0 / (4.0 * PI * PI * k2));
+      } else {
+        const int gx = min(x, a.Mx - x), gy = min(y, a.My - y), gz = min(kz, a.Mz - kz);
+        f = a.gsym[gx + (int64_t)(a.Mx / 2 + 1) * (gy + (int64_t)(a.My / 2 + 1) * gz)];
       }
-      v = mode == 0 ? (float)(-(double)rho / EPS0) : rho * h_ang * h_ang * h_ang;
+      float2 v = res[b * L + kz];
+      res[b * L + kz] = make_float2(v.x * f, v.y * f);
     }
-    out[idx] = make_float2(v, 0.f);
+    __syncthreads();
+    float2* other = res == b0 ? b1 : b0;
+    fft_lines_smem(res, other, a.plan, nb, tw, a.inv == 0, &res);
+  }
+  // ---- store ----
+  for (int i = threadIdx.x; i < nb * a.lstore; i += blockDim.x) {
+    int b, e;
+    if (lines_adjacent || MODE == PASS_X_OUT) { b = i % nb; e = i / nb; } else { e = i % a.lstore; b = i / a.lstore; }
+    const int64_t l = l0 + b;
+    const float2 v = res[b * L + e];
+    if constexpr (MODE == PASS_X_OUT) {
+      const int z = (int)(l % a.n1), y = (int)(l / a.n1);
+      a.out[(int64_t)e * a.ny * a.nz + (int64_t)y * a.nz + z] = v.x * a.scale;
+    } else {
+      a.data[(l % a.n1) * a.s1 + (l / a.n1) * a.s2 + e * a.se] = make_float2(v.x * a.scale, v.y * a.scale);
+    }
   }
 }
 
-// V_hat = -RHS_hat / (4 pi^2 |k|^2), k in cycles/Ang; k = 0 -> 0  (kernel_fft.cu:82-107)
-__global__ void periodic_scale_kernel(float2* __restrict__ c, int nx, int ny, int nz, float h_ang) {
-  const int64_t n = (int64_t)nx * ny * nz;
-  for (int64_t idx = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; idx < n; idx += (int64_t)gridDim.x * blockDim.x) {
-    const int i = (int)(idx % nx), j = (int)((idx / nx) % ny), k = (int)(idx / ((int64_t)nx * ny));
-    if (idx == 0) {
-      c[0] = make_float2(0.f, 0.f);
-      continue;
-    }
-    const float kx = (i > nx / 2 - 1 ? (float)(i - nx) : (float)i) / (nx * h_ang);
-    const float ky = (j > ny / 2 - 1 ? (float)(j - ny) : (float)j) / (ny * h_ang);
-    const float kz = (k > nz / 2 - 1 ? (float)(k - nz) : (float)k) / (nz * h_ang);
-    const float sc = (float)(-1.0 / (4.0 * 3.14159265358979323846 * 3.14159265358979323846 *
-                                     (double)(kx * kx + ky * ky + kz * kz)));
-    float2 v = c[idx];
-    v.x *= sc;
-    v.y *= sc;
-    c[idx] = v;
-  }
-}
-
-// Green's function on the padded grid (minimum image), real part only.
+// ---- Green's function ----------------------------------------------------------------
 __global__ void green_kernel(float2* __restrict__ g, int Mx, int My, int Mz, float h_ang) {
   const int64_t n = (int64_t)Mx * My * Mz;
-  const double pref = 1.0 / (4.0 * 3.14159265358979323846 * EPS0);
+  const double pref = 1.0 / (4.0 * PI * EPS0);
   for (int64_t idx = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; idx < n; idx += (int64_t)gridDim.x * blockDim.x) {
     const int64_t i = idx % Mx, j = (idx / Mx) % My, k = idx / ((int64_t)Mx * My);
     const double x = (double)min(i, Mx - i) * h_ang, y = (double)min(j, My - j) * h_ang,
@@ -276,59 +290,128 @@ __global__ void green_kernel(float2* __restrict__ g, int Mx, int My, int Mz, flo
   }
 }
 
-__global__ void take_real_kernel(const float2* __restrict__ in, float* __restrict__ out, int64_t n) {
-  for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x)
-    out[i] = in[i].x;
-}
-
-__global__ void mul_real_kernel(float2* __restrict__ c, const float* __restrict__ g, int64_t n) {
-  for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) {
-    float2 v = c[i];
-    const float s = g[i];
-    c[i] = make_float2(v.x * s, v.y * s);
-  }
-}
-
-// out[i*ny*nz + j*nz + k] = Re c[x=i, y=j, z=k] for the first (nx,ny,nz) of an Mx-by-My-by-Mz grid.
-__global__ void to_corder_kernel(const float2* __restrict__ c, int Mx, int My, int nx, int ny, int nz,
-                                 float* __restrict__ out) {
-  __shared__ float tile[32][33];
-  const int y = blockIdx.z;
-  const int x0 = blockIdx.x * 32, z0 = blockIdx.y * 32;
-  for (int r = threadIdx.y; r < 32; r += blockDim.y) {
-    const int z = z0 + r, x = x0 + threadIdx.x;
-    if (z < nz && x < nx) tile[r][threadIdx.x] = c[x + (int64_t)y * Mx + (int64_t)z * Mx * My].x;
-  }
-  __syncthreads();
-  for (int r = threadIdx.y; r < 32; r += blockDim.y) {
-    const int x = x0 + r, z = z0 + threadIdx.x;
-    if (z < nz && x < nx) out[(int64_t)x * ny * nz + (int64_t)y * nz + z] = tile[threadIdx.x][r];
+__global__ void green_octant_kernel(const float2* __restrict__ g, int Mx, int My, int Mz, float* __restrict__ out) {
+  const int ox = Mx / 2 + 1, oy = My / 2 + 1, oz = Mz / 2 + 1;
+  const int64_t n = (int64_t)ox * oy * oz;
+  for (int64_t idx = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; idx < n; idx += (int64_t)gridDim.x * blockDim.x) {
+    const int64_t i = idx % ox, j = (idx / ox) % oy, k = idx / ((int64_t)ox * oy);
+    out[idx] = g[i + j * Mx + k * (int64_t)Mx * My].x;
   }
 }
 
 // ---- host ------------------------------------------------------------------------------------
-struct GreenCache {
-  DevBuf g;
+static unsigned grid_blocks(int64_t n) { return (unsigned)std::min<int64_t>((n + 255) / 256, (int64_t)sm_count() * 16); }
+
+struct DevCache {
+  std::map<std::tuple<int, int>, DevBuf*> tw;                     // (L, device)
+  std::map<std::tuple<int, int, int, float, int>, DevBuf*> green; // (Mx, My, Mz, h, device)
 };
-static std::map<std::tuple<int, int, int, float, int>, DevBuf*>& green_cache() {
-  static std::map<std::tuple<int, int, int, float, int>, DevBuf*> m;
-  return m;
+static DevCache& cache() {
+  static DevCache c;
+  return c;
 }
 
-static qmt_status make_plan(int nx, int ny, int nz, Fft3D& f) {
-  f.nx = nx;
-  f.ny = ny;
-  f.nz = nz;
-  if (!factorize(nx, f.px) || !factorize(ny, f.py) || !factorize(nz, f.pz))
-    return fail(QMT_BAD_ARG, "FFT size has too many factors");
-  for (const Plan1D* p : {&f.px, &f.py, &f.pz})
-    for (int i = 0; i < p->nfac; ++i)
-      if (p->fac[i] > 127) return fail(QMT_BAD_ARG, "FFT size has a prime factor above 127");
-  if (std::max(nx, std::max(ny, nz)) > 4096) return fail(QMT_BAD_ARG, "FFT line longer than 4096");
+static qmt_status twiddles(int L, const float2** out) {
+  int dev = 0;
+  cudaGetDevice(&dev);
+  DevBuf*& b = cache().tw[std::make_tuple(L, dev)];
+  if (!b) {
+    std::vector<float2> h(L);
+    for (int m = 0; m < L; ++m) {
+      const double a = -2.0 * PI * (double)m / (double)L;
+      h[m] = make_float2((float)std::cos(a), (float)std::sin(a));
+    }
+    b = new DevBuf();
+    qmt_status st = b->reserve(L * sizeof(float2));
+    if (st) {
+      delete b;
+      b = nullptr;
+      return st;
+    }
+    QMT_CUDA(cudaMemcpy(b->ptr, h.data(), L * sizeof(float2), cudaMemcpyHostToDevice));
+  }
+  *out = b->as<float2>();
   return QMT_OK;
 }
 
-static unsigned grid_blocks(int64_t n) { return (unsigned)std::min<int64_t>((n + 255) / 256, (int64_t)sm_count() * 16); }
+template <int MODE>
+static qmt_status launch_mode(const PassArgs& a, unsigned blocks, size_t smem, cudaStream_t s) {
+  QMT_CUDA(cudaFuncSetAttribute(fft_pass_kernel<MODE>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+  fft_pass_kernel<MODE><<<blocks, 256, smem, s>>>(a);
+  QMT_CHECK_LAUNCH("fft_pass_kernel");
+  return QMT_OK;
+}
+
+static qmt_status launch_pass(int mode, PassArgs a, cudaStream_t s) {
+  a.B = std::max(1, std::min(16, 12288 / a.plan.L));
+  const float2* tw;
+  qmt_status st = twiddles(a.plan.L, &tw);
+  if (st) return st;
+  a.tw = tw;
+  size_t smem = ((size_t)a.plan.L * (1 + 2 * a.B)) * sizeof(float2);
+  if (mode == PASS_X_RHS) smem += 16 * (size_t)a.mol.natoms;
+  const unsigned blocks = (unsigned)((a.nlines + a.B - 1) / a.B);
+  if (blocks == 0) return QMT_OK;
+  switch (mode) {
+    case PASS_PLAIN: return launch_mode<PASS_PLAIN>(a, blocks, smem, s);
+    case PASS_X_RHS: return launch_mode<PASS_X_RHS>(a, blocks, smem, s);
+    case PASS_Z_MUL: return launch_mode<PASS_Z_MUL>(a, blocks, smem, s);
+    default: return launch_mode<PASS_X_OUT>(a, blocks, smem, s);
+  }
+}
+
+static qmt_status plan_of(int L, Plan1D& p) {
+  if (L < 2 || L > FFT_MAXLEN) return fail(QMT_BAD_ARG, "FFT line length out of range");
+  if (!factorize(L, p)) return fail(QMT_BAD_ARG, "FFT size has too many factors");
+  for (int i = 0; i < p.nfac; ++i)
+    if (p.fac[i] > 127) return fail(QMT_BAD_ARG, "FFT size has a prime factor above 127");
+  return QMT_OK;
+}
+
+// Hockney G_hat octant for (Mx, My, Mz, h): one unpruned forward 3D transform, cached.
+static qmt_status green_hat(int Mx, int My, int Mz, float h_ang, const Plan1D& px, const Plan1D& py,
+                            const Plan1D& pz, const float** out, cudaStream_t s) {
+  int dev = 0;
+  cudaGetDevice(&dev);
+  auto key = std::make_tuple(Mx, My, Mz, h_ang, dev);
+  auto it = cache().green.find(key);
+  if (it != cache().green.end()) {
+    *out = it->second->as<float>();
+    return QMT_OK;
+  }
+  const int64_t M = (int64_t)Mx * My * Mz;
+  DevBuf tmp;
+  qmt_status st = tmp.reserve(M * sizeof(float2));
+  if (st) return st;
+  float2* g = tmp.as<float2>();
+  green_kernel<<<grid_blocks(M), 256, 0, s>>>(g, Mx, My, Mz, h_ang);
+  QMT_CHECK_LAUNCH("green_kernel");
+  PassArgs a{};
+  a.data = g;
+  a.scale = 1.f;
+  a.inv = 0;
+  a.plan = px; a.n1 = My; a.s1 = Mx; a.s2 = (int64_t)Mx * My; a.se = 1; a.nlines = (int64_t)My * Mz;
+  a.lload = a.lstore = Mx;
+  if ((st = launch_pass(PASS_PLAIN, a, s))) return st;
+  a.plan = py; a.n1 = Mx; a.s1 = 1; a.s2 = (int64_t)Mx * My; a.se = Mx; a.nlines = (int64_t)Mx * Mz;
+  a.lload = a.lstore = My;
+  if ((st = launch_pass(PASS_PLAIN, a, s))) return st;
+  a.plan = pz; a.n1 = Mx; a.s1 = 1; a.s2 = Mx; a.se = (int64_t)Mx * My; a.nlines = (int64_t)Mx * My;
+  a.lload = a.lstore = Mz;
+  if ((st = launch_pass(PASS_PLAIN, a, s))) return st;
+  auto* gb = new DevBuf();
+  const int64_t no = (int64_t)(Mx / 2 + 1) * (My / 2 + 1) * (Mz / 2 + 1);
+  if ((st = gb->reserve(no * sizeof(float)))) {
+    delete gb;
+    return st;
+  }
+  green_octant_kernel<<<grid_blocks(no), 256, 0, s>>>(g, Mx, My, Mz, gb->as<float>());
+  QMT_CHECK_LAUNCH("green_octant_kernel");
+  QMT_CUDA(cudaStreamSynchronize(s));
+  cache().green[key] = gb;
+  *out = gb->as<float>();
+  return QMT_OK;
+}
 
 }  // namespace qmt
 
@@ -339,60 +422,61 @@ extern "C" qmt_status qmt_fft_poisson(qmt_mol* mol, int nx, int ny, int nz, floa
                                       float* out_dev, void* stream) {
   if (!mol || !q_dev || !out_dev || nx < 2 || ny < 2 || nz < 2 || !(step > 0.f) || !(sigma > 0.f) || cutoff < 0)
     return fail(QMT_BAD_ARG, "bad FFT Poisson arguments");
-  if (mol->natoms > 8192) return fail(QMT_BAD_ARG, "too many atoms");
+  if (mol->natoms > 4096) return fail(QMT_BAD_ARG, "too many atoms");
   cudaStream_t s = as_stream(stream);
-  const float h_ang = (float)(step / ANG2BOR);
-  const float oxa = (float)(ox / ANG2BOR), oya = (float)(oy / ANG2BOR), oza = (float)(oz / ANG2BOR);
-  const float cut2 = (cutoff * sigma) * (cutoff * sigma);
-  int Mx = nx, My = ny, Mz = nz;
-  if (padded) {
-    Mx = nice_at_least(2 * nx);
-    My = nice_at_least(2 * ny);
-    Mz = nice_at_least(2 * nz);
-  }
-  Fft3D plan;
-  qmt_status st = make_plan(Mx, My, Mz, plan);
-  if (st) return st;
+  const int Mx = padded ? nice_at_least(2 * nx) : nx;
+  const int My = padded ? nice_at_least(2 * ny) : ny;
+  const int Mz = padded ? nice_at_least(2 * nz) : nz;
+  Plan1D px, py, pz;
+  qmt_status st;
+  if ((st = plan_of(Mx, px)) || (st = plan_of(My, py)) || (st = plan_of(Mz, pz))) return st;
   const int64_t M = (int64_t)Mx * My * Mz;
-  if ((st = mol->d_work.reserve(M * sizeof(float2)))) return st;
+  // work grid: x-fastest, only the planes z < nz are ever touched
+  if ((st = mol->d_work.reserve((int64_t)Mx * My * nz * sizeof(float2)))) return st;
   float2* c = mol->d_work.as<float2>();
-  const size_t ash = 16 * (size_t)mol->natoms;
-  fft_rhs_kernel<<<grid_blocks(M), 256, ash, s>>>(mol->view(), q_dev, nx, ny, nz, h_ang, oxa, oya, oza, sigma, cut2,
-                                                  padded ? 1 : 0, Mx, My, Mz, c);
-  QMT_CHECK_LAUNCH("fft_rhs_kernel");
-  if ((st = fft3d(c, plan, false, s))) return st;
-  if (!padded) {
-    periodic_scale_kernel<<<grid_blocks(M), 256, 0, s>>>(c, Mx, My, Mz, h_ang);
-    QMT_CHECK_LAUNCH("periodic_scale_kernel");
-  } else {
-    int dev = 0;
-    cudaGetDevice(&dev);
-    auto key = std::make_tuple(Mx, My, Mz, h_ang, dev);
-    auto& cache = green_cache();
-    DevBuf*& gb = cache[key];
-    if (!gb) {
-      gb = new DevBuf();
-      DevBuf tmp;
-      if ((st = gb->reserve(M * sizeof(float))) || (st = tmp.reserve(M * sizeof(float2)))) {
-        delete gb;
-        gb = nullptr;
-        cache.erase(key);
-        return st;
-      }
-      green_kernel<<<grid_blocks(M), 256, 0, s>>>(tmp.as<float2>(), Mx, My, Mz, h_ang);
-      QMT_CHECK_LAUNCH("green_kernel");
-      if ((st = fft3d(tmp.as<float2>(), plan, false, s))) return st;
-      take_real_kernel<<<grid_blocks(M), 256, 0, s>>>(tmp.as<float2>(), gb->as<float>(), M);
-      QMT_CHECK_LAUNCH("take_real_kernel");
-      QMT_CUDA(cudaStreamSynchronize(s));
-      tmp.release();
-    }
-    mul_real_kernel<<<grid_blocks(M), 256, 0, s>>>(c, gb->as<float>(), M);
-    QMT_CHECK_LAUNCH("mul_real_kernel");
-  }
-  if ((st = fft3d(c, plan, true, s))) return st;
-  dim3 tb(32, 8), tg((nx + 31) / 32, (nz + 31) / 32, ny);
-  to_corder_kernel<<<tg, tb, 0, s>>>(c, Mx, My, nx, ny, nz, out_dev);
-  QMT_CHECK_LAUNCH("to_corder_kernel");
-  return QMT_OK;
+  const float h_ang = (float)(step / ANG2BOR);
+  const float* gsym = nullptr;
+  if (padded && (st = green_hat(Mx, My, Mz, h_ang, px, py, pz, &gsym, s))) return st;
+
+  PassArgs a{};
+  a.data = c;
+  a.mol = mol->view();
+  a.q = q_dev;
+  a.nx = nx;
+  a.ny = ny;
+  a.nz = nz;
+  a.h_ang = h_ang;
+  a.ox = (float)(ox / ANG2BOR);
+  a.oy = (float)(oy / ANG2BOR);
+  a.oz = (float)(oz / ANG2BOR);
+  a.norm = 1.0f / (sigma * sigma * sigma * 2.0f * (float)PI * sqrtf(2.0f * (float)PI));
+  a.i2s2 = 1.0f / (2.0f * sigma * sigma);
+  a.cut2 = (cutoff * sigma) * (cutoff * sigma);
+  a.periodic = padded ? 0 : 1;
+  a.gsym = gsym;
+  a.Mx = Mx;
+  a.My = My;
+  a.Mz = Mz;
+  a.out = out_dev;
+  a.scale = 1.f;
+  // 1. x forward with the RHS: lines (y < ny, z < nz), elements x < nx non-zero
+  a.plan = px; a.n1 = ny; a.s1 = Mx; a.s2 = (int64_t)Mx * My; a.se = 1; a.nlines = (int64_t)ny * nz;
+  a.lload = nx; a.lstore = Mx; a.inv = 0;
+  if ((st = launch_pass(PASS_X_RHS, a, s))) return st;
+  // 2. y forward on the planes z < nz: lines (x < Mx, z < nz), elements y < ny non-zero
+  a.plan = py; a.n1 = Mx; a.s1 = 1; a.s2 = (int64_t)Mx * My; a.se = Mx; a.nlines = (int64_t)Mx * nz;
+  a.lload = ny; a.lstore = My;
+  if ((st = launch_pass(PASS_PLAIN, a, s))) return st;
+  // 3. z forward, kernel multiply, z inverse: lines (x < Mx, y < My), store z < nz
+  a.plan = pz; a.n1 = Mx; a.s1 = 1; a.s2 = Mx; a.se = (int64_t)Mx * My; a.nlines = (int64_t)Mx * My;
+  a.lload = nz; a.lstore = nz;
+  if ((st = launch_pass(PASS_Z_MUL, a, s))) return st;
+  // 4. y inverse on the planes z < nz, store y < ny
+  a.plan = py; a.n1 = Mx; a.s1 = 1; a.s2 = (int64_t)Mx * My; a.se = Mx; a.nlines = (int64_t)Mx * nz;
+  a.lload = My; a.lstore = ny; a.inv = 1;
+  if ((st = launch_pass(PASS_PLAIN, a, s))) return st;
+  // 5. x inverse, 1/M^3, real part into the C-order output: lines (z < nz, y < ny)
+  a.plan = px; a.n1 = nz; a.s1 = (int64_t)Mx * My; a.s2 = Mx; a.se = 1; a.nlines = (int64_t)ny * nz;
+  a.lload = Mx; a.lstore = nx; a.inv = 1; a.scale = (float)(1.0 / (double)M);
+  return launch_pass(PASS_X_OUT, a, s);
 }

@@ -120,33 +120,18 @@ qmt_status qmt_mol::upload_dm(const float* dm, cudaStream_t s) {
   return QMT_OK;
 }
 
-extern "C" {
-
-const char* qmt_last_error(void) { return g_last_error.c_str(); }
-
-int qmt_abi_version(void) { return 1; }
-
-qmt_status qmt_init(int device) {
-  int n = 0;
-  cudaError_t e = cudaGetDeviceCount(&n);
-  if (e != cudaSuccess || n == 0) return fail(QMT_NO_DEVICE, "no CUDA device");
-  if (device < 0 || device >= n) return fail(QMT_BAD_ARG, "device index out of range");
-  QMT_CUDA(cudaSetDevice(device));
-  int major = 0;
-  QMT_CUDA(cudaDeviceGetAttribute(&major, cudaDevAttrComputeCapabilityMajor, device));
-  if (major != 10) return fail(QMT_NO_DEVICE, "libqmtools_b200 needs an sm_100 device");
-  return QMT_OK;
-}
-
-qmt_status qmt_mol_create(int natoms, const int32_t* types, const float* coords, int norbs,
-                          const int16_t* almos, int nparams, const float* alphas,
-                          const float* coeffs, const float* dm, void* stream, qmt_mol** out) {
-  if (!out || !types || !coords || !almos || !alphas || !coeffs || !dm)
-    return fail(QMT_BAD_ARG, "null argument");
-  *out = nullptr;
+// (Re)initialises `m` for a molecule; device buffers already held by `m` are reused.
+static qmt_status mol_init(qmt_mol* m, int natoms, const int32_t* types, const float* coords, int norbs,
+                           const int16_t* almos, int nparams, const float* alphas, const float* coeffs,
+                           const float* dm, cudaStream_t s) {
+  if (!types || !coords || !almos || !alphas || !coeffs || !dm) return fail(QMT_BAD_ARG, "null argument");
   if (natoms <= 0 || norbs <= 0 || nparams <= 0) return fail(QMT_BAD_ARG, "empty molecule");
-  cudaStream_t s = as_stream(stream);
-  auto* m = new qmt_mol();
+  m->shells.clear();
+  m->alpha.clear();
+  m->coeff.clear();
+  m->tc_prec = -1;
+  m->fused_prec = -1;
+  m->gto_ready = false;
   m->natoms = natoms;
   m->norbs = norbs;
   m->npad = (norbs + 31) / 32 * 32;
@@ -160,22 +145,18 @@ qmt_status qmt_mol_create(int natoms, const int32_t* types, const float* coords,
   while (f < norbs) {
     const int a = almos[4 * f + 0], L = almos[4 * f + 1], so = almos[4 * f + 3];
     if (a < 0 || a >= natoms) {
-      delete m;
       return fail(QMT_BAD_ARG, "ALMO atom index out of range");
     }
     if (L < 0 || L > MAX_L) {
-      delete m;
       return fail(QMT_UNSUPPORTED_L, "basis shell with L > 2");
     }
     if (f + 2 * L + 1 > norbs || so < 0 || so + MAXAOC > nparams) {
-      delete m;
       return fail(QMT_BAD_ARG, "truncated shell in ALMO table");
     }
     for (int k = 0; k < 2 * L + 1; ++k) {
       const int16_t* r = almos + 4 * (f + k);
       if (r[0] != a || r[1] != L || r[3] != so || r[2] != mord[L][k]) {
-        delete m;
-        return fail(QMT_BAD_ARG, "ALMO rows of a shell must follow the m order of the basis");
+          return fail(QMT_BAD_ARG, "ALMO rows of a shell must follow the m order of the basis");
       }
     }
     Shell sh{};
@@ -204,7 +185,6 @@ qmt_status qmt_mol_create(int natoms, const int32_t* types, const float* coords,
   }
   for (int sidx = 1; sidx < m->nshells; ++sidx)
     if (m->shells[sidx].atom < m->shells[sidx - 1].atom) {
-      delete m;
       return fail(QMT_BAD_ARG, "basis functions must be grouped by atom in atom order");
     }
   m->alpha64.assign(m->alpha.begin(), m->alpha.end());
@@ -225,11 +205,57 @@ qmt_status qmt_mol_create(int natoms, const int32_t* types, const float* coords,
       (st = upload(m->d_alpha64, m->alpha64.data(), m->alpha64.size() * sizeof(double), s)) ||
       (st = upload(m->d_coeff64, m->coeff64.data(), m->coeff64.size() * sizeof(double), s)) ||
       (st = m->upload_dm(dm, s))) {
+    return st;
+  }
+  // device scratch for sums and the sticky kernel error flag, cleared once here
+  if ((st = m->d_scalars.reserve(64 * sizeof(double)))) {
+    return st;
+  }
+  QMT_CUDA(cudaMemsetAsync(m->d_scalars.ptr, 0, 64 * sizeof(double), s));
+  QMT_CUDA(cudaStreamSynchronize(s));
+  return QMT_OK;
+}
+
+
+extern "C" {
+
+const char* qmt_last_error(void) { return g_last_error.c_str(); }
+
+int qmt_abi_version(void) { return 1; }
+
+qmt_status qmt_init(int device) {
+  int n = 0;
+  cudaError_t e = cudaGetDeviceCount(&n);
+  if (e != cudaSuccess || n == 0) return fail(QMT_NO_DEVICE, "no CUDA device");
+  if (device < 0 || device >= n) return fail(QMT_BAD_ARG, "device index out of range");
+  QMT_CUDA(cudaSetDevice(device));
+  int major = 0;
+  QMT_CUDA(cudaDeviceGetAttribute(&major, cudaDevAttrComputeCapabilityMajor, device));
+  if (major != 10) return fail(QMT_NO_DEVICE, "libqmtools_b200 needs an sm_100 device");
+  return QMT_OK;
+}
+
+qmt_status qmt_mol_create(int natoms, const int32_t* types, const float* coords, int norbs,
+                          const int16_t* almos, int nparams, const float* alphas,
+                          const float* coeffs, const float* dm, void* stream, qmt_mol** out) {
+  if (!out) return fail(QMT_BAD_ARG, "null argument");
+  *out = nullptr;
+  auto* m = new qmt_mol();
+  const qmt_status st = mol_init(m, natoms, types, coords, norbs, almos, nparams, alphas, coeffs, dm,
+                                 as_stream(stream));
+  if (st) {
     delete m;
     return st;
   }
   *out = m;
   return QMT_OK;
+}
+
+qmt_status qmt_mol_reset(qmt_mol* mol, int natoms, const int32_t* types, const float* coords, int norbs,
+                         const int16_t* almos, int nparams, const float* alphas, const float* coeffs,
+                         const float* dm, void* stream) {
+  if (!mol) return fail(QMT_BAD_ARG, "null argument");
+  return mol_init(mol, natoms, types, coords, norbs, almos, nparams, alphas, coeffs, dm, as_stream(stream));
 }
 
 qmt_status qmt_mol_set_coords(qmt_mol* mol, const float* coords, void* stream) {

@@ -71,9 +71,15 @@ struct MolView {
   const double* coeff64;
 };
 
+// Primitive screening: a primitive with alpha r^2 above the cut contributes less than
+// exp(-cut) of its contraction coefficient and is skipped -- 1.4e-11 for the FP32 paths
+// (far below FP32 round-off), 4e-18 for FP64.  A warp skips the exponential when all of
+// its points are beyond the cut.
+constexpr float kExpCut = 25.0f;
+constexpr double kExpCut64 = 40.0;
+
 // Writes the values of the shell's functions at displacement (dx,dy,dz) from its atom
-// into out[0..2L].  T = float or double.  Primitives with alpha*r^2 > cut contribute
-// below exp(-cut) relative and are skipped.
+// into out[0..2L].  T = float or double.
 template <typename T>
 __device__ __forceinline__ int shell_values(const Shell& sh, const T* __restrict__ al,
                                             const T* __restrict__ co, T dx, T dy, T dz,
@@ -82,7 +88,7 @@ __device__ __forceinline__ int shell_values(const Shell& sh, const T* __restrict
   T rad = T(0);
   for (int k = 0; k < sh.nprim; ++k) {
     const T e = al[sh.prim + k] * r2;
-    if (e < T(60)) rad += co[sh.prim + k] * exp(-e);
+    if (e < (sizeof(T) == 8 ? T(kExpCut64) : T(kExpCut))) rad += co[sh.prim + k] * exp(-e);
   }
   if (sh.L == 0) {
     out[0] = T(YS) * rad;

@@ -29,6 +29,7 @@ _pi = C.POINTER(C.c_int)
 SIGNATURES = {
     "qmt_init": [_i],
     "qmt_mol_create": [_i, _vp, _vp, _i, _vp, _i, _vp, _vp, _vp, _vp, C.POINTER(_vp)],
+    "qmt_mol_reset": [_vp, _i, _vp, _vp, _i, _vp, _i, _vp, _vp, _vp, _vp],
     "qmt_mol_set_coords": [_vp, _vp, _vp],
     "qmt_mol_set_dm": [_vp, _vp, _vp],
     "qmt_mol_destroy": [_vp],

@@ -71,7 +71,7 @@ def test_gto_ss_block_matches_reference_kernel(case, inputs):
     dm_ss = np.where(np.outer(s_only, s_only), mol.dm, 0).astype(np.float32)
     ref = oi.total_potential(pts, mol.coords, mol.types, mol.ALMOs, mol.basisset.alphas, mol.basisset.coeffs,
                              dm_ss)
-    assert rel_l2(g["hartree_gto_ss"][idx], ref) < 2e-6
+    assert rel_l2(g["hartree_gto_ss"][idx], ref) < 1e-5    # the reference kernel computes in FP32
 
 
 def test_sp_product_potential_matches_quadrature():

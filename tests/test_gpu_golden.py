@@ -53,7 +53,7 @@ def test_gto_ss_block_vs_reference(case, inputs, basis):
     m2.coords = mol.coords.copy()
     v = qmtools.Grid.emptyAs(grid)
     qmtools.QMTools.Compute_hartree(v, m2)
-    assert rel_l2(v.qube.ravel(), g["hartree_gto_ss"]) < 2e-6
+    assert rel_l2(v.qube.ravel(), g["hartree_gto_ss"]) < 1e-5   # the reference kernel is FP32
 
 
 def test_seed_jacobi_fft_vne_vs_reference(inputs):
