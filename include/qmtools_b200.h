@@ -154,6 +154,17 @@ qmt_status qmt_fft_poisson(qmt_mol* mol, int nx, int ny, int nz, float step,
 /* QMTools.Compute_qtot / gpu_total (qmtools/qmtools.py:2796-2803, kernel_utils.cu:68-98),
  * deterministic FP64 sum of n floats. */
 qmt_status qmt_grid_total(const float* q_dev, int64_t n, double* out, void* stream);
+/* Grid total that allocates nothing (no counterpart in the reference).  Same result as
+ * qmt_grid_total, for callers that must not allocate device memory: a host framework that
+ * owns all device memory through its own pool, or a serving loop that cannot accept the
+ * device-wide synchronisation cudaMalloc and cudaFree can cause.  The partial sums go to a
+ * fixed 32 KiB array compiled into the library, so n is limited to 33,554,432 points
+ * (QMT_BAD_ARG beyond that).  The first call on each device looks up that array's device
+ * address; make that first call before any stream capture begins.  All calls share the
+ * array; every slot a call reads it writes first, so nothing must be cleared, but calls
+ * whose work overlaps on the GPU (other streams, other host threads) race on it: order them.
+ * Synchronous like qmt_grid_total. */
+qmt_status qmt_grid_total_noalloc(const float* q_dev, int64_t n, double* out, void* stream);
 /* QMTools.Compute_qscale / gpu_rescale (qmtools/qmtools.py:2808-2813, kernel_utils.cu:54-65). */
 qmt_status qmt_grid_scale(float* q_dev, int64_t n, float factor, void* stream);
 /* QMTools.Compute_qdiff / gpu_qdiff(_rel) (qmtools/qmtools.py:2818-2831,

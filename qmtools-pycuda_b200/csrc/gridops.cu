@@ -455,3 +455,65 @@ qmt_status qmt_mol_trace_ps(qmt_mol* mol, double* trace_out, void* stream) {
 }
 
 }  // extern "C"
+
+// ---- grid total without allocation ----------------------------------------------------------
+// Same reduction as qmt_grid_total, but its partial sums live in a fixed array compiled into
+// the library instead of in memory obtained from cudaMalloc.  The array is part of the module
+// image: every GPU that loads the library holds its 32 KiB until the process exits.
+#include <mutex>
+
+namespace qmt {
+
+constexpr int64_t NOALLOC_MAX_BLOCKS = 4096;                          // first-pass partial sums
+constexpr int64_t NOALLOC_MAX_POINTS = NOALLOC_MAX_BLOCKS * RED_CHUNK;  // 33,554,432 grid points
+constexpr int NOALLOC_MAX_DEVICES = 64;
+
+// [0, NOALLOC_MAX_BLOCKS): one partial sum per first-pass block; [NOALLOC_MAX_BLOCKS]: the total.
+static __device__ __align__(256) double g_total_scratch[NOALLOC_MAX_BLOCKS + 32];
+
+static std::mutex g_total_scratch_mu;
+static double* g_total_scratch_dev[NOALLOC_MAX_DEVICES] = {};
+
+// Device address of g_total_scratch on the current device.  On the host the symbol only names
+// a host-side stand-in, so the address is looked up once per device with that device current.
+static qmt_status total_scratch(double** out) {
+  int dev = -1;
+  QMT_CUDA(cudaGetDevice(&dev));
+  if (dev < 0 || dev >= NOALLOC_MAX_DEVICES) return fail(QMT_BAD_ARG, "device ordinal out of range");
+  std::lock_guard<std::mutex> lock(g_total_scratch_mu);
+  if (!g_total_scratch_dev[dev]) {
+    void* p = nullptr;
+    const cudaError_t e = cudaGetSymbolAddress(&p, g_total_scratch);
+    if (e != cudaSuccess) return cuda_fail(e, "cudaGetSymbolAddress(g_total_scratch)");
+    g_total_scratch_dev[dev] = static_cast<double*>(p);
+  }
+  *out = g_total_scratch_dev[dev];
+  return QMT_OK;
+}
+
+}  // namespace qmt
+
+extern "C" qmt_status qmt_grid_total_noalloc(const float* q_dev, int64_t n, double* out, void* stream) {
+  using namespace qmt;
+  if (!q_dev || n <= 0 || !out) return fail(QMT_BAD_ARG, "bad reduction arguments");
+  if (n > NOALLOC_MAX_POINTS)
+    return fail(QMT_BAD_ARG, "qmt_grid_total_noalloc: " + std::to_string(n) +
+                                 " points exceed its fixed scratch limit of " +
+                                 std::to_string(NOALLOC_MAX_POINTS) + " points; use qmt_grid_total");
+  double* part = nullptr;
+  qmt_status st = total_scratch(&part);
+  if (st) return st;
+  double* res = part + NOALLOC_MAX_BLOCKS;
+  cudaStream_t s = as_stream(stream);
+  const int64_t nblk = (n + RED_CHUNK - 1) / RED_CHUNK;
+  // every slot read below is written earlier in this call, so nothing needs clearing
+  grid_reduce_kernel<0><<<(unsigned)nblk, RED_THREADS, 0, s>>>(q_dev, nullptr, n, part, nblk);
+  QMT_CHECK_LAUNCH("grid_reduce_kernel");
+  reduce_partials_kernel<<<1, 1024, 0, s>>>(part, nblk, res, 1, 0);
+  QMT_CHECK_LAUNCH("reduce_partials_kernel");
+  double h = 0.0;
+  QMT_CUDA(cudaMemcpyAsync(&h, res, sizeof(double), cudaMemcpyDeviceToHost, s));
+  QMT_CUDA(cudaStreamSynchronize(s));
+  *out = h;
+  return QMT_OK;
+}

@@ -43,6 +43,7 @@ SIGNATURES = {
     "qmt_jacobi_dirichlet": [_i, _i, _i, _f, _vp, _vp, _vp, _i, _i, _d, _pi, _pd, _vp],
     "qmt_fft_poisson": [_vp, _i, _i, _i, _f, _f, _f, _f, _f, _f, _i, _vp, _vp, _vp],
     "qmt_grid_total": [_vp, _i64, _pd, _vp],
+    "qmt_grid_total_noalloc": [_vp, _i64, _pd, _vp],
     "qmt_grid_scale": [_vp, _i64, _f, _vp],
     "qmt_grid_diff": [_vp, _vp, _i64, _i, _pd, _vp],
     "qmt_grid_errors": [_vp, _vp, _i64, _pd, _vp],
