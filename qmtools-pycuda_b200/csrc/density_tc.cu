@@ -615,17 +615,26 @@ static qmt_status run_tc(qmt_mol* m, const TcShape& sh, const PointMap& pm, int6
 // Per tile the phases are serial (A is resident and single-buffered); the U stream and
 // the MMA run asynchronously to the compute warps' work.
 // ---------------------------------------------------------------------------------------
+constexpr int MAX_FUSED_CHUNKS = 5;   // fused path: kpad <= 320
+
 struct FusedParams {
   MolView mol;
   PointMap pm;
   int64_t ntiles;
   int kpad, ksteps, nsplit, stages;
   int tri;                 // 1: upper-triangular U (half the work); 0: full symmetric P
+  int nchunks;             // kpad / 64 column chunks of A
+  int chunk_need[MAX_FUSED_CHUNKS];  // production items (atom halves) writing each chunk
   uint32_t a_bytes;        // one A piece: 128 rows x kpad x 2 B
   uint32_t b_slot;         // one U piece slot in a stage: kpad rows x 32 B
   uint32_t stage_bytes;
   uint32_t fmt;
-  const float* coeff_scaled;   // contraction coefficients times the shell's power-of-two scale
+  const int4* tab;         // packed shell records then primitive pairs (ensure_fused_operands)
+  int tab_words;           // 16-byte words of tab
+  int off_prim;            // byte offsets inside the staged tables: primitive pairs,
+  int off_ashell;          //   first shell of each atom,
+  int off_coords;          //   nuclear coordinates (float x, y, z)
+  int tab_bytes;           // shared-memory bytes of the staged tables
   float* qube;
   double* partials;
   double outscale;
@@ -698,7 +707,42 @@ __device__ __forceinline__ void unpack8(uint4 a, float* out) {
   }
 }
 
-constexpr int FUSED_NCW = 12;                 // compute warps (Phi production and epilogue)
+// Contracted radial parts sum_k c_k exp(-alpha_k r^2) (zero beyond the cut-off) of NP primitives
+// (alpha, c) at two points, in primitive order.  When the next shell of the atom has the same
+// exponents (pn != nullptr) its radial parts are formed from the same exponentials.
+template <int NP>
+__device__ __forceinline__ void radial_np(const float2* pa, const float2* pn, float q0, float q1, float& r0,
+                                          float& r1, float& n0, float& n1) {
+  float2 ac[NP];
+#pragma unroll
+  for (int k = 0; k < NP; ++k) ac[k] = pa[k];
+  float e0[NP], e1[NP];
+#pragma unroll
+  for (int k = 0; k < NP; ++k) {
+    const float x0 = ac[k].x * q0, x1 = ac[k].x * q1;
+    e0[k] = x0 < kExpCut ? expf(-x0) : 0.f;
+    e1[k] = x1 < kExpCut ? expf(-x1) : 0.f;
+  }
+  r0 = 0.f;
+  r1 = 0.f;
+#pragma unroll
+  for (int k = 0; k < NP; ++k) {
+    r0 = fmaf(ac[k].y, e0[k], r0);
+    r1 = fmaf(ac[k].y, e1[k], r1);
+  }
+  if (pn) {
+    n0 = 0.f;
+    n1 = 0.f;
+#pragma unroll
+    for (int k = 0; k < NP; ++k) {
+      const float d = pn[k].y;
+      n0 = fmaf(d, e0[k], n0);
+      n1 = fmaf(d, e1[k], n1);
+    }
+  }
+}
+
+constexpr int FUSED_NCW = 16;                 // compute warps (Phi production and epilogue)
 constexpr int FUSED_NCT = FUSED_NCW * 32;
 constexpr int FUSED_THREADS = 64 + FUSED_NCT;  // + TMA warp + MMA warp
 
@@ -708,7 +752,8 @@ __global__ void __launch_bounds__(FUSED_THREADS, 1)
                          const FusedParams p) {
   extern __shared__ uint8_t smem_dyn[];
   __shared__ __align__(8) uint64_t full_bar[MAX_STAGES], empty_bar[MAX_STAGES];
-  __shared__ __align__(8) uint64_t a_full, t_full, drain_bar;
+  __shared__ __align__(8) uint64_t chunk_bar[MAX_FUSED_CHUNKS], t_full, drain_bar;
+  __shared__ int item_ctr;
   __shared__ uint32_t tmem_slot;
   __shared__ double pos[128][3];
   __shared__ double rho_part[FUSED_NCW / 4][128];
@@ -729,7 +774,8 @@ __global__ void __launch_bounds__(FUSED_THREADS, 1)
       mbar_init(&full_bar[s], 1);
       mbar_init(&empty_bar[s], 1);
     }
-    mbar_init(&a_full, 1);
+    for (int c = 0; c < p.nchunks; ++c)
+      if (p.chunk_need[c] > 0) mbar_init(&chunk_bar[c], (uint32_t)p.chunk_need[c]);
     mbar_init(&t_full, 1);
     mbar_init(&drain_bar, 1);
     fence_mbar_init();
@@ -737,6 +783,13 @@ __global__ void __launch_bounds__(FUSED_THREADS, 1)
   // zero A once: padding columns and rows never written later stay zero
   for (uint32_t i = threadIdx.x; i < p.nsplit * p.a_bytes / 16; i += blockDim.x)
     reinterpret_cast<uint4*>(smem)[i] = make_uint4(0, 0, 0, 0);
+  // molecule tables in shared memory: the production loop reads them in dependent chains
+  uint8_t* tabs = stages + (size_t)p.stages * p.stage_bytes;
+  for (int i = threadIdx.x; i < p.tab_words; i += blockDim.x) reinterpret_cast<int4*>(tabs)[i] = __ldg(p.tab + i);
+  for (int i = threadIdx.x; i <= mol.natoms; i += blockDim.x)
+    reinterpret_cast<int*>(tabs + p.off_ashell)[i] = __ldg(mol.atom_shell + i);
+  for (int i = threadIdx.x; i < 3 * mol.natoms; i += blockDim.x)
+    reinterpret_cast<float*>(tabs + p.off_coords)[i] = __ldg(mol.coords + i);
   asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
   if (warp == 0 && lane == 0) {
     prefetch_tmap(&tmU_hi);
@@ -787,9 +840,15 @@ __global__ void __launch_bounds__(FUSED_THREADS, 1)
       bool ok = true;
       const uint32_t abase = smem_u32(A_hi), lbase = smem_u32(A_lo);
       for (int64_t t = blockIdx.x; t < p.ntiles && ok; t += gridDim.x, ++tile_it) {
-        if (!mbar_wait(&a_full, tile_it & 1u, &abort_flag)) break;
-        tc_fence_after();
         for (int ks = 0; ks < p.ksteps; ++ks, ++it) {
+          // columns 64c .. 64c+63 of A are complete once every item writing them arrived
+          if ((ks & 3) == 0 && p.chunk_need[ks >> 2] > 0) {
+            if (!mbar_wait(&chunk_bar[ks >> 2], tile_it & 1u, &abort_flag)) {
+              ok = false;
+              break;
+            }
+            tc_fence_after();
+          }
           const int s = it % p.stages;
           const uint32_t ph = (it / p.stages) & 1u;
           if (!mbar_wait(&full_bar[s], ph, &abort_flag)) {
@@ -821,6 +880,10 @@ __global__ void __launch_bounds__(FUSED_THREADS, 1)
     }
   } else {
     const int ct = threadIdx.x - 64;           // compute thread 0 .. FUSED_NCT-1
+    const int4* sh_s = reinterpret_cast<const int4*>(tabs);
+    const float2* pr_s = reinterpret_cast<const float2*>(tabs + p.off_prim);
+    const int* ash_s = reinterpret_cast<const int*>(tabs + p.off_ashell);
+    const float* crd_s = reinterpret_cast<const float*>(tabs + p.off_coords);
     const int cw = ct >> 5;                    // compute warp 0 .. FUSED_NCW-1
     const int q = warp & 3;                    // TMEM lane quadrant of this warp
     const int hh = cw >> 2;                    // epilogue column-chunk class 0 .. FUSED_NCW/4-1
@@ -836,43 +899,57 @@ __global__ void __launch_bounds__(FUSED_THREADS, 1)
         pos[ct][1] = y;
         pos[ct][2] = z;
       }
+      if (ct == 0) item_ctr = 0;
       named_barrier(1, FUSED_NCT);
-      // work item = (atom, half of the rows): warp-uniform atom data, two rows per thread
+      // work item = (atom, half of the rows), taken in atom order from a shared counter so that
+      // column chunks complete roughly in order and the warps stay balanced; two rows per thread
       // (lane and lane + 64 of its half) for independent exponential chains
-      for (int itm = cw; itm < 2 * mol.natoms; itm += FUSED_NCW) {
+      for (;;) {
+        int itm = 0;
+        if (lane == 0) itm = atomicAdd(&item_ctr, 1);
+        itm = __shfl_sync(0xffffffffu, itm, 0);
+        if (itm >= 2 * mol.natoms) break;
         const int a = itm >> 1;
+        const int s0 = ash_s[a], s1 = ash_s[a + 1];
+        if (s1 <= s0) continue;
         const int r0 = (itm & 1) * 32 + lane, r1 = r0 + 64;   // r1 sits 8192 B after r0 in A
-        const double ax = __ldg(mol.coords + 3 * a), ay = __ldg(mol.coords + 3 * a + 1),
-                     az = __ldg(mol.coords + 3 * a + 2);
+        const double ax = crd_s[3 * a], ay = crd_s[3 * a + 1], az = crd_s[3 * a + 2];
         const bool ok0 = pos[r0][0] < 1e29, ok1 = pos[r1][0] < 1e29;
         // FP64 displacement from the nucleus, rounded once (accuracy of steep exponents)
         const float x0 = (float)(pos[r0][0] - ax), y0 = (float)(pos[r0][1] - ay), z0 = (float)(pos[r0][2] - az);
         const float x1 = (float)(pos[r1][0] - ax), y1 = (float)(pos[r1][1] - ay), z1 = (float)(pos[r1][2] - az);
         const float q0 = x0 * x0 + y0 * y0 + z0 * z0, q1 = x1 * x1 + y1 * y1 + z1 * z1;
-        const int s0 = __ldg(mol.atom_shell + a), s1 = __ldg(mol.atom_shell + a + 1);
+        float nx0 = 0.f, nx1 = 0.f;   // radial parts of the next shell when it shares the exponents
+        int flast = 0;
         for (int sidx = s0; sidx < s1; ++sidx) {
-          const int4 sh = __ldg(reinterpret_cast<const int4*>(mol.shells + sidx));   // atom, L, nprim, prim
-          const int L = sh.y, np_ = sh.z, pr = sh.w;
-          const int f0 = __ldg(&mol.shells[sidx].func);
-          // up to 8 primitives fetched at once (independent loads), then 2 rows x 8 exponentials
-          float al[8], co[8];
-#pragma unroll
-          for (int k = 0; k < 8; ++k) {
-            al[k] = k < np_ ? __ldg(mol.alpha + pr + k) : 0.f;
-            co[k] = k < np_ ? __ldg(p.coeff_scaled + pr + k) : 0.f;
-          }
-          float rad0 = 0.f, rad1 = 0.f;
-#pragma unroll
-          for (int k = 0; k < 8; ++k) {
-            const float e0 = al[k] * q0, e1 = al[k] * q1;
-            if (k < np_ && e0 < kExpCut) rad0 = fmaf(co[k], expf(-e0), rad0);
-            if (k < np_ && e1 < kExpCut) rad1 = fmaf(co[k], expf(-e1), rad1);
-          }
-          for (int k = 8; k < np_; ++k) {
-            const float al2 = __ldg(mol.alpha + pr + k), co2 = __ldg(p.coeff_scaled + pr + k);
-            const float e0 = al2 * q0, e1 = al2 * q1;
-            if (e0 < kExpCut) rad0 = fmaf(co2, expf(-e0), rad0);
-            if (e1 < kExpCut) rad1 = fmaf(co2, expf(-e1), rad1);
+          const int4 rec = sh_s[sidx];   // prim, func, L | nprim << 8 | same_exp << 16 | next_same << 24, next prim
+          const int L = rec.z & 0xff, np_ = (rec.z >> 8) & 0xff, f0 = rec.y;
+          float rad0, rad1;
+          if (rec.z & 0x10000) {
+            rad0 = nx0;
+            rad1 = nx1;
+          } else {
+            const float2* pa = pr_s + rec.x;
+            const float2* pn = (rec.z >> 24) ? pr_s + rec.w : nullptr;
+            switch (np_) {
+              case 1: radial_np<1>(pa, pn, q0, q1, rad0, rad1, nx0, nx1); break;
+              case 2: radial_np<2>(pa, pn, q0, q1, rad0, rad1, nx0, nx1); break;
+              case 3: radial_np<3>(pa, pn, q0, q1, rad0, rad1, nx0, nx1); break;
+              case 4: radial_np<4>(pa, pn, q0, q1, rad0, rad1, nx0, nx1); break;
+              case 5: radial_np<5>(pa, pn, q0, q1, rad0, rad1, nx0, nx1); break;
+              case 6: radial_np<6>(pa, pn, q0, q1, rad0, rad1, nx0, nx1); break;
+              case 7: radial_np<7>(pa, pn, q0, q1, rad0, rad1, nx0, nx1); break;
+              case 8: radial_np<8>(pa, pn, q0, q1, rad0, rad1, nx0, nx1); break;
+              default:
+                rad0 = 0.f;
+                rad1 = 0.f;
+                for (int k = 0; k < np_; ++k) {
+                  const float2 ac = pa[k];
+                  const float a0 = ac.x * q0, a1 = ac.x * q1;
+                  rad0 = fmaf(ac.y, a0 < kExpCut ? expf(-a0) : 0.f, rad0);
+                  rad1 = fmaf(ac.y, a1 < kExpCut ? expf(-a1) : 0.f, rad1);
+                }
+            }
           }
           if (!ok0) rad0 = 0.f;
           if (!ok1) rad1 = 0.f;
@@ -894,6 +971,7 @@ __global__ void __launch_bounds__(FUSED_THREADS, 1)
             v1[3] = (float)YD2 * rad1 * (x1 * x1 - y1 * y1); v1[4] = c1 * x1 * y1;
           }
           const int nf = 2 * L + 1;
+          flast = f0 + nf - 1;
           bool skip = false;   // the function was stored with its predecessor
 #pragma unroll
           for (int k = 0; k < 5; ++k) {
@@ -915,39 +993,47 @@ __global__ void __launch_bounds__(FUSED_THREADS, 1)
             }
           }
         }
+        // publish: generic-proxy writes of A become visible to the tensor core, then one arrival
+        // per column chunk this atom wrote
+        asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+        __syncwarp();
+        if (lane == 0) {
+          const int cfirst = sh_s[s0].y >> 6, clast = flast >> 6;
+          for (int c = cfirst; c <= clast; ++c) mbar_arrive(&chunk_bar[c]);
+        }
       }
-      // generic-proxy writes of A must be visible to the tensor core
-      asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
-      tc_fence_before();
-      named_barrier(1, FUSED_NCT);
-      if (ct == 0) mbar_arrive(&a_full);
       // ---- epilogue -----------------------------------------------------------------------
       if (!mbar_wait(&t_full, tile_it & 1u, &abort_flag)) break;
       tc_fence_after();
-      double acc[4] = {0.0, 0.0, 0.0, 0.0};
-      for (int c = hh; c * 32 < p.kpad; c += FUSED_NCW / 4) {
-        const int col = c * 32;
-        float v[32], ph[32];
-        tmem_ld32(tmem + ((uint32_t)(q * 32) << 16) + (uint32_t)col, v);
+      double acc[2] = {0.0, 0.0};
+      for (int c = hh; c * 16 < p.kpad; c += FUSED_NCW / 4) {
+        const int col = c * 16;
+        float v[16], ph[16];
+        tmem_ld16(tmem + ((uint32_t)(q * 32) << 16) + (uint32_t)col, v);
         const int kc = col >> 6, u0 = (col & 63) >> 3;
         const uint8_t* rb = A_hi + kc * 16384 + (row >> 3) * 1024 + (row & 7) * 128;
 #pragma unroll
-        for (int u = 0; u < 4; ++u) unpack8<FMT>(*reinterpret_cast<const uint4*>(rb + (((u0 + u) ^ (row & 7)) * 16)), ph + 8 * u);
+        for (int u = 0; u < 2; ++u) unpack8<FMT>(*reinterpret_cast<const uint4*>(rb + (((u0 + u) ^ (row & 7)) * 16)), ph + 8 * u);
         if (two) {
           const uint8_t* rl = A_lo + kc * 16384 + (row >> 3) * 1024 + (row & 7) * 128;
 #pragma unroll
-          for (int u = 0; u < 4; ++u) {
+          for (int u = 0; u < 2; ++u) {
             float lo8[8];
             unpack8<FMT>(*reinterpret_cast<const uint4*>(rl + (((u0 + u) ^ (row & 7)) * 16)), lo8);
 #pragma unroll
             for (int e = 0; e < 8; ++e) ph[8 * u + e] += lo8[e];
           }
         }
+        // eight products per FP32 partial, partials summed in FP64 (the FP32 partials add
+        // ~3e-8 relative error; converting every product to FP64 ties up the conversion pipe)
+        float a32[2] = {0.f, 0.f};
 #pragma unroll
-        for (int k = 0; k < 32; ++k) acc[k & 3] = fma((double)ph[k], (double)v[k], acc[k & 3]);
+        for (int k = 0; k < 16; ++k) a32[k & 1] = fmaf(ph[k], v[k], a32[k & 1]);
+        acc[0] += (double)a32[0];
+        acc[1] += (double)a32[1];
       }
       tc_fence_before();
-      rho_part[hh][row] = (acc[0] + acc[1]) + (acc[2] + acc[3]);
+      rho_part[hh][row] = acc[0] + acc[1];
       named_barrier(1, FUSED_NCT);
       double mysum = 0.0;
       if (ct < p.pm.vpt) {
@@ -1033,19 +1119,49 @@ static qmt_status ensure_fused_operands(qmt_mol* m, int prec, const TcShape& sh,
     }
   // every function of a shell shares the shell's bound, hence its scale: fold it into the
   // contraction coefficients (exact, powers of two)
-  std::vector<float> cs(m->coeff.size());
+  // Shell records {prim, func, L | nprim << 8 | same_exp << 16 | next_same << 24, next shell's
+  // prim}, then one (alpha, coefficient x scale) pair per primitive.
+  const size_t nsh = m->shells.size(), npr = m->alpha.size();
+  std::vector<int4> tab(nsh + (npr + 1) / 2, make_int4(0, 0, 0, 0));
+  for (size_t i = 0; i < nsh; ++i) {
+    const Shell& a = m->shells[i];
+    if (a.nprim > 255 || a.L > 255) return fail(QMT_BAD_ARG, "shell too large for the fused density tables");
+    const bool nxt = i + 1 < nsh && m->shells[i + 1].same_exp;
+    tab[i] = make_int4(a.prim, a.func, a.L | (a.nprim << 8) | (a.same_exp << 16) | ((int)nxt << 24),
+                       nxt ? m->shells[i + 1].prim : 0);
+  }
+  float2* pt = reinterpret_cast<float2*>(tab.data() + nsh);
   for (const Shell& shl : m->shells)
-    for (int k = 0; k < shl.nprim; ++k) cs[shl.prim + k] = m->coeff[shl.prim + k] * fs[shl.func];
+    for (int k = 0; k < shl.nprim; ++k)
+      pt[shl.prim + k] = make_float2(m->alpha[shl.prim + k], m->coeff[shl.prim + k] * fs[shl.func]);
   qmt_status st;
   if ((st = m->d_fused_B.reserve(2 * piece))) return st;
-  if ((st = m->d_coeff_scaled.reserve(std::max<size_t>(1, cs.size()) * sizeof(float)))) return st;
+  if ((st = m->d_fused_tab.reserve(tab.size() * sizeof(int4)))) return st;
   QMT_CUDA(cudaMemcpyAsync(m->d_fused_B.ptr, host.data(), 2 * piece, cudaMemcpyHostToDevice, s));
-  if (!cs.empty())
-    QMT_CUDA(cudaMemcpyAsync(m->d_coeff_scaled.ptr, cs.data(), cs.size() * sizeof(float), cudaMemcpyHostToDevice, s));
+  QMT_CUDA(cudaMemcpyAsync(m->d_fused_tab.ptr, tab.data(), tab.size() * sizeof(int4), cudaMemcpyHostToDevice, s));
   QMT_CUDA(cudaStreamSynchronize(s));
   m->fused_g = g;
   m->fused_prec = key;
   return QMT_OK;
+}
+
+// Shared-memory bytes of the molecule tables staged by the fused kernel.
+static int fused_tab_bytes(const qmt_mol* m) {
+  const int words = (int)(m->shells.size() + (m->alpha.size() + 1) / 2);
+  return words * 16 + (m->natoms + 1 + 3) / 4 * 16 + (3 * m->natoms + 3) / 4 * 16;
+}
+
+// U pipeline stages that fit beside A and the tables (below 2: the fused path does not fit).
+template <int FMT>
+static int fused_stages(const TcShape& sh, int tab_bytes) {
+  int maxsm = 0, dev = 0;
+  cudaGetDevice(&dev);
+  cudaDeviceGetAttribute(&maxsm, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev);
+  cudaFuncAttributes fa;
+  if (cudaFuncGetAttributes(&fa, density_fused_kernel<FMT>) != cudaSuccess) return 0;
+  const long a_bytes = 128L * sh.kpad * 2, stage_bytes = (long)sh.nsplit * sh.kpad * 32;
+  const long avail = (long)maxsm - (long)fa.sharedSizeBytes - 1024 - sh.nsplit * a_bytes - tab_bytes;
+  return (int)std::max<long>(0, std::min<long>(MAX_STAGES, avail / stage_bytes));
 }
 
 template <int FMT>
@@ -1065,28 +1181,36 @@ static qmt_status run_fused(qmt_mol* m, const TcShape& sh, const PointMap& pm, i
   p.kpad = K;
   p.ksteps = K / 16;
   p.tri = g_fused_tri;
+  p.nchunks = K / 64;
+  if (p.nchunks > MAX_FUSED_CHUNKS) return fail(QMT_BAD_ARG, "fused density path supports kpad <= 320");
+  for (int a = 0; a < m->natoms; ++a) {
+    const int sa = m->atom_shell[a], sb = m->atom_shell[a + 1];
+    if (sb <= sa) continue;
+    const Shell& last = m->shells[sb - 1];
+    const int cfirst = m->shells[sa].func >> 6, clast = (last.func + 2 * last.L) >> 6;
+    for (int c = cfirst; c <= clast; ++c) p.chunk_need[c] += 2;   // two row halves per atom
+  }
   p.nsplit = sh.nsplit;
   p.a_bytes = 128u * K * 2u;
   p.b_slot = (uint32_t)K * 32u;
   p.stage_bytes = p.nsplit * p.b_slot;
   p.fmt = (uint32_t)sh.fmt;
-  p.coeff_scaled = m->d_coeff_scaled.as<float>();
+  p.tab = m->d_fused_tab.as<int4>();
+  p.tab_words = (int)(m->shells.size() + (m->alpha.size() + 1) / 2);
+  p.off_prim = (int)m->shells.size() * 16;
+  p.off_ashell = p.tab_words * 16;
+  p.off_coords = p.off_ashell + (m->natoms + 1 + 3) / 4 * 16;
+  p.tab_bytes = p.off_coords + (3 * m->natoms + 3) / 4 * 16;
   p.qube = qube;
   p.partials = m->d_partials.as<double>();
   p.outscale = outscale;
   p.inv_g2 = (g_fused_tri ? 2.0 : 1.0) * std::ldexp(1.0, -m->fused_g);
   p.err = reinterpret_cast<int*>(m->d_scalars.as<double>() + 8);
-  int maxsm = 0, dev = 0;
-  cudaGetDevice(&dev);
-  cudaDeviceGetAttribute(&maxsm, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev);
   auto kern = density_fused_kernel<FMT>;
-  cudaFuncAttributes fa;
-  QMT_CUDA(cudaFuncGetAttributes(&fa, kern));
-  const long avail = (long)maxsm - (long)fa.sharedSizeBytes - 1024 - (long)p.nsplit * p.a_bytes;
-  int stages = (int)std::min<long>(MAX_STAGES, avail / (long)p.stage_bytes);
+  const int stages = fused_stages<FMT>(sh, p.tab_bytes);
   if (stages < 2) return fail(QMT_BAD_ARG, "fused density tile does not fit in shared memory");
   p.stages = stages;
-  const size_t dyn = (size_t)p.nsplit * p.a_bytes + (size_t)stages * p.stage_bytes + 1024;
+  const size_t dyn = (size_t)p.nsplit * p.a_bytes + (size_t)stages * p.stage_bytes + p.tab_bytes + 1024;
   QMT_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)dyn));
   const int grid = (int)std::min<int64_t>(ntiles, sm_count());
   kern<<<grid, FUSED_THREADS, dyn, s>>>(tU_hi, tU_lo, p);
@@ -1106,9 +1230,14 @@ qmt_status density_tc(qmt_mol* mol, int nx, int ny, int nz, float step, float ox
   if ((st = make_point_map(nx, ny, nz, step, ox, oy, oz, subgrid, 128, pm, ntiles))) return st;
   if ((st = mol->d_partials.reserve(ntiles * sizeof(double)))) return st;
   const double outscale = 2.0 * (double)step * step * step / pm.s3;
-  const bool fusable = sh.fmt != FMT_TF32 && sh.kpad <= 320;
+  bool fusable = sh.fmt != FMT_TF32 && sh.kpad <= 320;
+  if (fusable) {
+    const int tb = fused_tab_bytes(mol);
+    fusable = (sh.fmt == FMT_F16 ? fused_stages<FMT_F16>(sh, tb) : fused_stages<FMT_BF16>(sh, tb)) >= 2;
+  }
   const bool fused = g_density_path == 2 ? fusable : (g_density_path == 1 ? false : fusable);
-  if (g_density_path == 2 && !fusable) return fail(QMT_BAD_ARG, "fused density path needs fp16/bf16 and N <= 320");
+  if (g_density_path == 2 && !fusable)
+    return fail(QMT_BAD_ARG, "fused density path needs fp16/bf16, N <= 320 and molecule tables that fit in shared memory");
   if (fused) {
     if ((st = ensure_fused_operands(mol, precision, sh, s))) return st;
     if (sh.fmt == FMT_F16) st = run_fused<FMT_F16>(mol, sh, pm, ntiles, qube, outscale, s);

@@ -79,7 +79,7 @@ using namespace qmt;
 qmt_mol::~qmt_mol() {
   for (DevBuf* b : {&d_coords, &d_types, &d_shells, &d_alpha, &d_coeff, &d_alpha64, &d_coeff64,
                     &d_P32, &d_P64, &d_Phi_hi, &d_Phi_lo, &d_tc_P, &d_fscale, &d_partials,
-                    &d_scalars, &d_pairs, &d_work, &d_atom_shell, &d_fused_B, &d_coeff_scaled})
+                    &d_scalars, &d_pairs, &d_work, &d_atom_shell, &d_fused_B, &d_fused_tab})
     b->release();
 }
 
@@ -172,6 +172,12 @@ static qmt_status mol_init(qmt_mol* m, int natoms, const int32_t* types, const f
       ++np;
     }
     sh.nprim = np;
+    if (!m->shells.empty()) {
+      const Shell& pv = m->shells.back();
+      bool same = pv.atom == a && pv.nprim == np && np <= 8;
+      for (int k = 0; same && k < np; ++k) same = m->alpha[pv.prim + k] == m->alpha[sh.prim + k];
+      sh.same_exp = same ? 1 : 0;
+    }
     const double bnd = shell_bound(L, m->alpha.data() + sh.prim, m->coeff.data() + sh.prim, np);
     for (int k = 0; k < 2 * L + 1; ++k) m->fbound[f + k] = bnd;
     m->shells.push_back(sh);

@@ -52,7 +52,8 @@ struct Shell {
   int nprim;
   int prim;    // offset into the primitive arrays
   int func;    // first basis function
-  int pad[3];
+  int same_exp;  // 1: same atom and the same exponents (at most 8) as the shell before it
+  int pad[2];
 };
 
 // ---- device-side molecule view --------------------------------------------------------
