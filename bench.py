@@ -18,9 +18,23 @@ synchronise on both sides; the reported time is the max over ranks.
 (coordinates and density matrix uploaded into the molecule handle, which re-derives its
 device operands) and reads the potential grid back to the host every step.
 
-`--impl reference` times the reference implementation of this path instead (see
-DESIGN.md: the reference is GPU-only CUDA C; its kernels are compiled from source into
-oracle/_ref when available, otherwise the CPU oracle port of its algorithm is timed).
+Beside the headline step, rank 0 also reports (not part of `value`):
+  * `plain_fp32`: the same step with the plain FP32 SIMT density path (the reference's
+    precision), and the speed-up of the mixed-precision path over it;
+  * `accuracy`: density rel-L2 / max-abs of the mixed path against this library's FP64
+    density, and the FP64 electron-count error;
+  * `batched`: 64 molecules of 5-60 atoms (grids = bounding box + 3 bohr per side at
+    0.15 bohr) through the continuous-batching engine, against serial plain FP32;
+  * `serving`: a Poisson request stream (atoms log-uniform 3-120) through the engine with
+    p50/p99 latency, against serial plain FP32;
+  * `cpu_baseline`: the FP64 NumPy/SciPy evaluation on a bounded sample, which also checks
+    the mixed result against it (density on the sampled planes, Hartree on the full grid).
+
+`--impl reference` times the reference's own implementation of this path.  The reference is
+GPU-only CUDA C driven from Python; its kernels, compiled from its sources into oracle/_ref,
+run here with the reference facade's launch shapes and host steps (density kernel, grid
+total and rescale, periodic cuFFT Poisson route).  Without those builds the FP64 CPU port
+of its algorithm is timed instead.
 """
 import argparse
 import json
@@ -50,8 +64,66 @@ def peaks():
     return 1590.0, 6650.0, "fallback"
 
 
+class NvmlClockSampler:
+    """SM clock and clock-event reasons polled through NVML every 10 ms in a thread."""
+
+    def __init__(self, local):
+        import pynvml
+        import torch
+        self.nv = pynvml
+        pynvml.nvmlInit()
+        uuid = "GPU-" + str(torch.cuda.get_device_properties(local).uuid)
+        self.h = pynvml.nvmlDeviceGetHandleByUUID(uuid.encode() if isinstance(uuid, str) else uuid)
+        self.max = float(pynvml.nvmlDeviceGetMaxClockInfo(self.h, pynvml.NVML_CLOCK_SM))
+        self.samples = []
+        self._stop = threading.Event()
+
+    def _run(self):
+        nv = self.nv
+        get_reasons = getattr(nv, "nvmlDeviceGetCurrentClocksEventReasons",
+                              getattr(nv, "nvmlDeviceGetCurrentClocksThrottleReasons", None))
+        while not self._stop.is_set():
+            try:
+                self.samples.append((float(nv.nvmlDeviceGetClockInfo(self.h, nv.NVML_CLOCK_SM)),
+                                     int(get_reasons(self.h)) if get_reasons else 0))
+            except Exception:
+                pass
+            self._stop.wait(0.01)
+
+    def __enter__(self):
+        self.th = threading.Thread(target=self._run, daemon=True)
+        self.th.start()
+        return self
+
+    def __exit__(self, *a):
+        self._stop.set()
+        self.th.join(timeout=2)
+
+    def summary(self):
+        nv = self.nv
+        bits = {"hw_slowdown": "HwSlowdown", "hw_thermal_slowdown": "HwThermalSlowdown",
+                "sw_thermal_slowdown": "SwThermalSlowdown", "sw_power_cap": "SwPowerCap"}
+        reasons = set()
+        for _, r in self.samples:
+            for name, suffix in bits.items():
+                b = getattr(nv, "nvmlClocksEventReason" + suffix, getattr(nv, "nvmlClocksThrottleReason" + suffix, 0))
+                if r & b:
+                    reasons.add(name)
+        if not self.samples:
+            return {"sm_mhz": None, "sm_max_mhz": self.max, "reasons": ["unsampled"], "samples": 0}
+        return {"sm_mhz": float(np.median([c for c, _ in self.samples])), "sm_max_mhz": self.max,
+                "reasons": sorted(reasons), "samples": len(self.samples), "source": "nvml 10 ms"}
+
+
+def clock_sampler(local):
+    try:
+        return NvmlClockSampler(local)
+    except Exception:
+        return ClockSampler(local)
+
+
 class ClockSampler:
-    """nvidia-smi clocks and throttle reasons sampled during the timed region."""
+    """nvidia-smi clocks and throttle reasons sampled during the timed region (NVML fallback)."""
 
     FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
               "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
@@ -145,12 +217,15 @@ def max_over_ranks(pg, v):
     return float(t.item())
 
 
-def cpu_baseline_c1(sm, basis, qmtools):
+def cpu_baseline_c1(sm, basis, qmtools, check=None):
     """FP64 NumPy/SciPy evaluation of the same step on a bounded sample, per grid point.
 
     Density: 4 z-planes (4*128^2 points) of the 128^3 grid through the oracle (chunked Phi,
     BLAS Phi@P, row-dot), extrapolated per point.  Hartree: one scipy.fft rfftn/irfftn
-    Hockney convolution on the full 256^3 padded grid with all host cores.
+    Hockney convolution on the full 256^3 padded grid with all host cores.  With `check`
+    (host copies of the mixed-precision results) the FP64 results also score them: density
+    on the sampled planes, and the FP64 Hockney potential of the same density on the full
+    grid.
     """
     import scipy.fft
     from oracle import density as od
@@ -161,8 +236,9 @@ def cpu_baseline_c1(sm, basis, qmtools):
     cores = os.cpu_count() or 1
     t0 = time.perf_counter()
     nzs = 4
+    z0 = nz // 2
     q = od.density_qube_unscaled((nx, ny, nz), np.float32(h), (ox, oy, oz), mol.coords, mol.ALMOs, basis.alphas,
-                                 basis.coeffs, mol.dm, zslab=(nz // 2, nz // 2 + nzs))
+                                 basis.coeffs, mol.dm, zslab=(z0, z0 + nzs))
     t_dens = (time.perf_counter() - t0) / q.size
     M = 2 * nx
     rho = np.zeros((M, M, M))
@@ -174,10 +250,77 @@ def cpu_baseline_c1(sm, basis, qmtools):
     t_fft = time.perf_counter() - t1
     npts = nx * ny * nz
     per_pt = t_dens + t_fft / npts
-    return {"value": 1.0 / per_pt, "unit": UNIT, "cores": cores, "kind": "port",
-            "sample": f"density on {nzs} z-planes ({nzs * nx * ny} pts, FP64 NumPy, extrapolated per point) + "
-                      f"one full {M}^3 scipy.fft Hockney convolution (workers={cores})",
-            "density_s_per_pt": t_dens, "fft_s": t_fft}
+    out = {"value": 1.0 / per_pt, "unit": UNIT, "cores": cores, "kind": "port",
+           "sample": f"density on {nzs} z-planes ({nzs * nx * ny} pts, FP64 NumPy, extrapolated per point) + "
+                     f"one full {M}^3 scipy.fft Hockney convolution (workers={cores})",
+           "density_s_per_pt": t_dens, "fft_s": t_fft}
+    if check is not None:
+        ref = np.asarray(q, dtype=np.float64).ravel()
+        got = check["q_raw"].reshape(nz, ny, nx)[z0:z0 + nzs].ravel().astype(np.float64)
+        vref = op.hockney_poisson(check["q"], (nx, ny, nz), h, (ox, oy, oz), mol.coords, mol.types, 0.2, 6)
+        vref = np.asarray(vref, dtype=np.float64).ravel()
+        vgot = check["v"].astype(np.float64).ravel()
+        out["check_vs_fp64"] = {
+            "density_rel_l2": float(np.linalg.norm(got - ref) / np.linalg.norm(ref)),
+            "density_max_abs": float(np.abs(got - ref).max()),
+            "density_points": int(ref.size),
+            "hartree_rel_l2": float(np.linalg.norm(vgot - vref) / np.linalg.norm(vref)),
+            "hartree_max_abs_volt": float(np.abs(vgot - vref).max())}
+    return out
+
+
+def _requests(mols, basis, qmtools, serving, arrivals=None):
+    out = []
+    for i, m in enumerate(mols):
+        out.append(serving.Request(m.molecule(basis, qmtools.Molecule), m.grid(qmtools.Grid),
+                                   arrival=0.0 if arrivals is None else arrivals[i], rid=i))
+    return out
+
+
+def _engine_run(serving, reqs, slots, precision, realtime):
+    import torch
+    eng = serving.Engine(slots=slots, precision=precision)
+    eng.run(reqs[:2], realtime=False)           # first-call set-up outside the timed run
+    for r in reqs[:2]:
+        r.t_admit = r.t_done = None
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    eng.run(reqs, realtime=realtime)
+    torch.cuda.synchronize()
+    wall = time.perf_counter() - t0
+    eng.close()
+    return wall
+
+
+def batched_and_serving(basis, qmtools, precision):
+    """C3-like batch and C4-like request stream through the continuous-batching engine."""
+    from qmtools import serving
+    from qmtools import synthetic as syn
+    res = {}
+    bm = syn.batch_molecules(64)
+    pts = sum(int(np.prod(m.grid_shape)) for m in bm)
+    t_mix = _engine_run(serving, _requests(bm, basis, qmtools, serving), 8, precision, False)
+    t_fp32 = _engine_run(serving, _requests(bm, basis, qmtools, serving), 1, "fp32", False)
+    res["batched"] = {"molecules": len(bm), "atoms": "uniform 5-60", "grid_pts": pts,
+                      "value": pts / t_mix, "unit": UNIT, "wall_s": t_mix, "slots": 8,
+                      "serial_plain_fp32": {"value": pts / t_fp32, "wall_s": t_fp32},
+                      "speedup_vs_serial_plain_fp32": t_fp32 / t_mix,
+                      "timing": "host wall clock around the whole batch (set-up, H2D, density, Hockney FFT, D2H)"}
+    rate, count = 200.0, 32
+    stream = syn.serving_stream(rate, count)
+    arr = [t for t, _ in stream]
+    mols = [m for _, m in stream]
+    pts = sum(int(np.prod(m.grid_shape)) for m in mols)
+    reqs = _requests(mols, basis, qmtools, serving, arr)
+    t_mix = _engine_run(serving, reqs, 8, precision, True)
+    lat = serving.latency_stats(reqs)
+    t_fp32 = _engine_run(serving, _requests(mols, basis, qmtools, serving), 1, "fp32", False)
+    res["serving"] = {"requests": count, "rate_req_s": rate, "atoms": "log-uniform 3-120", "grid_pts": pts,
+                      "p50_ms": lat["p50_ms"], "p99_ms": lat["p99_ms"], "mean_ms": lat["mean_ms"],
+                      "value": pts / t_mix, "unit": UNIT, "makespan_s": t_mix, "slots": 8,
+                      "serial_plain_fp32": {"value": pts / t_fp32, "wall_s": t_fp32},
+                      "speedup_vs_serial_plain_fp32": t_fp32 / t_mix}
+    return res
 
 
 def run_ours(args, world, rank, local, pg):
@@ -192,6 +335,11 @@ def run_ours(args, world, rank, local, pg):
     sm = syn.config_molecule("c1")
     mol = sm.molecule(basis, qmtools.Molecule)
     g = sm.grid(qmtools.Grid)
+    if args.grid:
+        # the same molecule on a smaller cube of the same spacing, centred on it (profiling cases)
+        c = np.asarray(sm.coords_bohr).mean(axis=0)
+        hb = sm.step_bohr
+        g = qmtools.Grid((1, args.grid, args.grid, args.grid), hb / qmtools.ANG2BOR, list(c - args.grid * hb / 2))
     nx, ny, nz, h, ox, oy, oz = g._geom()
     npts = nx * ny * nz
     qgrid = qmtools.Grid.emptyAs(g)
@@ -236,7 +384,7 @@ def run_ours(args, world, rank, local, pg):
         step()
     torch.cuda.synchronize()
     barrier(pg)
-    with ClockSampler(local) as clk:
+    with clock_sampler(local) as clk:
         ms, dens_ms = timed(step, args.steps, with_density_events=True)
     torch.cuda.synchronize()
     barrier(pg)
@@ -266,7 +414,8 @@ def run_ours(args, world, rank, local, pg):
         "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms, "higher_is_better": True,
         "scaling": "weak", "vs_baseline": None, "dtype": args.precision,
         "data": "synthetic (seeded geometry and density matrix; no public dataset exists for this path)",
-        "config": {"workload": WORKLOAD, "grid_pts_per_step": npts, "basis_functions": int(mol.norbs),
+        "config": {"workload": WORKLOAD if not args.grid else WORKLOAD.replace("128^3", f"{args.grid}^3"),
+                   "grid_pts_per_step": npts, "basis_functions": int(mol.norbs),
                    "density_precision": args.precision, "poisson": "Hockney free-space FFT, 256^3 padded, FP32",
                    "l2": "512 MiB flush written before every timed step", "parallelism": f"replicas x{world}"},
         "e2e": {"value": world * npts / (e2e_ms / 1000.0), "unit": UNIT,
@@ -283,31 +432,170 @@ def run_ours(args, world, rank, local, pg):
     out["roofline"] = {"bound": "tensor", "kernel": "qmt_density (basis + tcgen05 contraction + row-dot)",
                        "achieved": achieved, "peak": peak_tf, "unit": "TFLOP/s", "frac": achieved / peak_tf,
                        "peak_source": f"bf16_tflops burst, {kind}", "density_ms": dens_ms,
-                       "traffic": None}
+                       "traffic": profiled_traffic() if (args.precision == "fp16x3" and not args.grid) else None,
+                       "traffic_unit": "DRAM bytes per launch (ncu, dram__bytes_read.sum + dram__bytes_write.sum)"}
+    check = None
+    if world == 1 and not args.quick:
+        # plain FP32 SIMT density (the reference's precision) on the same step
+        p32 = N.PREC["fp32"]
+
+        def step32():
+            N.call("qmt_density", handle, nx, ny, nz, h, ox, oy, oz, 1, p32, 1, C.c_void_p(q.data_ptr()),
+                   C.byref(qsum), sh)
+            N.call("qmt_fft_poisson", handle, nx, ny, nz, h, ox, oy, oz, 0.2, 6.0, 1, C.c_void_p(q.data_ptr()),
+                   C.c_void_p(vout.data_ptr()), sh)
+
+        step32()
+        ms32, _ = timed(step32, 5)
+        out["plain_fp32"] = {"value": npts / (ms32 / 1000.0), "unit": UNIT, "ms_per_step": ms32,
+                             "speedup_of_mixed": ms32 / ms}
+        # accuracy of the mixed path against this library's FP64 density (raw electrons/voxel)
+        q64 = torch.empty_like(q)
+        s64, smx = C.c_double(), C.c_double()
+        N.call("qmt_density", handle, nx, ny, nz, h, ox, oy, oz, 1, N.PREC["fp64"], 0, C.c_void_p(q64.data_ptr()),
+               C.byref(s64), sh)
+        N.call("qmt_density", handle, nx, ny, nz, h, ox, oy, oz, 1, prec, 0, C.c_void_p(q.data_ptr()),
+               C.byref(smx), sh)
+        tr = C.c_double()
+        N.call("qmt_mol_trace_ps", handle, C.byref(tr), sh)
+        d = (q.double() - q64.double())
+        out["accuracy"] = {"density_rel_l2_vs_fp64": float(d.norm() / q64.double().norm()),
+                           "density_max_abs_vs_fp64": float(d.abs().max()),
+                           "grid_electrons_fp64": s64.value, "grid_electrons_mixed": smx.value,
+                           "electron_count_trace_ps_fp64": 2.0 * tr.value,
+                           "reference": "this library's FP64 density path (checked against the FP64 oracle by the tests)"}
+        q_raw = q.cpu().numpy()
+        step()
+        torch.cuda.synchronize()
+        check = {"q_raw": q_raw, "q": q.cpu().numpy(), "v": vout.cpu().numpy()}
+        out.update(batched_and_serving(basis, qmtools, args.precision))
     if rank == 0 and not args.no_cpu_baseline:
-        out["cpu_baseline"] = cpu_baseline_c1(sm, basis, qmtools)
+        out["cpu_baseline"] = cpu_baseline_c1(sm, basis, qmtools, check)
     return out
 
 
+def profiled_traffic():
+    """DRAM bytes (read + write) per launch of the fused density kernel at the bench size, from
+    the one-pass ncu capture summarised in profiles/density_fused_kernel_c1.md."""
+    import re
+    f = ROOT / "profiles" / "density_fused_kernel_c1.md"
+    if not f.exists():
+        return None
+    txt = f.read_text().split("## DRAM traffic at the bench size", 1)[-1]
+    rd = re.search(r"dram__bytes_read\.sum \| ([\d,]+) B", txt)
+    wr = re.search(r"dram__bytes_write\.sum \| ([\d,]+) B", txt)
+    if not (rd and wr):
+        return None
+    return int(rd.group(1).replace(",", "")) + int(wr.group(1).replace(",", ""))
+
+
 def kernel_launches_per_step(prec):
-    """Launches of this library's kernels per step (density + Hockney FFT)."""
-    # density: tensor-core path = staging + contraction per chunk, partial reduction, rescale
-    dens = 4 + 2 if prec not in ("fp32", "fp64") else 3
-    fft = 1 + 3 + 1 + 3 + 1    # RHS, 3 forward axis passes, G multiply, 3 inverse passes, C-order write
+    """Launches of this library's kernels per timed step (density + Hockney FFT)."""
+    dens = 3        # density kernel (fused tensor-core or SIMT), partial-sum reduction, rescale
+    fft = 5         # x forward with the RHS, y forward, z forward x G x z inverse, y inverse, x inverse
     return dens + fft
 
 
+def _ref_libs():
+    ref = ROOT / "oracle" / "_ref"
+    paths = [ref / "utils.so", ref / "c1_bench" / "density_s1.so", ref / "c1_bench" / "fft.so"]
+    return paths if all(p.exists() for p in paths) else None
+
+
+def run_reference_gpu(args, world, rank, local, paths):
+    """The reference path on the same B200: its density kernel (kernel_density.cu), grid total
+    and rescale (kernel_utils.cu) and the periodic FFT route (kernel_fft.cu around cuFFT), with
+    the launch shapes and host steps of its facade (Compute_density, Compute_hartree_fft)."""
+    import ctypes as C
+    import torch
+    import qmtools
+    from qmtools import synthetic as syn
+    qmtools.set_verbose(False)
+    torch.cuda.set_device(local)
+    ut, dl, fl_ = (C.CDLL(str(p)) for p in paths)
+    basis = qmtools.BasisSet(qmtools.BASIS_CCPVDZ)
+    sm = syn.config_molecule("c1")
+    mol = sm.molecule(basis, qmtools.Molecule)
+    g = sm.grid(qmtools.Grid)
+    nx, ny, nz = g.space_shape()
+    gx, gy, gz = g.GPUblocks
+    n = nx * ny * nz
+    h = float(g.step)
+    ox, oy, oz = (float(g.origin[k]) for k in "xyz")
+    dev = "cuda"
+    pin = lambda a, dt: torch.from_numpy(np.ascontiguousarray(a, dtype=dt).ravel()).pin_memory()
+    coords_h, dm_h = pin(mol.coords, np.float32), pin(mol.dm, np.float32)
+    coords, dm = coords_h.to(dev), dm_h.to(dev)
+    types = torch.from_numpy(np.ascontiguousarray(mol.types, dtype=np.int32)).to(dev)
+    almos = torch.from_numpy(np.ascontiguousarray(mol.ALMOs, dtype=np.int16)).to(dev)
+    alphas = torch.from_numpy(np.ascontiguousarray(basis.alphas, dtype=np.float32)).to(dev)
+    coeffs = torch.from_numpy(np.ascontiguousarray(basis.coeffs, dtype=np.float32)).to(dev)
+    q = torch.zeros(n, device=dev)
+    tot = torch.zeros(1, device=dev)
+    wr, c1, c2, v = (torch.zeros(k * n, device=dev) for k in (1, 2, 2, 1))
+    v_h = torch.empty(n, dtype=torch.float32).pin_memory()
+    vp = lambda t: C.c_void_p(t.data_ptr())
+    f = C.c_float
+
+    def step(e2e=False):
+        if e2e:
+            coords.copy_(coords_h, non_blocking=True)
+            dm.copy_(dm_h, non_blocking=True)
+        assert dl.ref_density(gx, gy, gz, f(h), f(ox), f(oy), f(oz), vp(coords), vp(alphas), vp(coeffs), vp(almos),
+                              vp(dm), vp(q)) == 0
+        assert ut.ref_total(gx, gy, gz, vp(q), vp(tot)) == 0
+        factor = np.float32(mol.qtot / float(tot.item()))
+        assert ut.ref_rescale(gx, gy, gz, vp(q), f(factor)) == 0
+        assert fl_.ref_fft_route(gx, gy, gz, nx, ny, nz, vp(q), vp(types), vp(coords), vp(wr), vp(c1), vp(c2),
+                                 vp(v)) == 0
+        if e2e:
+            v_h.copy_(v)
+        torch.cuda.synchronize()
+
+    def timed(k, e2e):
+        ts = []
+        for _ in range(k):
+            t0 = time.perf_counter()
+            step(e2e)
+            ts.append(time.perf_counter() - t0)
+        return float(np.mean(ts))
+
+    for _ in range(args.warmup):
+        step()
+    ms = 1000.0 * timed(args.steps, False)
+    e2e_ms = 1000.0 * timed(max(1, args.steps // 2), True)
+    v_ = n / (ms / 1000.0)
+    return {"metric": METRIC, "value": v_, "unit": UNIT, "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
+            "ms_per_step": ms, "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "fp32",
+            "data": "synthetic", "impl": "reference",
+            "config": {"workload": WORKLOAD.replace("density + Hockney FFT Poisson on 256^3",
+                                                   "density + periodic FFT Poisson on 128^3 (the reference's solve)"),
+                       "grid_pts_per_step": n, "timing": "host wall clock around each synchronised step"},
+            "cpu_baseline": {"value": v_, "unit": UNIT, "cores": 0, "kind": "reference",
+                             "sample": "the full step on the GPU: the reference's kernels compiled from its sources "
+                                       "for sm_100a (oracle/_ref/c1_bench), no host cores used"},
+            "e2e": {"value": n / (e2e_ms / 1000.0), "unit": UNIT,
+                    "h2d_bytes_per_step": int(4 * (coords_h.numel() + dm_h.numel())), "d2h_bytes_per_step": 4 * n}}
+
+
 def run_reference(args, world, rank, local, pg):
-    """The reference's implementation of this path, timed on the same workload."""
+    """The reference's implementation of this path, timed on the same workload (rank 0 only)."""
     if rank != 0:
         return None
+    paths = _ref_libs()
+    try:
+        import torch
+        has_gpu = torch.cuda.is_available()
+    except Exception:
+        has_gpu = False
+    if paths is not None and has_gpu:
+        return run_reference_gpu(args, world, rank, local, paths)
     import qmtools
     from qmtools import synthetic as syn
     qmtools.set_verbose(False)
     basis = qmtools.BasisSet(qmtools.BASIS_CCPVDZ)
     sm = syn.config_molecule("c1")
-    ref_lib = ROOT / "oracle" / "_ref"
-    # CPU oracle port of the reference algorithm (density per voxel centre + periodic FFT solve)
+    # CPU oracle port of the reference algorithm (FP64 density + FFT solve)
     samples = []
     for _ in range(args.warmup):
         cpu_baseline_c1(sm, basis, qmtools)
@@ -321,18 +609,19 @@ def run_reference(args, world, rank, local, pg):
             "scaling": "weak", "vs_baseline": None, "dtype": "fp64", "data": "synthetic", "impl": "reference",
             "config": {"workload": WORKLOAD},
             "cpu_baseline": cb, "e2e": {"value": v, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
-            "note": "oracle port (FP64 NumPy/SciPy) of the reference algorithm on the host cores"
-            + ("" if ref_lib.exists() else "; reference CUDA harness not built")}
+            "note": "FP64 CPU port of the reference algorithm on the host cores (reference kernel builds absent)"}
 
 
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
-    ap.add_argument("--steps", type=int, default=10)
+    ap.add_argument("--steps", type=int, default=50)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--precision", default="fp16x3")
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--quick", action="store_true", help="headline step only (no plain-FP32, batch, serving)")
+    ap.add_argument("--grid", type=int, default=0, help="cube edge of a smaller grid for the same molecule")
     args = ap.parse_args()
     args.warmup = max(args.warmup, 3)
     world, rank, local, pg = dist_setup()

@@ -3,9 +3,10 @@
 Loads the reference kernels compiled from their sources by oracle/build_ref.py
 (oracle/_ref/*.so), runs them on each parity case of oracle/ref_cases.py with the launch
 shapes and host-side steps of the reference facade (qmtools/qmtools.py), and writes the
-outputs to <outdir>/<case>.npz.  The committed tests/golden/*.npz were produced by
+outputs to <outdir>/<case>.npz (default golden_out).  The committed tests/golden/*.npz were
+produced by
 
-    python tests/golden/make_golden.py gpurun_out/golden
+    python tests/golden/make_golden.py <outdir>
 
 on a B200; tests/test_golden.py checks the oracle against them (CPU) and
 tests/test_gpu_golden.py checks the sm_100a kernels against them (GPU).
@@ -157,7 +158,7 @@ def run_case(case, outdir):
 
 
 def main():
-    outdir = Path(sys.argv[1] if len(sys.argv) > 1 else "gpurun_out/golden")
+    outdir = Path(sys.argv[1] if len(sys.argv) > 1 else "golden_out")
     outdir.mkdir(parents=True, exist_ok=True)
     cases = sys.argv[2:] or list(rc.CASES)
     for case in cases:
