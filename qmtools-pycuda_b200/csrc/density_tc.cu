@@ -624,6 +624,7 @@ struct FusedParams {
   int kpad, ksteps, nsplit, stages;
   int tri;                 // 1: upper-triangular U (half the work); 0: full symmetric P
   int nchunks;             // kpad / 64 column chunks of A
+  int box_rows;            // rows of one U box: 64 (triangular), else kpad or kpad / 2 (<= 256)
   int chunk_need[MAX_FUSED_CHUNKS];  // production items (atom halves) writing each chunk
   uint32_t a_bytes;        // one A piece: 128 rows x kpad x 2 B
   uint32_t b_slot;         // one U piece slot in a stage: kpad rows x 32 B
@@ -820,12 +821,13 @@ __global__ void __launch_bounds__(FUSED_THREADS, 1)
           }
           const int j0 = ks * 16;
           const int r0 = p.tri ? j0 : 0;            // first output column touched by this K-step
-          const int npc = (p.kpad - r0 + 63) / 64;  // 64-row pieces
+          const int bh = p.box_rows;                   // rows per TMA box (divides kpad - r0 when not tri)
+          const int npc = (p.kpad - r0 + bh - 1) / bh;
           uint8_t* st = stages + (size_t)s * p.stage_bytes;
-          mbar_expect_tx(&full_bar[s], (uint32_t)(npc * 64 * 32 * p.nsplit));
+          mbar_expect_tx(&full_bar[s], (uint32_t)(npc * bh * 32 * p.nsplit));
           for (int c = 0; c < npc; ++c) {
-            tma_load_2d(st + c * 2048, &tmU_hi, &full_bar[s], j0, r0 + 64 * c);
-            if (two) tma_load_2d(st + p.b_slot + c * 2048, &tmU_lo, &full_bar[s], j0, r0 + 64 * c);
+            tma_load_2d(st + c * bh * 32, &tmU_hi, &full_bar[s], j0, r0 + bh * c);
+            if (two) tma_load_2d(st + p.b_slot + c * bh * 32, &tmU_lo, &full_bar[s], j0, r0 + bh * c);
           }
           last_par[s] = (int)ph;
         }
@@ -919,6 +921,12 @@ __global__ void __launch_bounds__(FUSED_THREADS, 1)
         const float x0 = (float)(pos[r0][0] - ax), y0 = (float)(pos[r0][1] - ay), z0 = (float)(pos[r0][2] - az);
         const float x1 = (float)(pos[r1][0] - ax), y1 = (float)(pos[r1][1] - ay), z1 = (float)(pos[r1][2] - az);
         const float q0 = x0 * x0 + y0 * y0 + z0 * z0, q1 = x1 * x1 + y1 * y1 + z1 * z1;
+        // primitives with alpha * min_rows(r^2) >= the cut-off are zero at every row of the item:
+        // with exponents in descending order they are the leading ones of a shell and are skipped
+        // (the remaining terms are summed in the same order, so the result is unchanged)
+        float qmin = fminf(q0, q1);
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) qmin = fminf(qmin, __shfl_xor_sync(0xffffffffu, qmin, o));
         float nx0 = 0.f, nx1 = 0.f;   // radial parts of the next shell when it shares the exponents
         int flast = 0;
         for (int sidx = s0; sidx < s1; ++sidx) {
@@ -929,9 +937,15 @@ __global__ void __launch_bounds__(FUSED_THREADS, 1)
             rad0 = nx0;
             rad1 = nx1;
           } else {
-            const float2* pa = pr_s + rec.x;
-            const float2* pn = (rec.z >> 24) ? pr_s + rec.w : nullptr;
-            switch (np_) {
+            int sk = 0;
+            while (sk < np_ && pr_s[rec.x + sk].x * qmin >= kExpCut) ++sk;
+            const float2* pa = pr_s + rec.x + sk;
+            const float2* pn = (rec.z >> 24) ? pr_s + rec.w + sk : nullptr;
+            switch (np_ - sk) {
+              case 0:
+                rad0 = rad1 = 0.f;
+                nx0 = nx1 = 0.f;
+                break;
               case 1: radial_np<1>(pa, pn, q0, q1, rad0, rad1, nx0, nx1); break;
               case 2: radial_np<2>(pa, pn, q0, q1, rad0, rad1, nx0, nx1); break;
               case 3: radial_np<3>(pa, pn, q0, q1, rad0, rad1, nx0, nx1); break;
@@ -943,7 +957,7 @@ __global__ void __launch_bounds__(FUSED_THREADS, 1)
               default:
                 rad0 = 0.f;
                 rad1 = 0.f;
-                for (int k = 0; k < np_; ++k) {
+                for (int k = 0; k < np_ - sk; ++k) {
                   const float2 ac = pa[k];
                   const float a0 = ac.x * q0, a1 = ac.x * q1;
                   rad0 = fmaf(ac.y, a0 < kExpCut ? expf(-a0) : 0.f, rad0);
@@ -1071,12 +1085,13 @@ __global__ void __launch_bounds__(FUSED_THREADS, 1)
   }
 }
 
-static qmt_status make_map_sw32(CUtensorMap* m, const void* base, uint64_t inner, uint64_t outer) {
+static qmt_status make_map_sw32(CUtensorMap* m, const void* base, uint64_t inner, uint64_t outer,
+                                uint32_t box_rows = 64) {
   auto fn = encode_fn();
   if (!fn) return fail(QMT_CUDA_ERR, "cuTensorMapEncodeTiled unavailable");
   cuuint64_t dims[2] = {inner, outer};
   cuuint64_t strides[1] = {inner * 2};
-  cuuint32_t box[2] = {16, 64};
+  cuuint32_t box[2] = {16, box_rows};
   cuuint32_t estr[2] = {1, 1};
   CUresult r = fn(m, CU_TENSOR_MAP_DATA_TYPE_UINT16, 2, const_cast<void*>(base), dims, strides, box, estr,
                   CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_32B, CU_TENSOR_MAP_L2_PROMOTION_L2_256B,
@@ -1130,10 +1145,15 @@ static qmt_status ensure_fused_operands(qmt_mol* m, int prec, const TcShape& sh,
     tab[i] = make_int4(a.prim, a.func, a.L | (a.nprim << 8) | (a.same_exp << 16) | ((int)nxt << 24),
                        nxt ? m->shells[i + 1].prim : 0);
   }
+  // primitives of a shell in descending exponent order (the kernel skips the leading ones that
+  // vanish on a whole work item); basis files normally list them that way already
   float2* pt = reinterpret_cast<float2*>(tab.data() + nsh);
-  for (const Shell& shl : m->shells)
+  for (const Shell& shl : m->shells) {
     for (int k = 0; k < shl.nprim; ++k)
       pt[shl.prim + k] = make_float2(m->alpha[shl.prim + k], m->coeff[shl.prim + k] * fs[shl.func]);
+    std::stable_sort(pt + shl.prim, pt + shl.prim + shl.nprim,
+                     [](const float2& u, const float2& v) { return u.x > v.x; });
+  }
   qmt_status st;
   if ((st = m->d_fused_B.reserve(2 * piece))) return st;
   if ((st = m->d_fused_tab.reserve(tab.size() * sizeof(int4)))) return st;
@@ -1172,7 +1192,9 @@ static qmt_status run_fused(qmt_mol* m, const TcShape& sh, const PointMap& pm, i
   const size_t piece = (size_t)(K + 64) * K * 2;
   CUtensorMap tU_hi, tU_lo;
   const uint8_t* B = m->d_fused_B.as<uint8_t>();
-  if ((st = make_map_sw32(&tU_hi, B, K, K + 64)) || (st = make_map_sw32(&tU_lo, B + piece, K, K + 64)))
+  // fewer, taller boxes for the full matrix (a stage is one K-step of all kpad rows)
+  const uint32_t box_rows = g_fused_tri ? 64u : (K <= 256 ? (uint32_t)K : (uint32_t)K / 2);
+  if ((st = make_map_sw32(&tU_hi, B, K, K + 64, box_rows)) || (st = make_map_sw32(&tU_lo, B + piece, K, K + 64, box_rows)))
     return st;
   FusedParams p{};
   p.mol = m->view();
@@ -1182,6 +1204,7 @@ static qmt_status run_fused(qmt_mol* m, const TcShape& sh, const PointMap& pm, i
   p.ksteps = K / 16;
   p.tri = g_fused_tri;
   p.nchunks = K / 64;
+  p.box_rows = (int)box_rows;
   if (p.nchunks > MAX_FUSED_CHUNKS) return fail(QMT_BAD_ARG, "fused density path supports kpad <= 320");
   for (int a = 0; a < m->natoms; ++a) {
     const int sa = m->atom_shell[a], sb = m->atom_shell[a + 1];

@@ -6,76 +6,229 @@
 // Dirichlet mode (new): V'(interior) = (sum of 6 neighbours + 4 pi h^2 rho) / 6 and the
 // outer shell keeps its given values.
 //
-// Each CTA owns a 32 x 8 column of the x-y plane and marches along z holding the z-1, z,
-// z+1 values in registers; the x-y halo of the current plane goes through shared memory,
-// so every V value is read from memory about once per sweep.  The FP64 sum |V' - V| is
-// formed only on sweeps that feed a convergence check.
+// One cooperative, persistent launch runs every sweep.  A work item is four consecutive x
+// points (float4 loads of the row, the four neighbouring rows and Q): the grids of the path
+// (three fields up to 192^3 = 85 MB) stay in the 126 MB L2 across sweeps, so the stencil is
+// limited by L2 latency and wants many independent loads in flight rather than on-chip reuse.
+// Sweeps are separated by a grid barrier of this file (bounded wait: it raises an error flag
+// after 2 s).
+// V and its copy are rewritten by other CTAs between sweeps, so they are read through L2
+// (ld.global.cg), never through the non-coherent L1 paths.  On sweeps that feed a
+// convergence check each CTA sums |V' - V| in FP64 over its units; CTA 0 adds the CTA sums in
+// CTA order, so the residual is deterministic, and every CTA takes the same stop decision.
 #include "mol.cuh"
 #include "reduce.cuh"
 
 namespace qmt {
 
 constexpr int JX = 32, JY = 8;
+constexpr int JAC_THREADS = JX * JY;
+constexpr int JAC_BLOCKS_PER_SM = 4;
 
-template <bool DIRICHLET>
-__global__ void __launch_bounds__(JX* JY) jacobi_kernel(int nx, int ny, int nz, float h, float src_scale,
-                                                        const float* __restrict__ Q, const float* __restrict__ V,
-                                                        float* __restrict__ W, double* __restrict__ part) {
-  __shared__ float tile[JY + 2][JX + 2];
-  __shared__ double sh[8];
-  const int tx = threadIdx.x, ty = threadIdx.y;
-  const int x = blockIdx.x * JX + tx, y = blockIdx.y * JY + ty;
-  const bool in = x < nx && y < ny;
-  const int64_t plane = (int64_t)nx * ny;
-  const int64_t col = (int64_t)y * nx + x;
-  float vm = 0.f, vc = 0.f, vp = 0.f;
-  if (in) {
-    vc = V[col];
-    vp = nz > 1 ? V[col + plane] : 0.f;
-  }
-  double dsum = 0.0;
-  for (int z = 0; z < nz; ++z) {
-    __syncthreads();
-    tile[ty + 1][tx + 1] = vc;
-    if (tx == 0) tile[ty + 1][0] = (in && x > 0) ? V[z * plane + col - 1] : 0.f;
-    if (tx == JX - 1) tile[ty + 1][JX + 1] = (y < ny && x + 1 < nx) ? V[z * plane + col + 1] : 0.f;
-    if (ty == 0) tile[0][tx + 1] = (x < nx && y > 0) ? V[z * plane + col - nx] : 0.f;
-    if (ty == JY - 1) tile[JY + 1][tx + 1] = (x < nx && y + 1 < ny) ? V[z * plane + col + nx] : 0.f;
-    __syncthreads();
-    if (in) {
-      const int64_t g = z * plane + col;
-      const bool edge = x == 0 || x == nx - 1 || y == 0 || y == ny - 1 || z == 0 || z == nz - 1;
-      float out;
-      if constexpr (!DIRICHLET) {
-        float s = tile[ty + 1][tx] + tile[ty + 1][tx + 2];
-        s = s + tile[ty + 2][tx + 1];
-        s = s + tile[ty][tx + 1];
-        s = s + vp;
-        s = s + vm;
-        s = s - Q[g] / h;
-        out = edge ? 0.f : s / 6.0f;
-      } else {
-        const float s = tile[ty + 1][tx] + tile[ty + 1][tx + 2] + tile[ty + 2][tx + 1] + tile[ty][tx + 1] + vp + vm;
-        out = edge ? vc : (s + src_scale * Q[g]) * (1.0f / 6.0f);
+struct JacobiArgs {
+  int nx, ny, nz;
+  float h, src_scale;
+  const float* Q;
+  float* V;            // start value in, result out
+  float* T;            // second buffer
+  int vec4;            // nx % 4 == 0 and 16-byte aligned V, T, Q: groups of four x points
+  int max_sweeps, check_every;
+  double tol;
+  double* part;        // per-CTA partial sums
+  unsigned* bar;       // [0] arrivals, [1] generation
+  double* res;         // [0] residual of the last check
+  int* out;            // [0] sweeps done, [1] status: 0 running/cap, 1 converged, 2 not finite, 3 barrier timeout
+};
+
+__device__ __forceinline__ uint64_t jac_timer_ns() {
+  uint64_t t;
+  asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
+  return t;
+}
+
+// Sense-counting grid barrier for a cooperative launch (all CTAs co-resident).  Returns false
+// on every CTA once any CTA has waited more than 2 s or raised the flag.
+__device__ bool grid_barrier(unsigned* bar, int* flag, unsigned nblocks) {
+  __shared__ int ok_s;
+  __syncthreads();
+  if (threadIdx.x == 0 && threadIdx.y == 0) {
+    volatile unsigned* gen = bar + 1;
+    volatile int* vflag = flag;
+    const unsigned g = *gen;
+    __threadfence();
+    int ok = 1;
+    if (atomicAdd(bar, 1u) == nblocks - 1) {
+      atomicExch(bar, 0u);
+      __threadfence();
+      atomicAdd(bar + 1, 1u);
+    } else {
+      const uint64_t t0 = jac_timer_ns();
+      while (*gen == g) {
+        if (*vflag) {
+          ok = 0;
+          break;
+        }
+        if (jac_timer_ns() - t0 > 2000000000ull) {
+          atomicExch(flag, 1);
+          ok = 0;
+          break;
+        }
       }
-      W[g] = out;
-      if (part) dsum += fabs((double)out - (double)vc);
-      vm = vc;
-      vc = vp;
-      vp = (z + 2 < nz) ? V[g + 2 * plane] : 0.f;
+    }
+    __threadfence();
+    ok_s = ok && !*vflag;
+  }
+  __syncthreads();
+  return ok_s != 0;
+}
+
+// Update of one point from its six neighbours (in the reference's summation order).
+template <bool DIRICHLET>
+__device__ __forceinline__ float jac_point(float xm, float xp, float yp, float ym, float zp, float zm, float q,
+                                           float vc, bool edge, float h, float src_scale) {
+  if constexpr (!DIRICHLET) {
+    float s = xm + xp;
+    s = s + yp;
+    s = s + ym;
+    s = s + zp;
+    s = s + zm;
+    s = s - q / h;
+    return edge ? 0.f : s / 6.0f;
+  } else {
+    const float s = xm + xp + yp + ym + zp + zm;
+    return edge ? vc : (s + src_scale * q) * (1.0f / 6.0f);
+  }
+}
+
+__device__ __forceinline__ float4 ldcg4(const float* p) { return __ldcg(reinterpret_cast<const float4*>(p)); }
+
+// One sweep src -> dst.  Work items are groups of four consecutive x points (float4 loads of
+// the row, the four neighbouring rows and Q, scalar loads of the two x halo values), spread over
+// all CTAs; every load of a group is independent, so many are in flight per thread.  Returns
+// this thread's FP64 sum |dst - src| when `resid` is set.
+template <bool DIRICHLET>
+__device__ double sweep(const JacobiArgs& a, const float* src, float* dst, bool resid) {
+  const int nx = a.nx, ny = a.ny, nz = a.nz;
+  const int64_t row = nx, plane = (int64_t)nx * ny;
+  const int64_t nthreads = (int64_t)gridDim.x * JAC_THREADS;
+  const int64_t tid = (int64_t)blockIdx.x * JAC_THREADS + threadIdx.y * JX + threadIdx.x;
+  double dsum = 0.0;
+  if (a.vec4) {
+    const int nxq = nx >> 2;
+    const int64_t ngroups = (int64_t)nxq * ny * nz;
+    for (int64_t gi = tid; gi < ngroups; gi += nthreads) {
+      const int xq = (int)(gi % nxq);
+      const int64_t r = gi / nxq;
+      const int y = (int)(r % ny), z = (int)(r / ny);
+      const int x0 = xq * 4;
+      const int64_t b = z * plane + (int64_t)y * row + x0;
+      const float4 c = ldcg4(src + b);
+      const float4 zero = make_float4(0.f, 0.f, 0.f, 0.f);
+      const float4 ym = y > 0 ? ldcg4(src + b - row) : zero;
+      const float4 yp = y + 1 < ny ? ldcg4(src + b + row) : zero;
+      const float4 zm = z > 0 ? ldcg4(src + b - plane) : zero;
+      const float4 zp = z + 1 < nz ? ldcg4(src + b + plane) : zero;
+      const float4 q = __ldg(reinterpret_cast<const float4*>(a.Q + b));
+      const float xl = x0 > 0 ? __ldcg(src + b - 1) : 0.f;
+      const float xr = x0 + 4 < nx ? __ldcg(src + b + 4) : 0.f;
+      const bool eyz = y == 0 || y == ny - 1 || z == 0 || z == nz - 1;
+      float4 o;
+      o.x = jac_point<DIRICHLET>(xl, c.y, yp.x, ym.x, zp.x, zm.x, q.x, c.x, eyz || x0 == 0, a.h, a.src_scale);
+      o.y = jac_point<DIRICHLET>(c.x, c.z, yp.y, ym.y, zp.y, zm.y, q.y, c.y, eyz || x0 + 1 == nx - 1, a.h,
+                                 a.src_scale);
+      o.z = jac_point<DIRICHLET>(c.y, c.w, yp.z, ym.z, zp.z, zm.z, q.z, c.z, eyz || x0 + 2 == nx - 1, a.h,
+                                 a.src_scale);
+      o.w = jac_point<DIRICHLET>(c.z, xr, yp.w, ym.w, zp.w, zm.w, q.w, c.w, eyz || x0 + 3 == nx - 1, a.h,
+                                 a.src_scale);
+      __stcg(reinterpret_cast<float4*>(dst + b), o);
+      if (resid)
+        dsum += (fabs((double)o.x - (double)c.x) + fabs((double)o.y - (double)c.y)) +
+                (fabs((double)o.z - (double)c.z) + fabs((double)o.w - (double)c.w));
+    }
+  } else {
+    const int64_t n = plane * nz;
+    for (int64_t g = tid; g < n; g += nthreads) {
+      const int x = (int)(g % nx);
+      const int64_t r = g / nx;
+      const int y = (int)(r % ny), z = (int)(r / ny);
+      const float vc = __ldcg(src + g);
+      const float xm = x > 0 ? __ldcg(src + g - 1) : 0.f;
+      const float xp = x + 1 < nx ? __ldcg(src + g + 1) : 0.f;
+      const float ym = y > 0 ? __ldcg(src + g - row) : 0.f;
+      const float yp = y + 1 < ny ? __ldcg(src + g + row) : 0.f;
+      const float zm = z > 0 ? __ldcg(src + g - plane) : 0.f;
+      const float zp = z + 1 < nz ? __ldcg(src + g + plane) : 0.f;
+      const bool edge = x == 0 || x == nx - 1 || y == 0 || y == ny - 1 || z == 0 || z == nz - 1;
+      const float o = jac_point<DIRICHLET>(xm, xp, yp, ym, zp, zm, __ldg(a.Q + g), vc, edge, a.h, a.src_scale);
+      __stcg(dst + g, o);
+      if (resid) dsum += fabs((double)o - (double)vc);
     }
   }
-  if (part) {
-    const int lin = ty * JX + tx;
-    double v = dsum;
+  return dsum;
+}
+
+template <bool DIRICHLET>
+__global__ void __launch_bounds__(JAC_THREADS, JAC_BLOCKS_PER_SM) jacobi_persistent_kernel(JacobiArgs a) {
+  __shared__ double sh[JAC_THREADS / 32];
+  const unsigned nb = gridDim.x;
+  int* flag = a.out + 2;
+  double delta = INFINITY;
+  int sweeps = 0, pairs = 0, status = 0;
+  const int lin = threadIdx.y * JX + threadIdx.x;
+  while (sweeps + 2 <= a.max_sweeps) {
+    ++pairs;
+    const bool check = pairs % a.check_every == 0 || sweeps + 4 > a.max_sweeps;
+    sweep<DIRICHLET>(a, a.V, a.T, false);
+    if (!grid_barrier(a.bar, flag, nb)) {
+      status = 3;
+      break;
+    }
+    const double ds = sweep<DIRICHLET>(a, a.T, a.V, check);
+    sweeps += 2;
+    if (!check) {
+      if (!grid_barrier(a.bar, flag, nb)) {
+        status = 3;
+        break;
+      }
+      continue;
+    }
+    // FP64 residual: warp tree, warps in order, CTAs in order
+    double v = ds;
     for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
     if ((lin & 31) == 0) sh[lin >> 5] = v;
     __syncthreads();
     if (lin == 0) {
-      double r = 0;
-      for (int w = 0; w < JX * JY / 32; ++w) r += sh[w];
-      part[blockIdx.y * gridDim.x + blockIdx.x] = r;
+      double r = 0.0;
+      for (int w = 0; w < JAC_THREADS / 32; ++w) r += sh[w];
+      __stcg(a.part + blockIdx.x, r);
     }
+    if (!grid_barrier(a.bar, flag, nb)) {
+      status = 3;
+      break;
+    }
+    if (blockIdx.x == 0 && lin == 0) {
+      double r = 0.0;
+      for (unsigned b = 0; b < nb; ++b) r += __ldcg(a.part + b);
+      __stcg(a.res, r);
+    }
+    if (!grid_barrier(a.bar, flag, nb)) {
+      status = 3;
+      break;
+    }
+    delta = __ldcg(a.res);
+    if (!isfinite(delta)) {
+      status = 2;
+      break;
+    }
+    if (delta <= a.tol) {
+      status = 1;
+      break;
+    }
+  }
+  if (blockIdx.x == 0 && lin == 0) {
+    a.out[0] = sweeps;
+    a.out[1] = status;
+    __stcg(a.res + 1, delta);
   }
 }
 
@@ -85,47 +238,57 @@ static qmt_status run_jacobi(int nx, int ny, int nz, float step, const float* rh
                              double* delta_out, cudaStream_t s) {
   if (nx < 1 || ny < 1 || nz < 1 || !(step > 0.f) || !rho || !v || !t || max_sweeps < 0 || check_every < 1)
     return fail(QMT_BAD_ARG, "bad Jacobi arguments");
-  const dim3 blk(JX, JY), grd((nx + JX - 1) / JX, (ny + JY - 1) / JY);
-  const int64_t nblk = (int64_t)grd.x * grd.y;
+  const int nsm = sm_count();
+  int per_sm = 0;
+  auto kern = jacobi_persistent_kernel<DIRICHLET>;
+  QMT_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, JAC_THREADS, 0));
+  if (per_sm < 1) return fail(QMT_CUDA_ERR, "Jacobi kernel does not fit on an SM");
+  per_sm = std::min(per_sm, JAC_BLOCKS_PER_SM);
+  const int64_t capacity = (int64_t)nsm * per_sm;
+
+  JacobiArgs a{};
+  a.nx = nx;
+  a.ny = ny;
+  a.nz = nz;
+  a.h = DIRICHLET ? 0.f : step;
+  a.src_scale = DIRICHLET ? (float)(4.0 * 3.14159265358979323846 * (double)step * step) : 0.f;
+  a.Q = rho;
+  a.V = v;
+  a.T = t;
+  a.vec4 = (nx % 4 == 0) && ((reinterpret_cast<uintptr_t>(rho) | reinterpret_cast<uintptr_t>(v) |
+                                reinterpret_cast<uintptr_t>(t)) % 16 == 0);
+  a.max_sweeps = max_sweeps;
+  a.check_every = check_every;
+  a.tol = tol;
+  const int64_t items = a.vec4 ? (int64_t)(nx / 4) * ny * nz : (int64_t)nx * ny * nz;
+  const int grid = (int)std::max<int64_t>(1, std::min<int64_t>((items + JAC_THREADS - 1) / JAC_THREADS, capacity));
+
+  // scratch: CTA partial sums, barrier words, residuals, status words (grows, never freed)
   static thread_local DevBuf scratch;
-  qmt_status st = scratch.reserve((nblk + 8) * sizeof(double));
+  const size_t part_bytes = ((size_t)grid * sizeof(double) + 255) / 256 * 256;
+  qmt_status st = scratch.reserve(part_bytes + 256);
   if (st) return st;
-  double* part = scratch.as<double>();
-  double* res = part + nblk;
-  const float src = DIRICHLET ? (float)(4.0 * 3.14159265358979323846 * (double)step * step) : 0.f;
-  double delta = INFINITY;
-  int sweeps = 0, pairs = 0;
-  bool converged = false;
-  while (sweeps + 2 <= max_sweeps) {
-    ++pairs;
-    const bool check = pairs % check_every == 0 || sweeps + 4 > max_sweeps;
-    if constexpr (DIRICHLET) {
-      jacobi_kernel<true><<<grd, blk, 0, s>>>(nx, ny, nz, 0.f, src, rho, v, t, nullptr);
-      jacobi_kernel<true><<<grd, blk, 0, s>>>(nx, ny, nz, 0.f, src, rho, t, v, check ? part : nullptr);
-    } else {
-      jacobi_kernel<false><<<grd, blk, 0, s>>>(nx, ny, nz, step, 0.f, rho, v, t, nullptr);
-      jacobi_kernel<false><<<grd, blk, 0, s>>>(nx, ny, nz, step, 0.f, rho, t, v, check ? part : nullptr);
-    }
-    QMT_CHECK_LAUNCH("jacobi_kernel");
-    sweeps += 2;
-    if (check) {
-      if ((st = reduce_partials(part, nblk, res, 1, 0, s))) return st;
-      QMT_CUDA(cudaMemcpyAsync(&delta, res, sizeof(double), cudaMemcpyDeviceToHost, s));
-      QMT_CUDA(cudaStreamSynchronize(s));
-      if (!std::isfinite(delta)) {
-        if (sweeps_out) *sweeps_out = sweeps;
-        if (delta_out) *delta_out = delta;
-        return fail(QMT_NAN, "Jacobi residual is not finite");
-      }
-      if (delta <= tol) {
-        converged = true;
-        break;
-      }
-    }
+  uint8_t* base = scratch.as<uint8_t>();
+  a.part = reinterpret_cast<double*>(base);
+  a.res = reinterpret_cast<double*>(base + part_bytes);          // [0] check sum, [1] last residual
+  a.bar = reinterpret_cast<unsigned*>(base + part_bytes + 64);    // [0] arrivals, [1] generation
+  a.out = reinterpret_cast<int*>(base + part_bytes + 128);        // [0] sweeps, [1] status, [2] flag
+  QMT_CUDA(cudaMemsetAsync(base + part_bytes, 0, 256, s));
+  if (max_sweeps >= 2) {
+    void* params[] = {&a};
+    QMT_CUDA(cudaLaunchCooperativeKernel((const void*)kern, dim3(grid), dim3(JX, JY), params, 0, s));
   }
-  if (sweeps_out) *sweeps_out = sweeps;
+  int out[3] = {0, 0, 0};
+  double res[2] = {0.0, INFINITY};
+  QMT_CUDA(cudaMemcpyAsync(out, a.out, sizeof(out), cudaMemcpyDeviceToHost, s));
+  QMT_CUDA(cudaMemcpyAsync(res, a.res, sizeof(res), cudaMemcpyDeviceToHost, s));
+  QMT_CUDA(cudaStreamSynchronize(s));
+  const double delta = max_sweeps >= 2 ? res[1] : INFINITY;
+  if (sweeps_out) *sweeps_out = out[0];
   if (delta_out) *delta_out = delta;
-  if (!converged && tol > 0) return fail(QMT_NOT_CONVERGED, "Jacobi stopped at its sweep cap");
+  if (out[1] == 3 || out[2]) return fail(QMT_CUDA_ERR, "Jacobi grid barrier timed out");
+  if (out[1] == 2) return fail(QMT_NAN, "Jacobi residual is not finite");
+  if (out[1] != 1 && tol > 0) return fail(QMT_NOT_CONVERGED, "Jacobi stopped at its sweep cap");
   return QMT_OK;
 }
 
