@@ -280,9 +280,7 @@ def _requests(mols, basis, qmtools, serving, arrivals=None):
 def _engine_run(serving, reqs, slots, precision, realtime):
     import torch
     eng = serving.Engine(slots=slots, precision=precision)
-    eng.run(reqs[:2], realtime=False)           # first-call set-up outside the timed run
-    for r in reqs[:2]:
-        r.t_admit = r.t_done = None
+    eng.warm(reqs)                              # steady state: slots grown to the largest requests
     torch.cuda.synchronize()
     t0 = time.perf_counter()
     eng.run(reqs, realtime=realtime)
@@ -305,7 +303,8 @@ def batched_and_serving(basis, qmtools, precision):
                       "value": pts / t_mix, "unit": UNIT, "wall_s": t_mix, "slots": 8,
                       "serial_plain_fp32": {"value": pts / t_fp32, "wall_s": t_fp32},
                       "speedup_vs_serial_plain_fp32": t_fp32 / t_mix,
-                      "timing": "host wall clock around the whole batch (set-up, H2D, density, Hockney FFT, D2H)"}
+                      "timing": "host wall clock around the whole batch (set-up, H2D, density, Hockney FFT, D2H); "
+                                "slots grown to the largest requests beforehand"}
     rate, count = 200.0, 32
     stream = syn.serving_stream(rate, count)
     arr = [t for t, _ in stream]
@@ -469,8 +468,63 @@ def run_ours(args, world, rank, local, pg):
         torch.cuda.synchronize()
         check = {"q_raw": q_raw, "q": q.cpu().numpy(), "v": vout.cpu().numpy()}
         out.update(batched_and_serving(basis, qmtools, args.precision))
+        out["kernels"] = other_kernels(basis, qmtools, N, hbm, ms - dens_ms, {"n3": npts, "M": 2 * nx})
     if rank == 0 and not args.no_cpu_baseline:
         out["cpu_baseline"] = cpu_baseline_c1(sm, basis, qmtools, check)
+    return out
+
+
+def other_kernels(basis, qmtools, N, hbm_peak, fft_ms, nfft):
+    """Rooflines of the other kernels of the path (rank 0, not part of `value`)."""
+    import ctypes as C
+    import torch
+    from qmtools import synthetic as syn
+    s = C.c_void_p(torch.cuda.current_stream().cuda_stream)
+    out = {}
+    jac = {}
+    for name, n, sweeps in (("c0_64^3_2000_sweeps", 64, 2000), ("c1_128^3_400_sweeps", 128, 400)):
+        npts = n ** 3
+        rho = torch.rand(npts, device="cuda")
+        v = torch.zeros(npts, device="cuda")
+        t = torch.zeros(npts, device="cuda")
+        so, d = C.c_int(), C.c_double()
+        args = lambda k: (n, n, n, 0.2, C.c_void_p(rho.data_ptr()), C.c_void_p(v.data_ptr()),
+                          C.c_void_p(t.data_ptr()), k, 100, 0.0, C.byref(so), C.byref(d), s)
+        N.call("qmt_jacobi", *args(20))
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record()
+        N.call("qmt_jacobi", *args(sweeps))
+        e1.record()
+        torch.cuda.synchronize()
+        ms = e0.elapsed_time(e1)
+        gbs = 12.0 * npts * sweeps / (ms / 1e3) / 1e9
+        jac[name] = {"ms": ms, "us_per_sweep": 1e3 * ms / sweeps, "achieved_GBps": gbs,
+                     "frac_of_hbm_peak": gbs / hbm_peak}
+    out["jacobi"] = dict(jac, bytes_per_point_sweep=12, kernel="jacobi_persistent_kernel (one cooperative launch)")
+    if nfft is not None:
+        H = nfft["M"] ** 2 * (nfft["M"] // 2 + 1)
+        fbytes = 8.0 * nfft["n3"] + 100.0 * H
+        out["fft_hockney"] = {"ms": fft_ms, "algorithmic_bytes": fbytes,
+                              "achieved_GBps": fbytes / (fft_ms / 1e3) / 1e9,
+                              "frac_of_hbm_peak": fbytes / (fft_ms / 1e3) / 1e9 / hbm_peak,
+                              "definition": "8 n^3 + 100 H bytes, H = M^2 (M/2+1), M = 2n"}
+        sm = syn.config_molecule("c1")
+        mol = sm.molecule(basis, qmtools.Molecule)
+        g = sm.grid(qmtools.Grid)
+        nx, ny, nz, h, ox, oy, oz = g._geom()
+        v = torch.zeros(nx * ny * nz, device="cuda")
+        call = lambda: N.call("qmt_hartree_gto_boundary", mol.handle, nx, ny, nz, h, ox, oy, oz,
+                              C.c_void_p(v.data_ptr()), s)
+        call()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record()
+        call()
+        e1.record()
+        torch.cuda.synchronize()
+        nb = nx * ny * nz - (nx - 2) * (ny - 2) * (nz - 2)
+        ms = e0.elapsed_time(e1)
+        out["gto_boundary_c1"] = {"ms": ms, "boundary_points": nb, "points_per_s": nb / (ms / 1e3),
+                                  "precision": "FP64 McMurchie-Davidson"}
     return out
 
 
@@ -622,9 +676,20 @@ def main():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--quick", action="store_true", help="headline step only (no plain-FP32, batch, serving)")
     ap.add_argument("--grid", type=int, default=0, help="cube edge of a smaller grid for the same molecule")
+    ap.add_argument("--only", default="", choices=["", "jacobi"], help="run one kernel family alone (profiling)")
     args = ap.parse_args()
     args.warmup = max(args.warmup, 3)
     world, rank, local, pg = dist_setup()
+    if args.only == "jacobi":
+        # the Jacobi solve alone (64^3 for 2000 sweeps, 128^3 for 400): its profiling case
+        import torch
+        import qmtools
+        from qmtools import _native as N
+        qmtools.set_verbose(False)
+        torch.cuda.set_device(local)
+        N.ensure_device(None)
+        print(json.dumps(other_kernels(None, qmtools, N, peaks()[1], 0.0, None)["jacobi"]))
+        return
     try:
         if args.impl == "reference":
             out = run_reference(args, world, rank, local, pg)

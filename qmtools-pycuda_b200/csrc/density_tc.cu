@@ -468,7 +468,7 @@ static qmt_status make_map(CUtensorMap* m, const void* base, int esize, uint64_t
   return QMT_OK;
 }
 
-static void split_host(double x, int fmt, void* hi, void* lo, size_t idx) {
+__host__ __device__ inline void split_host(double x, int fmt, void* hi, void* lo, size_t idx) {
   if (fmt == FMT_TF32) {
     const uint32_t h = tf32_round_bits((float)x);
     const uint32_t l = tf32_round_bits((float)(x - (double)bits_f32(h)));
@@ -487,6 +487,57 @@ static void split_host(double x, int fmt, void* hi, void* lo, size_t idx) {
   }
 }
 
+// Scaled, split density matrix on the device: element (r, c), r, c < n, at r * K + c holds
+// P_rc 2^(g - s_r - s_c) split into hi + lo (inv_s = 2^-s, exact powers of two, so this equals
+// ldexp of the same exponents); `tri` keeps c <= r and halves the diagonal.  The pieces must be
+// cleared beforehand (padding stays zero).
+__global__ void split_P_kernel(const double* __restrict__ P, int np, int n, int K, const double* __restrict__ inv_s,
+                               double two_g, int tri, int fmt, uint8_t* hi, uint8_t* lo) {
+  const int64_t tot = (int64_t)n * n;
+  for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < tot; i += (int64_t)gridDim.x * blockDim.x) {
+    const int r = (int)(i / n), c = (int)(i % n);
+    if (tri && c > r) continue;
+    double v = P[(size_t)c * np + r] * two_g * inv_s[r] * inv_s[c];
+    if (tri && c == r) v *= 0.5;
+    split_host(v, fmt, hi, lo, (size_t)r * K + c);
+  }
+}
+
+// Device scales 2^-s_j (K doubles) for split_P_kernel, and the exponent g that puts
+// max |P_jk 2^(-s_j-s_k)| near 2^14.
+static qmt_status split_scales(qmt_mol* m, const std::vector<int>& sj, int K, int* g_out, cudaStream_t s) {
+  const int n = m->norbs, np = m->npad;
+  std::vector<double> inv(K, 1.0);
+  for (int j = 0; j < n; ++j) inv[j] = std::ldexp(1.0, -sj[j]);
+  double mx = 0;
+  for (int j = 0; j < n; ++j) {
+    const double* row = m->P64.data() + (size_t)j * np;
+    double rm = 0;
+    for (int k = 0; k < n; ++k) rm = std::max(rm, std::fabs(row[k]) * inv[k]);
+    mx = std::max(mx, rm * inv[j]);
+  }
+  int g = mx > 0 ? (int)std::floor(std::log2(16000.0 / mx)) : 0;
+  *g_out = std::max(-100, std::min(100, g));
+  qmt_status st = m->d_split_scale.reserve(K * sizeof(double));
+  if (st) return st;
+  // pageable uploads return once the data is staged, so `inv` may go
+  QMT_CUDA(cudaMemcpyAsync(m->d_split_scale.ptr, inv.data(), K * sizeof(double), cudaMemcpyHostToDevice, s));
+  return QMT_OK;
+}
+
+static qmt_status launch_split(qmt_mol* m, int K, int g, int tri, int fmt, void* hi, void* lo, size_t piece_bytes,
+                               cudaStream_t s) {
+  QMT_CUDA(cudaMemsetAsync(hi, 0, piece_bytes, s));
+  QMT_CUDA(cudaMemsetAsync(lo, 0, piece_bytes, s));
+  const int64_t tot = (int64_t)m->norbs * m->norbs;
+  const int blocks = (int)std::min<int64_t>((tot + 255) / 256, (int64_t)sm_count() * 8);
+  split_P_kernel<<<std::max(blocks, 1), 256, 0, s>>>(m->d_P64.as<double>(), m->npad, m->norbs, K,
+                                                     m->d_split_scale.as<double>(), std::ldexp(1.0, g), tri, fmt,
+                                                     reinterpret_cast<uint8_t*>(hi), reinterpret_cast<uint8_t*>(lo));
+  QMT_CHECK_LAUNCH("split_P_kernel");
+  return QMT_OK;
+}
+
 // Builds the scaled, split density matrix and the Phi column scales for `prec`.
 static qmt_status ensure_tc_operands(qmt_mol* m, int prec, const TcShape& sh, cudaStream_t s) {
   if (m->tc_prec == prec) return QMT_OK;
@@ -499,25 +550,14 @@ static qmt_status ensure_tc_operands(qmt_mol* m, int prec, const TcShape& sh, cu
     sj[j] = std::max(-60, std::min(60, sj[j]));
     fs[j] = (float)std::ldexp(1.0, sj[j]);
   }
-  double mx = 0;
-  for (int j = 0; j < n; ++j)
-    for (int k = 0; k < n; ++k)
-      mx = std::max(mx, std::fabs(std::ldexp(m->P64[(size_t)j * np + k], -sj[j] - sj[k])));
-  int g = mx > 0 ? (int)std::floor(std::log2(16000.0 / mx)) : 0;
-  g = std::max(-100, std::min(100, g));
+  int g = 0;
+  qmt_status st = split_scales(m, sj, K, &g, s);
+  if (st) return st;
   const size_t piece = (size_t)sh.nrows_b * K * sh.esize;
-  std::vector<uint8_t> host(2 * piece, 0);
-  for (int j = 0; j < n; ++j)
-    for (int k = 0; k < n; ++k) {
-      const double v = std::ldexp(m->P64[(size_t)j * np + k], g - sj[j] - sj[k]);
-      split_host(v, sh.fmt, host.data(), host.data() + piece, (size_t)j * K + k);
-    }
-  qmt_status st;
   if ((st = m->d_tc_P.reserve(2 * piece))) return st;
   if ((st = m->d_fscale.reserve(K * sizeof(float)))) return st;
-  QMT_CUDA(cudaMemcpyAsync(m->d_tc_P.ptr, host.data(), 2 * piece, cudaMemcpyHostToDevice, s));
   QMT_CUDA(cudaMemcpyAsync(m->d_fscale.ptr, fs.data(), K * sizeof(float), cudaMemcpyHostToDevice, s));
-  QMT_CUDA(cudaStreamSynchronize(s));
+  if ((st = launch_split(m, K, g, 0, sh.fmt, m->d_tc_P.ptr, m->d_tc_P.as<uint8_t>() + piece, piece, s))) return st;
   m->tc_g = g;
   m->tc_prec = prec;
   return QMT_OK;
@@ -1116,22 +1156,15 @@ static qmt_status ensure_fused_operands(qmt_mol* m, int prec, const TcShape& sh,
     sj[j] = std::max(-60, std::min(60, (int)std::floor(std::log2(16000.0 / b))));
     fs[j] = (float)std::ldexp(1.0, sj[j]);
   }
-  double mx = 0;
-  for (int j = 0; j < n; ++j)
-    for (int k = j; k < n; ++k)
-      mx = std::max(mx, std::fabs(std::ldexp(m->P64[(size_t)j * np + k], -sj[j] - sj[k])));
-  int g = mx > 0 ? (int)std::floor(std::log2(16000.0 / mx)) : 0;
-  g = std::max(-100, std::min(100, g));
+  int g = 0;
+  qmt_status st = split_scales(m, sj, K, &g, s);
+  if (st) return st;
   const int rows = K + 64;
   const size_t piece = (size_t)rows * K * 2;
-  std::vector<uint8_t> host(2 * piece, 0);
-  for (int nn = 0; nn < n; ++nn)
-    for (int j = 0; j < n; ++j) {
-      if (g_fused_tri && j > nn) continue;
-      double v = std::ldexp(m->P64[(size_t)j * np + nn], g - sj[j] - sj[nn]);
-      if (g_fused_tri && j == nn) v *= 0.5;
-      split_host(v, sh.fmt, host.data(), host.data() + piece, (size_t)nn * K + j);
-    }
+  if ((st = m->d_fused_B.reserve(2 * piece))) return st;
+  if ((st = launch_split(m, K, g, g_fused_tri, sh.fmt, m->d_fused_B.ptr, m->d_fused_B.as<uint8_t>() + piece, piece,
+                         s)))
+    return st;
   // every function of a shell shares the shell's bound, hence its scale: fold it into the
   // contraction coefficients (exact, powers of two)
   // Shell records {prim, func, L | nprim << 8 | same_exp << 16 | next_same << 24, next shell's
@@ -1154,12 +1187,9 @@ static qmt_status ensure_fused_operands(qmt_mol* m, int prec, const TcShape& sh,
     std::stable_sort(pt + shl.prim, pt + shl.prim + shl.nprim,
                      [](const float2& u, const float2& v) { return u.x > v.x; });
   }
-  qmt_status st;
-  if ((st = m->d_fused_B.reserve(2 * piece))) return st;
   if ((st = m->d_fused_tab.reserve(tab.size() * sizeof(int4)))) return st;
-  QMT_CUDA(cudaMemcpyAsync(m->d_fused_B.ptr, host.data(), 2 * piece, cudaMemcpyHostToDevice, s));
+  // pageable uploads return once the data is staged, so the host vectors may go
   QMT_CUDA(cudaMemcpyAsync(m->d_fused_tab.ptr, tab.data(), tab.size() * sizeof(int4), cudaMemcpyHostToDevice, s));
-  QMT_CUDA(cudaStreamSynchronize(s));
   m->fused_g = g;
   m->fused_prec = key;
   return QMT_OK;

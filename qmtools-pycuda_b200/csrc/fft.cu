@@ -26,6 +26,8 @@
 #include <map>
 #include <tuple>
 
+#include <mutex>
+
 #include "mol.cuh"
 
 namespace qmt {
@@ -302,9 +304,23 @@ __global__ void green_octant_kernel(const float2* __restrict__ g, int Mx, int My
 // ---- host ------------------------------------------------------------------------------------
 static unsigned grid_blocks(int64_t n) { return (unsigned)std::min<int64_t>((n + 255) / 256, (int64_t)sm_count() * 16); }
 
+struct GreenEntry {
+  DevBuf* buf;
+  uint64_t used;      // last use, for least-recently-used eviction
+};
+
+// Device-side caches shared by all calls: twiddle tables per (length, device), transformed
+// Green's functions per (padded shape, step, device) with at most GREEN_CACHE_MAX entries, and
+// one growing scratch grid per device for building them.  `tw_mu` guards the twiddles and
+// `green_mu` the rest; building a Green's function takes green_mu and then (through its FFT
+// passes) tw_mu, never the other way round.
+constexpr size_t GREEN_CACHE_MAX = 16;
 struct DevCache {
-  std::map<std::tuple<int, int>, DevBuf*> tw;                     // (L, device)
-  std::map<std::tuple<int, int, int, float, int>, DevBuf*> green; // (Mx, My, Mz, h, device)
+  std::mutex tw_mu, green_mu;
+  std::map<std::tuple<int, int>, DevBuf*> tw;                         // (L, device)
+  std::map<std::tuple<int, int, int, float, int>, GreenEntry> green;  // (Mx, My, Mz, h, device)
+  std::map<int, DevBuf*> green_tmp;                                   // device -> scratch
+  uint64_t clock = 0;
 };
 static DevCache& cache() {
   static DevCache c;
@@ -314,6 +330,7 @@ static DevCache& cache() {
 static qmt_status twiddles(int L, const float2** out) {
   int dev = 0;
   cudaGetDevice(&dev);
+  std::lock_guard<std::mutex> lock(cache().tw_mu);
   DevBuf*& b = cache().tw[std::make_tuple(L, dev)];
   if (!b) {
     std::vector<float2> h(L);
@@ -374,16 +391,20 @@ static qmt_status green_hat(int Mx, int My, int Mz, float h_ang, const Plan1D& p
   int dev = 0;
   cudaGetDevice(&dev);
   auto key = std::make_tuple(Mx, My, Mz, h_ang, dev);
-  auto it = cache().green.find(key);
-  if (it != cache().green.end()) {
-    *out = it->second->as<float>();
+  DevCache& c = cache();
+  std::lock_guard<std::mutex> lock(c.green_mu);
+  auto it = c.green.find(key);
+  if (it != c.green.end()) {
+    it->second.used = ++c.clock;
+    *out = it->second.buf->as<float>();
     return QMT_OK;
   }
   const int64_t M = (int64_t)Mx * My * Mz;
-  DevBuf tmp;
-  qmt_status st = tmp.reserve(M * sizeof(float2));
+  DevBuf*& tmp = c.green_tmp[dev];
+  if (!tmp) tmp = new DevBuf();
+  qmt_status st = tmp->reserve(M * sizeof(float2));   // grows only: no allocation in steady state
   if (st) return st;
-  float2* g = tmp.as<float2>();
+  float2* g = tmp->as<float2>();
   green_kernel<<<grid_blocks(M), 256, 0, s>>>(g, Mx, My, Mz, h_ang);
   QMT_CHECK_LAUNCH("green_kernel");
   PassArgs a{};
@@ -407,8 +428,17 @@ static qmt_status green_hat(int Mx, int My, int Mz, float h_ang, const Plan1D& p
   }
   green_octant_kernel<<<grid_blocks(no), 256, 0, s>>>(g, Mx, My, Mz, gb->as<float>());
   QMT_CHECK_LAUNCH("green_octant_kernel");
+  // the scratch grid is reused by the next build: finish this one first
   QMT_CUDA(cudaStreamSynchronize(s));
-  cache().green[key] = gb;
+  if (c.green.size() >= GREEN_CACHE_MAX) {
+    auto lru = c.green.begin();
+    for (auto e = c.green.begin(); e != c.green.end(); ++e)
+      if (e->second.used < lru->second.used) lru = e;
+    lru->second.buf->release();   // cudaFree waits for kernels still reading it
+    delete lru->second.buf;
+    c.green.erase(lru);
+  }
+  c.green[key] = GreenEntry{gb, ++c.clock};
   *out = gb->as<float>();
   return QMT_OK;
 }

@@ -37,6 +37,7 @@ struct qmt_mol {
   int fused_prec = -1;          // precision of the fused-path operands below
   int fused_g = 0;
   qmt::DevBuf d_fused_B;        // scaled density matrix pieces for the fused path (hi then lo)
+  qmt::DevBuf d_split_scale;    // 2^-s_j per function for the device split of the density matrix
   qmt::DevBuf d_fused_tab;      // fused path: packed shell records, then (alpha, scaled coefficient) pairs
   qmt::DevBuf d_coords, d_types, d_shells, d_alpha, d_coeff, d_alpha64, d_coeff64;
   qmt::DevBuf d_P32, d_P64;

@@ -205,6 +205,23 @@ class Engine:
                 time.sleep(5e-5)
         return requests
 
+    def warm(self, requests):
+        """Grow every slot to the largest of `requests` (device grids, pinned host buffers and the
+        molecule handle's operands), so that serving them later allocates nothing.  Growing a
+        device buffer calls cudaMalloc/cudaFree, which synchronise the whole device."""
+        import dataclasses
+        picks = {max(requests, key=lambda r: r.npts).rid,
+                 max(requests, key=lambda r: int(r.molecule.norbs)).rid,
+                 max(requests, key=lambda r: footprint(r, self.precision)).rid}
+        big = [r for r in requests if r.rid in picks]
+        for slot in self.slots:
+            for r in big:
+                r2 = dataclasses.replace(r, density=None, potential=None, t_admit=None, t_done=None)
+                self._launch(slot, r2)
+                slot.event.synchronize()
+                self._retire(slot, 0.0)
+        self.in_use = 0
+
     def close(self):
         for s in self.slots:
             if s.handle is not None:
