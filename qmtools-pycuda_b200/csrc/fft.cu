@@ -43,7 +43,17 @@ struct Plan1D {
   int L;
   int nfac;
   int fac[FFT_MAXFAC];
+  // per stage: Ns (product of the earlier radices) and exact multiply-high divisors
+  // ceil(2^32 / d) for d = L / R and d = Ns (dividends stay below 2^16, divisors <= 2048;
+  // d == 1 does not fit in 32 bits and is handled without the multiply)
+  int ns[FFT_MAXFAC];
+  unsigned m_nbf[FFT_MAXFAC], m_ns[FFT_MAXFAC];
+  unsigned m_len;   // ceil(2^32 / L)
 };
+
+constexpr int FFT_CAND = 24;   // nuclei listed per x line for the right-hand side
+
+__device__ __forceinline__ unsigned fdiv(unsigned n, unsigned m) { return __umulhi(n, m); }
 
 static bool factorize(int L, Plan1D& p) {
   p.L = L;
@@ -127,16 +137,18 @@ __device__ __forceinline__ void radix_stage(const float2* __restrict__ s, float2
 __device__ void fft_lines_smem(float2* src, float2* dst, const Plan1D& plan, int nb, const float2* tw, bool inv,
                                float2** result) {
   const int L = plan.L;
-  int Ns = 1;
   for (int st = 0; st < plan.nfac; ++st) {
     const int R = plan.fac[st];
     const int nbf = L / R;
+    const int Ns = plan.ns[st];
+    const unsigned mnbf = plan.m_nbf[st], mns = plan.m_ns[st];
     for (int w = threadIdx.x; w < nb * nbf; w += blockDim.x) {
-      const int b = w / nbf, j = w - b * nbf;
+      const int b = nbf == 1 ? w : (int)fdiv((unsigned)w, mnbf), j = w - b * nbf;
       const float2* s = src + b * L;
       float2* d = dst + b * L;
-      const int k = j % Ns;
-      const int idxD = (j / Ns) * Ns * R + k;
+      const int jq = Ns == 1 ? j : (int)fdiv((unsigned)j, mns);
+      const int k = j - jq * Ns;
+      const int idxD = jq * Ns * R + k;
       switch (R) {
         case 2: radix_stage<2>(s, d, j, k, idxD, nbf, Ns, tw, L, inv); break;
         case 3: radix_stage<3>(s, d, j, k, idxD, nbf, Ns, tw, L, inv); break;
@@ -161,7 +173,6 @@ __device__ void fft_lines_smem(float2* src, float2* dst, const Plan1D& plan, int
     float2* t = src;
     src = dst;
     dst = t;
-    Ns *= R;
   }
   *result = src;
 }
@@ -211,39 +222,75 @@ __global__ void __launch_bounds__(256) fft_pass_kernel(const PassArgs a) {
   const int64_t rem = a.nlines - l0;
   const int nb = rem < a.B ? (int)rem : a.B;
   const bool lines_adjacent = a.s1 == 1;
+  // per-line data, computed once per CTA (B <= 16 lines)
+  __shared__ int64_t lbase[16];          // element 0 of the line in the work grid / output
+  __shared__ int lx[16], ly[16];         // the line's two grid coordinates (RHS, multiply, output)
+  __shared__ int ncand[16];              // RHS: nuclei within the cut-off of the line, or -1 for all
+  __shared__ int cand[16][FFT_CAND];
+  __syncthreads();   // twiddles and nuclei are in shared memory
+  if (threadIdx.x < nb) {
+    const int b = threadIdx.x;
+    const int64_t l = l0 + b;
+    const int c0 = (int)(l % a.n1), c1 = (int)(l / a.n1);
+    lx[b] = c0;
+    ly[b] = c1;
+    lbase[b] = (int64_t)c0 * a.s1 + (int64_t)c1 * a.s2;
+    if constexpr (MODE == PASS_X_RHS) {
+      // line (y = c0, z = c1) along x: keep the nuclei whose (y, z) distance passes the cut-off
+      const float py = a.oy + (c0 + 0.5f) * a.h_ang, pz = a.oz + (c1 + 0.5f) * a.h_ang;
+      int cnt = 0;
+      for (int at = 0; at < a.mol.natoms; ++at) {
+        const float cy = py - sat[4 * at + 1], cz = pz - sat[4 * at + 2];
+        if (cy * cy + cz * cz <= a.cut2 * 1.0001f) {   // superset of the per-point test below
+          if (cnt < FFT_CAND) cand[b][cnt] = at;
+          ++cnt;
+        }
+      }
+      ncand[b] = cnt <= FFT_CAND ? cnt : -1;
+    }
+  }
   __syncthreads();
   // ---- load ----
-  for (int i = threadIdx.x; i < nb * L; i += blockDim.x) {
-    int b, e;
-    if (lines_adjacent) { b = i % nb; e = i / nb; } else { e = i % L; b = i / L; }
-    const int64_t l = l0 + b;
+  auto load_one = [&](int b, int e) {
     float2 v = make_float2(0.f, 0.f);
     if (e < a.lload) {
       if constexpr (MODE == PASS_X_RHS) {
-        const int y = (int)(l % a.n1), z = (int)(l / a.n1), x = e;
+        const int y = lx[b], z = ly[b], x = e;
         const float px = a.ox + (x + 0.5f) * a.h_ang, py = a.oy + (y + 0.5f) * a.h_ang,
                     pz = a.oz + (z + 0.5f) * a.h_ang;
         float rho = a.q[x + (int64_t)y * a.nx + (int64_t)z * a.nx * a.ny] / (-a.h_ang * a.h_ang * a.h_ang);
-        for (int at = 0; at < a.mol.natoms; ++at) {
+        const int nc = ncand[b];
+        const int cnt = nc < 0 ? a.mol.natoms : nc;
+        for (int c = 0; c < cnt; ++c) {
+          const int at = nc < 0 ? c : cand[b][c];
           const float cx = px - sat[4 * at], cy = py - sat[4 * at + 1], cz = pz - sat[4 * at + 2];
           const float r2 = cx * cx + cy * cy + cz * cz;
           if (r2 <= a.cut2) rho += sat[4 * at + 3] * a.norm * expf(-r2 * a.i2s2);
         }
         v.x = a.periodic ? (float)(-(double)rho / EPS0) : rho * a.h_ang * a.h_ang * a.h_ang;
       } else {
-        v = a.data[(l % a.n1) * a.s1 + (l / a.n1) * a.s2 + e * a.se];
+        v = a.data[lbase[b] + (int64_t)e * a.se];
       }
     }
     b0[b * L + e] = v;
+  };
+  if (lines_adjacent) {
+    // 16 adjacent lines side by side: one 128-byte row of the grid per element index
+    const int b = threadIdx.x & 15;
+    for (int e = threadIdx.x >> 4; e < L; e += 16)
+      if (b < nb) load_one(b, e);
+  } else {
+    for (int b = 0; b < nb; ++b)
+      for (int e = threadIdx.x; e < L; e += blockDim.x) load_one(b, e);
   }
   __syncthreads();
   float2* res;
   fft_lines_smem(b0, b1, a.plan, nb, tw, a.inv != 0, &res);
   if constexpr (MODE == PASS_Z_MUL) {
+    const int hx = a.Mx / 2 + 1, hy = a.My / 2 + 1;
     for (int i = threadIdx.x; i < nb * L; i += blockDim.x) {
-      const int b = i / L, kz = i % L;
-      const int64_t l = l0 + b;
-      const int x = (int)(l % a.n1), y = (int)(l / a.n1);
+      const int b = (int)fdiv((unsigned)i, a.plan.m_len), kz = i - b * L;
+      const int x = lx[b], y = ly[b];
       float f;
       if (a.periodic) {
         // kernel_fft.cu:90-104: k in cycles/Ang, negative frequencies above N/2 - 1, k = 0 -> 0
@@ -254,7 +301,7 @@ __global__ void __launch_bounds__(256) fft_pass_kernel(const PassArgs a) {
         f = (x == 0 && y == 0 && kz == 0) ? 0.f : (float)(-1.0 / (4.0 * PI * PI * k2));
       } else {
         const int gx = min(x, a.Mx - x), gy = min(y, a.My - y), gz = min(kz, a.Mz - kz);
-        f = a.gsym[gx + (int64_t)(a.Mx / 2 + 1) * (gy + (int64_t)(a.My / 2 + 1) * gz)];
+        f = __ldg(a.gsym + gx + (int64_t)hx * (gy + (int64_t)hy * gz));
       }
       float2 v = res[b * L + kz];
       res[b * L + kz] = make_float2(v.x * f, v.y * f);
@@ -264,17 +311,22 @@ __global__ void __launch_bounds__(256) fft_pass_kernel(const PassArgs a) {
     fft_lines_smem(res, other, a.plan, nb, tw, a.inv == 0, &res);
   }
   // ---- store ----
-  for (int i = threadIdx.x; i < nb * a.lstore; i += blockDim.x) {
-    int b, e;
-    if (lines_adjacent || MODE == PASS_X_OUT) { b = i % nb; e = i / nb; } else { e = i % a.lstore; b = i / a.lstore; }
-    const int64_t l = l0 + b;
+  auto store_one = [&](int b, int e) {
     const float2 v = res[b * L + e];
     if constexpr (MODE == PASS_X_OUT) {
-      const int z = (int)(l % a.n1), y = (int)(l / a.n1);
-      a.out[(int64_t)e * a.ny * a.nz + (int64_t)y * a.nz + z] = v.x * a.scale;
+      // line (z = lx, y = ly) along x into the C-order output
+      a.out[(int64_t)e * a.ny * a.nz + (int64_t)ly[b] * a.nz + lx[b]] = v.x * a.scale;
     } else {
-      a.data[(l % a.n1) * a.s1 + (l / a.n1) * a.s2 + e * a.se] = make_float2(v.x * a.scale, v.y * a.scale);
+      a.data[lbase[b] + (int64_t)e * a.se] = make_float2(v.x * a.scale, v.y * a.scale);
     }
+  };
+  if (lines_adjacent || MODE == PASS_X_OUT) {
+    const int b = threadIdx.x & 15;
+    for (int e = threadIdx.x >> 4; e < a.lstore; e += 16)
+      if (b < nb) store_one(b, e);
+  } else {
+    for (int b = 0; b < nb; ++b)
+      for (int e = threadIdx.x; e < a.lstore; e += blockDim.x) store_one(b, e);
   }
 }
 
@@ -380,8 +432,16 @@ static qmt_status launch_pass(int mode, PassArgs a, cudaStream_t s) {
 static qmt_status plan_of(int L, Plan1D& p) {
   if (L < 2 || L > FFT_MAXLEN) return fail(QMT_BAD_ARG, "FFT line length out of range");
   if (!factorize(L, p)) return fail(QMT_BAD_ARG, "FFT size has too many factors");
-  for (int i = 0; i < p.nfac; ++i)
+  p.m_len = (unsigned)(((1ull << 32) + (uint64_t)L - 1) / (uint64_t)L);
+  int ns = 1;
+  for (int i = 0; i < p.nfac; ++i) {
     if (p.fac[i] > 127) return fail(QMT_BAD_ARG, "FFT size has a prime factor above 127");
+    const uint64_t nbf = (uint64_t)(L / p.fac[i]);
+    p.ns[i] = ns;
+    p.m_nbf[i] = nbf > 1 ? (unsigned)(((1ull << 32) + nbf - 1) / nbf) : 0u;
+    p.m_ns[i] = ns > 1 ? (unsigned)(((1ull << 32) + (uint64_t)ns - 1) / (uint64_t)ns) : 0u;
+    ns *= p.fac[i];
+  }
   return QMT_OK;
 }
 
