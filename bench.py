@@ -501,6 +501,26 @@ def other_kernels(basis, qmtools, N, hbm_peak, fft_ms, nfft):
         jac[name] = {"ms": ms, "us_per_sweep": 1e3 * ms / sweeps, "achieved_GBps": gbs,
                      "frac_of_hbm_peak": gbs / hbm_peak}
     out["jacobi"] = dict(jac, bytes_per_point_sweep=12, kernel="jacobi_persistent_kernel (one cooperative launch)")
+    # GA single-shot automaton: 26 neighbour MLPs (4 hidden layers of 16) per voxel, 96^3 grid
+    n, nl = 96, 4
+    npts = n ** 3
+    qube = torch.rand(2 * npts, device="cuda")
+    qo = torch.empty(npts, device="cuda")
+    p = ((2 * np.random.default_rng(0).random(272 * nl + 29) - 1) * 0.5).astype(np.float32)
+    call = lambda: N.call("qmt_nn_singleshot", n, n, n, 0.2, C.c_void_p(qube.data_ptr()),
+                          C.c_void_p(qo.data_ptr()), C.c_void_p(p.ctypes.data), int(p.size), nl, s)
+    call()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record()
+    for _ in range(5):
+        call()
+    e1.record()
+    torch.cuda.synchronize()
+    ms = e0.elapsed_time(e1) / 5
+    fma = 26.0 * (272 * nl + 17)
+    out["automaton_nnss_96^3_nl4"] = {"ms": ms, "voxels_per_s": npts / (ms / 1e3),
+                                      "fp32_tflops": 2 * fma * npts / (ms / 1e3) / 1e12,
+                                      "flop_definition": "2 x 26 x (272 NL + 17) FMA per voxel (tanh not counted)"}
     if nfft is not None:
         H = nfft["M"] ** 2 * (nfft["M"] // 2 + 1)
         fbytes = 8.0 * nfft["n3"] + 100.0 * H

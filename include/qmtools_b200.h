@@ -196,6 +196,18 @@ qmt_status qmt_vne_pseudo(qmt_mol* mol, int nx, int ny, int nz, float step,
                           int maxiters, float* res_dev, float* out_dev, int* iters_out,
                           void* stream);
 
+/* ---- GA single-shot automaton --------------------------------------------------------- */
+/* AutomatonSingleShot.Evaluate's kernel (qmtools/automaton_nn_singleshot.py:78-183,
+ * gpu_automaton_nn_singleshot, kernel_nn_ss.cu:33-178): qout_dev[v] =
+ * field1(v) * sum over the 26 neighbours u (periodic) of MLP(field1(v), field1(u))^2
+ * rsqrt(|u - v|_1) / gridstep * 0.05234482976098482.  qube_dev holds two fields of
+ * nx*ny*nz floats (field 0 is not read); params is a HOST array of 272*nlayers + 29 floats
+ * (the reference's DNASIZE), nlayers 1..8; gridstep is the double the reference writes into
+ * its kernel source (the grid step in bohr as printed from float32).  Asynchronous. */
+qmt_status qmt_nn_singleshot(int nx, int ny, int nz, double gridstep, const float* qube_dev,
+                             float* qout_dev, const float* params, int nparams, int nlayers,
+                             void* stream);
+
 #ifdef __cplusplus
 }
 #endif

@@ -98,6 +98,21 @@ def vne_classic_src(mol, grid, divisions):
                      ("PYCUDA_NDIV", _ff(divisions)), ("PYCUDA_dx", _ff(grid.step / divisions))])
 
 
+def nn_ss_src(grid, nlayers):
+    # AutomatonSingleShot.__WriteCode (qmtools/automaton_nn_singleshot.py:195-207), then the
+    # common substitutions of Evaluate (qmtools/automaton_nn_singleshot.py:108-113) on the
+    # two-field compute grid (Grid.npts is a uint32, Grid.step a float32, qmtools/qmtools.py:218-221)
+    import numpy
+    t = (REF_CUDA / "kernel_nn_ss.cu").read_text()
+    dna = 16 * 16 * nlayers + 16 * nlayers + (16 * 1 + 1) + 12
+    t = subst(t, [("PYCUDA_DNASIZE", _ff(dna)), ("PYCUDA_NL1", _ff(nlayers)), ("PYCUDA_NL2", _ff(0)),
+                  ("PYCUDA_ABS_A", _ff(0)), ("PYCUDA_ABS_B", _ff(0))])
+    npts = numpy.uint32(grid.shape[1] * grid.shape[2] * grid.shape[3])
+    return subst(t, [("PYCUDA_NX", _ff(grid.shape[1])), ("PYCUDA_NY", _ff(grid.shape[2])),
+                     ("PYCUDA_NZ", _ff(grid.shape[3])), ("PYCUDA_NPTS", _ff(npts)),
+                     ("PYCUDA_GRIDSTEP", _ff(grid.step))])
+
+
 def targets():
     """[(output .so path, generated source text, launcher include, extra libs)]."""
     from oracle import ref_cases as rc
@@ -119,6 +134,8 @@ def targets():
         if spec.get("vne"):
             out.append((d / "vne.so", vne_src(mol, grid, rc.VNE_PARAMS["adsorb"], rc.VNE_PARAMS["diff"]),
                         "vne.inc", []))
+        for nl in spec.get("nn_ss", []):
+            out.append((d / f"nn_ss_l{nl}.so", nn_ss_src(grid, nl), "nn_ss.inc", []))
         if spec.get("vne_classic"):
             out.append((d / "vne_classic.so", vne_classic_src(mol, grid, spec["vne_classic"]), "vne_classic.inc",
                         []))

@@ -58,11 +58,12 @@ def case_inputs(name, basis=None):
 # case -> kernel families to build: density subgrids, and which other families
 CASES = {
     "c0_32": {"density": [1, 2], "hartree_gto": True, "hartree_iter": True, "fft": True, "vne": True,
-              "vne_classic": 3},
+              "vne_classic": 3, "nn_ss": [4, 1]},
     "c0_16": {"density": [1, 3], "hartree_gto": True},
     "c1_24": {"density": [1], "hartree_gto": True},
     "sample": {"density": [1], "hartree_gto": False},
     "c1_bench": {"density": [1], "fft": True},
 }
 VNE_PARAMS = {"adsorb": 0.05, "diff": 0.02}
+NN_SEED = 4242          # seeded pseudo-field and parameters of the automaton cases
 FFT_PARAMS = {"sigma": 0.2, "cutoff": 6}

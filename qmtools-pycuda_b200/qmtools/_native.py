@@ -51,6 +51,7 @@ SIGNATURES = {
     "qmt_vne_point": [_vp, _i, _i, _i, _f, _f, _f, _f, _i, _vp, _vp],
     "qmt_vne_classic": [_vp, _i, _i, _i, _f, _f, _f, _f, _i, _vp, _vp],
     "qmt_vne_pseudo": [_vp, _i, _i, _i, _f, _f, _f, _f, _f, _f, _d, _i, _vp, _vp, _pi, _vp],
+    "qmt_nn_singleshot": [_i, _i, _i, _d, _vp, _vp, _vp, _i, _i, _vp],
 }
 OTHER = {"qmt_last_error": ([], C.c_char_p), "qmt_abi_version": ([], C.c_int)}
 

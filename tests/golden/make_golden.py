@@ -157,12 +157,47 @@ def run_case(case, outdir):
     return path
 
 
+def run_nn_ss(case, outdir):
+    """The single-shot automaton kernel on seeded inputs, as AutomatonSingleShot.Evaluate
+    launches it (qmtools/automaton_nn_singleshot.py:90-140): a two-field grid (field 0 zero,
+    field 1 the pseudo-field), the element's parameters in cParams, 8x8x8 blocks."""
+    import torch
+    import qmtools
+    qmtools.set_verbose(False)
+    _, grid = rc.case_inputs(case)
+    nx, ny, nz = grid.space_shape()
+    gx, gy, gz = grid.GPUblocks
+    n = nx * ny * nz
+    out = {"shape": np.array([nx, ny, nz]), "step": np.float32(grid.step)}
+    for nl in rc.CASES[case].get("nn_ss", []):
+        rng = np.random.default_rng(rc.NN_SEED + nl)
+        field1 = rng.uniform(0.0, 1.0, size=n).astype(np.float32)
+        dna = 16 * 16 * nl + 16 * nl + (16 * 1 + 1) + 12
+        params = ((2 * rng.random(dna) - 1) * 1.0).astype(np.float32)
+        qube = torch.zeros(2 * n, device="cuda")
+        qube[n:] = torch.from_numpy(field1).cuda()
+        qout = torch.zeros(n, device="cuda")
+        L = lib(REF / case / f"nn_ss_l{nl}.so")
+        assert L.ref_nn_ss(gx, gy, gz, vp(qube), vp(qout), params.ctypes.data_as(C.c_void_p), dna) == 0
+        out[f"nn_ss_l{nl}_field1"] = field1
+        out[f"nn_ss_l{nl}_params"] = params
+        out[f"nn_ss_l{nl}_out"] = qout.cpu().numpy()
+    path = Path(outdir) / f"{case}.nn_ss.npz"
+    np.savez_compressed(path, **out)
+    return path
+
+
 def main():
-    outdir = Path(sys.argv[1] if len(sys.argv) > 1 else "golden_out")
+    args = [a for a in sys.argv[1:] if not a.startswith("--")]
+    outdir = Path(args[0] if args else "golden_out")
     outdir.mkdir(parents=True, exist_ok=True)
-    cases = sys.argv[2:] or list(rc.CASES)
+    cases = args[1:] or list(rc.CASES)
     for case in cases:
-        print("wrote", run_case(case, outdir), flush=True)
+        if "--nn-ss" in sys.argv:
+            if rc.CASES[case].get("nn_ss"):
+                print("wrote", run_nn_ss(case, outdir), flush=True)
+        else:
+            print("wrote", run_case(case, outdir), flush=True)
 
 
 if __name__ == "__main__":

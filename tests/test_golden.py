@@ -140,3 +140,21 @@ def test_seed_jacobi_fft_vne_match_reference_kernels(inputs):
     assert abs(g["qdiff_rel0"] - og.qdiff(a, b)) < 1e-4 * og.qdiff(a, b)
     # the kernel returns sum |a-b|/b; Compute_qdiff multiplies by 100 (qmtools/qmtools.py:2829)
     assert abs(100 * g["qdiff_rel1"] - og.qdiff(a, b, rel=True)) < 1e-3 * og.qdiff(a, b, rel=True)
+
+
+@pytest.mark.parametrize("nl", [1, 4])
+def test_automaton_oracle_matches_reference_kernel(nl):
+    """The single-shot automaton oracle against gpu_automaton_nn_singleshot's own output
+    (kernel_nn_ss.cu, tests/golden/c0_32.nn_ss.npz; FP32 kernel vs FP64-emulated oracle)."""
+    from oracle import automaton as oa
+    g = np.load(GOLDEN / "c0_32.nn_ss.npz")
+    shape = tuple(int(v) for v in g["shape"])
+    gs = float(str(np.float32(g["step"])))
+    got = oa.nn_singleshot_grid(g[f"nn_ss_l{nl}_field1"], shape, g[f"nn_ss_l{nl}_params"], nl, gs)
+    assert rel_l2(got, g[f"nn_ss_l{nl}_out"]) < 1e-6
+
+
+def test_automaton_neighbour_order_covers_the_26_neighbours():
+    from oracle import automaton as oa
+    nb = oa.neighbour_order()
+    assert len(nb) == 26 and len({t[:3] for t in nb}) == 26 and (0, 0, 0) not in {t[:3] for t in nb}
