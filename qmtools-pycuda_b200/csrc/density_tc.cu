@@ -783,6 +783,86 @@ __device__ __forceinline__ void radial_np(const float2* pa, const float2* pn, fl
   }
 }
 
+// ---- fixed atom layouts ----------------------------------------------------------------------
+// Atoms whose shells follow a known layout are produced by fully unrolled code (one dispatch per
+// atom, every table load independent); others take the generic shell loop.  Per-primitive
+// screening skips exponentials that vanish on all rows of the item; the terms are summed in the
+// same order as the generic loop, so the values are identical.
+enum { SHAPE_GENERIC = 0, SHAPE_S3S1P1 = 1, SHAPE_S8S8S1P3P1D1 = 2 };
+
+template <int NP>
+__device__ __forceinline__ void exps2(const float2* pa, float q0, float q1, float qmin, float (&e0)[NP],
+                                      float (&e1)[NP], float (&c)[NP]) {
+  float2 ac[NP];
+#pragma unroll
+  for (int k = 0; k < NP; ++k) ac[k] = pa[k];
+#pragma unroll
+  for (int k = 0; k < NP; ++k) {
+    c[k] = ac[k].y;
+    e0[k] = 0.f;
+    e1[k] = 0.f;
+    if (ac[k].x * qmin < kExpCut) {   // uniform over the warp: qmin is the item's minimum
+      const float x0 = ac[k].x * q0, x1 = ac[k].x * q1;
+      e0[k] = x0 < kExpCut ? expf(-x0) : 0.f;
+      e1[k] = x1 < kExpCut ? expf(-x1) : 0.f;
+    }
+  }
+}
+
+template <int NP>
+__device__ __forceinline__ void contract2(const float (&c)[NP], const float (&e0)[NP], const float (&e1)[NP],
+                                          float& r0, float& r1) {
+  r0 = 0.f;
+  r1 = 0.f;
+#pragma unroll
+  for (int k = 0; k < NP; ++k) {
+    r0 = fmaf(c[k], e0[k], r0);
+    r1 = fmaf(c[k], e1[k], r1);
+  }
+}
+
+// Values of a shell of angular momentum L at the two rows, stored at functions j0.. (hi/lo).
+template <int FMT, int L>
+__device__ __forceinline__ void shell_out(float rad0, float rad1, float x0, float y0, float z0, float x1, float y1,
+                                          float z1, int j0, int r0, uint8_t* A_hi, uint8_t* A_lo, bool two) {
+  constexpr int NF = 2 * L + 1;
+  float v0[NF], v1[NF];
+  if constexpr (L == 0) {
+    v0[0] = (float)YS * rad0;
+    v1[0] = (float)YS * rad1;
+  } else if constexpr (L == 1) {
+    const float c0 = (float)YP * rad0, c1 = (float)YP * rad1;
+    v0[0] = c0 * z0; v0[1] = c0 * x0; v0[2] = c0 * y0;
+    v1[0] = c1 * z1; v1[1] = c1 * x1; v1[2] = c1 * y1;
+  } else {
+    const float c0 = (float)YD1 * rad0, c1 = (float)YD1 * rad1;
+    v0[0] = (float)YD0 * rad0 * (2.f * z0 * z0 - x0 * x0 - y0 * y0);
+    v0[1] = c0 * x0 * z0; v0[2] = c0 * z0 * y0;
+    v0[3] = (float)YD2 * rad0 * (x0 * x0 - y0 * y0); v0[4] = c0 * x0 * y0;
+    v1[0] = (float)YD0 * rad1 * (2.f * z1 * z1 - x1 * x1 - y1 * y1);
+    v1[1] = c1 * x1 * z1; v1[2] = c1 * z1 * y1;
+    v1[3] = (float)YD2 * rad1 * (x1 * x1 - y1 * y1); v1[4] = c1 * x1 * y1;
+  }
+  bool skip = false;
+#pragma unroll
+  for (int k = 0; k < NF; ++k) {
+    if (skip) {
+      skip = false;
+      continue;
+    }
+    const int j = j0 + k;
+    const uint32_t off = a_offset(r0, j);
+    if (k + 1 < NF && (j & 1) == 0) {
+      store_pair16<FMT>(A_hi, A_lo, off, v0[k], v0[k + 1], two);
+      store_pair16<FMT>(A_hi, A_lo, off + 8192u, v1[k], v1[k + 1], two);
+      skip = true;
+    } else {
+      store_split16<FMT>(A_hi, A_lo, off, v0[k], two);
+      store_split16<FMT>(A_hi, A_lo, off + 8192u, v1[k], two);
+    }
+  }
+}
+
 constexpr int FUSED_NCW = 16;                 // compute warps (Phi production and epilogue)
 constexpr int FUSED_NCT = FUSED_NCW * 32;
 constexpr int FUSED_THREADS = 64 + FUSED_NCT;  // + TMA warp + MMA warp
@@ -826,9 +906,8 @@ __global__ void __launch_bounds__(FUSED_THREADS, 1)
     reinterpret_cast<uint4*>(smem)[i] = make_uint4(0, 0, 0, 0);
   // molecule tables in shared memory: the production loop reads them in dependent chains
   uint8_t* tabs = stages + (size_t)p.stages * p.stage_bytes;
+  // shell records, primitive pairs and per-atom words (first shell | layout << 24)
   for (int i = threadIdx.x; i < p.tab_words; i += blockDim.x) reinterpret_cast<int4*>(tabs)[i] = __ldg(p.tab + i);
-  for (int i = threadIdx.x; i <= mol.natoms; i += blockDim.x)
-    reinterpret_cast<int*>(tabs + p.off_ashell)[i] = __ldg(mol.atom_shell + i);
   for (int i = threadIdx.x; i < 3 * mol.natoms; i += blockDim.x)
     reinterpret_cast<float*>(tabs + p.off_coords)[i] = __ldg(mol.coords + i);
   asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
@@ -952,7 +1031,8 @@ __global__ void __launch_bounds__(FUSED_THREADS, 1)
         itm = __shfl_sync(0xffffffffu, itm, 0);
         if (itm >= 2 * mol.natoms) break;
         const int a = itm >> 1;
-        const int s0 = ash_s[a], s1 = ash_s[a + 1];
+        const int as0 = ash_s[a];
+        const int s0 = as0 & 0xffffff, s1 = ash_s[a + 1] & 0xffffff, shape = as0 >> 24;
         if (s1 <= s0) continue;
         const int r0 = (itm & 1) * 32 + lane, r1 = r0 + 64;   // r1 sits 8192 B after r0 in A
         const double ax = crd_s[3 * a], ay = crd_s[3 * a + 1], az = crd_s[3 * a + 2];
@@ -969,7 +1049,71 @@ __global__ void __launch_bounds__(FUSED_THREADS, 1)
         for (int o = 16; o > 0; o >>= 1) qmin = fminf(qmin, __shfl_xor_sync(0xffffffffu, qmin, o));
         float nx0 = 0.f, nx1 = 0.f;   // radial parts of the next shell when it shares the exponents
         int flast = 0;
-        for (int sidx = s0; sidx < s1; ++sidx) {
+        if (shape != SHAPE_GENERIC) {
+          const int4 rec0 = sh_s[s0];
+          const float2* pa = pr_s + rec0.x;
+          const int f0 = rec0.y;
+          float rA0, rA1;
+          if (shape == SHAPE_S3S1P1) {
+            {
+              float e0[3], e1[3], c[3];
+              exps2<3>(pa, q0, q1, qmin, e0, e1, c);
+              contract2<3>(c, e0, e1, rA0, rA1);
+            }
+            float rB0, rB1, rC0, rC1;
+            {
+              float e0[1], e1[1], c[1];
+              exps2<1>(pa + 3, q0, q1, qmin, e0, e1, c);
+              contract2<1>(c, e0, e1, rB0, rB1);
+              exps2<1>(pa + 4, q0, q1, qmin, e0, e1, c);
+              contract2<1>(c, e0, e1, rC0, rC1);
+            }
+            if (!ok0) rA0 = rB0 = rC0 = 0.f;
+            if (!ok1) rA1 = rB1 = rC1 = 0.f;
+            shell_out<FMT, 0>(rA0, rA1, x0, y0, z0, x1, y1, z1, f0, r0, A_hi, A_lo, two);
+            shell_out<FMT, 0>(rB0, rB1, x0, y0, z0, x1, y1, z1, f0 + 1, r0, A_hi, A_lo, two);
+            shell_out<FMT, 1>(rC0, rC1, x0, y0, z0, x1, y1, z1, f0 + 2, r0, A_hi, A_lo, two);
+            flast = f0 + 4;
+          } else {
+            float rB0, rB1;
+            {
+              float e0[8], e1[8], c[8], d[8];
+              exps2<8>(pa, q0, q1, qmin, e0, e1, c);
+              contract2<8>(c, e0, e1, rA0, rA1);
+#pragma unroll
+              for (int k = 0; k < 8; ++k) d[k] = pa[8 + k].y;   // second s shell: same exponents
+              contract2<8>(d, e0, e1, rB0, rB1);
+            }
+            float rC0, rC1, rD0, rD1, rE0, rE1, rF0, rF1;
+            {
+              float e0[1], e1[1], c[1];
+              exps2<1>(pa + 16, q0, q1, qmin, e0, e1, c);
+              contract2<1>(c, e0, e1, rC0, rC1);
+            }
+            {
+              float e0[3], e1[3], c[3];
+              exps2<3>(pa + 17, q0, q1, qmin, e0, e1, c);
+              contract2<3>(c, e0, e1, rD0, rD1);
+            }
+            {
+              float e0[1], e1[1], c[1];
+              exps2<1>(pa + 20, q0, q1, qmin, e0, e1, c);
+              contract2<1>(c, e0, e1, rE0, rE1);
+              exps2<1>(pa + 21, q0, q1, qmin, e0, e1, c);
+              contract2<1>(c, e0, e1, rF0, rF1);
+            }
+            if (!ok0) rA0 = rB0 = rC0 = rD0 = rE0 = rF0 = 0.f;
+            if (!ok1) rA1 = rB1 = rC1 = rD1 = rE1 = rF1 = 0.f;
+            shell_out<FMT, 0>(rA0, rA1, x0, y0, z0, x1, y1, z1, f0, r0, A_hi, A_lo, two);
+            shell_out<FMT, 0>(rB0, rB1, x0, y0, z0, x1, y1, z1, f0 + 1, r0, A_hi, A_lo, two);
+            shell_out<FMT, 0>(rC0, rC1, x0, y0, z0, x1, y1, z1, f0 + 2, r0, A_hi, A_lo, two);
+            shell_out<FMT, 1>(rD0, rD1, x0, y0, z0, x1, y1, z1, f0 + 3, r0, A_hi, A_lo, two);
+            shell_out<FMT, 1>(rE0, rE1, x0, y0, z0, x1, y1, z1, f0 + 6, r0, A_hi, A_lo, two);
+            shell_out<FMT, 2>(rF0, rF1, x0, y0, z0, x1, y1, z1, f0 + 9, r0, A_hi, A_lo, two);
+            flast = f0 + 13;
+          }
+        }
+        for (int sidx = shape != SHAPE_GENERIC ? s1 : s0; sidx < s1; ++sidx) {
           const int4 rec = sh_s[sidx];   // prim, func, L | nprim << 8 | same_exp << 16 | next_same << 24, next prim
           const int L = rec.z & 0xff, np_ = (rec.z >> 8) & 0xff, f0 = rec.y;
           float rad0, rad1;
@@ -1170,7 +1314,8 @@ static qmt_status ensure_fused_operands(qmt_mol* m, int prec, const TcShape& sh,
   // Shell records {prim, func, L | nprim << 8 | same_exp << 16 | next_same << 24, next shell's
   // prim}, then one (alpha, coefficient x scale) pair per primitive.
   const size_t nsh = m->shells.size(), npr = m->alpha.size();
-  std::vector<int4> tab(nsh + (npr + 1) / 2, make_int4(0, 0, 0, 0));
+  const size_t atoms_off = nsh + (npr + 1) / 2;   // int4 index of the per-atom words
+  std::vector<int4> tab(atoms_off + (m->natoms + 1 + 3) / 4, make_int4(0, 0, 0, 0));
   for (size_t i = 0; i < nsh; ++i) {
     const Shell& a = m->shells[i];
     if (a.nprim > 255 || a.L > 255) return fail(QMT_BAD_ARG, "shell too large for the fused density tables");
@@ -1186,6 +1331,25 @@ static qmt_status ensure_fused_operands(qmt_mol* m, int prec, const TcShape& sh,
       pt[shl.prim + k] = make_float2(m->alpha[shl.prim + k], m->coeff[shl.prim + k] * fs[shl.func]);
     std::stable_sort(pt + shl.prim, pt + shl.prim + shl.nprim,
                      [](const float2& u, const float2& v) { return u.x > v.x; });
+  }
+  // per-atom words: first shell, and the atom's layout when it is one of the unrolled ones
+  int* aw = reinterpret_cast<int*>(tab.data() + atoms_off);
+  auto is = [&](int sidx, int L, int np, int same) {
+    const Shell& x = m->shells[sidx];
+    return x.L == L && x.nprim == np && x.same_exp == same;
+  };
+  for (int a = 0; a <= m->natoms; ++a) {
+    const int sa = m->atom_shell[a];
+    int shape = SHAPE_GENERIC;
+    if (a < m->natoms) {
+      const int ns = m->atom_shell[a + 1] - sa;
+      if (ns == 3 && is(sa, 0, 3, 0) && is(sa + 1, 0, 1, 0) && is(sa + 2, 1, 1, 0)) shape = SHAPE_S3S1P1;
+      if (ns == 6 && is(sa, 0, 8, 0) && is(sa + 1, 0, 8, 1) && is(sa + 2, 0, 1, 0) && is(sa + 3, 1, 3, 0) &&
+          is(sa + 4, 1, 1, 0) && is(sa + 5, 2, 1, 0))
+        shape = SHAPE_S8S8S1P3P1D1;
+    }
+    if (sa >= (1 << 24)) return fail(QMT_BAD_ARG, "too many shells for the fused density tables");
+    aw[a] = sa | (shape << 24);
   }
   if ((st = m->d_fused_tab.reserve(tab.size() * sizeof(int4)))) return st;
   // pageable uploads return once the data is staged, so the host vectors may go
@@ -1249,10 +1413,10 @@ static qmt_status run_fused(qmt_mol* m, const TcShape& sh, const PointMap& pm, i
   p.stage_bytes = p.nsplit * p.b_slot;
   p.fmt = (uint32_t)sh.fmt;
   p.tab = m->d_fused_tab.as<int4>();
-  p.tab_words = (int)(m->shells.size() + (m->alpha.size() + 1) / 2);
   p.off_prim = (int)m->shells.size() * 16;
-  p.off_ashell = p.tab_words * 16;
-  p.off_coords = p.off_ashell + (m->natoms + 1 + 3) / 4 * 16;
+  p.off_ashell = (int)(m->shells.size() + (m->alpha.size() + 1) / 2) * 16;
+  p.tab_words = p.off_ashell / 16 + (m->natoms + 1 + 3) / 4;
+  p.off_coords = p.tab_words * 16;
   p.tab_bytes = p.off_coords + (3 * m->natoms + 3) / 4 * 16;
   p.qube = qube;
   p.partials = m->d_partials.as<double>();
