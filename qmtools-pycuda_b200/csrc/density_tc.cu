@@ -94,72 +94,6 @@ __device__ __forceinline__ void split_store(float x, void* hi, void* lo, int64_t
 }
 
 // ---------------------------------------------------------------------------------------
-// Stage 1: basis functions of 128-row tiles into operand pieces.
-// ---------------------------------------------------------------------------------------
-template <int FMT>
-__global__ void __launch_bounds__(256) basis_stage_kernel(MolView mol, PointMap pm, int64_t tile0,
-                                                          int ntiles, int kpad,
-                                                          const float* __restrict__ fscale,
-                                                          void* __restrict__ out_hi,
-                                                          void* __restrict__ out_lo, int two) {
-  constexpr int ROWS = 128, CW = 64;
-  __shared__ float buf[ROWS][CW + 1];
-  __shared__ double pts[ROWS][3];
-  __shared__ int srange[2];
-  for (int t = blockIdx.x; t < ntiles; t += gridDim.x) {
-    const int64_t tile = tile0 + t;
-    __syncthreads();
-    if (threadIdx.x < ROWS) {
-      double x, y, z;
-      int64_t vox;
-      if (!tile_point<double>(pm, tile, threadIdx.x, x, y, z, vox)) x = y = z = 1e30;
-      pts[threadIdx.x][0] = x;
-      pts[threadIdx.x][1] = y;
-      pts[threadIdx.x][2] = z;
-    }
-    for (int w0 = 0; w0 < kpad; w0 += CW) {
-      for (int i = threadIdx.x; i < ROWS * CW; i += blockDim.x) buf[i / CW][i % CW] = 0.f;
-      if (threadIdx.x == 0) {
-        int s0 = mol.nshells, s1 = 0;
-        for (int s = 0; s < mol.nshells; ++s) {
-          const Shell& sh = mol.shells[s];
-          if (sh.func < w0 + CW && sh.func + 2 * sh.L + 1 > w0) {
-            s0 = min(s0, s);
-            s1 = max(s1, s + 1);
-          }
-        }
-        srange[0] = s0;
-        srange[1] = s1;
-      }
-      __syncthreads();
-      const int s0 = srange[0], ns = max(0, srange[1] - s0);
-      for (int it = threadIdx.x; it < ROWS * ns; it += blockDim.x) {
-        const int r = it % ROWS;
-        const double px = pts[r][0];
-        if (px > 1e29) continue;
-        const Shell sh = mol.shells[s0 + it / ROWS];
-        float v[5];
-        // FP64 displacement from the nucleus, rounded once (accuracy of steep exponents)
-        const int n = shell_values<float>(sh, mol.alpha, mol.coeff, (float)(px - (double)mol.coords[3 * sh.atom]),
-                                          (float)(pts[r][1] - (double)mol.coords[3 * sh.atom + 1]),
-                                          (float)(pts[r][2] - (double)mol.coords[3 * sh.atom + 2]), v);
-        for (int k = 0; k < n; ++k) {
-          const int j = sh.func + k;
-          if (j >= w0 && j < w0 + CW) buf[r][j - w0] = v[k] * fscale[j];
-        }
-      }
-      __syncthreads();
-      for (int i = threadIdx.x; i < ROWS * CW; i += blockDim.x) {
-        const int r = i / CW, c = i % CW;
-        if (w0 + c < kpad)
-          split_store<FMT>(buf[r][c], out_hi, out_lo, ((int64_t)t * ROWS + r) * kpad + w0 + c, two != 0);
-      }
-      __syncthreads();
-    }
-  }
-}
-
-// ---------------------------------------------------------------------------------------
 // Stage 2: tcgen05 contraction with the fused row-dot epilogue.
 // ---------------------------------------------------------------------------------------
 struct TcParams {
@@ -538,103 +472,6 @@ static qmt_status launch_split(qmt_mol* m, int K, int g, int tri, int fmt, void*
   return QMT_OK;
 }
 
-// Builds the scaled, split density matrix and the Phi column scales for `prec`.
-static qmt_status ensure_tc_operands(qmt_mol* m, int prec, const TcShape& sh, cudaStream_t s) {
-  if (m->tc_prec == prec) return QMT_OK;
-  const int n = m->norbs, np = m->npad, K = sh.kpad;
-  std::vector<int> sj(K, 0);
-  std::vector<float> fs(K, 0.f);
-  for (int j = 0; j < n; ++j) {
-    const double b = std::max(m->fbound[j], 1e-30);
-    sj[j] = (int)std::floor(std::log2(16000.0 / b));
-    sj[j] = std::max(-60, std::min(60, sj[j]));
-    fs[j] = (float)std::ldexp(1.0, sj[j]);
-  }
-  int g = 0;
-  qmt_status st = split_scales(m, sj, K, &g, s);
-  if (st) return st;
-  const size_t piece = (size_t)sh.nrows_b * K * sh.esize;
-  if ((st = m->d_tc_P.reserve(2 * piece))) return st;
-  if ((st = m->d_fscale.reserve(K * sizeof(float)))) return st;
-  QMT_CUDA(cudaMemcpyAsync(m->d_fscale.ptr, fs.data(), K * sizeof(float), cudaMemcpyHostToDevice, s));
-  if ((st = launch_split(m, K, g, 0, sh.fmt, m->d_tc_P.ptr, m->d_tc_P.as<uint8_t>() + piece, piece, s))) return st;
-  m->tc_g = g;
-  m->tc_prec = prec;
-  return QMT_OK;
-}
-
-template <int FMT>
-static qmt_status run_tc(qmt_mol* m, const TcShape& sh, const PointMap& pm, int64_t ntiles, int prec,
-                         float* qube, double outscale, cudaStream_t s) {
-  qmt_status st;
-  const size_t tile_bytes = (size_t)128 * sh.kpad * sh.esize;
-  const int nsm = sm_count();
-  // staging chunk: bounded to ~2 GiB, a multiple of the SM count when larger than one wave
-  int64_t chunk = std::max<int64_t>(1, ((size_t)2 << 30) / (tile_bytes * sh.nsplit));
-  if (chunk > nsm) chunk = chunk / nsm * nsm;
-  chunk = std::min<int64_t>(chunk, ntiles);
-  if ((st = m->d_Phi_hi.reserve(chunk * tile_bytes))) return st;
-  if (sh.nsplit == 2 && (st = m->d_Phi_lo.reserve(chunk * tile_bytes))) return st;
-  void* lo_ptr = sh.nsplit == 2 ? m->d_Phi_lo.ptr : m->d_Phi_hi.ptr;
-
-  CUtensorMap tA_hi, tA_lo, tB_hi, tB_lo;
-  const uint8_t* Pb = m->d_tc_P.as<uint8_t>();
-  const size_t piece = (size_t)sh.nrows_b * sh.kpad * sh.esize;
-  if ((st = make_map(&tA_hi, m->d_Phi_hi.ptr, sh.esize, sh.kpad, (uint64_t)chunk * 128, sh.ke, 128)) ||
-      (st = make_map(&tA_lo, lo_ptr, sh.esize, sh.kpad, (uint64_t)chunk * 128, sh.ke, 128)) ||
-      (st = make_map(&tB_hi, Pb, sh.esize, sh.kpad, sh.nrows_b, sh.ke, sh.pw)) ||
-      (st = make_map(&tB_lo, Pb + piece, sh.esize, sh.kpad, sh.nrows_b, sh.ke, sh.pw)))
-    return st;
-
-  TcParams p{};
-  p.pm = pm;
-  p.kpad = sh.kpad;
-  p.kchunks = sh.kpad / sh.ke;
-  p.npanels = sh.npanels;
-  p.pw = sh.pw;
-  p.nsplit = sh.nsplit;
-  p.esize = sh.esize;
-  p.a_bytes = 128u * 128u;
-  p.b_bytes = (uint32_t)sh.pw * 128u;
-  p.stage_bytes = sh.nsplit * (p.a_bytes + p.b_bytes);
-  p.tx_bytes = p.stage_bytes;
-  p.idesc = make_idesc((uint32_t)sh.fmt, 128, (uint32_t)sh.pw);
-  p.phi_hi = m->d_Phi_hi.ptr;
-  p.phi_lo = lo_ptr;
-  p.qube = qube;
-  p.partials = m->d_partials.as<double>();
-  p.outscale = outscale;
-  p.inv_g = std::ldexp(1.0, -m->tc_g);
-  p.err = reinterpret_cast<int*>(m->d_scalars.as<double>() + 8);
-
-  int maxsm = 0, dev = 0;
-  cudaGetDevice(&dev);
-  cudaDeviceGetAttribute(&maxsm, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev);
-  const int static_bytes = 4096;
-  int stages = (int)((maxsm - static_bytes - 1024) / p.stage_bytes);
-  stages = std::min(stages, MAX_STAGES);
-  if (stages < 2) return fail(QMT_BAD_ARG, "tensor-core stage does not fit in shared memory");
-  p.stages = stages;
-  const size_t dyn = (size_t)stages * p.stage_bytes + 1024;
-  auto kern = density_mma_kernel<FMT>;
-  QMT_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)dyn));
-
-  for (int64_t t0 = 0; t0 < ntiles; t0 += chunk) {
-    const int nt = (int)std::min<int64_t>(chunk, ntiles - t0);
-    const int gb = (int)std::min<int64_t>(nt, (int64_t)nsm * 4);
-    basis_stage_kernel<FMT><<<gb, 256, 0, s>>>(m->view(), pm, t0, nt, sh.kpad, m->d_fscale.as<float>(),
-                                               m->d_Phi_hi.ptr, lo_ptr, sh.nsplit == 2);
-    QMT_CHECK_LAUNCH("basis_stage_kernel");
-    p.tile0 = t0;
-    p.ntiles = nt;
-    const int gm = (int)std::min<int64_t>(nt, nsm);
-    kern<<<gm, 192, dyn, s>>>(tA_hi, tA_lo, tB_hi, tB_lo, p);
-    QMT_CHECK_LAUNCH("density_mma_kernel");
-  }
-  (void)prec;
-  return QMT_OK;
-}
-
 // ---------------------------------------------------------------------------------------
 // Fused path (kind::f16 formats, K <= 320): Phi' never leaves shared memory.
 //
@@ -670,7 +507,7 @@ struct FusedParams {
   uint32_t b_slot;         // one U piece slot in a stage: kpad rows x 32 B
   uint32_t stage_bytes;
   uint32_t fmt;
-  const int4* tab;         // packed shell records then primitive pairs (ensure_fused_operands)
+  const int4* tab;         // molecule tables (ensure_mol_tables)
   int tab_words;           // 16-byte words of tab
   int off_prim;            // byte offsets inside the staged tables: primitive pairs,
   int off_ashell;          //   first shell of each atom,
@@ -821,44 +658,373 @@ __device__ __forceinline__ void contract2(const float (&c)[NP], const float (&e0
   }
 }
 
-// Values of a shell of angular momentum L at the two rows, stored at functions j0.. (hi/lo).
-template <int FMT, int L>
-__device__ __forceinline__ void shell_out(float rad0, float rad1, float x0, float y0, float z0, float x1, float y1,
-                                          float z1, int j0, int r0, uint8_t* A_hi, uint8_t* A_lo, bool two) {
-  constexpr int NF = 2 * L + 1;
-  float v0[NF], v1[NF];
+// Real solid-harmonic values of one shell at the two rows, from the radial parts and the
+// displacements: L = 0, 1, 2 fixed, or L = -1 for the runtime angular momentum `lrt` (<= 2).
+__device__ __forceinline__ void sh_s_vals(float rad, float* v) { v[0] = (float)YS * rad; }
+__device__ __forceinline__ void sh_p_vals(float rad, float x, float y, float z, float* v) {
+  const float c = (float)YP * rad;
+  v[0] = c * z; v[1] = c * x; v[2] = c * y;
+}
+__device__ __forceinline__ void sh_d_vals(float rad, float x, float y, float z, float* v) {
+  const float c = (float)YD1 * rad;
+  v[0] = (float)YD0 * rad * (2.f * z * z - x * x - y * y);
+  v[1] = c * x * z; v[2] = c * z * y;
+  v[3] = (float)YD2 * rad * (x * x - y * y); v[4] = c * x * y;
+}
+
+template <int L>
+__device__ __forceinline__ void shell_vals(int lrt, float rad0, float rad1, float x0, float y0, float z0, float x1,
+                                           float y1, float z1, float (&v0)[L < 0 ? 5 : 2 * L + 1],
+                                           float (&v1)[L < 0 ? 5 : 2 * L + 1]) {
   if constexpr (L == 0) {
-    v0[0] = (float)YS * rad0;
-    v1[0] = (float)YS * rad1;
+    sh_s_vals(rad0, v0);
+    sh_s_vals(rad1, v1);
   } else if constexpr (L == 1) {
-    const float c0 = (float)YP * rad0, c1 = (float)YP * rad1;
-    v0[0] = c0 * z0; v0[1] = c0 * x0; v0[2] = c0 * y0;
-    v1[0] = c1 * z1; v1[1] = c1 * x1; v1[2] = c1 * y1;
+    sh_p_vals(rad0, x0, y0, z0, v0);
+    sh_p_vals(rad1, x1, y1, z1, v1);
+  } else if constexpr (L == 2) {
+    sh_d_vals(rad0, x0, y0, z0, v0);
+    sh_d_vals(rad1, x1, y1, z1, v1);
+  } else if (lrt == 0) {
+    sh_s_vals(rad0, v0);
+    sh_s_vals(rad1, v1);
+  } else if (lrt == 1) {
+    sh_p_vals(rad0, x0, y0, z0, v0);
+    sh_p_vals(rad1, x1, y1, z1, v1);
   } else {
-    const float c0 = (float)YD1 * rad0, c1 = (float)YD1 * rad1;
-    v0[0] = (float)YD0 * rad0 * (2.f * z0 * z0 - x0 * x0 - y0 * y0);
-    v0[1] = c0 * x0 * z0; v0[2] = c0 * z0 * y0;
-    v0[3] = (float)YD2 * rad0 * (x0 * x0 - y0 * y0); v0[4] = c0 * x0 * y0;
-    v1[0] = (float)YD0 * rad1 * (2.f * z1 * z1 - x1 * x1 - y1 * y1);
-    v1[1] = c1 * x1 * z1; v1[2] = c1 * z1 * y1;
-    v1[3] = (float)YD2 * rad1 * (x1 * x1 - y1 * y1); v1[4] = c1 * x1 * y1;
+    sh_d_vals(rad0, x0, y0, z0, v0);
+    sh_d_vals(rad1, x1, y1, z1, v1);
   }
-  bool skip = false;
+}
+
+// Output of the fused kernel's production: rows r0 and r0 + 64 of the 128-byte swizzled K-major
+// A tile (hi and lo pieces).  put() takes the nf (<= NF) values of one shell at functions j0..
+template <int FMT>
+struct SwizzledRowsOut {
+  uint8_t* hi;
+  uint8_t* lo;
+  int r0;
+  bool two;
+  template <int NF>
+  __device__ __forceinline__ void put(int j0, int nf, const float (&v0)[NF], const float (&v1)[NF]) const {
+    bool skip = false;   // the function was stored with its predecessor
 #pragma unroll
-  for (int k = 0; k < NF; ++k) {
-    if (skip) {
-      skip = false;
-      continue;
+    for (int k = 0; k < NF; ++k) {
+      if (k >= nf) break;
+      if (skip) {
+        skip = false;
+        continue;
+      }
+      const int j = j0 + k;
+      const uint32_t off = a_offset(r0, j);
+      // two consecutive functions in the same 16-byte unit: one 4-byte store per piece
+      if (k + 1 < nf && (j & 1) == 0) {
+        store_pair16<FMT>(hi, lo, off, v0[k], v0[k + 1], two);
+        store_pair16<FMT>(hi, lo, off + 8192u, v1[k], v1[k + 1], two);   // row r0 + 64
+        skip = true;
+      } else {
+        store_split16<FMT>(hi, lo, off, v0[k], two);
+        store_split16<FMT>(hi, lo, off + 8192u, v1[k], two);
+      }
     }
-    const int j = j0 + k;
-    const uint32_t off = a_offset(r0, j);
-    if (k + 1 < NF && (j & 1) == 0) {
-      store_pair16<FMT>(A_hi, A_lo, off, v0[k], v0[k + 1], two);
-      store_pair16<FMT>(A_hi, A_lo, off + 8192u, v1[k], v1[k + 1], two);
-      skip = true;
+  }
+};
+
+// Output of the staging kernel's production: FP32 rows r0 and r0 + 64 of a shared-memory window
+// of STAGE_W columns starting at function c0 (functions outside the window are dropped; rows
+// without a sample point get zeros).
+constexpr int STAGE_W = 128;        // columns of one staging window
+constexpr int STAGE_LD = STAGE_W + 1;  // row stride (odd: lanes on consecutive rows hit distinct banks)
+
+struct WindowRowsOut {
+  float* b0;   // row r0 of the window buffer
+  float* b1;   // row r0 + 64
+  int c0;
+  bool ok0, ok1;
+  template <int NF>
+  __device__ __forceinline__ void put(int j0, int nf, const float (&v0)[NF], const float (&v1)[NF]) const {
+#pragma unroll
+    for (int k = 0; k < NF; ++k) {
+      if (k >= nf) break;
+      const int j = j0 + k - c0;
+      if ((unsigned)j < (unsigned)STAGE_W) {
+        b0[j] = ok0 ? v0[k] : 0.f;
+        b1[j] = ok1 ? v1[k] : 0.f;
+      }
+    }
+  }
+};
+
+// Values of every function of atom `a` at rows r0 and r0 + 64 of a 128-row tile (FP64 positions
+// in `pos`, 1e30 for rows without a point), handed to `out` shell by shell.  Tables as staged
+// by the kernels: shell records, (alpha, scaled coefficient) pairs in descending alpha order,
+// per-atom words (first shell | layout << 24), float nuclear coordinates.  The whole warp works
+// on the atom (lanes r0 = half * 32 + lane).  Returns the atom's last function.
+template <class Out>
+__device__ __forceinline__ int atom_rows(const int4* sh_s, const float2* pr_s, const int* ash_s, const float* crd_s,
+                                         int a, const double (*pos)[3], int r0, const Out& out) {
+  const int as0 = ash_s[a];
+  const int s0 = as0 & 0xffffff, s1 = ash_s[a + 1] & 0xffffff, shape = as0 >> 24;
+  const int r1 = r0 + 64;
+  const double ax = crd_s[3 * a], ay = crd_s[3 * a + 1], az = crd_s[3 * a + 2];
+  const bool ok0 = pos[r0][0] < 1e29, ok1 = pos[r1][0] < 1e29;
+  // FP64 displacement from the nucleus, rounded once (accuracy of steep exponents)
+  const float x0 = (float)(pos[r0][0] - ax), y0 = (float)(pos[r0][1] - ay), z0 = (float)(pos[r0][2] - az);
+  const float x1 = (float)(pos[r1][0] - ax), y1 = (float)(pos[r1][1] - ay), z1 = (float)(pos[r1][2] - az);
+  const float q0 = x0 * x0 + y0 * y0 + z0 * z0, q1 = x1 * x1 + y1 * y1 + z1 * z1;
+  // primitives with alpha * min_rows(r^2) >= the cut-off are zero at every row of the item:
+  // with exponents in descending order they are the leading ones of a shell and are skipped
+  // (the remaining terms are summed in the same order, so the result is unchanged)
+  float qmin = fminf(q0, q1);
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) qmin = fminf(qmin, __shfl_xor_sync(0xffffffffu, qmin, o));
+  float nx0 = 0.f, nx1 = 0.f;   // radial parts of the next shell when it shares the exponents
+  int flast = 0;
+  if (shape != SHAPE_GENERIC) {
+    const int4 rec0 = sh_s[s0];
+    const float2* pa = pr_s + rec0.x;
+    const int f0 = rec0.y;
+    float rA0, rA1;
+    float s_0[1], s_1[1], p_0[3], p_1[3];
+    if (shape == SHAPE_S3S1P1) {
+      {
+        float e0[3], e1[3], c[3];
+        exps2<3>(pa, q0, q1, qmin, e0, e1, c);
+        contract2<3>(c, e0, e1, rA0, rA1);
+      }
+      float rB0, rB1, rC0, rC1;
+      {
+        float e0[1], e1[1], c[1];
+        exps2<1>(pa + 3, q0, q1, qmin, e0, e1, c);
+        contract2<1>(c, e0, e1, rB0, rB1);
+        exps2<1>(pa + 4, q0, q1, qmin, e0, e1, c);
+        contract2<1>(c, e0, e1, rC0, rC1);
+      }
+      if (!ok0) rA0 = rB0 = rC0 = 0.f;
+      if (!ok1) rA1 = rB1 = rC1 = 0.f;
+      shell_vals<0>(0, rA0, rA1, x0, y0, z0, x1, y1, z1, s_0, s_1);
+      out.put(f0, 1, s_0, s_1);
+      shell_vals<0>(0, rB0, rB1, x0, y0, z0, x1, y1, z1, s_0, s_1);
+      out.put(f0 + 1, 1, s_0, s_1);
+      shell_vals<1>(1, rC0, rC1, x0, y0, z0, x1, y1, z1, p_0, p_1);
+      out.put(f0 + 2, 3, p_0, p_1);
+      flast = f0 + 4;
     } else {
-      store_split16<FMT>(A_hi, A_lo, off, v0[k], two);
-      store_split16<FMT>(A_hi, A_lo, off + 8192u, v1[k], two);
+      float rB0, rB1;
+      {
+        float e0[8], e1[8], c[8], d[8];
+        exps2<8>(pa, q0, q1, qmin, e0, e1, c);
+        contract2<8>(c, e0, e1, rA0, rA1);
+#pragma unroll
+        for (int k = 0; k < 8; ++k) d[k] = pa[8 + k].y;   // second s shell: same exponents
+        contract2<8>(d, e0, e1, rB0, rB1);
+      }
+      float rC0, rC1, rD0, rD1, rE0, rE1, rF0, rF1;
+      {
+        float e0[1], e1[1], c[1];
+        exps2<1>(pa + 16, q0, q1, qmin, e0, e1, c);
+        contract2<1>(c, e0, e1, rC0, rC1);
+      }
+      {
+        float e0[3], e1[3], c[3];
+        exps2<3>(pa + 17, q0, q1, qmin, e0, e1, c);
+        contract2<3>(c, e0, e1, rD0, rD1);
+      }
+      {
+        float e0[1], e1[1], c[1];
+        exps2<1>(pa + 20, q0, q1, qmin, e0, e1, c);
+        contract2<1>(c, e0, e1, rE0, rE1);
+        exps2<1>(pa + 21, q0, q1, qmin, e0, e1, c);
+        contract2<1>(c, e0, e1, rF0, rF1);
+      }
+      if (!ok0) rA0 = rB0 = rC0 = rD0 = rE0 = rF0 = 0.f;
+      if (!ok1) rA1 = rB1 = rC1 = rD1 = rE1 = rF1 = 0.f;
+      shell_vals<0>(0, rA0, rA1, x0, y0, z0, x1, y1, z1, s_0, s_1);
+      out.put(f0, 1, s_0, s_1);
+      shell_vals<0>(0, rB0, rB1, x0, y0, z0, x1, y1, z1, s_0, s_1);
+      out.put(f0 + 1, 1, s_0, s_1);
+      shell_vals<0>(0, rC0, rC1, x0, y0, z0, x1, y1, z1, s_0, s_1);
+      out.put(f0 + 2, 1, s_0, s_1);
+      shell_vals<1>(1, rD0, rD1, x0, y0, z0, x1, y1, z1, p_0, p_1);
+      out.put(f0 + 3, 3, p_0, p_1);
+      shell_vals<1>(1, rE0, rE1, x0, y0, z0, x1, y1, z1, p_0, p_1);
+      out.put(f0 + 6, 3, p_0, p_1);
+      float d_0[5], d_1[5];
+      shell_vals<2>(2, rF0, rF1, x0, y0, z0, x1, y1, z1, d_0, d_1);
+      out.put(f0 + 9, 5, d_0, d_1);
+      flast = f0 + 13;
+    }
+  }
+  for (int sidx = shape != SHAPE_GENERIC ? s1 : s0; sidx < s1; ++sidx) {
+    const int4 rec = sh_s[sidx];   // prim, func, L | nprim << 8 | same_exp << 16 | next_same << 24, next prim
+    const int L = rec.z & 0xff, np_ = (rec.z >> 8) & 0xff, f0 = rec.y;
+    float rad0, rad1;
+    if (rec.z & 0x10000) {
+      rad0 = nx0;
+      rad1 = nx1;
+    } else {
+      int sk = 0;
+      while (sk < np_ && pr_s[rec.x + sk].x * qmin >= kExpCut) ++sk;
+      const float2* pa = pr_s + rec.x + sk;
+      const float2* pn = (rec.z >> 24) ? pr_s + rec.w + sk : nullptr;
+      switch (np_ - sk) {
+        case 0:
+          rad0 = rad1 = 0.f;
+          nx0 = nx1 = 0.f;
+          break;
+        case 1: radial_np<1>(pa, pn, q0, q1, rad0, rad1, nx0, nx1); break;
+        case 2: radial_np<2>(pa, pn, q0, q1, rad0, rad1, nx0, nx1); break;
+        case 3: radial_np<3>(pa, pn, q0, q1, rad0, rad1, nx0, nx1); break;
+        case 4: radial_np<4>(pa, pn, q0, q1, rad0, rad1, nx0, nx1); break;
+        case 5: radial_np<5>(pa, pn, q0, q1, rad0, rad1, nx0, nx1); break;
+        case 6: radial_np<6>(pa, pn, q0, q1, rad0, rad1, nx0, nx1); break;
+        case 7: radial_np<7>(pa, pn, q0, q1, rad0, rad1, nx0, nx1); break;
+        case 8: radial_np<8>(pa, pn, q0, q1, rad0, rad1, nx0, nx1); break;
+        default:
+          rad0 = 0.f;
+          rad1 = 0.f;
+          for (int k = 0; k < np_ - sk; ++k) {
+            const float2 ac = pa[k];
+            const float a0 = ac.x * q0, a1 = ac.x * q1;
+            rad0 = fmaf(ac.y, a0 < kExpCut ? expf(-a0) : 0.f, rad0);
+            rad1 = fmaf(ac.y, a1 < kExpCut ? expf(-a1) : 0.f, rad1);
+          }
+      }
+    }
+    if (!ok0) rad0 = 0.f;
+    if (!ok1) rad1 = 0.f;
+    float v0[5], v1[5];
+    shell_vals<-1>(L, rad0, rad1, x0, y0, z0, x1, y1, z1, v0, v1);
+    const int nf = 2 * L + 1;
+    flast = f0 + nf - 1;
+    out.put(f0, nf, v0, v1);
+  }
+  return flast;
+}
+
+// ---------------------------------------------------------------------------------------
+// Staged path, stage 1: Phi' of 128-row tiles into operand pieces in HBM.
+//
+// Persistent CTAs take whole tiles; a tile is produced in windows of STAGE_W columns.  Per
+// window the warps take (atom, row half) items of the atoms with functions in the window from
+// a shared counter and write FP32 values into the window buffer (atom_rows, the producer of
+// the fused kernel); then the CTA converts the window to hi = fmt(Phi'), lo = fmt(Phi' - hi)
+// and writes it with coalesced stores to the row-major [row][kpad] pieces.  Padding columns
+// (>= norbs) and rows without a point are zero.
+// ---------------------------------------------------------------------------------------
+struct StageParams {
+  PointMap pm;
+  int64_t tile0;           // first tile of this chunk
+  int ntiles;              // tiles of this chunk
+  int kpad, norbs, nwin;   // nwin = ceil(kpad / STAGE_W)
+  const int4* tab;         // molecule tables (ensure_mol_tables)
+  const float* coords;     // nuclear coordinates, 3 per atom
+  int ncoords;             // 3 * natoms
+  const int2* win;         // atoms [x, y) with functions in each window
+  int tab_words;           // 16-byte words of shell records, primitive pairs and atom words
+  int off_prim, off_ashell, off_coords;   // byte offsets of the tables
+  int tab_bytes;           // shared-memory bytes of the staged tables (0: read from global memory)
+  void* out_hi;
+  void* out_lo;
+  int two;
+};
+
+constexpr int STAGE_THREADS = 256;
+
+template <int FMT>
+__device__ __forceinline__ void split_store2(float x0, float x1, void* hi, void* lo, int64_t idx, bool two) {
+  if constexpr (FMT == FMT_TF32) {
+    const uint32_t h0 = tf32_round_bits(x0), h1 = tf32_round_bits(x1);
+    reinterpret_cast<uint2*>(reinterpret_cast<uint32_t*>(hi) + idx)[0] = make_uint2(h0, h1);
+    if (two)
+      reinterpret_cast<uint2*>(reinterpret_cast<uint32_t*>(lo) + idx)[0] =
+          make_uint2(tf32_round_bits(x0 - bits_f32(h0)), tf32_round_bits(x1 - bits_f32(h1)));
+  } else if constexpr (FMT == FMT_F16) {
+    const __half2 h = __floats2half2_rn(x0, x1);
+    reinterpret_cast<__half2*>(reinterpret_cast<__half*>(hi) + idx)[0] = h;
+    if (two) {
+      const float2 hf = __half22float2(h);
+      reinterpret_cast<__half2*>(reinterpret_cast<__half*>(lo) + idx)[0] = __floats2half2_rn(x0 - hf.x, x1 - hf.y);
+    }
+  } else {
+    const __nv_bfloat162 h = __floats2bfloat162_rn(x0, x1);
+    reinterpret_cast<__nv_bfloat162*>(reinterpret_cast<__nv_bfloat16*>(hi) + idx)[0] = h;
+    if (two) {
+      const float2 hf = __bfloat1622float2(h);
+      reinterpret_cast<__nv_bfloat162*>(reinterpret_cast<__nv_bfloat16*>(lo) + idx)[0] =
+          __floats2bfloat162_rn(x0 - hf.x, x1 - hf.y);
+    }
+  }
+}
+
+template <int FMT>
+__global__ void __launch_bounds__(STAGE_THREADS, 2) basis_window_kernel(const StageParams p) {
+  extern __shared__ __align__(16) uint8_t smem_dyn[];
+  __shared__ double pos[128][3];
+  __shared__ int item_ctr;
+  const int lane = threadIdx.x & 31;
+  const bool two = p.two != 0;
+  float* buf = reinterpret_cast<float*>(smem_dyn + p.tab_bytes);   // [128][STAGE_LD]
+  const int4* sh_s;
+  const float2* pr_s;
+  const int* ash_s;
+  const float* crd_s;
+  if (p.tab_bytes > 0) {
+    for (int i = threadIdx.x; i < p.tab_words; i += blockDim.x) reinterpret_cast<int4*>(smem_dyn)[i] = __ldg(p.tab + i);
+    for (int i = threadIdx.x; i < p.ncoords; i += blockDim.x)
+      reinterpret_cast<float*>(smem_dyn + p.off_coords)[i] = __ldg(p.coords + i);
+    sh_s = reinterpret_cast<const int4*>(smem_dyn);
+    pr_s = reinterpret_cast<const float2*>(smem_dyn + p.off_prim);
+    ash_s = reinterpret_cast<const int*>(smem_dyn + p.off_ashell);
+    crd_s = reinterpret_cast<const float*>(smem_dyn + p.off_coords);
+  } else {
+    const uint8_t* g = reinterpret_cast<const uint8_t*>(p.tab);
+    sh_s = p.tab;
+    pr_s = reinterpret_cast<const float2*>(g + p.off_prim);
+    ash_s = reinterpret_cast<const int*>(g + p.off_ashell);
+    crd_s = p.coords;
+  }
+  for (int t = blockIdx.x; t < p.ntiles; t += gridDim.x) {
+    // positions: every reader of the previous tile's positions passed the barrier that ends
+    // the last window's production
+    if (threadIdx.x < 128) {
+      double x, y, z;
+      int64_t vox;
+      if (!tile_point<double>(p.pm, p.tile0 + t, threadIdx.x, x, y, z, vox)) x = y = z = 1e30;
+      pos[threadIdx.x][0] = x;
+      pos[threadIdx.x][1] = y;
+      pos[threadIdx.x][2] = z;
+    }
+    for (int w = 0; w < p.nwin; ++w) {
+      if (threadIdx.x == 0) item_ctr = 0;
+      __syncthreads();   // positions and tables ready, window buffer free, counter reset
+      const int2 ar = __ldg(p.win + w);
+      const int c0 = w * STAGE_W;
+      const int nitems = 2 * (ar.y - ar.x);
+      for (;;) {
+        int itm = 0;
+        if (lane == 0) itm = atomicAdd(&item_ctr, 1);
+        itm = __shfl_sync(0xffffffffu, itm, 0);
+        if (itm >= nitems) break;
+        const int a = ar.x + (itm >> 1);
+        if ((ash_s[a + 1] & 0xffffff) <= (ash_s[a] & 0xffffff)) continue;
+        const int r0 = (itm & 1) * 32 + lane;
+        atom_rows(sh_s, pr_s, ash_s, crd_s, a, pos, r0,
+                  WindowRowsOut{buf + r0 * STAGE_LD, buf + (r0 + 64) * STAGE_LD, c0, pos[r0][0] < 1e29,
+                                pos[r0 + 64][0] < 1e29});
+      }
+      __syncthreads();
+      // write-out: a warp covers 64 consecutive columns of a row (two per lane)
+      const int ncol = min(STAGE_W, p.kpad - c0);   // 128 or 64
+      const int nval = p.norbs - c0;                // columns beyond hold padding zeros
+      const int lp = ncol == STAGE_W ? 6 : 5;       // log2(column pairs per row)
+      const int64_t rowbase = (int64_t)t * 128;
+      for (int i = threadIdx.x; i < (128 << lp); i += blockDim.x) {
+        const int r = i >> lp, c = (i & ((1 << lp) - 1)) * 2;
+        const float v0 = c < nval ? buf[r * STAGE_LD + c] : 0.f;
+        const float v1 = c + 1 < nval ? buf[r * STAGE_LD + c + 1] : 0.f;
+        split_store2<FMT>(v0, v1, p.out_hi, p.out_lo, (rowbase + r) * p.kpad + c0 + c, two);
+      }
     }
   }
 }
@@ -1031,166 +1197,10 @@ __global__ void __launch_bounds__(FUSED_THREADS, 1)
         itm = __shfl_sync(0xffffffffu, itm, 0);
         if (itm >= 2 * mol.natoms) break;
         const int a = itm >> 1;
-        const int as0 = ash_s[a];
-        const int s0 = as0 & 0xffffff, s1 = ash_s[a + 1] & 0xffffff, shape = as0 >> 24;
-        if (s1 <= s0) continue;
-        const int r0 = (itm & 1) * 32 + lane, r1 = r0 + 64;   // r1 sits 8192 B after r0 in A
-        const double ax = crd_s[3 * a], ay = crd_s[3 * a + 1], az = crd_s[3 * a + 2];
-        const bool ok0 = pos[r0][0] < 1e29, ok1 = pos[r1][0] < 1e29;
-        // FP64 displacement from the nucleus, rounded once (accuracy of steep exponents)
-        const float x0 = (float)(pos[r0][0] - ax), y0 = (float)(pos[r0][1] - ay), z0 = (float)(pos[r0][2] - az);
-        const float x1 = (float)(pos[r1][0] - ax), y1 = (float)(pos[r1][1] - ay), z1 = (float)(pos[r1][2] - az);
-        const float q0 = x0 * x0 + y0 * y0 + z0 * z0, q1 = x1 * x1 + y1 * y1 + z1 * z1;
-        // primitives with alpha * min_rows(r^2) >= the cut-off are zero at every row of the item:
-        // with exponents in descending order they are the leading ones of a shell and are skipped
-        // (the remaining terms are summed in the same order, so the result is unchanged)
-        float qmin = fminf(q0, q1);
-#pragma unroll
-        for (int o = 16; o > 0; o >>= 1) qmin = fminf(qmin, __shfl_xor_sync(0xffffffffu, qmin, o));
-        float nx0 = 0.f, nx1 = 0.f;   // radial parts of the next shell when it shares the exponents
-        int flast = 0;
-        if (shape != SHAPE_GENERIC) {
-          const int4 rec0 = sh_s[s0];
-          const float2* pa = pr_s + rec0.x;
-          const int f0 = rec0.y;
-          float rA0, rA1;
-          if (shape == SHAPE_S3S1P1) {
-            {
-              float e0[3], e1[3], c[3];
-              exps2<3>(pa, q0, q1, qmin, e0, e1, c);
-              contract2<3>(c, e0, e1, rA0, rA1);
-            }
-            float rB0, rB1, rC0, rC1;
-            {
-              float e0[1], e1[1], c[1];
-              exps2<1>(pa + 3, q0, q1, qmin, e0, e1, c);
-              contract2<1>(c, e0, e1, rB0, rB1);
-              exps2<1>(pa + 4, q0, q1, qmin, e0, e1, c);
-              contract2<1>(c, e0, e1, rC0, rC1);
-            }
-            if (!ok0) rA0 = rB0 = rC0 = 0.f;
-            if (!ok1) rA1 = rB1 = rC1 = 0.f;
-            shell_out<FMT, 0>(rA0, rA1, x0, y0, z0, x1, y1, z1, f0, r0, A_hi, A_lo, two);
-            shell_out<FMT, 0>(rB0, rB1, x0, y0, z0, x1, y1, z1, f0 + 1, r0, A_hi, A_lo, two);
-            shell_out<FMT, 1>(rC0, rC1, x0, y0, z0, x1, y1, z1, f0 + 2, r0, A_hi, A_lo, two);
-            flast = f0 + 4;
-          } else {
-            float rB0, rB1;
-            {
-              float e0[8], e1[8], c[8], d[8];
-              exps2<8>(pa, q0, q1, qmin, e0, e1, c);
-              contract2<8>(c, e0, e1, rA0, rA1);
-#pragma unroll
-              for (int k = 0; k < 8; ++k) d[k] = pa[8 + k].y;   // second s shell: same exponents
-              contract2<8>(d, e0, e1, rB0, rB1);
-            }
-            float rC0, rC1, rD0, rD1, rE0, rE1, rF0, rF1;
-            {
-              float e0[1], e1[1], c[1];
-              exps2<1>(pa + 16, q0, q1, qmin, e0, e1, c);
-              contract2<1>(c, e0, e1, rC0, rC1);
-            }
-            {
-              float e0[3], e1[3], c[3];
-              exps2<3>(pa + 17, q0, q1, qmin, e0, e1, c);
-              contract2<3>(c, e0, e1, rD0, rD1);
-            }
-            {
-              float e0[1], e1[1], c[1];
-              exps2<1>(pa + 20, q0, q1, qmin, e0, e1, c);
-              contract2<1>(c, e0, e1, rE0, rE1);
-              exps2<1>(pa + 21, q0, q1, qmin, e0, e1, c);
-              contract2<1>(c, e0, e1, rF0, rF1);
-            }
-            if (!ok0) rA0 = rB0 = rC0 = rD0 = rE0 = rF0 = 0.f;
-            if (!ok1) rA1 = rB1 = rC1 = rD1 = rE1 = rF1 = 0.f;
-            shell_out<FMT, 0>(rA0, rA1, x0, y0, z0, x1, y1, z1, f0, r0, A_hi, A_lo, two);
-            shell_out<FMT, 0>(rB0, rB1, x0, y0, z0, x1, y1, z1, f0 + 1, r0, A_hi, A_lo, two);
-            shell_out<FMT, 0>(rC0, rC1, x0, y0, z0, x1, y1, z1, f0 + 2, r0, A_hi, A_lo, two);
-            shell_out<FMT, 1>(rD0, rD1, x0, y0, z0, x1, y1, z1, f0 + 3, r0, A_hi, A_lo, two);
-            shell_out<FMT, 1>(rE0, rE1, x0, y0, z0, x1, y1, z1, f0 + 6, r0, A_hi, A_lo, two);
-            shell_out<FMT, 2>(rF0, rF1, x0, y0, z0, x1, y1, z1, f0 + 9, r0, A_hi, A_lo, two);
-            flast = f0 + 13;
-          }
-        }
-        for (int sidx = shape != SHAPE_GENERIC ? s1 : s0; sidx < s1; ++sidx) {
-          const int4 rec = sh_s[sidx];   // prim, func, L | nprim << 8 | same_exp << 16 | next_same << 24, next prim
-          const int L = rec.z & 0xff, np_ = (rec.z >> 8) & 0xff, f0 = rec.y;
-          float rad0, rad1;
-          if (rec.z & 0x10000) {
-            rad0 = nx0;
-            rad1 = nx1;
-          } else {
-            int sk = 0;
-            while (sk < np_ && pr_s[rec.x + sk].x * qmin >= kExpCut) ++sk;
-            const float2* pa = pr_s + rec.x + sk;
-            const float2* pn = (rec.z >> 24) ? pr_s + rec.w + sk : nullptr;
-            switch (np_ - sk) {
-              case 0:
-                rad0 = rad1 = 0.f;
-                nx0 = nx1 = 0.f;
-                break;
-              case 1: radial_np<1>(pa, pn, q0, q1, rad0, rad1, nx0, nx1); break;
-              case 2: radial_np<2>(pa, pn, q0, q1, rad0, rad1, nx0, nx1); break;
-              case 3: radial_np<3>(pa, pn, q0, q1, rad0, rad1, nx0, nx1); break;
-              case 4: radial_np<4>(pa, pn, q0, q1, rad0, rad1, nx0, nx1); break;
-              case 5: radial_np<5>(pa, pn, q0, q1, rad0, rad1, nx0, nx1); break;
-              case 6: radial_np<6>(pa, pn, q0, q1, rad0, rad1, nx0, nx1); break;
-              case 7: radial_np<7>(pa, pn, q0, q1, rad0, rad1, nx0, nx1); break;
-              case 8: radial_np<8>(pa, pn, q0, q1, rad0, rad1, nx0, nx1); break;
-              default:
-                rad0 = 0.f;
-                rad1 = 0.f;
-                for (int k = 0; k < np_ - sk; ++k) {
-                  const float2 ac = pa[k];
-                  const float a0 = ac.x * q0, a1 = ac.x * q1;
-                  rad0 = fmaf(ac.y, a0 < kExpCut ? expf(-a0) : 0.f, rad0);
-                  rad1 = fmaf(ac.y, a1 < kExpCut ? expf(-a1) : 0.f, rad1);
-                }
-            }
-          }
-          if (!ok0) rad0 = 0.f;
-          if (!ok1) rad1 = 0.f;
-          float v0[5], v1[5];
-          if (L == 0) {
-            v0[0] = (float)YS * rad0;
-            v1[0] = (float)YS * rad1;
-          } else if (L == 1) {
-            const float c0 = (float)YP * rad0, c1 = (float)YP * rad1;
-            v0[0] = c0 * z0; v0[1] = c0 * x0; v0[2] = c0 * y0;
-            v1[0] = c1 * z1; v1[1] = c1 * x1; v1[2] = c1 * y1;
-          } else {
-            const float c0 = (float)YD1 * rad0, c1 = (float)YD1 * rad1;
-            v0[0] = (float)YD0 * rad0 * (2.f * z0 * z0 - x0 * x0 - y0 * y0);
-            v0[1] = c0 * x0 * z0; v0[2] = c0 * z0 * y0;
-            v0[3] = (float)YD2 * rad0 * (x0 * x0 - y0 * y0); v0[4] = c0 * x0 * y0;
-            v1[0] = (float)YD0 * rad1 * (2.f * z1 * z1 - x1 * x1 - y1 * y1);
-            v1[1] = c1 * x1 * z1; v1[2] = c1 * z1 * y1;
-            v1[3] = (float)YD2 * rad1 * (x1 * x1 - y1 * y1); v1[4] = c1 * x1 * y1;
-          }
-          const int nf = 2 * L + 1;
-          flast = f0 + nf - 1;
-          bool skip = false;   // the function was stored with its predecessor
-#pragma unroll
-          for (int k = 0; k < 5; ++k) {
-            if (k >= nf) break;
-            if (skip) {
-              skip = false;
-              continue;
-            }
-            const int j = f0 + k;
-            const uint32_t off = a_offset(r0, j);
-            // two consecutive functions in the same 16-byte unit: one 4-byte store per piece
-            if (k + 1 < nf && (j & 1) == 0) {
-              store_pair16<FMT>(A_hi, A_lo, off, v0[k], v0[k + 1], two);
-              store_pair16<FMT>(A_hi, A_lo, off + 8192u, v1[k], v1[k + 1], two);
-              skip = true;
-            } else {
-              store_split16<FMT>(A_hi, A_lo, off, v0[k], two);
-              store_split16<FMT>(A_hi, A_lo, off + 8192u, v1[k], two);
-            }
-          }
-        }
+        const int s0 = ash_s[a] & 0xffffff;
+        if ((ash_s[a + 1] & 0xffffff) <= s0) continue;
+        const int flast = atom_rows(sh_s, pr_s, ash_s, crd_s, a, pos, (itm & 1) * 32 + lane,
+                                    SwizzledRowsOut<FMT>{A_hi, A_lo, (itm & 1) * 32 + lane, two});
         // publish: generic-proxy writes of A become visible to the tensor core, then one arrival
         // per column chunk this atom wrote
         asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
@@ -1284,6 +1294,95 @@ static qmt_status make_map_sw32(CUtensorMap* m, const void* base, uint64_t inner
   return QMT_OK;
 }
 
+// Molecule tables of the producers (fused and staging kernels), in 16-byte words:
+//   shell records {prim, func, L | nprim << 8 | same_exp << 16 | next_same << 24, next shell's
+//   prim}; (alpha, coefficient x column scale) pairs, descending alpha within a shell; per-atom
+//   words (first shell | layout << 24), natoms + 1 of them; then, per STAGE_W-column window of
+//   the kpad columns, the atoms [first, end) with a function in the window (int2).
+struct MolTabLayout {
+  int off_prim, off_ashell;   // byte offsets
+  int words;                  // words up to and including the atom words
+  int off_win;                // word index of the window ranges
+  int nwin, total_words;
+};
+
+static MolTabLayout mol_tab_layout(const qmt_mol* m, int K) {
+  MolTabLayout l{};
+  const int nsh = (int)m->shells.size(), npr = (int)m->alpha.size();
+  l.off_prim = nsh * 16;
+  l.off_ashell = (nsh + (npr + 1) / 2) * 16;
+  l.words = l.off_ashell / 16 + (m->natoms + 1 + 3) / 4;
+  l.off_win = l.words;
+  l.nwin = (K + STAGE_W - 1) / STAGE_W;
+  l.total_words = l.off_win + (l.nwin + 1) / 2;
+  return l;
+}
+
+static qmt_status ensure_mol_tables(qmt_mol* m, const std::vector<float>& fs, int K, cudaStream_t s) {
+  const MolTabLayout lay = mol_tab_layout(m, K);
+  const size_t nsh = m->shells.size();
+  std::vector<int4> tab(lay.total_words, make_int4(0, 0, 0, 0));
+  for (size_t i = 0; i < nsh; ++i) {
+    const Shell& a = m->shells[i];
+    if (a.nprim > 255 || a.L > 255) return fail(QMT_BAD_ARG, "shell too large for the density tables");
+    const bool nxt = i + 1 < nsh && m->shells[i + 1].same_exp;
+    tab[i] = make_int4(a.prim, a.func, a.L | (a.nprim << 8) | (a.same_exp << 16) | ((int)nxt << 24),
+                       nxt ? m->shells[i + 1].prim : 0);
+  }
+  // every function of a shell shares the shell's bound, hence its scale: fold it into the
+  // contraction coefficients (exact, powers of two).  Primitives of a shell in descending
+  // exponent order (the kernels skip the leading ones that vanish on a whole work item);
+  // basis files normally list them that way already.
+  float2* pt = reinterpret_cast<float2*>(tab.data() + nsh);
+  for (const Shell& shl : m->shells) {
+    for (int k = 0; k < shl.nprim; ++k)
+      pt[shl.prim + k] = make_float2(m->alpha[shl.prim + k], m->coeff[shl.prim + k] * fs[shl.func]);
+    std::stable_sort(pt + shl.prim, pt + shl.prim + shl.nprim,
+                     [](const float2& u, const float2& v) { return u.x > v.x; });
+  }
+  // per-atom words: first shell, and the atom's layout when it is one of the unrolled ones
+  int* aw = reinterpret_cast<int*>(tab.data() + lay.off_ashell / 16);
+  auto is = [&](int sidx, int L, int np, int same) {
+    const Shell& x = m->shells[sidx];
+    return x.L == L && x.nprim == np && x.same_exp == same;
+  };
+  for (int a = 0; a <= m->natoms; ++a) {
+    const int sa = m->atom_shell[a];
+    int shape = SHAPE_GENERIC;
+    if (a < m->natoms) {
+      const int ns = m->atom_shell[a + 1] - sa;
+      if (ns == 3 && is(sa, 0, 3, 0) && is(sa + 1, 0, 1, 0) && is(sa + 2, 1, 1, 0)) shape = SHAPE_S3S1P1;
+      if (ns == 6 && is(sa, 0, 8, 0) && is(sa + 1, 0, 8, 1) && is(sa + 2, 0, 1, 0) && is(sa + 3, 1, 3, 0) &&
+          is(sa + 4, 1, 1, 0) && is(sa + 5, 2, 1, 0))
+        shape = SHAPE_S8S8S1P3P1D1;
+    }
+    if (sa >= (1 << 24)) return fail(QMT_BAD_ARG, "too many shells for the density tables");
+    aw[a] = sa | (shape << 24);
+  }
+  // staging windows: atoms whose functions [first, last] meet [c0, c0 + STAGE_W)
+  int2* wr = reinterpret_cast<int2*>(tab.data() + lay.off_win);
+  for (int w = 0; w < lay.nwin; ++w) {
+    const int c0 = w * STAGE_W, c1 = c0 + STAGE_W;
+    int first = m->natoms, end = 0;
+    for (int a = 0; a < m->natoms; ++a) {
+      const int sa = m->atom_shell[a], sb = m->atom_shell[a + 1];
+      if (sb <= sa) continue;
+      const Shell& last = m->shells[sb - 1];
+      const int f0 = m->shells[sa].func, f1 = last.func + 2 * last.L;
+      if (f1 >= c0 && f0 < c1) {
+        first = std::min(first, a);
+        end = a + 1;
+      }
+    }
+    wr[w] = first < end ? make_int2(first, end) : make_int2(0, 0);
+  }
+  qmt_status st;
+  if ((st = m->d_fused_tab.reserve(tab.size() * sizeof(int4)))) return st;
+  // pageable uploads return once the data is staged, so the host vectors may go
+  QMT_CUDA(cudaMemcpyAsync(m->d_fused_tab.ptr, tab.data(), tab.size() * sizeof(int4), cudaMemcpyHostToDevice, s));
+  return QMT_OK;
+}
+
 // Upper-triangular scaled density matrix for the fused path: row n (output column) holds
 // U_jn for j <= n, i.e. Ptilde_jn for j < n and Ptilde_nn / 2 on the diagonal.  Rows are
 // padded to kpad + 64 so every 64-row TMA box stays inside the tensor.
@@ -1292,7 +1391,7 @@ static int g_fused_tri = 0;   // upper-triangular variant of the fused path (off
 static qmt_status ensure_fused_operands(qmt_mol* m, int prec, const TcShape& sh, cudaStream_t s) {
   const int key = prec * 2 + g_fused_tri;
   if (m->fused_prec == key) return QMT_OK;
-  const int n = m->norbs, np = m->npad, K = sh.kpad;
+  const int n = m->norbs, K = sh.kpad;
   std::vector<int> sj(K, 0);
   std::vector<float> fs(K, 0.f);
   for (int j = 0; j < n; ++j) {
@@ -1309,51 +1408,7 @@ static qmt_status ensure_fused_operands(qmt_mol* m, int prec, const TcShape& sh,
   if ((st = launch_split(m, K, g, g_fused_tri, sh.fmt, m->d_fused_B.ptr, m->d_fused_B.as<uint8_t>() + piece, piece,
                          s)))
     return st;
-  // every function of a shell shares the shell's bound, hence its scale: fold it into the
-  // contraction coefficients (exact, powers of two)
-  // Shell records {prim, func, L | nprim << 8 | same_exp << 16 | next_same << 24, next shell's
-  // prim}, then one (alpha, coefficient x scale) pair per primitive.
-  const size_t nsh = m->shells.size(), npr = m->alpha.size();
-  const size_t atoms_off = nsh + (npr + 1) / 2;   // int4 index of the per-atom words
-  std::vector<int4> tab(atoms_off + (m->natoms + 1 + 3) / 4, make_int4(0, 0, 0, 0));
-  for (size_t i = 0; i < nsh; ++i) {
-    const Shell& a = m->shells[i];
-    if (a.nprim > 255 || a.L > 255) return fail(QMT_BAD_ARG, "shell too large for the fused density tables");
-    const bool nxt = i + 1 < nsh && m->shells[i + 1].same_exp;
-    tab[i] = make_int4(a.prim, a.func, a.L | (a.nprim << 8) | (a.same_exp << 16) | ((int)nxt << 24),
-                       nxt ? m->shells[i + 1].prim : 0);
-  }
-  // primitives of a shell in descending exponent order (the kernel skips the leading ones that
-  // vanish on a whole work item); basis files normally list them that way already
-  float2* pt = reinterpret_cast<float2*>(tab.data() + nsh);
-  for (const Shell& shl : m->shells) {
-    for (int k = 0; k < shl.nprim; ++k)
-      pt[shl.prim + k] = make_float2(m->alpha[shl.prim + k], m->coeff[shl.prim + k] * fs[shl.func]);
-    std::stable_sort(pt + shl.prim, pt + shl.prim + shl.nprim,
-                     [](const float2& u, const float2& v) { return u.x > v.x; });
-  }
-  // per-atom words: first shell, and the atom's layout when it is one of the unrolled ones
-  int* aw = reinterpret_cast<int*>(tab.data() + atoms_off);
-  auto is = [&](int sidx, int L, int np, int same) {
-    const Shell& x = m->shells[sidx];
-    return x.L == L && x.nprim == np && x.same_exp == same;
-  };
-  for (int a = 0; a <= m->natoms; ++a) {
-    const int sa = m->atom_shell[a];
-    int shape = SHAPE_GENERIC;
-    if (a < m->natoms) {
-      const int ns = m->atom_shell[a + 1] - sa;
-      if (ns == 3 && is(sa, 0, 3, 0) && is(sa + 1, 0, 1, 0) && is(sa + 2, 1, 1, 0)) shape = SHAPE_S3S1P1;
-      if (ns == 6 && is(sa, 0, 8, 0) && is(sa + 1, 0, 8, 1) && is(sa + 2, 0, 1, 0) && is(sa + 3, 1, 3, 0) &&
-          is(sa + 4, 1, 1, 0) && is(sa + 5, 2, 1, 0))
-        shape = SHAPE_S8S8S1P3P1D1;
-    }
-    if (sa >= (1 << 24)) return fail(QMT_BAD_ARG, "too many shells for the fused density tables");
-    aw[a] = sa | (shape << 24);
-  }
-  if ((st = m->d_fused_tab.reserve(tab.size() * sizeof(int4)))) return st;
-  // pageable uploads return once the data is staged, so the host vectors may go
-  QMT_CUDA(cudaMemcpyAsync(m->d_fused_tab.ptr, tab.data(), tab.size() * sizeof(int4), cudaMemcpyHostToDevice, s));
+  if ((st = ensure_mol_tables(m, fs, K, s))) return st;
   m->fused_g = g;
   m->fused_prec = key;
   return QMT_OK;
@@ -1432,6 +1487,131 @@ static qmt_status run_fused(qmt_mol* m, const TcShape& sh, const PointMap& pm, i
   const int grid = (int)std::min<int64_t>(ntiles, sm_count());
   kern<<<grid, FUSED_THREADS, dyn, s>>>(tU_hi, tU_lo, p);
   QMT_CHECK_LAUNCH("density_fused_kernel");
+  return QMT_OK;
+}
+
+// Builds the scaled, split density matrix and the Phi column scales for `prec`.
+static qmt_status ensure_tc_operands(qmt_mol* m, int prec, const TcShape& sh, cudaStream_t s) {
+  if (m->tc_prec == prec) return QMT_OK;
+  const int n = m->norbs, K = sh.kpad;
+  std::vector<int> sj(K, 0);
+  std::vector<float> fs(K, 0.f);
+  for (int j = 0; j < n; ++j) {
+    const double b = std::max(m->fbound[j], 1e-30);
+    sj[j] = (int)std::floor(std::log2(16000.0 / b));
+    sj[j] = std::max(-60, std::min(60, sj[j]));
+    fs[j] = (float)std::ldexp(1.0, sj[j]);
+  }
+  int g = 0;
+  qmt_status st = split_scales(m, sj, K, &g, s);
+  if (st) return st;
+  const size_t piece = (size_t)sh.nrows_b * K * sh.esize;
+  if ((st = m->d_tc_P.reserve(2 * piece))) return st;
+  if ((st = ensure_mol_tables(m, fs, K, s))) return st;
+  if ((st = launch_split(m, K, g, 0, sh.fmt, m->d_tc_P.ptr, m->d_tc_P.as<uint8_t>() + piece, piece, s))) return st;
+  m->tc_g = g;
+  m->tc_prec = prec;
+  return QMT_OK;
+}
+
+template <int FMT>
+static qmt_status run_tc(qmt_mol* m, const TcShape& sh, const PointMap& pm, int64_t ntiles, int prec,
+                         float* qube, double outscale, cudaStream_t s) {
+  qmt_status st;
+  const size_t tile_bytes = (size_t)128 * sh.kpad * sh.esize;
+  const int nsm = sm_count();
+  // staging chunk: bounded to ~2 GiB, a multiple of the SM count when larger than one wave
+  int64_t chunk = std::max<int64_t>(1, ((size_t)2 << 30) / (tile_bytes * sh.nsplit));
+  if (chunk > nsm) chunk = chunk / nsm * nsm;
+  chunk = std::min<int64_t>(chunk, ntiles);
+  if ((st = m->d_Phi_hi.reserve(chunk * tile_bytes))) return st;
+  if (sh.nsplit == 2 && (st = m->d_Phi_lo.reserve(chunk * tile_bytes))) return st;
+  void* lo_ptr = sh.nsplit == 2 ? m->d_Phi_lo.ptr : m->d_Phi_hi.ptr;
+
+  CUtensorMap tA_hi, tA_lo, tB_hi, tB_lo;
+  const uint8_t* Pb = m->d_tc_P.as<uint8_t>();
+  const size_t piece = (size_t)sh.nrows_b * sh.kpad * sh.esize;
+  if ((st = make_map(&tA_hi, m->d_Phi_hi.ptr, sh.esize, sh.kpad, (uint64_t)chunk * 128, sh.ke, 128)) ||
+      (st = make_map(&tA_lo, lo_ptr, sh.esize, sh.kpad, (uint64_t)chunk * 128, sh.ke, 128)) ||
+      (st = make_map(&tB_hi, Pb, sh.esize, sh.kpad, sh.nrows_b, sh.ke, sh.pw)) ||
+      (st = make_map(&tB_lo, Pb + piece, sh.esize, sh.kpad, sh.nrows_b, sh.ke, sh.pw)))
+    return st;
+
+  TcParams p{};
+  p.pm = pm;
+  p.kpad = sh.kpad;
+  p.kchunks = sh.kpad / sh.ke;
+  p.npanels = sh.npanels;
+  p.pw = sh.pw;
+  p.nsplit = sh.nsplit;
+  p.esize = sh.esize;
+  p.a_bytes = 128u * 128u;
+  p.b_bytes = (uint32_t)sh.pw * 128u;
+  p.stage_bytes = sh.nsplit * (p.a_bytes + p.b_bytes);
+  p.tx_bytes = p.stage_bytes;
+  p.idesc = make_idesc((uint32_t)sh.fmt, 128, (uint32_t)sh.pw);
+  p.phi_hi = m->d_Phi_hi.ptr;
+  p.phi_lo = lo_ptr;
+  p.qube = qube;
+  p.partials = m->d_partials.as<double>();
+  p.outscale = outscale;
+  p.inv_g = std::ldexp(1.0, -m->tc_g);
+  p.err = reinterpret_cast<int*>(m->d_scalars.as<double>() + 8);
+
+  int maxsm = 0, dev = 0;
+  cudaGetDevice(&dev);
+  cudaDeviceGetAttribute(&maxsm, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev);
+  const int static_bytes = 4096;
+  int stages = (int)((maxsm - static_bytes - 1024) / p.stage_bytes);
+  stages = std::min(stages, MAX_STAGES);
+  if (stages < 2) return fail(QMT_BAD_ARG, "tensor-core stage does not fit in shared memory");
+  p.stages = stages;
+  const size_t dyn = (size_t)stages * p.stage_bytes + 1024;
+  auto kern = density_mma_kernel<FMT>;
+  QMT_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)dyn));
+
+  // staging kernel: molecule tables in shared memory unless they would keep two CTAs off an SM
+  const MolTabLayout lay = mol_tab_layout(m, sh.kpad);
+  StageParams sp{};
+  sp.pm = pm;
+  sp.kpad = sh.kpad;
+  sp.norbs = m->norbs;
+  sp.nwin = lay.nwin;
+  sp.tab = m->d_fused_tab.as<int4>();
+  sp.coords = m->d_coords.as<float>();
+  sp.ncoords = 3 * m->natoms;
+  sp.win = reinterpret_cast<const int2*>(sp.tab + lay.off_win);
+  sp.tab_words = lay.words;
+  sp.off_prim = lay.off_prim;
+  sp.off_ashell = lay.off_ashell;
+  sp.off_coords = lay.words * 16;
+  sp.tab_bytes = sp.off_coords + (3 * m->natoms + 3) / 4 * 16;
+  sp.out_hi = m->d_Phi_hi.ptr;
+  sp.out_lo = lo_ptr;
+  sp.two = sh.nsplit == 2;
+  const int buf_bytes = 128 * STAGE_LD * 4;
+  if (sp.tab_bytes + buf_bytes > (maxsm - 8192) / 2) sp.tab_bytes = 0;
+  const size_t sdyn = (size_t)sp.tab_bytes + buf_bytes;
+  auto skern = basis_window_kernel<FMT>;
+  QMT_CUDA(cudaFuncSetAttribute(skern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sdyn));
+  int stage_ctas = 0;
+  QMT_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&stage_ctas, skern, STAGE_THREADS, sdyn));
+  stage_ctas = std::max(1, stage_ctas);
+
+  for (int64_t t0 = 0; t0 < ntiles; t0 += chunk) {
+    const int nt = (int)std::min<int64_t>(chunk, ntiles - t0);
+    sp.tile0 = t0;
+    sp.ntiles = nt;
+    const int gb = (int)std::min<int64_t>(nt, (int64_t)nsm * stage_ctas);
+    skern<<<gb, STAGE_THREADS, sdyn, s>>>(sp);
+    QMT_CHECK_LAUNCH("basis_window_kernel");
+    p.tile0 = t0;
+    p.ntiles = nt;
+    const int gm = (int)std::min<int64_t>(nt, nsm);
+    kern<<<gm, 192, dyn, s>>>(tA_hi, tA_lo, tB_hi, tB_lo, p);
+    QMT_CHECK_LAUNCH("density_mma_kernel");
+  }
+  (void)prec;
   return QMT_OK;
 }
 

@@ -45,7 +45,6 @@ struct qmt_mol {
   int tc_prec = -1;             // precision the operands below were built for
   int tc_g = 0;                 // global exponent of the scaled density matrix
   qmt::DevBuf d_tc_P;           // split, scaled density matrix (hi then lo)
-  qmt::DevBuf d_fscale;         // per-function power-of-two scale of Phi
   qmt::DevBuf d_Phi_hi, d_Phi_lo;
   // scratch
   qmt::DevBuf d_partials, d_scalars, d_work;
