@@ -32,6 +32,7 @@ qmt_status make_point_map(int nx, int ny, int nz, float step, float ox, float oy
   pm.ox = ox;
   pm.oy = oy;
   pm.oz = oz;
+  pm.inv_s = 1.0 / subgrid;
   ntiles = (pm.nvox + pm.vpt - 1) / pm.vpt;
   return QMT_OK;
 }

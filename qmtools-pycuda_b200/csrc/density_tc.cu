@@ -499,12 +499,15 @@ struct FusedParams {
   PointMap pm;
   int64_t ntiles;
   int kpad, ksteps, nsplit, stages;
+  int n16;                 // functions rounded up to 16: K of the MMAs and N (output columns)
+  int full_cols;           // columns held in 64-column 128-byte swizzled chunks (n16 rounded down
+                           // to 64); the rest in 16-column 32-byte swizzled blocks
   int tri;                 // 1: upper-triangular U (half the work); 0: full symmetric P
-  int nchunks;             // kpad / 64 column chunks of A
-  int box_rows;            // rows of one U box: 64 (triangular), else kpad or kpad / 2 (<= 256)
+  int nchunks;             // ceil(n16 / 64) column chunks of A (the last may be the 16-column blocks)
+  int box_rows;            // rows of one U box: 64 (triangular), else n16 or n16 / 2 (<= 256)
   int chunk_need[MAX_FUSED_CHUNKS];  // production items (atom halves) writing each chunk
-  uint32_t a_bytes;        // one A piece: 128 rows x kpad x 2 B
-  uint32_t b_slot;         // one U piece slot in a stage: kpad rows x 32 B
+  uint32_t a_bytes;        // one A piece: 128 rows x n16 x 2 B
+  uint32_t b_slot;         // one U piece slot in a stage: n16 (triangular: kpad) rows x 32 B
   uint32_t stage_bytes;
   uint32_t fmt;
   const int4* tab;         // molecule tables (ensure_mol_tables)
@@ -520,12 +523,23 @@ struct FusedParams {
   int* err;
 };
 
-// Byte offset of element (row, j) in the 128-byte swizzled K-major A tile.
-__device__ __forceinline__ uint32_t a_offset(int row, int j) {
-  const int kc = j >> 6, e = j & 63;
-  const int u = (e >> 3) ^ (row & 7);
-  return (uint32_t)(kc * 16384 + (row >> 3) * 1024 + (row & 7) * 128 + u * 16 + (e & 7) * 2);
+// Byte offset of element (row, j) in the K-major A tile: columns below `full_cols` in 64-column
+// chunks with the 128-byte swizzle (8-row atoms of 1024 B, 16-byte unit u at u ^ (row & 7)),
+// the rest in 16-column blocks with the 32-byte swizzle (8-row atoms of 256 B, unit u at
+// u ^ ((row >> 2) & 1)), so that a tile holds n16 rather than kpad columns.
+__device__ __forceinline__ uint32_t a_offset(int row, int j, int full_cols) {
+  if (j < full_cols) {
+    const int kc = j >> 6, e = j & 63;
+    const int u = (e >> 3) ^ (row & 7);
+    return (uint32_t)(kc * 16384 + (row >> 3) * 1024 + (row & 7) * 128 + u * 16 + (e & 7) * 2);
+  }
+  const int t = j - full_cols, e = t & 15;
+  const int u = (e >> 3) ^ ((row >> 2) & 1);
+  return (uint32_t)(full_cols * 256 + (t >> 4) * 4096 + (row >> 3) * 256 + (row & 7) * 32 + u * 16 + (e & 7) * 2);
 }
+
+// Offset from row r to row r + 64 of the same column (the row's bits 0-2 are unchanged).
+__device__ __forceinline__ uint32_t a_row64(int j, int full_cols) { return j < full_cols ? 8192u : 2048u; }
 
 __device__ __forceinline__ uint64_t sw32_kmajor_desc(uint32_t saddr) {
   uint64_t d = 0;
@@ -704,6 +718,7 @@ struct SwizzledRowsOut {
   uint8_t* hi;
   uint8_t* lo;
   int r0;
+  int full_cols;
   bool two;
   template <int NF>
   __device__ __forceinline__ void put(int j0, int nf, const float (&v0)[NF], const float (&v1)[NF]) const {
@@ -716,15 +731,16 @@ struct SwizzledRowsOut {
         continue;
       }
       const int j = j0 + k;
-      const uint32_t off = a_offset(r0, j);
+      const uint32_t off = a_offset(r0, j, full_cols);
+      const uint32_t off1 = off + a_row64(j, full_cols);   // row r0 + 64
       // two consecutive functions in the same 16-byte unit: one 4-byte store per piece
       if (k + 1 < nf && (j & 1) == 0) {
         store_pair16<FMT>(hi, lo, off, v0[k], v0[k + 1], two);
-        store_pair16<FMT>(hi, lo, off + 8192u, v1[k], v1[k + 1], two);   // row r0 + 64
+        store_pair16<FMT>(hi, lo, off1, v1[k], v1[k + 1], two);
         skip = true;
       } else {
         store_split16<FMT>(hi, lo, off, v0[k], two);
-        store_split16<FMT>(hi, lo, off + 8192u, v1[k], two);
+        store_split16<FMT>(hi, lo, off1, v1[k], two);
       }
     }
   }
@@ -1106,8 +1122,8 @@ __global__ void __launch_bounds__(FUSED_THREADS, 1)
           }
           const int j0 = ks * 16;
           const int r0 = p.tri ? j0 : 0;            // first output column touched by this K-step
-          const int bh = p.box_rows;                   // rows per TMA box (divides kpad - r0 when not tri)
-          const int npc = (p.kpad - r0 + bh - 1) / bh;
+          const int bh = p.box_rows;                   // rows per TMA box (divides n16 when not tri)
+          const int npc = (p.n16 - r0 + bh - 1) / bh;
           uint8_t* st = stages + (size_t)s * p.stage_bytes;
           mbar_expect_tx(&full_bar[s], (uint32_t)(npc * bh * 32 * p.nsplit));
           for (int c = 0; c < npc; ++c) {
@@ -1145,17 +1161,22 @@ __global__ void __launch_bounds__(FUSED_THREADS, 1)
           tc_fence_after();
           const int j0 = ks * 16;
           const int r0 = p.tri ? j0 : 0;
-          const uint32_t aoff = (uint32_t)((j0 >> 6) * 16384 + ((j0 & 63) >> 4) * 32);
+          // A K-step: 32 bytes inside a 128-byte swizzled chunk, or a whole 32-byte swizzled block
+          const bool in_full = j0 < p.full_cols;
+          const uint32_t aoff = in_full ? (uint32_t)((j0 >> 6) * 16384 + ((j0 & 63) >> 4) * 32)
+                                        : (uint32_t)(p.full_cols * 256 + ((j0 - p.full_cols) >> 4) * 4096);
+          const uint64_t ahi = in_full ? sw128_kmajor_desc(abase + aoff) : sw32_kmajor_desc(abase + aoff);
+          const uint64_t alo = in_full ? sw128_kmajor_desc(lbase + aoff) : sw32_kmajor_desc(lbase + aoff);
           const uint32_t bst = smem_u32(stages + (size_t)s * p.stage_bytes);
-          for (int c0 = r0; c0 < p.kpad; c0 += 256) {
-            const int n = min(256, p.kpad - c0);
+          for (int c0 = r0; c0 < p.n16; c0 += 256) {
+            const int n = min(256, p.n16 - c0);
             const uint32_t idesc = make_idesc(p.fmt, 128, (uint32_t)n);
             const uint32_t boff = (uint32_t)(c0 - r0) * 32u;
             const uint32_t d = tmem + (uint32_t)c0;
-            mma_f16(d, sw128_kmajor_desc(abase + aoff), sw32_kmajor_desc(bst + boff), idesc, ks > 0 ? 1u : 0u);
+            mma_f16(d, ahi, sw32_kmajor_desc(bst + boff), idesc, ks > 0 ? 1u : 0u);
             if (two) {
-              mma_f16(d, sw128_kmajor_desc(abase + aoff), sw32_kmajor_desc(bst + p.b_slot + boff), idesc, 1u);
-              mma_f16(d, sw128_kmajor_desc(lbase + aoff), sw32_kmajor_desc(bst + boff), idesc, 1u);
+              mma_f16(d, ahi, sw32_kmajor_desc(bst + p.b_slot + boff), idesc, 1u);
+              mma_f16(d, alo, sw32_kmajor_desc(bst + boff), idesc, 1u);
             }
           }
           tc_commit(&empty_bar[s]);
@@ -1200,7 +1221,7 @@ __global__ void __launch_bounds__(FUSED_THREADS, 1)
         const int s0 = ash_s[a] & 0xffffff;
         if ((ash_s[a + 1] & 0xffffff) <= s0) continue;
         const int flast = atom_rows(sh_s, pr_s, ash_s, crd_s, a, pos, (itm & 1) * 32 + lane,
-                                    SwizzledRowsOut<FMT>{A_hi, A_lo, (itm & 1) * 32 + lane, two});
+                                    SwizzledRowsOut<FMT>{A_hi, A_lo, (itm & 1) * 32 + lane, p.full_cols, two});
         // publish: generic-proxy writes of A become visible to the tensor core, then one arrival
         // per column chunk this atom wrote
         asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
@@ -1214,20 +1235,31 @@ __global__ void __launch_bounds__(FUSED_THREADS, 1)
       if (!mbar_wait(&t_full, tile_it & 1u, &abort_flag)) break;
       tc_fence_after();
       double acc[2] = {0.0, 0.0};
-      for (int c = hh; c * 16 < p.kpad; c += FUSED_NCW / 4) {
+      for (int c = hh; c * 16 < p.n16; c += FUSED_NCW / 4) {
         const int col = c * 16;
         float v[16], ph[16];
         tmem_ld16(tmem + ((uint32_t)(q * 32) << 16) + (uint32_t)col, v);
-        const int kc = col >> 6, u0 = (col & 63) >> 3;
-        const uint8_t* rb = A_hi + kc * 16384 + (row >> 3) * 1024 + (row & 7) * 128;
+        // the row's two 16-byte units of columns col .. col + 15 (layouts of a_offset)
+        uint32_t rbase, uo[2];
+        if (col < p.full_cols) {
+          const int u0 = (col & 63) >> 3;
+          rbase = (uint32_t)((col >> 6) * 16384 + (row >> 3) * 1024 + (row & 7) * 128);
+          uo[0] = (uint32_t)((u0 ^ (row & 7)) * 16);
+          uo[1] = (uint32_t)(((u0 + 1) ^ (row & 7)) * 16);
+        } else {
+          rbase = (uint32_t)(p.full_cols * 256 + ((col - p.full_cols) >> 4) * 4096 + (row >> 3) * 256 + (row & 7) * 32);
+          uo[0] = (uint32_t)(((row >> 2) & 1) * 16);
+          uo[1] = 16u - uo[0];
+        }
+        const uint8_t* rb = A_hi + rbase;
 #pragma unroll
-        for (int u = 0; u < 2; ++u) unpack8<FMT>(*reinterpret_cast<const uint4*>(rb + (((u0 + u) ^ (row & 7)) * 16)), ph + 8 * u);
+        for (int u = 0; u < 2; ++u) unpack8<FMT>(*reinterpret_cast<const uint4*>(rb + uo[u]), ph + 8 * u);
         if (two) {
-          const uint8_t* rl = A_lo + kc * 16384 + (row >> 3) * 1024 + (row & 7) * 128;
+          const uint8_t* rl = A_lo + rbase;
 #pragma unroll
           for (int u = 0; u < 2; ++u) {
             float lo8[8];
-            unpack8<FMT>(*reinterpret_cast<const uint4*>(rl + (((u0 + u) ^ (row & 7)) * 16)), lo8);
+            unpack8<FMT>(*reinterpret_cast<const uint4*>(rl + uo[u]), lo8);
 #pragma unroll
             for (int e = 0; e < 8; ++e) ph[8 * u + e] += lo8[e];
           }
@@ -1420,15 +1452,21 @@ static int fused_tab_bytes(const qmt_mol* m) {
   return words * 16 + (m->natoms + 1 + 3) / 4 * 16 + (3 * m->natoms + 3) / 4 * 16;
 }
 
+// Functions rounded up to 16 (K-steps of the fused MMAs), bytes of one A piece and of one U
+// piece slot in a stage.
+static int fused_n16(const qmt_mol* m) { return (m->norbs + 15) / 16 * 16; }
+static uint32_t fused_a_bytes(int n16) { return 128u * (uint32_t)n16 * 2u; }
+static uint32_t fused_b_slot(int kpad, int n16) { return (uint32_t)(g_fused_tri ? kpad : n16) * 32u; }
+
 // U pipeline stages that fit beside A and the tables (below 2: the fused path does not fit).
 template <int FMT>
-static int fused_stages(const TcShape& sh, int tab_bytes) {
+static int fused_stages(const TcShape& sh, int n16, int tab_bytes) {
   int maxsm = 0, dev = 0;
   cudaGetDevice(&dev);
   cudaDeviceGetAttribute(&maxsm, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev);
   cudaFuncAttributes fa;
   if (cudaFuncGetAttributes(&fa, density_fused_kernel<FMT>) != cudaSuccess) return 0;
-  const long a_bytes = 128L * sh.kpad * 2, stage_bytes = (long)sh.nsplit * sh.kpad * 32;
+  const long a_bytes = fused_a_bytes(n16), stage_bytes = (long)sh.nsplit * fused_b_slot(sh.kpad, n16);
   const long avail = (long)maxsm - (long)fa.sharedSizeBytes - 1024 - sh.nsplit * a_bytes - tab_bytes;
   return (int)std::max<long>(0, std::min<long>(MAX_STAGES, avail / stage_bytes));
 }
@@ -1437,12 +1475,12 @@ template <int FMT>
 static qmt_status run_fused(qmt_mol* m, const TcShape& sh, const PointMap& pm, int64_t ntiles, float* qube,
                             double outscale, cudaStream_t s) {
   qmt_status st;
-  const int K = sh.kpad;
+  const int K = sh.kpad, n16 = fused_n16(m);
   const size_t piece = (size_t)(K + 64) * K * 2;
   CUtensorMap tU_hi, tU_lo;
   const uint8_t* B = m->d_fused_B.as<uint8_t>();
-  // fewer, taller boxes for the full matrix (a stage is one K-step of all kpad rows)
-  const uint32_t box_rows = g_fused_tri ? 64u : (K <= 256 ? (uint32_t)K : (uint32_t)K / 2);
+  // fewer, taller boxes for the full matrix (a stage is one K-step of all n16 output columns)
+  const uint32_t box_rows = g_fused_tri ? 64u : (n16 <= 256 ? (uint32_t)n16 : (uint32_t)n16 / 2);
   if ((st = make_map_sw32(&tU_hi, B, K, K + 64, box_rows)) || (st = make_map_sw32(&tU_lo, B + piece, K, K + 64, box_rows)))
     return st;
   FusedParams p{};
@@ -1450,9 +1488,11 @@ static qmt_status run_fused(qmt_mol* m, const TcShape& sh, const PointMap& pm, i
   p.pm = pm;
   p.ntiles = ntiles;
   p.kpad = K;
-  p.ksteps = K / 16;
+  p.n16 = n16;
+  p.full_cols = n16 / 64 * 64;
+  p.ksteps = n16 / 16;
   p.tri = g_fused_tri;
-  p.nchunks = K / 64;
+  p.nchunks = (n16 + 63) / 64;
   p.box_rows = (int)box_rows;
   if (p.nchunks > MAX_FUSED_CHUNKS) return fail(QMT_BAD_ARG, "fused density path supports kpad <= 320");
   for (int a = 0; a < m->natoms; ++a) {
@@ -1463,8 +1503,8 @@ static qmt_status run_fused(qmt_mol* m, const TcShape& sh, const PointMap& pm, i
     for (int c = cfirst; c <= clast; ++c) p.chunk_need[c] += 2;   // two row halves per atom
   }
   p.nsplit = sh.nsplit;
-  p.a_bytes = 128u * K * 2u;
-  p.b_slot = (uint32_t)K * 32u;
+  p.a_bytes = fused_a_bytes(n16);
+  p.b_slot = fused_b_slot(K, n16);
   p.stage_bytes = p.nsplit * p.b_slot;
   p.fmt = (uint32_t)sh.fmt;
   p.tab = m->d_fused_tab.as<int4>();
@@ -1479,7 +1519,7 @@ static qmt_status run_fused(qmt_mol* m, const TcShape& sh, const PointMap& pm, i
   p.inv_g2 = (g_fused_tri ? 2.0 : 1.0) * std::ldexp(1.0, -m->fused_g);
   p.err = reinterpret_cast<int*>(m->d_scalars.as<double>() + 8);
   auto kern = density_fused_kernel<FMT>;
-  const int stages = fused_stages<FMT>(sh, p.tab_bytes);
+  const int stages = fused_stages<FMT>(sh, n16, p.tab_bytes);
   if (stages < 2) return fail(QMT_BAD_ARG, "fused density tile does not fit in shared memory");
   p.stages = stages;
   const size_t dyn = (size_t)p.nsplit * p.a_bytes + (size_t)stages * p.stage_bytes + p.tab_bytes + 1024;
@@ -1630,7 +1670,8 @@ qmt_status density_tc(qmt_mol* mol, int nx, int ny, int nz, float step, float ox
   bool fusable = sh.fmt != FMT_TF32 && sh.kpad <= 320;
   if (fusable) {
     const int tb = fused_tab_bytes(mol);
-    fusable = (sh.fmt == FMT_F16 ? fused_stages<FMT_F16>(sh, tb) : fused_stages<FMT_BF16>(sh, tb)) >= 2;
+    const int n16 = fused_n16(mol);
+    fusable = (sh.fmt == FMT_F16 ? fused_stages<FMT_F16>(sh, n16, tb) : fused_stages<FMT_BF16>(sh, n16, tb)) >= 2;
   }
   const bool fused = g_density_path == 2 ? fusable : (g_density_path == 1 ? false : fusable);
   if (g_density_path == 2 && !fusable)

@@ -121,23 +121,39 @@ struct PointMap {
   int64_t nvox;
   float h;
   float ox, oy, oz;
+  double inv_s;   // 1 / s
 };
 
 template <typename T>
 __device__ __forceinline__ bool tile_point(const PointMap& pm, int64_t tile, int row,
                                            T& x, T& y, T& z, int64_t& vox) {
-  const int v = row / pm.s3;
-  const int sub = row - v * pm.s3;
+  int v = row, sub = 0;
+  if (pm.s3 > 1) {
+    v = row / pm.s3;
+    sub = row - v * pm.s3;
+  }
   if (v >= pm.vpt) return false;
   vox = tile * pm.vpt + v;
   if (vox >= pm.nvox) return false;
-  const int64_t ix = vox % pm.nx;
-  const int64_t iy = (vox / pm.nx) % pm.ny;
-  const int64_t iz = vox / ((int64_t)pm.nx * pm.ny);
-  const int sx = sub % pm.s;
-  const int sy = (sub / pm.s) % pm.s;
-  const int sz = sub / (pm.s * pm.s);
-  const T inv = T(1) / T(pm.s);
+  int64_t ix, iy, iz;
+  if (pm.nvox <= 0x7fffffffLL) {   // 32-bit index arithmetic (exact, several times cheaper)
+    const uint32_t vv = (uint32_t)vox, nx = (uint32_t)pm.nx, ny = (uint32_t)pm.ny;
+    const uint32_t qy = vv / nx, qz = qy / ny;
+    ix = vv - qy * nx;
+    iy = qy - qz * ny;
+    iz = qz;
+  } else {
+    ix = vox % pm.nx;
+    iy = (vox / pm.nx) % pm.ny;
+    iz = vox / ((int64_t)pm.nx * pm.ny);
+  }
+  int sx = 0, sy = 0, sz = 0;
+  if (pm.s > 1) {
+    sx = sub % pm.s;
+    sy = (sub / pm.s) % pm.s;
+    sz = sub / (pm.s * pm.s);
+  }
+  const T inv = T(pm.inv_s);
   const T h = T(pm.h);
   x = T(pm.ox) + (T(ix) + (T(sx) + T(0.5)) * inv) * h;
   y = T(pm.oy) + (T(iy) + (T(sy) + T(0.5)) * inv) * h;
