@@ -425,15 +425,21 @@ __host__ __device__ inline void split_host(double x, int fmt, void* hi, void* lo
 // P_rc 2^(g - s_r - s_c) split into hi + lo (inv_s = 2^-s, exact powers of two, so this equals
 // ldexp of the same exponents); `tri` keeps c <= r and halves the diagonal.  The pieces must be
 // cleared beforehand (padding stays zero).
+// Element (r, c) goes to r * K + c (row-major), or, with blk_rows > 0, to the K-step blocks of
+// the fused path: block c / 16 holds blk_rows rows of 32 bytes (the 16 columns of one K-step),
+// each row's two 16-byte units exchanged when bit 2 of the row is set -- the 32-byte swizzled
+// K-major image that the MMA reads from shared memory, so that a stage is one contiguous copy.
 __global__ void split_P_kernel(const double* __restrict__ P, int np, int n, int K, const double* __restrict__ inv_s,
-                               double two_g, int tri, int fmt, uint8_t* hi, uint8_t* lo) {
+                               double two_g, int tri, int fmt, int blk_rows, uint8_t* hi, uint8_t* lo) {
   const int64_t tot = (int64_t)n * n;
   for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < tot; i += (int64_t)gridDim.x * blockDim.x) {
     const int r = (int)(i / n), c = (int)(i % n);
     if (tri && c > r) continue;
     double v = P[(size_t)c * np + r] * two_g * inv_s[r] * inv_s[c];
     if (tri && c == r) v *= 0.5;
-    split_host(v, fmt, hi, lo, (size_t)r * K + c);
+    const int e = c & 15, pe = ((((e >> 3) ^ (r >> 2)) & 1) << 3) | (e & 7);   // swizzled position in the row
+    const size_t idx = blk_rows > 0 ? ((size_t)(c >> 4) * blk_rows + r) * 16 + pe : (size_t)r * K + c;
+    split_host(v, fmt, hi, lo, idx);
   }
 }
 
@@ -459,14 +465,14 @@ static qmt_status split_scales(qmt_mol* m, const std::vector<int>& sj, int K, in
   return QMT_OK;
 }
 
-static qmt_status launch_split(qmt_mol* m, int K, int g, int tri, int fmt, void* hi, void* lo, size_t piece_bytes,
-                               cudaStream_t s) {
+static qmt_status launch_split(qmt_mol* m, int K, int g, int tri, int fmt, int blk_rows, void* hi, void* lo,
+                               size_t piece_bytes, cudaStream_t s) {
   QMT_CUDA(cudaMemsetAsync(hi, 0, piece_bytes, s));
   QMT_CUDA(cudaMemsetAsync(lo, 0, piece_bytes, s));
   const int64_t tot = (int64_t)m->norbs * m->norbs;
   const int blocks = (int)std::min<int64_t>((tot + 255) / 256, (int64_t)sm_count() * 8);
   split_P_kernel<<<std::max(blocks, 1), 256, 0, s>>>(m->d_P64.as<double>(), m->npad, m->norbs, K,
-                                                     m->d_split_scale.as<double>(), std::ldexp(1.0, g), tri, fmt,
+                                                     m->d_split_scale.as<double>(), std::ldexp(1.0, g), tri, fmt, blk_rows,
                                                      reinterpret_cast<uint8_t*>(hi), reinterpret_cast<uint8_t*>(lo));
   QMT_CHECK_LAUNCH("split_P_kernel");
   return QMT_OK;
@@ -482,7 +488,9 @@ static qmt_status launch_split(qmt_mol* m, int K, int g, int tri, int fmt, void*
 //   those of Phi P, so the FP32 tensor-core accumulation loses about a factor 2 in accuracy.
 //
 // CTA layout (one per SM, persistent over 128-row tiles), 10 warps:
-//   warp 0     TMA producer of U (32-byte swizzled, one 16-element K-step per stage);
+//   warp 0     producer of U: one bulk copy per stage and piece of a K-step block that HBM
+//              already holds in the 32-byte swizzled layout (tensor-map boxes of 32-byte rows
+//              ran the copy engine at ~40 GB/s per SM; contiguous copies do not);
 //              U is the same for every tile, so it streams ahead across tiles;
 //   warp 1     TMEM allocation and the single MMA-issuing thread;
 //   warps 2-9  evaluate Phi' for the tile straight into the 128-byte swizzled K-major
@@ -499,14 +507,15 @@ struct FusedParams {
   PointMap pm;
   int64_t ntiles;
   int kpad, ksteps, nsplit, stages;
-  int n16;                 // functions rounded up to 16: K of the MMAs and N (output columns)
-  int full_cols;           // columns held in 64-column 128-byte swizzled chunks (n16 rounded down
-                           // to 64); the rest in 16-column 32-byte swizzled blocks
+  int n16;                 // functions rounded up to 16: K of the MMAs and N (output columns); the
+                           // K-steps beyond it only hold zero padding and are skipped
   int tri;                 // 1: upper-triangular U (half the work); 0: full symmetric P
-  int nchunks;             // ceil(n16 / 64) column chunks of A (the last may be the 16-column blocks)
-  int box_rows;            // rows of one U box: 64 (triangular), else n16 or n16 / 2 (<= 256)
+  int nchunks;             // ceil(n16 / 64) column chunks of A
+  int u_rows;              // rows of one K-step block of U in HBM (kpad + 64)
+  const uint8_t* u_hi;     // U pieces in K-step blocks (split_P_kernel with blk_rows = u_rows)
+  const uint8_t* u_lo;
   int chunk_need[MAX_FUSED_CHUNKS];  // production items (atom halves) writing each chunk
-  uint32_t a_bytes;        // one A piece: 128 rows x n16 x 2 B
+  uint32_t a_bytes;        // one A piece: 128 rows x kpad x 2 B
   uint32_t b_slot;         // one U piece slot in a stage: n16 (triangular: kpad) rows x 32 B
   uint32_t stage_bytes;
   uint32_t fmt;
@@ -523,23 +532,16 @@ struct FusedParams {
   int* err;
 };
 
-// Byte offset of element (row, j) in the K-major A tile: columns below `full_cols` in 64-column
-// chunks with the 128-byte swizzle (8-row atoms of 1024 B, 16-byte unit u at u ^ (row & 7)),
-// the rest in 16-column blocks with the 32-byte swizzle (8-row atoms of 256 B, unit u at
-// u ^ ((row >> 2) & 1)), so that a tile holds n16 rather than kpad columns.
-__device__ __forceinline__ uint32_t a_offset(int row, int j, int full_cols) {
-  if (j < full_cols) {
-    const int kc = j >> 6, e = j & 63;
-    const int u = (e >> 3) ^ (row & 7);
-    return (uint32_t)(kc * 16384 + (row >> 3) * 1024 + (row & 7) * 128 + u * 16 + (e & 7) * 2);
-  }
-  const int t = j - full_cols, e = t & 15;
-  const int u = (e >> 3) ^ ((row >> 2) & 1);
-  return (uint32_t)(full_cols * 256 + (t >> 4) * 4096 + (row >> 3) * 256 + (row & 7) * 32 + u * 16 + (e & 7) * 2);
+// Byte offset of element (row, j) in the 128-byte swizzled K-major A tile (64-column chunks of
+// 8-row atoms of 1024 B, 16-byte unit u of a row at u ^ (row & 7)).  Row r + 64 of a column sits
+// 8192 B after row r.  (Holding the padding of the last chunk in 32-byte swizzled 16-column
+// blocks instead saves 8 KB of shared memory but the extra branch in this store path slowed
+// production by more than the third U stage it made room for gained.)
+__device__ __forceinline__ uint32_t a_offset(int row, int j) {
+  const int kc = j >> 6, e = j & 63;
+  const int u = (e >> 3) ^ (row & 7);
+  return (uint32_t)(kc * 16384 + (row >> 3) * 1024 + (row & 7) * 128 + u * 16 + (e & 7) * 2);
 }
-
-// Offset from row r to row r + 64 of the same column (the row's bits 0-2 are unchanged).
-__device__ __forceinline__ uint32_t a_row64(int j, int full_cols) { return j < full_cols ? 8192u : 2048u; }
 
 __device__ __forceinline__ uint64_t sw32_kmajor_desc(uint32_t saddr) {
   uint64_t d = 0;
@@ -718,7 +720,6 @@ struct SwizzledRowsOut {
   uint8_t* hi;
   uint8_t* lo;
   int r0;
-  int full_cols;
   bool two;
   template <int NF>
   __device__ __forceinline__ void put(int j0, int nf, const float (&v0)[NF], const float (&v1)[NF]) const {
@@ -731,8 +732,8 @@ struct SwizzledRowsOut {
         continue;
       }
       const int j = j0 + k;
-      const uint32_t off = a_offset(r0, j, full_cols);
-      const uint32_t off1 = off + a_row64(j, full_cols);   // row r0 + 64
+      const uint32_t off = a_offset(r0, j);
+      const uint32_t off1 = off + 8192u;   // row r0 + 64
       // two consecutive functions in the same 16-byte unit: one 4-byte store per piece
       if (k + 1 < nf && (j & 1) == 0) {
         store_pair16<FMT>(hi, lo, off, v0[k], v0[k + 1], two);
@@ -1049,10 +1050,97 @@ constexpr int FUSED_NCW = 16;                 // compute warps (Phi production a
 constexpr int FUSED_NCT = FUSED_NCW * 32;
 constexpr int FUSED_THREADS = 64 + FUSED_NCT;  // + TMA warp + MMA warp
 
+// The single-thread roles of the fused kernel (warp 0 lane 0 and warp 1 lane 0).
+
+// U producer: streams the K-step blocks of U into the stage ring (one bulk copy per stage and
+// piece, already in the 32-byte swizzled layout; stage slots and r0 are multiples of 256 bytes
+// and 16 rows).  On an abort it waits (bounded) for its copies in flight before returning.
+__device__ __forceinline__ void fused_produce_u(const FusedParams* pp, uint8_t* stages, uint64_t* full_bar,
+                                             uint64_t* empty_bar, volatile int* abort_flag) {
+  const FusedParams& p = *pp;
+  const bool two = p.nsplit == 2;
+  uint32_t it = 0, issued = 0, par = 0;   // bit s: stage s has a copy in flight / its phase parity
+  bool ok = true;
+  for (int64_t t = blockIdx.x; t < p.ntiles && ok; t += gridDim.x) {
+    for (int ks = 0; ks < p.ksteps; ++ks, ++it) {
+      const int s = it % p.stages;
+      const uint32_t ph = (it / p.stages) & 1u;
+      if (!mbar_wait(&empty_bar[s], ph ^ 1u, abort_flag)) {
+        ok = false;
+        break;
+      }
+      const int r0 = p.tri ? ks * 16 : 0;   // first output column touched by this K-step
+      const uint32_t bytes = (uint32_t)(p.n16 - r0) * 32u;
+      const size_t src = ((size_t)ks * p.u_rows + r0) * 32u;
+      uint8_t* st = stages + (size_t)s * p.stage_bytes;
+      mbar_expect_tx(&full_bar[s], bytes * (uint32_t)p.nsplit);
+      bulk_load(st, p.u_hi + src, bytes, &full_bar[s]);
+      if (two) bulk_load(st + p.b_slot, p.u_lo + src, bytes, &full_bar[s]);
+      issued |= 1u << s;
+      par = (par & ~(1u << s)) | (ph << s);
+    }
+  }
+  if (!ok)
+    for (int s = 0; s < p.stages; ++s)
+      if ((issued >> s) & 1u) mbar_wait(&full_bar[s], (par >> s) & 1u, abort_flag, 100000000ull);
+}
+
+// MMA issuer: per tile, per K-step (after its column chunk of A is complete and its U stage has
+// landed) the split products T' += A_hi U_hi + A_hi U_lo + A_lo U_hi into TMEM; frees the stage
+// with a commit, and signals t_full after the tile's last K-step.
+__device__ __forceinline__ void fused_issue_mma(const FusedParams* pp, uint32_t abase, uint32_t lbase, uint8_t* stages,
+                                             uint32_t tmem, uint64_t* full_bar, uint64_t* empty_bar,
+                                             uint64_t* chunk_bar, uint64_t* t_full, uint64_t* drain_bar,
+                                             volatile int* abort_flag) {
+  const FusedParams& p = *pp;
+  const bool two = p.nsplit == 2;
+  uint32_t it = 0, tile_it = 0;
+  bool ok = true;
+  for (int64_t t = blockIdx.x; t < p.ntiles && ok; t += gridDim.x, ++tile_it) {
+    for (int ks = 0; ks < p.ksteps; ++ks, ++it) {
+      // columns 64c .. 64c+63 of A are complete once every item writing them arrived
+      if ((ks & 3) == 0 && p.chunk_need[ks >> 2] > 0) {
+        if (!mbar_wait(&chunk_bar[ks >> 2], tile_it & 1u, abort_flag)) {
+          ok = false;
+          break;
+        }
+        tc_fence_after();
+      }
+      const int s = it % p.stages;
+      const uint32_t ph = (it / p.stages) & 1u;
+      if (!mbar_wait(&full_bar[s], ph, abort_flag)) {
+        ok = false;
+        break;
+      }
+      tc_fence_after();
+      const int j0 = ks * 16;
+      const int r0 = p.tri ? j0 : 0;
+      // A K-step: 32 bytes inside a 128-byte swizzled chunk
+      const uint32_t aoff = (uint32_t)((j0 >> 6) * 16384 + ((j0 & 63) >> 4) * 32);
+      const uint64_t ahi = sw128_kmajor_desc(abase + aoff), alo = sw128_kmajor_desc(lbase + aoff);
+      const uint32_t bst = smem_u32(stages + (size_t)s * p.stage_bytes);
+      for (int c0 = r0; c0 < p.n16; c0 += 256) {
+        const int n = min(256, p.n16 - c0);
+        const uint32_t idesc = make_idesc(p.fmt, 128, (uint32_t)n);
+        const uint32_t boff = (uint32_t)(c0 - r0) * 32u;
+        const uint32_t d = tmem + (uint32_t)c0;
+        mma_f16(d, ahi, sw32_kmajor_desc(bst + boff), idesc, ks > 0 ? 1u : 0u);
+        if (two) {
+          mma_f16(d, ahi, sw32_kmajor_desc(bst + p.b_slot + boff), idesc, 1u);
+          mma_f16(d, alo, sw32_kmajor_desc(bst + boff), idesc, 1u);
+        }
+      }
+      tc_commit(&empty_bar[s]);
+    }
+    if (ok) tc_commit(t_full);
+  }
+  tc_commit(drain_bar);
+  mbar_wait(drain_bar, 0u, abort_flag, 500000000ull);
+}
+
 template <int FMT>
 __global__ void __launch_bounds__(FUSED_THREADS, 1)
-    density_fused_kernel(const __grid_constant__ CUtensorMap tmU_hi, const __grid_constant__ CUtensorMap tmU_lo,
-                         const FusedParams p) {
+    density_fused_kernel(const __grid_constant__ FusedParams p) {
   extern __shared__ uint8_t smem_dyn[];
   __shared__ __align__(8) uint64_t full_bar[MAX_STAGES], empty_bar[MAX_STAGES];
   __shared__ __align__(8) uint64_t chunk_bar[MAX_FUSED_CHUNKS], t_full, drain_bar;
@@ -1093,10 +1181,6 @@ __global__ void __launch_bounds__(FUSED_THREADS, 1)
   for (int i = threadIdx.x; i < 3 * mol.natoms; i += blockDim.x)
     reinterpret_cast<float*>(tabs + p.off_coords)[i] = __ldg(mol.coords + i);
   asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
-  if (warp == 0 && lane == 0) {
-    prefetch_tmap(&tmU_hi);
-    if (two) prefetch_tmap(&tmU_lo);
-  }
   if (warp == 1) {
     tmem_alloc(&tmem_slot, 512);
     tmem_relinquish();
@@ -1107,85 +1191,11 @@ __global__ void __launch_bounds__(FUSED_THREADS, 1)
   const uint32_t tmem = tmem_slot;
 
   if (warp == 0) {
-    if (lane == 0) {
-      uint32_t it = 0;
-      int last_par[MAX_STAGES];
-      for (int s = 0; s < MAX_STAGES; ++s) last_par[s] = -1;
-      bool ok = true;
-      for (int64_t t = blockIdx.x; t < p.ntiles && ok; t += gridDim.x) {
-        for (int ks = 0; ks < p.ksteps; ++ks, ++it) {
-          const int s = it % p.stages;
-          const uint32_t ph = (it / p.stages) & 1u;
-          if (!mbar_wait(&empty_bar[s], ph ^ 1u, &abort_flag)) {
-            ok = false;
-            break;
-          }
-          const int j0 = ks * 16;
-          const int r0 = p.tri ? j0 : 0;            // first output column touched by this K-step
-          const int bh = p.box_rows;                   // rows per TMA box (divides n16 when not tri)
-          const int npc = (p.n16 - r0 + bh - 1) / bh;
-          uint8_t* st = stages + (size_t)s * p.stage_bytes;
-          mbar_expect_tx(&full_bar[s], (uint32_t)(npc * bh * 32 * p.nsplit));
-          for (int c = 0; c < npc; ++c) {
-            tma_load_2d(st + c * bh * 32, &tmU_hi, &full_bar[s], j0, r0 + bh * c);
-            if (two) tma_load_2d(st + p.b_slot + c * bh * 32, &tmU_lo, &full_bar[s], j0, r0 + bh * c);
-          }
-          last_par[s] = (int)ph;
-        }
-      }
-      if (!ok)
-        for (int s = 0; s < p.stages; ++s)
-          if (last_par[s] >= 0) mbar_wait(&full_bar[s], (uint32_t)last_par[s], &abort_flag, 100000000ull);
-    }
+    if (lane == 0) fused_produce_u(&p, stages, full_bar, empty_bar, &abort_flag);
   } else if (warp == 1) {
-    if (lane == 0) {
-      uint32_t it = 0, tile_it = 0;
-      bool ok = true;
-      const uint32_t abase = smem_u32(A_hi), lbase = smem_u32(A_lo);
-      for (int64_t t = blockIdx.x; t < p.ntiles && ok; t += gridDim.x, ++tile_it) {
-        for (int ks = 0; ks < p.ksteps; ++ks, ++it) {
-          // columns 64c .. 64c+63 of A are complete once every item writing them arrived
-          if ((ks & 3) == 0 && p.chunk_need[ks >> 2] > 0) {
-            if (!mbar_wait(&chunk_bar[ks >> 2], tile_it & 1u, &abort_flag)) {
-              ok = false;
-              break;
-            }
-            tc_fence_after();
-          }
-          const int s = it % p.stages;
-          const uint32_t ph = (it / p.stages) & 1u;
-          if (!mbar_wait(&full_bar[s], ph, &abort_flag)) {
-            ok = false;
-            break;
-          }
-          tc_fence_after();
-          const int j0 = ks * 16;
-          const int r0 = p.tri ? j0 : 0;
-          // A K-step: 32 bytes inside a 128-byte swizzled chunk, or a whole 32-byte swizzled block
-          const bool in_full = j0 < p.full_cols;
-          const uint32_t aoff = in_full ? (uint32_t)((j0 >> 6) * 16384 + ((j0 & 63) >> 4) * 32)
-                                        : (uint32_t)(p.full_cols * 256 + ((j0 - p.full_cols) >> 4) * 4096);
-          const uint64_t ahi = in_full ? sw128_kmajor_desc(abase + aoff) : sw32_kmajor_desc(abase + aoff);
-          const uint64_t alo = in_full ? sw128_kmajor_desc(lbase + aoff) : sw32_kmajor_desc(lbase + aoff);
-          const uint32_t bst = smem_u32(stages + (size_t)s * p.stage_bytes);
-          for (int c0 = r0; c0 < p.n16; c0 += 256) {
-            const int n = min(256, p.n16 - c0);
-            const uint32_t idesc = make_idesc(p.fmt, 128, (uint32_t)n);
-            const uint32_t boff = (uint32_t)(c0 - r0) * 32u;
-            const uint32_t d = tmem + (uint32_t)c0;
-            mma_f16(d, ahi, sw32_kmajor_desc(bst + boff), idesc, ks > 0 ? 1u : 0u);
-            if (two) {
-              mma_f16(d, ahi, sw32_kmajor_desc(bst + p.b_slot + boff), idesc, 1u);
-              mma_f16(d, alo, sw32_kmajor_desc(bst + boff), idesc, 1u);
-            }
-          }
-          tc_commit(&empty_bar[s]);
-        }
-        if (ok) tc_commit(&t_full);
-      }
-      tc_commit(&drain_bar);
-      mbar_wait(&drain_bar, 0u, &abort_flag, 500000000ull);
-    }
+    if (lane == 0)
+      fused_issue_mma(&p, smem_u32(A_hi), smem_u32(A_lo), stages, tmem, full_bar, empty_bar, chunk_bar, &t_full,
+                      &drain_bar, &abort_flag);
   } else {
     const int ct = threadIdx.x - 64;           // compute thread 0 .. FUSED_NCT-1
     const int4* sh_s = reinterpret_cast<const int4*>(tabs);
@@ -1221,7 +1231,7 @@ __global__ void __launch_bounds__(FUSED_THREADS, 1)
         const int s0 = ash_s[a] & 0xffffff;
         if ((ash_s[a + 1] & 0xffffff) <= s0) continue;
         const int flast = atom_rows(sh_s, pr_s, ash_s, crd_s, a, pos, (itm & 1) * 32 + lane,
-                                    SwizzledRowsOut<FMT>{A_hi, A_lo, (itm & 1) * 32 + lane, p.full_cols, two});
+                                    SwizzledRowsOut<FMT>{A_hi, A_lo, (itm & 1) * 32 + lane, two});
         // publish: generic-proxy writes of A become visible to the tensor core, then one arrival
         // per column chunk this atom wrote
         asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
@@ -1239,18 +1249,10 @@ __global__ void __launch_bounds__(FUSED_THREADS, 1)
         const int col = c * 16;
         float v[16], ph[16];
         tmem_ld16(tmem + ((uint32_t)(q * 32) << 16) + (uint32_t)col, v);
-        // the row's two 16-byte units of columns col .. col + 15 (layouts of a_offset)
-        uint32_t rbase, uo[2];
-        if (col < p.full_cols) {
-          const int u0 = (col & 63) >> 3;
-          rbase = (uint32_t)((col >> 6) * 16384 + (row >> 3) * 1024 + (row & 7) * 128);
-          uo[0] = (uint32_t)((u0 ^ (row & 7)) * 16);
-          uo[1] = (uint32_t)(((u0 + 1) ^ (row & 7)) * 16);
-        } else {
-          rbase = (uint32_t)(p.full_cols * 256 + ((col - p.full_cols) >> 4) * 4096 + (row >> 3) * 256 + (row & 7) * 32);
-          uo[0] = (uint32_t)(((row >> 2) & 1) * 16);
-          uo[1] = 16u - uo[0];
-        }
+        // the row's two 16-byte units of columns col .. col + 15 (layout of a_offset)
+        const int u0 = (col & 63) >> 3;
+        const uint32_t rbase = (uint32_t)((col >> 6) * 16384 + (row >> 3) * 1024 + (row & 7) * 128);
+        const uint32_t uo[2] = {(uint32_t)((u0 ^ (row & 7)) * 16), (uint32_t)(((u0 + 1) ^ (row & 7)) * 16)};
         const uint8_t* rb = A_hi + rbase;
 #pragma unroll
         for (int u = 0; u < 2; ++u) unpack8<FMT>(*reinterpret_cast<const uint4*>(rb + uo[u]), ph + 8 * u);
@@ -1309,21 +1311,6 @@ __global__ void __launch_bounds__(FUSED_THREADS, 1)
     tc_fence_after();
     tmem_dealloc(tmem, 512);
   }
-}
-
-static qmt_status make_map_sw32(CUtensorMap* m, const void* base, uint64_t inner, uint64_t outer,
-                                uint32_t box_rows = 64) {
-  auto fn = encode_fn();
-  if (!fn) return fail(QMT_CUDA_ERR, "cuTensorMapEncodeTiled unavailable");
-  cuuint64_t dims[2] = {inner, outer};
-  cuuint64_t strides[1] = {inner * 2};
-  cuuint32_t box[2] = {16, box_rows};
-  cuuint32_t estr[2] = {1, 1};
-  CUresult r = fn(m, CU_TENSOR_MAP_DATA_TYPE_UINT16, 2, const_cast<void*>(base), dims, strides, box, estr,
-                  CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_32B, CU_TENSOR_MAP_L2_PROMOTION_L2_256B,
-                  CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
-  if (r != CUDA_SUCCESS) return fail(QMT_CUDA_ERR, "cuTensorMapEncodeTiled failed");
-  return QMT_OK;
 }
 
 // Molecule tables of the producers (fused and staging kernels), in 16-byte words:
@@ -1416,8 +1403,9 @@ static qmt_status ensure_mol_tables(qmt_mol* m, const std::vector<float>& fs, in
 }
 
 // Upper-triangular scaled density matrix for the fused path: row n (output column) holds
-// U_jn for j <= n, i.e. Ptilde_jn for j < n and Ptilde_nn / 2 on the diagonal.  Rows are
-// padded to kpad + 64 so every 64-row TMA box stays inside the tensor.
+// U_jn for j <= n, i.e. Ptilde_jn for j < n and Ptilde_nn / 2 on the diagonal.  Both variants are
+// stored as K-step blocks of kpad + 64 rows x 16 columns in the 32-byte swizzled image of a stage
+// (split_P_kernel), read by one contiguous copy per stage and piece.
 static int g_fused_tri = 0;   // upper-triangular variant of the fused path (off by default)
 
 static qmt_status ensure_fused_operands(qmt_mol* m, int prec, const TcShape& sh, cudaStream_t s) {
@@ -1437,8 +1425,8 @@ static qmt_status ensure_fused_operands(qmt_mol* m, int prec, const TcShape& sh,
   const int rows = K + 64;
   const size_t piece = (size_t)rows * K * 2;
   if ((st = m->d_fused_B.reserve(2 * piece))) return st;
-  if ((st = launch_split(m, K, g, g_fused_tri, sh.fmt, m->d_fused_B.ptr, m->d_fused_B.as<uint8_t>() + piece, piece,
-                         s)))
+  if ((st = launch_split(m, K, g, g_fused_tri, sh.fmt, K + 64, m->d_fused_B.ptr, m->d_fused_B.as<uint8_t>() + piece,
+                         piece, s)))
     return st;
   if ((st = ensure_mol_tables(m, fs, K, s))) return st;
   m->fused_g = g;
@@ -1452,10 +1440,10 @@ static int fused_tab_bytes(const qmt_mol* m) {
   return words * 16 + (m->natoms + 1 + 3) / 4 * 16 + (3 * m->natoms + 3) / 4 * 16;
 }
 
-// Functions rounded up to 16 (K-steps of the fused MMAs), bytes of one A piece and of one U
-// piece slot in a stage.
+// Functions rounded up to 16 (K-steps of the fused MMAs), bytes of one A piece (kpad columns)
+// and of one U piece slot in a stage.
 static int fused_n16(const qmt_mol* m) { return (m->norbs + 15) / 16 * 16; }
-static uint32_t fused_a_bytes(int n16) { return 128u * (uint32_t)n16 * 2u; }
+static uint32_t fused_a_bytes(int kpad) { return 128u * (uint32_t)kpad * 2u; }
 static uint32_t fused_b_slot(int kpad, int n16) { return (uint32_t)(g_fused_tri ? kpad : n16) * 32u; }
 
 // U pipeline stages that fit beside A and the tables (below 2: the fused path does not fit).
@@ -1466,7 +1454,7 @@ static int fused_stages(const TcShape& sh, int n16, int tab_bytes) {
   cudaDeviceGetAttribute(&maxsm, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev);
   cudaFuncAttributes fa;
   if (cudaFuncGetAttributes(&fa, density_fused_kernel<FMT>) != cudaSuccess) return 0;
-  const long a_bytes = fused_a_bytes(n16), stage_bytes = (long)sh.nsplit * fused_b_slot(sh.kpad, n16);
+  const long a_bytes = fused_a_bytes(sh.kpad), stage_bytes = (long)sh.nsplit * fused_b_slot(sh.kpad, n16);
   const long avail = (long)maxsm - (long)fa.sharedSizeBytes - 1024 - sh.nsplit * a_bytes - tab_bytes;
   return (int)std::max<long>(0, std::min<long>(MAX_STAGES, avail / stage_bytes));
 }
@@ -1474,26 +1462,21 @@ static int fused_stages(const TcShape& sh, int n16, int tab_bytes) {
 template <int FMT>
 static qmt_status run_fused(qmt_mol* m, const TcShape& sh, const PointMap& pm, int64_t ntiles, float* qube,
                             double outscale, cudaStream_t s) {
-  qmt_status st;
   const int K = sh.kpad, n16 = fused_n16(m);
   const size_t piece = (size_t)(K + 64) * K * 2;
-  CUtensorMap tU_hi, tU_lo;
   const uint8_t* B = m->d_fused_B.as<uint8_t>();
-  // fewer, taller boxes for the full matrix (a stage is one K-step of all n16 output columns)
-  const uint32_t box_rows = g_fused_tri ? 64u : (n16 <= 256 ? (uint32_t)n16 : (uint32_t)n16 / 2);
-  if ((st = make_map_sw32(&tU_hi, B, K, K + 64, box_rows)) || (st = make_map_sw32(&tU_lo, B + piece, K, K + 64, box_rows)))
-    return st;
   FusedParams p{};
   p.mol = m->view();
   p.pm = pm;
   p.ntiles = ntiles;
   p.kpad = K;
   p.n16 = n16;
-  p.full_cols = n16 / 64 * 64;
+  p.u_rows = K + 64;
+  p.u_hi = B;
+  p.u_lo = B + piece;
   p.ksteps = n16 / 16;
   p.tri = g_fused_tri;
   p.nchunks = (n16 + 63) / 64;
-  p.box_rows = (int)box_rows;
   if (p.nchunks > MAX_FUSED_CHUNKS) return fail(QMT_BAD_ARG, "fused density path supports kpad <= 320");
   for (int a = 0; a < m->natoms; ++a) {
     const int sa = m->atom_shell[a], sb = m->atom_shell[a + 1];
@@ -1503,7 +1486,7 @@ static qmt_status run_fused(qmt_mol* m, const TcShape& sh, const PointMap& pm, i
     for (int c = cfirst; c <= clast; ++c) p.chunk_need[c] += 2;   // two row halves per atom
   }
   p.nsplit = sh.nsplit;
-  p.a_bytes = fused_a_bytes(n16);
+  p.a_bytes = fused_a_bytes(K);
   p.b_slot = fused_b_slot(K, n16);
   p.stage_bytes = p.nsplit * p.b_slot;
   p.fmt = (uint32_t)sh.fmt;
@@ -1525,7 +1508,7 @@ static qmt_status run_fused(qmt_mol* m, const TcShape& sh, const PointMap& pm, i
   const size_t dyn = (size_t)p.nsplit * p.a_bytes + (size_t)stages * p.stage_bytes + p.tab_bytes + 1024;
   QMT_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)dyn));
   const int grid = (int)std::min<int64_t>(ntiles, sm_count());
-  kern<<<grid, FUSED_THREADS, dyn, s>>>(tU_hi, tU_lo, p);
+  kern<<<grid, FUSED_THREADS, dyn, s>>>(p);
   QMT_CHECK_LAUNCH("density_fused_kernel");
   return QMT_OK;
 }
@@ -1548,7 +1531,7 @@ static qmt_status ensure_tc_operands(qmt_mol* m, int prec, const TcShape& sh, cu
   const size_t piece = (size_t)sh.nrows_b * K * sh.esize;
   if ((st = m->d_tc_P.reserve(2 * piece))) return st;
   if ((st = ensure_mol_tables(m, fs, K, s))) return st;
-  if ((st = launch_split(m, K, g, 0, sh.fmt, m->d_tc_P.ptr, m->d_tc_P.as<uint8_t>() + piece, piece, s))) return st;
+  if ((st = launch_split(m, K, g, 0, sh.fmt, 0, m->d_tc_P.ptr, m->d_tc_P.as<uint8_t>() + piece, piece, s))) return st;
   m->tc_g = g;
   m->tc_prec = prec;
   return QMT_OK;
