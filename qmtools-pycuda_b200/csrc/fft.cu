@@ -13,8 +13,10 @@
 //   its octant [0, M/2]^3 is stored, cached per (M, h, device).
 //
 // 1D transforms are mixed-radix Stockham (self-sorting) FFTs of batches of lines in shared
-// memory, twiddles from a per-length table computed in FP64 on the host.  A solve is five
-// passes over an x-fastest complex work grid:
+// memory, twiddles from a per-length table computed in FP64 on the host; 256-point lines (the
+// padded grids of 128^3 boxes) take a register kernel instead (16 x 16 four-step, one
+// shared-memory exchange per transform).  A solve is five passes over an x-fastest complex work
+// grid:
 //   1. x forward, with the RHS assembled on the fly from q and the nuclei (only lines and
 //      elements inside the physical box are non-zero: y < ny, z < nz, x < nx);
 //   2. y forward on the z < nz planes (elements y >= ny are zero and not read);
@@ -330,6 +332,196 @@ __global__ void __launch_bounds__(256) fft_pass_kernel(const PassArgs a) {
   }
 }
 
+// ---- length-256 lines in registers -----------------------------------------------------------
+// 256 = 16 x 16 (four-step): thread t of a line holds elements t + 16 m (m = 0..15), forms the
+// 16-point DFT over m, multiplies by W256^(t k1), exchanges through shared memory so that it
+// holds the 16 values of its k1 = t, and forms the 16-point DFT over them; it then holds
+// X[t + 16 k2] (k2 = 0..15), the same element pattern as its input.  16 lines x 16 threads per
+// CTA; global loads and stores are issued 16 per thread back to back.
+struct Tw16 {
+  float2 w1, w2, w3, w6, w9;   // W16^p = table entry 16 p (conjugated for the inverse)
+};
+
+__device__ __forceinline__ Tw16 tw16(const float2* tw, bool inv) {
+  return Tw16{twid(tw, 16, inv), twid(tw, 32, inv), twid(tw, 48, inv), twid(tw, 96, inv), twid(tw, 144, inv)};
+}
+
+// In-place 4-point DFT (forward: W4 = -i; inverse: +i).
+__device__ __forceinline__ void dft4(float2& a0, float2& a1, float2& a2, float2& a3, bool inv) {
+  const float2 t0 = cadd(a0, a2), t1 = csub(a0, a2), t2 = cadd(a1, a3), t3 = csub(a1, a3);
+  const float2 t3r = inv ? make_float2(-t3.y, t3.x) : make_float2(t3.y, -t3.x);
+  a0 = cadd(t0, t2);
+  a2 = csub(t0, t2);
+  a1 = cadd(t1, t3r);
+  a3 = csub(t1, t3r);
+}
+
+// 16-point DFT of x[0..15] (4 x 4), result in natural order.
+__device__ __forceinline__ void dft16(float2 (&x)[16], const Tw16& w, bool inv) {
+#pragma unroll
+  for (int m2 = 0; m2 < 4; ++m2) dft4(x[m2], x[4 + m2], x[8 + m2], x[12 + m2], inv);
+  // x[m2 + 4 k1] holds the m2-th partial DFT at k1: twiddle W16^(m2 k1)
+  x[5] = cmul(x[5], w.w1);
+  x[9] = cmul(x[9], w.w2);
+  x[13] = cmul(x[13], w.w3);
+  x[6] = cmul(x[6], w.w2);
+  x[10] = inv ? make_float2(-x[10].y, x[10].x) : make_float2(x[10].y, -x[10].x);   // W16^4 = -+i
+  x[14] = cmul(x[14], w.w6);
+  x[7] = cmul(x[7], w.w3);
+  x[11] = cmul(x[11], w.w6);
+  x[15] = cmul(x[15], w.w9);
+#pragma unroll
+  for (int k1 = 0; k1 < 4; ++k1) dft4(x[4 * k1], x[4 * k1 + 1], x[4 * k1 + 2], x[4 * k1 + 3], inv);
+  // x[4 k1 + k2] holds X[k1 + 4 k2]
+  float2 y[16];
+#pragma unroll
+  for (int k1 = 0; k1 < 4; ++k1)
+#pragma unroll
+    for (int k2 = 0; k2 < 4; ++k2) y[k1 + 4 * k2] = x[4 * k1 + k2];
+#pragma unroll
+  for (int k = 0; k < 16; ++k) x[k] = y[k];
+}
+
+constexpr int F256_S = 273;   // line stride of the exchange buffer (odd: no bank conflicts either way)
+constexpr int F256_R = 17;    // row stride inside a line (odd)
+
+// One 256-point transform of the thread's line b (thread t of it); `buf` is the CTA's exchange
+// buffer (16 x F256_S), free on entry (the barrier below orders it after earlier readers).
+__device__ __forceinline__ void fft256_regs(float2 (&x)[16], const float2* tw, float2* buf, int b, int t, bool inv) {
+  const Tw16 w = tw16(tw, inv);
+  dft16(x, w, inv);
+#pragma unroll
+  for (int k1 = 1; k1 < 16; ++k1) x[k1] = cmul(x[k1], twid(tw, (t * k1) & 255, inv));
+  __syncthreads();
+#pragma unroll
+  for (int k1 = 0; k1 < 16; ++k1) buf[b * F256_S + k1 * F256_R + t] = x[k1];
+  __syncthreads();
+#pragma unroll
+  for (int u = 0; u < 16; ++u) x[u] = buf[b * F256_S + t * F256_R + u];
+  dft16(x, w, inv);
+}
+
+template <int MODE>
+__global__ void __launch_bounds__(256) fft256_pass_kernel(const PassArgs a) {
+  constexpr int L = 256;
+  extern __shared__ float2 fsm[];
+  float2* tw = fsm;
+  float2* buf = fsm + L;
+  float* sat = reinterpret_cast<float*>(buf + 16 * F256_S);   // atoms (PASS_X_RHS)
+  for (int i = threadIdx.x; i < L; i += blockDim.x) tw[i] = a.tw[i];
+  if constexpr (MODE == PASS_X_RHS) {
+    for (int i = threadIdx.x; i < a.mol.natoms; i += blockDim.x) {
+      sat[4 * i] = a.mol.coords[3 * i] * (float)R_BOHR;
+      sat[4 * i + 1] = a.mol.coords[3 * i + 1] * (float)R_BOHR;
+      sat[4 * i + 2] = a.mol.coords[3 * i + 2] * (float)R_BOHR;
+      sat[4 * i + 3] = (float)a.mol.types[i];
+    }
+  }
+  const int64_t l0 = (int64_t)blockIdx.x * 16;
+  const int64_t rem = a.nlines - l0;
+  const int nb = rem < 16 ? (int)rem : 16;
+  __shared__ int64_t lbase[16];
+  __shared__ int lx[16], ly[16];
+  __shared__ int ncand[16];
+  __shared__ int cand[16][FFT_CAND];
+  __syncthreads();
+  if (threadIdx.x < nb) {
+    const int bb = threadIdx.x;
+    const int64_t l = l0 + bb;
+    const int c0 = (int)(l % a.n1), c1 = (int)(l / a.n1);
+    lx[bb] = c0;
+    ly[bb] = c1;
+    lbase[bb] = (int64_t)c0 * a.s1 + (int64_t)c1 * a.s2;
+    if constexpr (MODE == PASS_X_RHS) {
+      const float py = a.oy + (c0 + 0.5f) * a.h_ang, pz = a.oz + (c1 + 0.5f) * a.h_ang;
+      int cnt = 0;
+      for (int at = 0; at < a.mol.natoms; ++at) {
+        const float cy = py - sat[4 * at + 1], cz = pz - sat[4 * at + 2];
+        if (cy * cy + cz * cz <= a.cut2 * 1.0001f) {
+          if (cnt < FFT_CAND) cand[bb][cnt] = at;
+          ++cnt;
+        }
+      }
+      ncand[bb] = cnt <= FFT_CAND ? cnt : -1;
+    }
+  }
+  __syncthreads();
+  // lines adjacent in memory: a half-warp spans the 16 lines at one element (128 contiguous
+  // bytes); lines contiguous: a half-warp spans 16 consecutive elements of one line
+  const bool bfast = a.s1 == 1;
+  const int b = bfast ? (threadIdx.x & 15) : (threadIdx.x >> 4);
+  const int t = bfast ? (threadIdx.x >> 4) : (threadIdx.x & 15);
+  const bool live = b < nb;
+  float2 x[16];
+#pragma unroll
+  for (int m = 0; m < 16; ++m) {
+    const int e = t + 16 * m;
+    float2 v = make_float2(0.f, 0.f);
+    if (live && e < a.lload) {
+      if constexpr (MODE == PASS_X_RHS) {
+        const int y = lx[b], z = ly[b], xx = e;
+        const float px = a.ox + (xx + 0.5f) * a.h_ang, py = a.oy + (y + 0.5f) * a.h_ang,
+                    pz = a.oz + (z + 0.5f) * a.h_ang;
+        float rho = a.q[xx + (int64_t)y * a.nx + (int64_t)z * a.nx * a.ny] / (-a.h_ang * a.h_ang * a.h_ang);
+        const int nc = ncand[b];
+        const int cnt = nc < 0 ? a.mol.natoms : nc;
+        for (int c = 0; c < cnt; ++c) {
+          const int at = nc < 0 ? c : cand[b][c];
+          const float cx = px - sat[4 * at], cy = py - sat[4 * at + 1], cz = pz - sat[4 * at + 2];
+          const float r2 = cx * cx + cy * cy + cz * cz;
+          if (r2 <= a.cut2) rho += sat[4 * at + 3] * a.norm * expf(-r2 * a.i2s2);
+        }
+        v.x = a.periodic ? (float)(-(double)rho / EPS0) : rho * a.h_ang * a.h_ang * a.h_ang;
+      } else {
+        v = a.data[lbase[b] + (int64_t)e * a.se];
+      }
+    }
+    x[m] = v;
+  }
+  fft256_regs(x, tw, buf, b, t, a.inv != 0);
+  if constexpr (MODE == PASS_Z_MUL) {
+    const int hx = a.Mx / 2 + 1, hy = a.My / 2 + 1;
+    const int xg = lx[b], yg = ly[b];
+#pragma unroll
+    for (int k2 = 0; k2 < 16; ++k2) {
+      const int kz = t + 16 * k2;
+      float f;
+      if (a.periodic) {
+        // kernel_fft.cu:90-104: k in cycles/Ang, negative frequencies above N/2 - 1, k = 0 -> 0
+        const float kx = (xg > a.Mx / 2 - 1 ? (float)(xg - a.Mx) : (float)xg) / (a.Mx * a.h_ang);
+        const float ky = (yg > a.My / 2 - 1 ? (float)(yg - a.My) : (float)yg) / (a.My * a.h_ang);
+        const float kk = (kz > a.Mz / 2 - 1 ? (float)(kz - a.Mz) : (float)kz) / (a.Mz * a.h_ang);
+        const double k2d = (double)(kx * kx + ky * ky + kk * kk);
+        f = (xg == 0 && yg == 0 && kz == 0) ? 0.f : (float)(-1.0 / (4.0 * PI * PI * k2d));
+      } else {
+        const int gx = min(xg, a.Mx - xg), gy = min(yg, a.My - yg), gz = min(kz, a.Mz - kz);
+        f = live ? __ldg(a.gsym + gx + (int64_t)hx * (gy + (int64_t)hy * gz)) : 0.f;
+      }
+      x[k2] = make_float2(x[k2].x * f, x[k2].y * f);
+    }
+    fft256_regs(x, tw, buf, b, t, a.inv == 0);
+  }
+  if constexpr (MODE == PASS_X_OUT) {
+    // line (z = lx, y = ly) along x into the C-order output: regroup through shared memory so
+    // that a half-warp writes 16 consecutive z of one x
+    __syncthreads();
+#pragma unroll
+    for (int k2 = 0; k2 < 16; ++k2) buf[b * F256_S + t + 16 * k2] = x[k2];
+    __syncthreads();
+    const int bo = threadIdx.x & 15;
+    if (bo < nb)
+      for (int e = threadIdx.x >> 4; e < a.lstore; e += 16)
+        a.out[(int64_t)e * a.ny * a.nz + (int64_t)ly[bo] * a.nz + lx[bo]] = buf[bo * F256_S + e].x * a.scale;
+  } else {
+#pragma unroll
+    for (int k2 = 0; k2 < 16; ++k2) {
+      const int e = t + 16 * k2;
+      if (live && e < a.lstore)
+        a.data[lbase[b] + (int64_t)e * a.se] = make_float2(x[k2].x * a.scale, x[k2].y * a.scale);
+    }
+  }
+}
+
 // ---- Green's function ----------------------------------------------------------------
 __global__ void green_kernel(float2* __restrict__ g, int Mx, int My, int Mz, float h_ang) {
   const int64_t n = (int64_t)Mx * My * Mz;
@@ -411,12 +603,33 @@ static qmt_status launch_mode(const PassArgs& a, unsigned blocks, size_t smem, c
   return QMT_OK;
 }
 
+template <int MODE>
+static qmt_status launch_mode256(const PassArgs& a, unsigned blocks, size_t smem, cudaStream_t s) {
+  QMT_CUDA(cudaFuncSetAttribute(fft256_pass_kernel<MODE>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+  fft256_pass_kernel<MODE><<<blocks, 256, smem, s>>>(a);
+  QMT_CHECK_LAUNCH("fft256_pass_kernel");
+  return QMT_OK;
+}
+
 static qmt_status launch_pass(int mode, PassArgs a, cudaStream_t s) {
   a.B = std::max(1, std::min(16, 12288 / a.plan.L));
   const float2* tw;
   qmt_status st = twiddles(a.plan.L, &tw);
   if (st) return st;
   a.tw = tw;
+  if (a.plan.L == 256) {   // register kernel for 256-point lines
+    a.B = 16;
+    size_t smem = ((size_t)256 + 16 * F256_S) * sizeof(float2);
+    if (mode == PASS_X_RHS) smem += 16 * (size_t)a.mol.natoms;
+    const unsigned blocks = (unsigned)((a.nlines + 15) / 16);
+    if (blocks == 0) return QMT_OK;
+    switch (mode) {
+      case PASS_PLAIN: return launch_mode256<PASS_PLAIN>(a, blocks, smem, s);
+      case PASS_X_RHS: return launch_mode256<PASS_X_RHS>(a, blocks, smem, s);
+      case PASS_Z_MUL: return launch_mode256<PASS_Z_MUL>(a, blocks, smem, s);
+      default: return launch_mode256<PASS_X_OUT>(a, blocks, smem, s);
+    }
+  }
   size_t smem = ((size_t)a.plan.L * (1 + 2 * a.B)) * sizeof(float2);
   if (mode == PASS_X_RHS) smem += 16 * (size_t)a.mol.natoms;
   const unsigned blocks = (unsigned)((a.nlines + a.B - 1) / a.B);
