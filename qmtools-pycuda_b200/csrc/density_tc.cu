@@ -108,7 +108,7 @@ struct TcParams {
   float* qube;
   double* partials;
   double outscale;
-  double inv_g;
+  const double* gsc;   // device {max, 2^g, 2^-g} of the split density matrix
   int* err;
 };
 
@@ -342,7 +342,7 @@ __global__ void __launch_bounds__(192, 1)
         mbar_arrive(&tempty[buf]);
       }
       if (!ok) break;
-      rho_s[row] = acc * p.inv_g;
+      rho_s[row] = acc * p.gsc[2];
       named_barrier(1, 128);
       double mysum = 0.0;
       if (et < p.pm.vpt) {
@@ -430,8 +430,9 @@ __host__ __device__ inline void split_host(double x, int fmt, void* hi, void* lo
 // each row's two 16-byte units exchanged when bit 2 of the row is set -- the 32-byte swizzled
 // K-major image that the MMA reads from shared memory, so that a stage is one contiguous copy.
 __global__ void split_P_kernel(const double* __restrict__ P, int np, int n, int K, const double* __restrict__ inv_s,
-                               double two_g, int tri, int fmt, int blk_rows, uint8_t* hi, uint8_t* lo) {
+                               const double* __restrict__ gsc, int tri, int fmt, int blk_rows, uint8_t* hi, uint8_t* lo) {
   const int64_t tot = (int64_t)n * n;
+  const double two_g = gsc[1];
   for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < tot; i += (int64_t)gridDim.x * blockDim.x) {
     const int r = (int)(i / n), c = (int)(i % n);
     if (tri && c > r) continue;
@@ -443,36 +444,84 @@ __global__ void split_P_kernel(const double* __restrict__ P, int np, int n, int 
   }
 }
 
-// Device scales 2^-s_j (K doubles) for split_P_kernel, and the exponent g that puts
-// max |P_jk 2^(-s_j-s_k)| near 2^14.
-static qmt_status split_scales(qmt_mol* m, const std::vector<int>& sj, int K, int* g_out, cudaStream_t s) {
-  const int n = m->norbs, np = m->npad;
-  std::vector<double> inv(K, 1.0);
-  for (int j = 0; j < n; ++j) inv[j] = std::ldexp(1.0, -sj[j]);
-  double mx = 0;
-  for (int j = 0; j < n; ++j) {
-    const double* row = m->P64.data() + (size_t)j * np;
-    double rm = 0;
-    for (int k = 0; k < n; ++k) rm = std::max(rm, std::fabs(row[k]) * inv[k]);
-    mx = std::max(mx, rm * inv[j]);
+// max_jk |P_jk| 2^(-s_j - s_k) over the n x n block, as the bits of a non-negative double
+// (ordered like the values), into gsc[0].
+__global__ void split_max_kernel(const double* __restrict__ P, int np, int n, const double* __restrict__ inv_s,
+                                 unsigned long long* gsc_bits) {
+  __shared__ double red[32];
+  double mx = 0.0;
+  const int64_t tot = (int64_t)n * n;
+  for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < tot; i += (int64_t)gridDim.x * blockDim.x) {
+    const int j = (int)(i / n), k = (int)(i - (int64_t)j * n);
+    mx = fmax(mx, fabs(P[(size_t)j * np + k]) * inv_s[k] * inv_s[j]);
   }
-  int g = mx > 0 ? (int)std::floor(std::log2(16000.0 / mx)) : 0;
-  *g_out = std::max(-100, std::min(100, g));
+  for (int o = 16; o > 0; o >>= 1) mx = fmax(mx, __shfl_xor_sync(0xffffffffu, mx, o));
+  if ((threadIdx.x & 31) == 0) red[threadIdx.x >> 5] = mx;
+  __syncthreads();
+  if (threadIdx.x < 32) {
+    mx = threadIdx.x < (blockDim.x >> 5) ? red[threadIdx.x] : 0.0;
+    for (int o = 16; o > 0; o >>= 1) mx = fmax(mx, __shfl_xor_sync(0xffffffffu, mx, o));
+    if (threadIdx.x == 0) atomicMax(gsc_bits, (unsigned long long)__double_as_longlong(mx));
+  }
+}
+
+// The exponent g that puts that maximum near 2^14 (g in [-100, 100], 0 for a zero matrix):
+// gsc[1] = 2^g, gsc[2] = 2^-g.
+__global__ void split_exp_kernel(double* gsc) {
+  const double mx = __longlong_as_double((long long)reinterpret_cast<const unsigned long long*>(gsc)[0]);
+  int g = mx > 0 ? (int)floor(log2(16000.0 / mx)) : 0;
+  g = max(-100, min(100, g));
+  gsc[1] = ldexp(1.0, g);
+  gsc[2] = ldexp(1.0, -g);
+}
+
+// Column scales 2^s_j (fs, folded into the producer tables) and 2^-s_j (device, for the split)
+// and the producer tables: they depend on the basis only, so they are built once per molecule.
+static qmt_status ensure_mol_tables(qmt_mol* m, const std::vector<float>& fs, int K, cudaStream_t s);
+static qmt_status ensure_basis_operands(qmt_mol* m, int K, cudaStream_t s) {
+  if (m->basis_ops_ready) return QMT_OK;
+  const int n = m->norbs;
+  std::vector<float> fs(K, 0.f);
+  std::vector<double> inv(K, 1.0);
+  for (int j = 0; j < n; ++j) {
+    const double b = std::max(m->fbound[j], 1e-30);
+    const int sj = std::max(-60, std::min(60, (int)std::floor(std::log2(16000.0 / b))));
+    fs[j] = (float)std::ldexp(1.0, sj);
+    inv[j] = std::ldexp(1.0, -sj);
+  }
   qmt_status st = m->d_split_scale.reserve(K * sizeof(double));
   if (st) return st;
   // pageable uploads return once the data is staged, so `inv` may go
   QMT_CUDA(cudaMemcpyAsync(m->d_split_scale.ptr, inv.data(), K * sizeof(double), cudaMemcpyHostToDevice, s));
+  if ((st = ensure_mol_tables(m, fs, K, s))) return st;
+  m->basis_ops_ready = true;
   return QMT_OK;
 }
 
-static qmt_status launch_split(qmt_mol* m, int K, int g, int tri, int fmt, int blk_rows, void* hi, void* lo,
+// Exponent of the scaled density matrix, on the device (no host round trip).
+static qmt_status split_exponent(qmt_mol* m, cudaStream_t s) {
+  qmt_status st = m->d_gscale.reserve(4 * sizeof(double));
+  if (st) return st;
+  QMT_CUDA(cudaMemsetAsync(m->d_gscale.ptr, 0, sizeof(double), s));
+  const int64_t tot = (int64_t)m->norbs * m->norbs;
+  const int blocks = (int)std::min<int64_t>((tot + 255) / 256, (int64_t)sm_count() * 2);
+  split_max_kernel<<<std::max(blocks, 1), 256, 0, s>>>(m->d_P64.as<double>(), m->npad, m->norbs,
+                                                       m->d_split_scale.as<double>(),
+                                                       reinterpret_cast<unsigned long long*>(m->d_gscale.ptr));
+  QMT_CHECK_LAUNCH("split_max_kernel");
+  split_exp_kernel<<<1, 1, 0, s>>>(m->d_gscale.as<double>());
+  QMT_CHECK_LAUNCH("split_exp_kernel");
+  return QMT_OK;
+}
+
+static qmt_status launch_split(qmt_mol* m, int K, int tri, int fmt, int blk_rows, void* hi, void* lo,
                                size_t piece_bytes, cudaStream_t s) {
   QMT_CUDA(cudaMemsetAsync(hi, 0, piece_bytes, s));
   QMT_CUDA(cudaMemsetAsync(lo, 0, piece_bytes, s));
   const int64_t tot = (int64_t)m->norbs * m->norbs;
   const int blocks = (int)std::min<int64_t>((tot + 255) / 256, (int64_t)sm_count() * 8);
   split_P_kernel<<<std::max(blocks, 1), 256, 0, s>>>(m->d_P64.as<double>(), m->npad, m->norbs, K,
-                                                     m->d_split_scale.as<double>(), std::ldexp(1.0, g), tri, fmt, blk_rows,
+                                                     m->d_split_scale.as<double>(), m->d_gscale.as<double>(), tri, fmt, blk_rows,
                                                      reinterpret_cast<uint8_t*>(hi), reinterpret_cast<uint8_t*>(lo));
   QMT_CHECK_LAUNCH("split_P_kernel");
   return QMT_OK;
@@ -528,7 +577,8 @@ struct FusedParams {
   float* qube;
   double* partials;
   double outscale;
-  double inv_g2;           // 2 * 2^-g
+  const double* gsc;       // device {max, 2^g, 2^-g} of the split density matrix
+  double g_mul;            // 2 (triangular U) or 1
   int* err;
 };
 
@@ -1287,7 +1337,7 @@ __global__ void __launch_bounds__(FUSED_THREADS, 1)
         }
         const int64_t vox = t * p.pm.vpt + ct;
         if (vox < p.pm.nvox) {
-          const float qv = (float)(r * p.inv_g2 * p.outscale);
+          const float qv = (float)(r * (p.g_mul * p.gsc[2]) * p.outscale);
           p.qube[vox] = qv;
           mysum = qv;
         }
@@ -1411,25 +1461,15 @@ static int g_fused_tri = 0;   // upper-triangular variant of the fused path (off
 static qmt_status ensure_fused_operands(qmt_mol* m, int prec, const TcShape& sh, cudaStream_t s) {
   const int key = prec * 2 + g_fused_tri;
   if (m->fused_prec == key) return QMT_OK;
-  const int n = m->norbs, K = sh.kpad;
-  std::vector<int> sj(K, 0);
-  std::vector<float> fs(K, 0.f);
-  for (int j = 0; j < n; ++j) {
-    const double b = std::max(m->fbound[j], 1e-30);
-    sj[j] = std::max(-60, std::min(60, (int)std::floor(std::log2(16000.0 / b))));
-    fs[j] = (float)std::ldexp(1.0, sj[j]);
-  }
-  int g = 0;
-  qmt_status st = split_scales(m, sj, K, &g, s);
-  if (st) return st;
+  const int K = sh.kpad;
+  qmt_status st;
+  if ((st = ensure_basis_operands(m, K, s)) || (st = split_exponent(m, s))) return st;
   const int rows = K + 64;
   const size_t piece = (size_t)rows * K * 2;
   if ((st = m->d_fused_B.reserve(2 * piece))) return st;
-  if ((st = launch_split(m, K, g, g_fused_tri, sh.fmt, K + 64, m->d_fused_B.ptr, m->d_fused_B.as<uint8_t>() + piece,
+  if ((st = launch_split(m, K, g_fused_tri, sh.fmt, K + 64, m->d_fused_B.ptr, m->d_fused_B.as<uint8_t>() + piece,
                          piece, s)))
     return st;
-  if ((st = ensure_mol_tables(m, fs, K, s))) return st;
-  m->fused_g = g;
   m->fused_prec = key;
   return QMT_OK;
 }
@@ -1499,7 +1539,8 @@ static qmt_status run_fused(qmt_mol* m, const TcShape& sh, const PointMap& pm, i
   p.qube = qube;
   p.partials = m->d_partials.as<double>();
   p.outscale = outscale;
-  p.inv_g2 = (g_fused_tri ? 2.0 : 1.0) * std::ldexp(1.0, -m->fused_g);
+  p.gsc = m->d_gscale.as<double>();
+  p.g_mul = g_fused_tri ? 2.0 : 1.0;
   p.err = reinterpret_cast<int*>(m->d_scalars.as<double>() + 8);
   auto kern = density_fused_kernel<FMT>;
   const int stages = fused_stages<FMT>(sh, n16, p.tab_bytes);
@@ -1516,23 +1557,12 @@ static qmt_status run_fused(qmt_mol* m, const TcShape& sh, const PointMap& pm, i
 // Builds the scaled, split density matrix and the Phi column scales for `prec`.
 static qmt_status ensure_tc_operands(qmt_mol* m, int prec, const TcShape& sh, cudaStream_t s) {
   if (m->tc_prec == prec) return QMT_OK;
-  const int n = m->norbs, K = sh.kpad;
-  std::vector<int> sj(K, 0);
-  std::vector<float> fs(K, 0.f);
-  for (int j = 0; j < n; ++j) {
-    const double b = std::max(m->fbound[j], 1e-30);
-    sj[j] = (int)std::floor(std::log2(16000.0 / b));
-    sj[j] = std::max(-60, std::min(60, sj[j]));
-    fs[j] = (float)std::ldexp(1.0, sj[j]);
-  }
-  int g = 0;
-  qmt_status st = split_scales(m, sj, K, &g, s);
-  if (st) return st;
+  const int K = sh.kpad;
+  qmt_status st;
+  if ((st = ensure_basis_operands(m, K, s)) || (st = split_exponent(m, s))) return st;
   const size_t piece = (size_t)sh.nrows_b * K * sh.esize;
   if ((st = m->d_tc_P.reserve(2 * piece))) return st;
-  if ((st = ensure_mol_tables(m, fs, K, s))) return st;
-  if ((st = launch_split(m, K, g, 0, sh.fmt, 0, m->d_tc_P.ptr, m->d_tc_P.as<uint8_t>() + piece, piece, s))) return st;
-  m->tc_g = g;
+  if ((st = launch_split(m, K, 0, sh.fmt, 0, m->d_tc_P.ptr, m->d_tc_P.as<uint8_t>() + piece, piece, s))) return st;
   m->tc_prec = prec;
   return QMT_OK;
 }
@@ -1578,7 +1608,7 @@ static qmt_status run_tc(qmt_mol* m, const TcShape& sh, const PointMap& pm, int6
   p.qube = qube;
   p.partials = m->d_partials.as<double>();
   p.outscale = outscale;
-  p.inv_g = std::ldexp(1.0, -m->tc_g);
+  p.gsc = m->d_gscale.as<double>();
   p.err = reinterpret_cast<int*>(m->d_scalars.as<double>() + 8);
 
   int maxsm = 0, dev = 0;

@@ -336,6 +336,7 @@ static qmt_status build_pairs(qmt_mol* m, cudaStream_t s) {
   std::vector<Acc> acc;
   std::unordered_map<std::string, int> index;
   const int ns = m->nshells, np = m->npad;
+  const std::vector<double>& P64 = m->host_P64();
   for (int iA = 0; iA < ns; ++iA) {
     const Shell& A = m->shells[iA];
     const double Ax = m->coords[3 * A.atom], Ay = m->coords[3 * A.atom + 1], Az = m->coords[3 * A.atom + 2];
@@ -347,7 +348,7 @@ static qmt_status build_pairs(qmt_mol* m, cudaStream_t s) {
       double pmax = 0;
       for (int k1 = 0; k1 < 2 * A.L + 1; ++k1)
         for (int k2 = 0; k2 < 2 * B.L + 1; ++k2)
-          pmax = std::max(pmax, std::fabs(m->P64[(size_t)(A.func + k1) * np + B.func + k2]));
+          pmax = std::max(pmax, std::fabs(P64[(size_t)(A.func + k1) * np + B.func + k2]));
       if (pmax == 0) continue;
       for (int ia = 0; ia < A.nprim; ++ia)
         for (int ib = 0; ib < B.nprim; ++ib) {
@@ -370,7 +371,7 @@ static qmt_status build_pairs(qmt_mol* m, cudaStream_t s) {
             int e1[3][3];
             const int n1 = cart_host(A.L, k1, c1, e1);
             for (int k2 = 0; k2 < 2 * B.L + 1; ++k2) {
-              const double w = m->P64[(size_t)(A.func + k1) * np + B.func + k2];
+              const double w = P64[(size_t)(A.func + k1) * np + B.func + k2];
               if (w == 0) continue;
               double c2[3];
               int e2[3][3];

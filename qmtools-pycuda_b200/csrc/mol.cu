@@ -79,8 +79,42 @@ using namespace qmt;
 qmt_mol::~qmt_mol() {
   for (DevBuf* b : {&d_coords, &d_types, &d_shells, &d_alpha, &d_coeff, &d_alpha64, &d_coeff64,
                     &d_P32, &d_P64, &d_Phi_hi, &d_Phi_lo, &d_tc_P, &d_partials,
-                    &d_scalars, &d_pairs, &d_work, &d_atom_shell, &d_fused_B, &d_fused_tab, &d_split_scale})
+                    &d_scalars, &d_pairs, &d_work, &d_atom_shell, &d_fused_B, &d_fused_tab, &d_split_scale,
+                    &d_dm_raw, &d_gscale})
     b->release();
+  if (dm_stage_ev) cudaEventDestroy(dm_stage_ev);
+  if (h_dm_stage) cudaFreeHost(h_dm_stage);
+}
+
+namespace qmt {
+// P (npad x npad, FP64 and FP32) symmetric from the lower triangle of the caller's matrix,
+// zero in the padding.
+__global__ void sym_dm_kernel(const float* __restrict__ raw, int n, int np, double* __restrict__ P64,
+                              float* __restrict__ P32) {
+  const int64_t tot = (int64_t)np * np;
+  for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < tot; i += (int64_t)gridDim.x * blockDim.x) {
+    const int r = (int)(i / np), c = (int)(i - (int64_t)r * np);
+    float v = 0.f;
+    if (r < n && c < n) v = c <= r ? raw[(size_t)r * n + c] : raw[(size_t)c * n + r];
+    P64[i] = v;
+    P32[i] = v;
+  }
+}
+}  // namespace qmt
+
+const std::vector<double>& qmt_mol::host_P64() {
+  if (!p64_host_valid) {
+    const int n = norbs, np = npad;
+    P64.assign((size_t)np * np, 0.0);
+    for (int p = 0; p < n; ++p)
+      for (int q = 0; q <= p; ++q) {
+        const double v = h_dm_stage[(size_t)p * n + q];
+        P64[(size_t)p * np + q] = v;
+        P64[(size_t)q * np + p] = v;
+      }
+    p64_host_valid = true;
+  }
+  return P64;
 }
 
 static qmt_status upload(DevBuf& b, const void* src, size_t n, cudaStream_t s) {
@@ -99,21 +133,41 @@ qmt_status qmt_mol::upload_coords(const float* c, cudaStream_t s) {
 
 qmt_status qmt_mol::upload_dm(const float* dm, cudaStream_t s) {
   const int n = norbs, np = npad;
-  P64.assign((size_t)np * np, 0.0);
-  for (int p = 0; p < n; ++p)
-    for (int q = 0; q <= p; ++q) {
-      const float v = dm[(size_t)p * n + q];
-      if (!std::isfinite(v)) return fail(QMT_NAN, "non-finite density matrix entry");
-      P64[(size_t)p * np + q] = v;
-      P64[(size_t)q * np + p] = v;
+  const size_t bytes = (size_t)n * n * sizeof(float);
+  // the lower triangle is the matrix (the reference reads it that way)
+  for (int p = 0; p < n; ++p) {
+    const float* row = dm + (size_t)p * n;
+    for (int q = 0; q <= p; ++q)
+      if (!std::isfinite(row[q])) return fail(QMT_NAN, "non-finite density matrix entry");
+  }
+  // pinned staging copy (also the host's copy of the matrix), reused once the previous upload
+  // from it has completed
+  if (!dm_stage_ev) QMT_CUDA(cudaEventCreateWithFlags(&dm_stage_ev, cudaEventDisableTiming));
+  if (h_dm_stage_bytes < bytes) {
+    if (h_dm_stage) {
+      QMT_CUDA(cudaEventSynchronize(dm_stage_ev));
+      cudaFreeHost(h_dm_stage);
+      h_dm_stage = nullptr;
+      h_dm_stage_bytes = 0;
     }
-  std::vector<float> P32(P64.begin(), P64.end());
-  qmt_status st = upload(d_P64, P64.data(), P64.size() * sizeof(double), s);
-  if (st) return st;
-  st = upload(d_P32, P32.data(), P32.size() * sizeof(float), s);
-  if (st) return st;
-  // host copies must outlive the async copies: synchronise before the vectors go away
-  QMT_CUDA(cudaStreamSynchronize(s));
+    QMT_CUDA(cudaHostAlloc(reinterpret_cast<void**>(&h_dm_stage), bytes, cudaHostAllocDefault));
+    h_dm_stage_bytes = bytes;
+  } else {
+    QMT_CUDA(cudaEventSynchronize(dm_stage_ev));
+  }
+  std::memcpy(h_dm_stage, dm, bytes);
+  p64_host_valid = false;
+  qmt_status st;
+  if ((st = d_dm_raw.reserve(bytes)) || (st = d_P64.reserve((size_t)np * np * sizeof(double))) ||
+      (st = d_P32.reserve((size_t)np * np * sizeof(float))))
+    return st;
+  QMT_CUDA(cudaMemcpyAsync(d_dm_raw.ptr, h_dm_stage, bytes, cudaMemcpyHostToDevice, s));
+  QMT_CUDA(cudaEventRecord(dm_stage_ev, s));
+  const int64_t tot = (int64_t)np * np;
+  const int blocks = (int)std::min<int64_t>((tot + 255) / 256, (int64_t)sm_count() * 4);
+  sym_dm_kernel<<<std::max(blocks, 1), 256, 0, s>>>(d_dm_raw.as<float>(), n, np, d_P64.as<double>(),
+                                                    d_P32.as<float>());
+  QMT_CHECK_LAUNCH("sym_dm_kernel");
   tc_prec = -1;
   fused_prec = -1;
   gto_ready = false;
@@ -132,6 +186,7 @@ static qmt_status mol_init(qmt_mol* m, int natoms, const int32_t* types, const f
   m->tc_prec = -1;
   m->fused_prec = -1;
   m->gto_ready = false;
+  m->basis_ops_ready = false;
   m->natoms = natoms;
   m->norbs = norbs;
   m->npad = (norbs + 31) / 32 * 32;
@@ -267,9 +322,9 @@ qmt_status qmt_mol_reset(qmt_mol* mol, int natoms, const int32_t* types, const f
 qmt_status qmt_mol_set_coords(qmt_mol* mol, const float* coords, void* stream) {
   if (!mol || !coords) return fail(QMT_BAD_ARG, "null argument");
   cudaStream_t s = as_stream(stream);
+  // the pageable upload returns once the data is staged, so no synchronisation is needed
   qmt_status st = mol->upload_coords(coords, s);
   if (st) return st;
-  QMT_CUDA(cudaStreamSynchronize(s));
   mol->gto_ready = false;
   return QMT_OK;
 }

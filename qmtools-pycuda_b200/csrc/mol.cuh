@@ -30,12 +30,20 @@ struct qmt_mol {
   std::vector<int> atom_shell;  // shells of atom a are [atom_shell[a], atom_shell[a+1])
   std::vector<float> alpha, coeff;
   std::vector<double> alpha64, coeff64;
-  std::vector<double> P64;      // symmetric (from the lower triangle), npad x npad
+  std::vector<double> P64;      // symmetric (from the lower triangle), npad x npad; host copy built on
+                                // demand from the staged matrix (host_P64), the device copies by a kernel
+  bool p64_host_valid = false;
+  const std::vector<double>& host_P64();
+  float* h_dm_stage = nullptr;  // pinned copy of the caller's density matrix (the latest upload)
+  size_t h_dm_stage_bytes = 0;
+  cudaEvent_t dm_stage_ev = nullptr;   // the upload from the staging copy completed
+  qmt::DevBuf d_dm_raw;         // the matrix as given, norbs x norbs
+  bool basis_ops_ready = false; // column scales and producer tables (depend on the basis only)
+  qmt::DevBuf d_gscale;         // device {max, 2^g, 2^-g} of the split density matrix
   std::vector<double> fbound;   // per-function bound on |phi|
 
   qmt::DevBuf d_atom_shell;
   int fused_prec = -1;          // precision of the fused-path operands below
-  int fused_g = 0;
   qmt::DevBuf d_fused_B;        // scaled density matrix pieces for the fused path (hi then lo)
   qmt::DevBuf d_split_scale;    // 2^-s_j per function for the device split of the density matrix
   qmt::DevBuf d_fused_tab;      // fused path: packed shell records, then (alpha, scaled coefficient) pairs
@@ -43,7 +51,6 @@ struct qmt_mol {
   qmt::DevBuf d_P32, d_P64;
   // tensor-core operands
   int tc_prec = -1;             // precision the operands below were built for
-  int tc_g = 0;                 // global exponent of the scaled density matrix
   qmt::DevBuf d_tc_P;           // split, scaled density matrix (hi then lo)
   qmt::DevBuf d_Phi_hi, d_Phi_lo;
   // scratch
