@@ -82,8 +82,6 @@ qmt_mol::~qmt_mol() {
                     &d_scalars, &d_pairs, &d_work, &d_atom_shell, &d_fused_B, &d_fused_tab, &d_split_scale,
                     &d_dm_raw, &d_gscale})
     b->release();
-  if (dm_stage_ev) cudaEventDestroy(dm_stage_ev);
-  if (h_dm_stage) cudaFreeHost(h_dm_stage);
 }
 
 namespace qmt {
@@ -108,7 +106,7 @@ const std::vector<double>& qmt_mol::host_P64() {
     P64.assign((size_t)np * np, 0.0);
     for (int p = 0; p < n; ++p)
       for (int q = 0; q <= p; ++q) {
-        const double v = h_dm_stage[(size_t)p * n + q];
+        const double v = dm_host[(size_t)p * n + q];
         P64[(size_t)p * np + q] = v;
         P64[(size_t)q * np + p] = v;
       }
@@ -140,29 +138,15 @@ qmt_status qmt_mol::upload_dm(const float* dm, cudaStream_t s) {
     for (int q = 0; q <= p; ++q)
       if (!std::isfinite(row[q])) return fail(QMT_NAN, "non-finite density matrix entry");
   }
-  // pinned staging copy (also the host's copy of the matrix), reused once the previous upload
-  // from it has completed
-  if (!dm_stage_ev) QMT_CUDA(cudaEventCreateWithFlags(&dm_stage_ev, cudaEventDisableTiming));
-  if (h_dm_stage_bytes < bytes) {
-    if (h_dm_stage) {
-      QMT_CUDA(cudaEventSynchronize(dm_stage_ev));
-      cudaFreeHost(h_dm_stage);
-      h_dm_stage = nullptr;
-      h_dm_stage_bytes = 0;
-    }
-    QMT_CUDA(cudaHostAlloc(reinterpret_cast<void**>(&h_dm_stage), bytes, cudaHostAllocDefault));
-    h_dm_stage_bytes = bytes;
-  } else {
-    QMT_CUDA(cudaEventSynchronize(dm_stage_ev));
-  }
-  std::memcpy(h_dm_stage, dm, bytes);
+  // host copy (the analytic-potential path reads it); the pageable upload returns once the data
+  // is staged, so the copy may be overwritten by the next call without synchronisation
+  dm_host.assign(dm, dm + (size_t)n * n);
   p64_host_valid = false;
   qmt_status st;
   if ((st = d_dm_raw.reserve(bytes)) || (st = d_P64.reserve((size_t)np * np * sizeof(double))) ||
       (st = d_P32.reserve((size_t)np * np * sizeof(float))))
     return st;
-  QMT_CUDA(cudaMemcpyAsync(d_dm_raw.ptr, h_dm_stage, bytes, cudaMemcpyHostToDevice, s));
-  QMT_CUDA(cudaEventRecord(dm_stage_ev, s));
+  QMT_CUDA(cudaMemcpyAsync(d_dm_raw.ptr, dm_host.data(), bytes, cudaMemcpyHostToDevice, s));
   const int64_t tot = (int64_t)np * np;
   const int blocks = (int)std::min<int64_t>((tot + 255) / 256, (int64_t)sm_count() * 4);
   sym_dm_kernel<<<std::max(blocks, 1), 256, 0, s>>>(d_dm_raw.as<float>(), n, np, d_P64.as<double>(),

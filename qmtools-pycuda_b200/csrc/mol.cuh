@@ -34,9 +34,7 @@ struct qmt_mol {
                                 // demand from the staged matrix (host_P64), the device copies by a kernel
   bool p64_host_valid = false;
   const std::vector<double>& host_P64();
-  float* h_dm_stage = nullptr;  // pinned copy of the caller's density matrix (the latest upload)
-  size_t h_dm_stage_bytes = 0;
-  cudaEvent_t dm_stage_ev = nullptr;   // the upload from the staging copy completed
+  std::vector<float> dm_host;   // the caller's density matrix as given (latest upload)
   qmt::DevBuf d_dm_raw;         // the matrix as given, norbs x norbs
   bool basis_ops_ready = false; // column scales and producer tables (depend on the basis only)
   qmt::DevBuf d_gscale;         // device {max, 2^g, 2^-g} of the split density matrix
