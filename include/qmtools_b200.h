@@ -78,9 +78,11 @@ qmt_status qmt_mol_create(int natoms, const int32_t* types, const float* coords,
 qmt_status qmt_mol_reset(qmt_mol* mol, int natoms, const int32_t* types, const float* coords,
                          int norbs, const int16_t* almos, int nparams, const float* alphas,
                          const float* coeffs, const float* dm, void* stream);
-/* Molecule.Translate upload (qmtools/qmtools.py:182-188): new coords[natoms*3] bohr. */
+/* Molecule.Translate upload (qmtools/qmtools.py:182-188): new coords[natoms*3] bohr.
+ * Stream-ordered: returns once the host array has been copied; later calls on `stream` see it. */
 qmt_status qmt_mol_set_coords(qmt_mol* mol, const float* coords, void* stream);
-/* New density matrix (same norbs). */
+/* New density matrix (same norbs).  Stream-ordered like qmt_mol_set_coords: the caller's array
+ * may be reused on return; the device operands are re-derived on `stream`. */
 qmt_status qmt_mol_set_dm(qmt_mol* mol, const float* dm, void* stream);
 qmt_status qmt_mol_destroy(qmt_mol* mol);
 /* FP64 Tr(P S) with the analytic overlap S, computed on the device (new; no reference
