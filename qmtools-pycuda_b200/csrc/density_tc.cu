@@ -1295,10 +1295,13 @@ __global__ void __launch_bounds__(FUSED_THREADS, 1)
       if (!mbar_wait(&t_full, tile_it & 1u, &abort_flag)) break;
       tc_fence_after();
       double acc[2] = {0.0, 0.0};
+      const uint32_t trow = tmem + ((uint32_t)(q * 32) << 16);
       for (int c = hh; c * 16 < p.n16; c += FUSED_NCW / 4) {
         const int col = c * 16;
-        float v[16], ph[16];
-        tmem_ld16(tmem + ((uint32_t)(q * 32) << 16) + (uint32_t)col, v);
+        // the TMEM load of T' is in flight while the row's Phi' units are read from shared memory
+        uint32_t tv[16];
+        tmem_ld16_issue(trow + (uint32_t)col, tv);
+        float ph[16];
         // the row's two 16-byte units of columns col .. col + 15 (layout of a_offset)
         const int u0 = (col & 63) >> 3;
         const uint32_t rbase = (uint32_t)((col >> 6) * 16384 + (row >> 3) * 1024 + (row & 7) * 128);
@@ -1316,11 +1319,12 @@ __global__ void __launch_bounds__(FUSED_THREADS, 1)
             for (int e = 0; e < 8; ++e) ph[8 * u + e] += lo8[e];
           }
         }
+        tmem_ld16_wait(tv);
         // eight products per FP32 partial, partials summed in FP64 (the FP32 partials add
         // ~3e-8 relative error; converting every product to FP64 ties up the conversion pipe)
         float a32[2] = {0.f, 0.f};
 #pragma unroll
-        for (int k = 0; k < 16; ++k) a32[k & 1] = fmaf(ph[k], v[k], a32[k & 1]);
+        for (int k = 0; k < 16; ++k) a32[k & 1] = fmaf(ph[k], __uint_as_float(tv[k]), a32[k & 1]);
         acc[0] += (double)a32[0];
         acc[1] += (double)a32[1];
       }
