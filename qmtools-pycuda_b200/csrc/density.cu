@@ -33,7 +33,16 @@ qmt_status make_point_map(int nx, int ny, int nz, float step, float ox, float oy
   pm.oy = oy;
   pm.oz = oz;
   pm.inv_s = 1.0 / subgrid;
-  ntiles = (pm.nvox + pm.vpt - 1) / pm.vpt;
+  pm.blocked = pm.vpt == 128 ? 1 : 0;
+  if (pm.blocked) {
+    pm.nbx = (nx + 7) / 8;
+    pm.nby = (ny + 3) / 4;
+    ntiles = (int64_t)pm.nbx * pm.nby * ((nz + 3) / 4);
+    if (ntiles >= (int64_t)1 << 31) return fail(QMT_BAD_ARG, "grid too large");
+  } else {
+    pm.nbx = pm.nby = 0;
+    ntiles = (pm.nvox + pm.vpt - 1) / pm.vpt;
+  }
   return QMT_OK;
 }
 
@@ -158,8 +167,8 @@ __global__ void __launch_bounds__(256) density_simt_kernel(MolView mol, PointMap
     if (tid < pm.vpt) {
       T acc = T(0);
       for (int s = 0; s < pm.s3; ++s) acc += rho_s[tid * pm.s3 + s];
-      const int64_t vox = tile * pm.vpt + tid;
-      if (vox < pm.nvox) {
+      int64_t vox, ix, iy, iz;
+      if (tile_voxel(pm, tile, tid, vox, ix, iy, iz)) {
         const float q = (float)((double)acc * outscale);
         qube[vox] = q;
         mysum = q;

@@ -348,8 +348,8 @@ __global__ void __launch_bounds__(192, 1)
       if (et < p.pm.vpt) {
         double r = 0.0;
         for (int s = 0; s < p.pm.s3; ++s) r += rho_s[et * p.pm.s3 + s];
-        const int64_t vox = (p.tile0 + t) * p.pm.vpt + et;
-        if (vox < p.pm.nvox) {
+        int64_t vox, ix, iy, iz;
+        if (tile_voxel(p.pm, p.tile0 + t, et, vox, ix, iy, iz)) {
           const float qv = (float)(r * p.outscale);
           p.qube[vox] = qv;
           mysum = qv;
@@ -1339,8 +1339,8 @@ __global__ void __launch_bounds__(FUSED_THREADS, 1)
 #pragma unroll
           for (int h3 = 0; h3 < FUSED_NCW / 4; ++h3) r += rho_part[h3][rr];
         }
-        const int64_t vox = t * p.pm.vpt + ct;
-        if (vox < p.pm.nvox) {
+        int64_t vox, ix, iy, iz;
+        if (tile_voxel(p.pm, t, ct, vox, ix, iy, iz)) {
           const float qv = (float)(r * (p.g_mul * p.gsc[2]) * p.outscale);
           p.qube[vox] = qv;
           mysum = qv;

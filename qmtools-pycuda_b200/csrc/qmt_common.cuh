@@ -111,8 +111,11 @@ __device__ __forceinline__ int shell_values(const Shell& sh, const T* __restrict
   return 5;
 }
 
-// Point of row `row` of a density tile: voxels are taken in flat x-fastest order,
-// `vpt` voxels per tile, s^3 sub-points per voxel (sub-point index fastest).
+// Points of a density tile.  With subgrid 1 (128 voxels per tile) a tile is an 8 x 4 x 4 block
+// of voxels (row v -> x + (v & 7), y + ((v >> 3) & 3), z + (v >> 5)), so that the rows of a work
+// item are close together and primitive screening over them skips more; otherwise voxels are
+// taken in flat x-fastest order, `vpt` per tile.  Each voxel has s^3 sub-points (sub-point index
+// fastest within the voxel's rows).
 struct PointMap {
   int nx, ny, nz;
   int s;          // subgrid
@@ -122,20 +125,27 @@ struct PointMap {
   float h;
   float ox, oy, oz;
   double inv_s;   // 1 / s
+  int blocked;    // 8 x 4 x 4 voxel blocks (vpt == 128)
+  int nbx, nby;   // blocks along x and y
 };
 
-template <typename T>
-__device__ __forceinline__ bool tile_point(const PointMap& pm, int64_t tile, int row,
-                                           T& x, T& y, T& z, int64_t& vox) {
-  int v = row, sub = 0;
-  if (pm.s3 > 1) {
-    v = row / pm.s3;
-    sub = row - v * pm.s3;
-  }
+// Voxel v (< vpt) of `tile`: grid indices and flat x-fastest index; false outside the grid.
+__device__ __forceinline__ bool tile_voxel(const PointMap& pm, int64_t tile, int v, int64_t& vox, int64_t& ix,
+                                           int64_t& iy, int64_t& iz) {
   if (v >= pm.vpt) return false;
+  if (pm.blocked) {
+    const uint32_t tt = (uint32_t)tile;   // fewer than 2^31 tiles (checked on the host)
+    const uint32_t q1 = tt / (uint32_t)pm.nbx, bz = q1 / (uint32_t)pm.nby;
+    const uint32_t bx = tt - q1 * (uint32_t)pm.nbx, by = q1 - bz * (uint32_t)pm.nby;
+    ix = (int64_t)(bx * 8 + (v & 7));
+    iy = (int64_t)(by * 4 + ((v >> 3) & 3));
+    iz = (int64_t)(bz * 4 + (v >> 5));
+    if (ix >= pm.nx || iy >= pm.ny || iz >= pm.nz) return false;
+    vox = ix + (int64_t)pm.nx * (iy + (int64_t)pm.ny * iz);
+    return true;
+  }
   vox = tile * pm.vpt + v;
   if (vox >= pm.nvox) return false;
-  int64_t ix, iy, iz;
   if (pm.nvox <= 0x7fffffffLL) {   // 32-bit index arithmetic (exact, several times cheaper)
     const uint32_t vv = (uint32_t)vox, nx = (uint32_t)pm.nx, ny = (uint32_t)pm.ny;
     const uint32_t qy = vv / nx, qz = qy / ny;
@@ -147,6 +157,19 @@ __device__ __forceinline__ bool tile_point(const PointMap& pm, int64_t tile, int
     iy = (vox / pm.nx) % pm.ny;
     iz = vox / ((int64_t)pm.nx * pm.ny);
   }
+  return true;
+}
+
+template <typename T>
+__device__ __forceinline__ bool tile_point(const PointMap& pm, int64_t tile, int row,
+                                           T& x, T& y, T& z, int64_t& vox) {
+  int v = row, sub = 0;
+  if (pm.s3 > 1) {
+    v = row / pm.s3;
+    sub = row - v * pm.s3;
+  }
+  int64_t ix, iy, iz;
+  if (!tile_voxel(pm, tile, v, vox, ix, iy, iz)) return false;
   int sx = 0, sy = 0, sz = 0;
   if (pm.s > 1) {
     sx = sub % pm.s;
