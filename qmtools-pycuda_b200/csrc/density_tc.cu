@@ -76,23 +76,6 @@ __host__ __device__ inline float bits_f32(uint32_t u) {
 #endif
 }
 
-template <int FMT>
-__device__ __forceinline__ void split_store(float x, void* hi, void* lo, int64_t idx, bool two) {
-  if constexpr (FMT == FMT_TF32) {
-    const uint32_t h = tf32_round_bits(x);
-    reinterpret_cast<uint32_t*>(hi)[idx] = h;
-    if (two) reinterpret_cast<uint32_t*>(lo)[idx] = tf32_round_bits(x - bits_f32(h));
-  } else if constexpr (FMT == FMT_F16) {
-    const __half h = __float2half_rn(x);
-    reinterpret_cast<__half*>(hi)[idx] = h;
-    if (two) reinterpret_cast<__half*>(lo)[idx] = __float2half_rn(x - __half2float(h));
-  } else {
-    const __nv_bfloat16 h = __float2bfloat16_rn(x);
-    reinterpret_cast<__nv_bfloat16*>(hi)[idx] = h;
-    if (two) reinterpret_cast<__nv_bfloat16*>(lo)[idx] = __float2bfloat16_rn(x - __bfloat162float(h));
-  }
-}
-
 // ---------------------------------------------------------------------------------------
 // Stage 2: tcgen05 contraction with the fused row-dot epilogue.
 // ---------------------------------------------------------------------------------------
@@ -1098,7 +1081,7 @@ __global__ void __launch_bounds__(STAGE_THREADS, 2) basis_window_kernel(const St
 
 constexpr int FUSED_NCW = 16;                 // compute warps (Phi production and epilogue)
 constexpr int FUSED_NCT = FUSED_NCW * 32;
-constexpr int FUSED_THREADS = 64 + FUSED_NCT;  // + TMA warp + MMA warp
+constexpr int FUSED_THREADS = 64 + FUSED_NCT;  // + U-producer warp + MMA warp
 
 // The single-thread roles of the fused kernel (warp 0 lane 0 and warp 1 lane 0).
 
