@@ -550,20 +550,26 @@ static unsigned grid_blocks(int64_t n) { return (unsigned)std::min<int64_t>((n +
 
 struct GreenEntry {
   DevBuf* buf;
-  uint64_t used;      // last use, for least-recently-used eviction
+  uint64_t used;        // last use, for least-recently-used eviction
+  size_t bytes;
+  cudaEvent_t ready;    // recorded after the build, on the stream that built it
 };
 
 // Device-side caches shared by all calls: twiddle tables per (length, device), transformed
-// Green's functions per (padded shape, step, device) with at most GREEN_CACHE_MAX entries, and
-// one growing scratch grid per device for building them.  `tw_mu` guards the twiddles and
-// `green_mu` the rest; building a Green's function takes green_mu and then (through its FFT
-// passes) tw_mu, never the other way round.
-constexpr size_t GREEN_CACHE_MAX = 16;
+// Green's functions per (padded shape, step, device) up to GREEN_CACHE_BYTES of octants, and one
+// growing scratch grid per device for building them.  `tw_mu` guards the twiddles and `green_mu`
+// the rest; building a Green's function takes green_mu and then (through its FFT passes) tw_mu,
+// never the other way round.  No host synchronisation: a solve on another stream waits for a
+// cached octant's `ready` event on the device, and a build waits for the previous build's use
+// of the scratch grid (`tmp_done`) the same way.
+constexpr size_t GREEN_CACHE_BYTES = (size_t)4 << 30;
 struct DevCache {
   std::mutex tw_mu, green_mu;
   std::map<std::tuple<int, int>, DevBuf*> tw;                         // (L, device)
   std::map<std::tuple<int, int, int, float, int>, GreenEntry> green;  // (Mx, My, Mz, h, device)
   std::map<int, DevBuf*> green_tmp;                                   // device -> scratch
+  std::map<int, cudaEvent_t> tmp_done;                                // device -> last build's end
+  size_t green_bytes = 0;
   uint64_t clock = 0;
 };
 static DevCache& cache() {
@@ -589,6 +595,7 @@ static qmt_status twiddles(int L, const float2** out) {
       b = nullptr;
       return st;
     }
+    // synchronous: the table is shared by every stream (built once per length and device)
     QMT_CUDA(cudaMemcpy(b->ptr, h.data(), L * sizeof(float2), cudaMemcpyHostToDevice));
   }
   *out = b->as<float2>();
@@ -669,14 +676,20 @@ static qmt_status green_hat(int Mx, int My, int Mz, float h_ang, const Plan1D& p
   auto it = c.green.find(key);
   if (it != c.green.end()) {
     it->second.used = ++c.clock;
+    QMT_CUDA(cudaStreamWaitEvent(s, it->second.ready, 0));   // built on another stream, maybe
     *out = it->second.buf->as<float>();
     return QMT_OK;
   }
   const int64_t M = (int64_t)Mx * My * Mz;
   DevBuf*& tmp = c.green_tmp[dev];
   if (!tmp) tmp = new DevBuf();
+  cudaEvent_t& tmp_done = c.tmp_done[dev];
+  if (!tmp_done) QMT_CUDA(cudaEventCreateWithFlags(&tmp_done, cudaEventDisableTiming));
+  // growing the scratch frees the old one (cudaFree waits for its users); otherwise the previous
+  // build's use of it is ordered before this one on the device
   qmt_status st = tmp->reserve(M * sizeof(float2));   // grows only: no allocation in steady state
   if (st) return st;
+  QMT_CUDA(cudaStreamWaitEvent(s, tmp_done, 0));
   float2* g = tmp->as<float2>();
   green_kernel<<<grid_blocks(M), 256, 0, s>>>(g, Mx, My, Mz, h_ang);
   QMT_CHECK_LAUNCH("green_kernel");
@@ -701,17 +714,23 @@ static qmt_status green_hat(int Mx, int My, int Mz, float h_ang, const Plan1D& p
   }
   green_octant_kernel<<<grid_blocks(no), 256, 0, s>>>(g, Mx, My, Mz, gb->as<float>());
   QMT_CHECK_LAUNCH("green_octant_kernel");
-  // the scratch grid is reused by the next build: finish this one first
-  QMT_CUDA(cudaStreamSynchronize(s));
-  if (c.green.size() >= GREEN_CACHE_MAX) {
+  QMT_CUDA(cudaEventRecord(tmp_done, s));
+  cudaEvent_t ready;
+  QMT_CUDA(cudaEventCreateWithFlags(&ready, cudaEventDisableTiming));
+  QMT_CUDA(cudaEventRecord(ready, s));
+  const size_t nbytes = (size_t)no * sizeof(float);
+  while (!c.green.empty() && c.green_bytes + nbytes > GREEN_CACHE_BYTES) {
     auto lru = c.green.begin();
     for (auto e = c.green.begin(); e != c.green.end(); ++e)
       if (e->second.used < lru->second.used) lru = e;
     lru->second.buf->release();   // cudaFree waits for kernels still reading it
     delete lru->second.buf;
+    cudaEventDestroy(lru->second.ready);
+    c.green_bytes -= lru->second.bytes;
     c.green.erase(lru);
   }
-  c.green[key] = GreenEntry{gb, ++c.clock};
+  c.green[key] = GreenEntry{gb, ++c.clock, nbytes, ready};
+  c.green_bytes += nbytes;
   *out = gb->as<float>();
   return QMT_OK;
 }
