@@ -55,6 +55,38 @@ def test_density_c0_all_precisions(c0, prec):
     assert abs(out.qsum - ref.sum()) <= max(10 * TOL[prec], 1e-9) * abs(ref.sum())
 
 
+@pytest.mark.parametrize("density_path", [1, 2])
+@pytest.mark.parametrize("shape", [(13, 7, 5), (33, 17, 9), (8, 4, 4)])
+def test_density_partial_tile_blocks(c0, density_path, shape):
+    """Grids that are not a multiple of the 8 x 4 x 4 voxel tiles, through the C ABI (the Grid
+    class only makes multiples of 8): staged and fused paths, and the SIMT path for fp32.  Every
+    voxel is written once and the edge tiles' unused rows nowhere."""
+    import ctypes as C
+    import torch
+    from qmtools import _native as N
+    sm, mol = c0
+    nx, ny, nz = shape
+    h = 0.45
+    c = np.asarray(sm.coords_bohr).mean(axis=0)
+    o = (c - np.array(shape) * h / 2).astype(np.float32)   # the kernel's float32 origin
+    ref = od.density_qube_unscaled((nx, ny, nz), np.float32(h), tuple(float(v) for v in o), mol.coords, mol.ALMOs,
+                                   mol.basisset.alphas, mol.basisset.coeffs, mol.dm, 1)
+    q = torch.full((nx * ny * nz + 64,), -7.0, dtype=torch.float32, device="cuda")   # sentinel tail
+    N.call("qmt_set_density_path", density_path)
+    try:
+        for prec in ("fp16x3", "fp32"):
+            s = C.c_double()
+            N.call("qmt_density", mol.handle, nx, ny, nz, C.c_float(h), C.c_float(o[0]), C.c_float(o[1]),
+                   C.c_float(o[2]), 1, N.PREC[prec], 0, C.c_void_p(q.data_ptr()), C.byref(s), N.stream_handle())
+            got = q.cpu().numpy()
+            assert np.all(got[nx * ny * nz:] == -7.0), "write beyond the grid"
+            err = rel_l2(got[:nx * ny * nz], ref)
+            assert err <= TOL[prec], f"{prec} {shape}: rel-L2 {err:.3e}"
+            assert abs(s.value - ref.sum()) <= 10 * TOL[prec] * abs(ref.sum())
+    finally:
+        N.call("qmt_set_density_path", 0)
+
+
 @pytest.mark.parametrize("prec", ["fp32", "fp16x3", "tf32x3", "bf16x3"])
 def test_density_two_panels(c1, prec):
     """N = 294 needs two output panels in the tensor-core kernel."""
@@ -141,3 +173,37 @@ def test_fused_path_subgrids_and_small_basis(c0, density_path, sub):
     ref = _oracle(g, mol, subgrid=sub)
     out = qmtools.QMTools.Compute_density(g, mol, subgrid=sub, precision="fp16x3", rescale=False)
     assert rel_l2(out.qube.ravel(), ref) <= TOL["fp16x3"] * (3 if density_path == 3 else 1)
+
+
+def test_set_dm_and_translate_update_the_handle(basis):
+    """A handle whose density matrix is replaced (and restored) and whose molecule is moved gives
+    the density of a molecule built with those inputs: the device copies, the split operands and
+    the host copy read by the analytic potential all follow the upload."""
+    sm = syn.config_molecule("c0")
+    mol = sm.molecule(basis, qmtools.Molecule)
+    g = _small_grid(sm, 24, 0.45)
+    qmtools.QMTools.Compute_density(g, mol, precision="fp16x3", rescale=False)   # operands built
+    v0 = qmtools.Grid((1, 8, 8, 8), 0.9 / qmtools.ANG2BOR, list(np.asarray(sm.coords_bohr).mean(axis=0) - 3.6))
+    qmtools.QMTools.Compute_hartree(v0, mol)                                     # host copy built
+    rng = np.random.default_rng(5)
+    dm1 = np.array(mol.dm, dtype=np.float64)
+    dm2 = dm1 * (1.0 + 0.1 * rng.standard_normal(dm1.shape))
+    dm2 = 0.5 * (dm2 + dm2.T)
+    for dm in (dm2, dm1, dm2):
+        mol.set_dm(dm)
+        ref = _oracle(g, mol)
+        for prec in ("fp16x3", "fp64"):
+            got = qmtools.QMTools.Compute_density(g, mol, precision=prec, rescale=False).qube.ravel()
+            assert rel_l2(got, ref) <= TOL[prec], prec
+        fresh = qmtools.Molecule(sm.xyz_list(), np.array(dm, dtype=np.float32), basis)
+        va = qmtools.Grid.emptyAs(v0)
+        vb = qmtools.Grid.emptyAs(v0)
+        qmtools.QMTools.Compute_hartree(va, mol)
+        qmtools.QMTools.Compute_hartree(vb, fresh)
+        assert rel_l2(va.qube.ravel(), vb.qube.ravel()) <= 1e-12
+        fresh.release()
+    mol.Translate(0.2, -0.1, 0.05)
+    ref = _oracle(g, mol)
+    got = qmtools.QMTools.Compute_density(g, mol, precision="fp16x3", rescale=False).qube.ravel()
+    assert rel_l2(got, ref) <= TOL["fp16x3"]
+    mol.release()

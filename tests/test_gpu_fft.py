@@ -28,7 +28,10 @@ def _density(mol, shape, step, centre):
     return qmtools.QMTools.Compute_density(g, mol, precision="fp32")
 
 
-@pytest.mark.parametrize("shape", [(32, 32, 32), (24, 40, 56), (136, 16, 24), (48, 8, 88)])
+# 256-point lines (one axis each) take the register kernel in every pass mode; other lengths the
+# shared-memory one
+@pytest.mark.parametrize("shape", [(32, 32, 32), (24, 40, 56), (136, 16, 24), (48, 8, 88),
+                                   (256, 16, 8), (16, 256, 8), (8, 16, 256)])
 def test_periodic_matches_numpy(c0, shape):
     sm, mol = c0
     q = _density(mol, shape, 0.35, np.asarray(sm.coords_bohr).mean(axis=0))
@@ -39,7 +42,7 @@ def test_periodic_matches_numpy(c0, shape):
     assert rel_l2(got, ref) < TOL
 
 
-@pytest.mark.parametrize("shape", [(32, 32, 32), (24, 16, 40)])
+@pytest.mark.parametrize("shape", [(32, 32, 32), (24, 16, 40), (128, 8, 16), (8, 128, 16), (16, 8, 128)])
 def test_hockney_matches_numpy(c0, shape):
     sm, mol = c0
     q = _density(mol, shape, 0.4, np.asarray(sm.coords_bohr).mean(axis=0))
