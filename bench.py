@@ -433,6 +433,14 @@ def run_ours(args, world, rank, local, pg):
                        "peak_source": f"bf16_tflops burst, {kind}", "density_ms": dens_ms,
                        "traffic": profiled_traffic() if (args.precision == "fp16x3" and not args.grid) else None,
                        "traffic_unit": "DRAM bytes per launch (ncu, dram__bytes_read.sum + dram__bytes_write.sum)"}
+    # the basis evaluation's exponentials, counted separately (npts x primitives of all shells,
+    # before screening): what bounds the SIMT half of the kernel
+    almos = np.asarray(mol.ALMOs).reshape(-1, 4)
+    shells = {(int(r[0]), int(r[3])) for r in almos}
+    co = np.asarray(mol.basisset.coeffs)
+    nprim = sum(int(np.count_nonzero(co[so:so + 20])) for _, so in shells)
+    out["roofline"]["exponentials_per_launch"] = int(npts * nprim)
+    out["roofline"]["exponentials_per_s"] = npts * nprim / (dens_ms / 1000.0)
     check = None
     if world == 1 and not args.quick:
         # plain FP32 SIMT density (the reference's precision) on the same step
