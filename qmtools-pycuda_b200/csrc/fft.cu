@@ -13,10 +13,10 @@
 //   its octant [0, M/2]^3 is stored, cached per (M, h, device).
 //
 // 1D transforms are mixed-radix Stockham (self-sorting) FFTs of batches of lines in shared
-// memory, twiddles from a per-length table computed in FP64 on the host; 256-point lines (the
-// padded grids of 128^3 boxes) take a register kernel instead (16 x 16 four-step, one
-// shared-memory exchange per transform).  A solve is five passes over an x-fastest complex work
-// grid:
+// memory, twiddles from a per-length table computed in FP64 on the host; 256- and 128-point
+// lines (the padded axes of 128- and 64-voxel boxes) take register kernels instead (16 x 16 and
+// 16 x 8 four-step, one shared-memory exchange per transform).  A solve is five passes over an
+// x-fastest complex work grid:
 //   1. x forward, with the RHS assembled on the fly from q and the nuclei (only lines and
 //      elements inside the physical box are non-zero: y < ny, z < nz, x < nx);
 //   2. y forward on the z < nz planes (elements y >= ny are zero and not read);
@@ -332,18 +332,22 @@ __global__ void __launch_bounds__(256) fft_pass_kernel(const PassArgs a) {
   }
 }
 
-// ---- length-256 lines in registers -----------------------------------------------------------
-// 256 = 16 x 16 (four-step): thread t of a line holds elements t + 16 m (m = 0..15), forms the
-// 16-point DFT over m, multiplies by W256^(t k1), exchanges through shared memory so that it
-// holds the 16 values of its k1 = t, and forms the 16-point DFT over them; it then holds
-// X[t + 16 k2] (k2 = 0..15), the same element pattern as its input.  16 lines x 16 threads per
-// CTA; global loads and stores are issued 16 per thread back to back.
+// ---- 256- and 128-point lines in registers -----------------------------------------------
+// Four-step transforms with every thread holding 16 elements e = t + TPL m (m = 0..15) of its
+// line, TPL = L / 16 threads per line, 256 / TPL lines per CTA: the 16-point DFT over m, the
+// twiddle W_L^(t k1), one exchange through shared memory, then the DFTs over t.  L = 256: thread
+// t forms the 16-point DFT of k1 = t (16 values); L = 128: the two 8-point DFTs of k1 = t and
+// t + 8.  Either way the thread then holds X[t + TPL m'] in register m', the same element pattern
+// as its input, so global loads and stores are issued 16 per thread back to back.
 struct Tw16 {
-  float2 w1, w2, w3, w6, w9;   // W16^p = table entry 16 p (conjugated for the inverse)
+  float2 w1, w2, w3, w6, w9;   // W16^p = table entry (L/16) p (conjugated for the inverse)
 };
 
+template <int L>
 __device__ __forceinline__ Tw16 tw16(const float2* tw, bool inv) {
-  return Tw16{twid(tw, 16, inv), twid(tw, 32, inv), twid(tw, 48, inv), twid(tw, 96, inv), twid(tw, 144, inv)};
+  constexpr int st = L / 16;
+  return Tw16{twid(tw, st, inv), twid(tw, 2 * st, inv), twid(tw, 3 * st, inv), twid(tw, 6 * st, inv),
+              twid(tw, 9 * st, inv)};
 }
 
 // In-place 4-point DFT (forward: W4 = -i; inverse: +i).
@@ -382,32 +386,80 @@ __device__ __forceinline__ void dft16(float2 (&x)[16], const Tw16& w, bool inv) 
   for (int k = 0; k < 16; ++k) x[k] = y[k];
 }
 
-constexpr int F256_S = 273;   // line stride of the exchange buffer (odd: no bank conflicts either way)
-constexpr int F256_R = 17;    // row stride inside a line (odd)
-
-// One 256-point transform of the thread's line b (thread t of it); `buf` is the CTA's exchange
-// buffer (16 x F256_S), free on entry (the barrier below orders it after earlier readers).
-__device__ __forceinline__ void fft256_regs(float2 (&x)[16], const float2* tw, float2* buf, int b, int t, bool inv) {
-  const Tw16 w = tw16(tw, inv);
-  dft16(x, w, inv);
-#pragma unroll
-  for (int k1 = 1; k1 < 16; ++k1) x[k1] = cmul(x[k1], twid(tw, (t * k1) & 255, inv));
-  __syncthreads();
-#pragma unroll
-  for (int k1 = 0; k1 < 16; ++k1) buf[b * F256_S + k1 * F256_R + t] = x[k1];
-  __syncthreads();
-#pragma unroll
-  for (int u = 0; u < 16; ++u) x[u] = buf[b * F256_S + t * F256_R + u];
-  dft16(x, w, inv);
+// 8-point DFT of y[0..7] (even/odd 4-point DFTs), result in natural order; w1, w3 = W8^1, W8^3.
+__device__ __forceinline__ void dft8(float2 (&y)[8], float2 w1, float2 w3, bool inv) {
+  float2 a0 = y[0], a1 = y[2], a2 = y[4], a3 = y[6];
+  float2 b0 = y[1], b1 = y[3], b2 = y[5], b3 = y[7];
+  dft4(a0, a1, a2, a3, inv);
+  dft4(b0, b1, b2, b3, inv);
+  b1 = cmul(b1, w1);
+  b2 = inv ? make_float2(-b2.y, b2.x) : make_float2(b2.y, -b2.x);   // W8^2 = -+i
+  b3 = cmul(b3, w3);
+  y[0] = cadd(a0, b0);
+  y[1] = cadd(a1, b1);
+  y[2] = cadd(a2, b2);
+  y[3] = cadd(a3, b3);
+  y[4] = csub(a0, b0);
+  y[5] = csub(a1, b1);
+  y[6] = csub(a2, b2);
+  y[7] = csub(a3, b3);
 }
 
-template <int MODE>
-__global__ void __launch_bounds__(256) fft256_pass_kernel(const PassArgs a) {
-  constexpr int L = 256;
+// Exchange-buffer geometry per length: element (k1, t) of line b at b S + k1 R + t.  R and S are
+// chosen so that neither thread mapping (lines or elements fastest) has bank conflicts.
+template <int L> struct RegFft;
+template <> struct RegFft<256> {
+  static constexpr int TPL = 16, LINES = 16, R = 17, S_MAX = 273;
+  static __device__ __forceinline__ int S(bool) { return 273; }
+};
+template <> struct RegFft<128> {
+  static constexpr int TPL = 8, LINES = 32, R = 9, S_MAX = 152;
+  static __device__ __forceinline__ int S(bool bfast) { return bfast ? 143 : 152; }
+};
+
+// One transform of the thread's line b (thread t of it); `buf` is the CTA's exchange buffer,
+// free on entry (the barrier below orders it after earlier readers).
+template <int L>
+__device__ __forceinline__ void fft_regs(float2 (&x)[16], const float2* tw, float2* buf, int b, int t, int S,
+                                         bool inv) {
+  constexpr int R = RegFft<L>::R;
+  const Tw16 w = tw16<L>(tw, inv);
+  dft16(x, w, inv);
+#pragma unroll
+  for (int k1 = 1; k1 < 16; ++k1) x[k1] = cmul(x[k1], twid(tw, (t * k1) & (L - 1), inv));
+  __syncthreads();
+#pragma unroll
+  for (int k1 = 0; k1 < 16; ++k1) buf[b * S + k1 * R + t] = x[k1];
+  __syncthreads();
+  if constexpr (L == 256) {
+#pragma unroll
+    for (int u = 0; u < 16; ++u) x[u] = buf[b * S + t * R + u];
+    dft16(x, w, inv);
+  } else {
+    const float2 w1 = twid(tw, L / 8, inv), w3 = twid(tw, 3 * L / 8, inv);
+    float2 ya[8], yb[8];
+#pragma unroll
+    for (int u = 0; u < 8; ++u) {
+      ya[u] = buf[b * S + t * R + u];
+      yb[u] = buf[b * S + (t + 8) * R + u];
+    }
+    dft8(ya, w1, w3, inv);
+    dft8(yb, w1, w3, inv);
+#pragma unroll
+    for (int k2 = 0; k2 < 8; ++k2) {
+      x[2 * k2] = ya[k2];       // X[t + 16 k2]     = element t + 8 (2 k2)
+      x[2 * k2 + 1] = yb[k2];   // X[t + 8 + 16 k2] = element t + 8 (2 k2 + 1)
+    }
+  }
+}
+
+template <int MODE, int L>
+__global__ void __launch_bounds__(256) fft_reg_pass_kernel(const PassArgs a) {
+  constexpr int TPL = RegFft<L>::TPL, LINES = RegFft<L>::LINES;
   extern __shared__ float2 fsm[];
   float2* tw = fsm;
   float2* buf = fsm + L;
-  float* sat = reinterpret_cast<float*>(buf + 16 * F256_S);   // atoms (PASS_X_RHS)
+  float* sat = reinterpret_cast<float*>(buf + LINES * RegFft<L>::S_MAX);   // atoms (PASS_X_RHS)
   for (int i = threadIdx.x; i < L; i += blockDim.x) tw[i] = a.tw[i];
   if constexpr (MODE == PASS_X_RHS) {
     for (int i = threadIdx.x; i < a.mol.natoms; i += blockDim.x) {
@@ -417,13 +469,13 @@ __global__ void __launch_bounds__(256) fft256_pass_kernel(const PassArgs a) {
       sat[4 * i + 3] = (float)a.mol.types[i];
     }
   }
-  const int64_t l0 = (int64_t)blockIdx.x * 16;
+  const int64_t l0 = (int64_t)blockIdx.x * LINES;
   const int64_t rem = a.nlines - l0;
-  const int nb = rem < 16 ? (int)rem : 16;
-  __shared__ int64_t lbase[16];
-  __shared__ int lx[16], ly[16];
-  __shared__ int ncand[16];
-  __shared__ int cand[16][FFT_CAND];
+  const int nb = rem < LINES ? (int)rem : LINES;
+  __shared__ int64_t lbase[LINES];
+  __shared__ int lx[LINES], ly[LINES];
+  __shared__ int ncand[LINES];
+  __shared__ int cand[LINES][FFT_CAND];
   __syncthreads();
   if (threadIdx.x < nb) {
     const int bb = threadIdx.x;
@@ -446,16 +498,17 @@ __global__ void __launch_bounds__(256) fft256_pass_kernel(const PassArgs a) {
     }
   }
   __syncthreads();
-  // lines adjacent in memory: a half-warp spans the 16 lines at one element (128 contiguous
-  // bytes); lines contiguous: a half-warp spans 16 consecutive elements of one line
+  // lines adjacent in memory: a half-warp spans 16 lines at one element; lines contiguous: it
+  // spans consecutive elements of one (L = 256) or two (L = 128) lines
   const bool bfast = a.s1 == 1;
-  const int b = bfast ? (threadIdx.x & 15) : (threadIdx.x >> 4);
-  const int t = bfast ? (threadIdx.x >> 4) : (threadIdx.x & 15);
+  const int b = bfast ? (int)(threadIdx.x % LINES) : (int)(threadIdx.x / TPL);
+  const int t = bfast ? (int)(threadIdx.x / LINES) : (int)(threadIdx.x % TPL);
+  const int S = RegFft<L>::S(bfast);
   const bool live = b < nb;
   float2 x[16];
 #pragma unroll
   for (int m = 0; m < 16; ++m) {
-    const int e = t + 16 * m;
+    const int e = t + TPL * m;
     float2 v = make_float2(0.f, 0.f);
     if (live && e < a.lload) {
       if constexpr (MODE == PASS_X_RHS) {
@@ -478,13 +531,13 @@ __global__ void __launch_bounds__(256) fft256_pass_kernel(const PassArgs a) {
     }
     x[m] = v;
   }
-  fft256_regs(x, tw, buf, b, t, a.inv != 0);
+  fft_regs<L>(x, tw, buf, b, t, S, a.inv != 0);
   if constexpr (MODE == PASS_Z_MUL) {
     const int hx = a.Mx / 2 + 1, hy = a.My / 2 + 1;
     const int xg = lx[b], yg = ly[b];
 #pragma unroll
-    for (int k2 = 0; k2 < 16; ++k2) {
-      const int kz = t + 16 * k2;
+    for (int m = 0; m < 16; ++m) {
+      const int kz = t + TPL * m;
       float f;
       if (a.periodic) {
         // kernel_fft.cu:90-104: k in cycles/Ang, negative frequencies above N/2 - 1, k = 0 -> 0
@@ -497,27 +550,28 @@ __global__ void __launch_bounds__(256) fft256_pass_kernel(const PassArgs a) {
         const int gx = min(xg, a.Mx - xg), gy = min(yg, a.My - yg), gz = min(kz, a.Mz - kz);
         f = live ? __ldg(a.gsym + gx + (int64_t)hx * (gy + (int64_t)hy * gz)) : 0.f;
       }
-      x[k2] = make_float2(x[k2].x * f, x[k2].y * f);
+      x[m] = make_float2(x[m].x * f, x[m].y * f);
     }
-    fft256_regs(x, tw, buf, b, t, a.inv == 0);
+    fft_regs<L>(x, tw, buf, b, t, S, a.inv == 0);
   }
   if constexpr (MODE == PASS_X_OUT) {
     // line (z = lx, y = ly) along x into the C-order output: regroup through shared memory so
-    // that a half-warp writes 16 consecutive z of one x
+    // that a warp writes consecutive z of one x
+    constexpr int S2 = L + 1;
     __syncthreads();
 #pragma unroll
-    for (int k2 = 0; k2 < 16; ++k2) buf[b * F256_S + t + 16 * k2] = x[k2];
+    for (int m = 0; m < 16; ++m) buf[b * S2 + t + TPL * m] = x[m];
     __syncthreads();
-    const int bo = threadIdx.x & 15;
+    const int bo = (int)(threadIdx.x % LINES);
     if (bo < nb)
-      for (int e = threadIdx.x >> 4; e < a.lstore; e += 16)
-        a.out[(int64_t)e * a.ny * a.nz + (int64_t)ly[bo] * a.nz + lx[bo]] = buf[bo * F256_S + e].x * a.scale;
+      for (int e = (int)(threadIdx.x / LINES); e < a.lstore; e += TPL)
+        a.out[(int64_t)e * a.ny * a.nz + (int64_t)ly[bo] * a.nz + lx[bo]] = buf[bo * S2 + e].x * a.scale;
   } else {
 #pragma unroll
-    for (int k2 = 0; k2 < 16; ++k2) {
-      const int e = t + 16 * k2;
+    for (int m = 0; m < 16; ++m) {
+      const int e = t + TPL * m;
       if (live && e < a.lstore)
-        a.data[lbase[b] + (int64_t)e * a.se] = make_float2(x[k2].x * a.scale, x[k2].y * a.scale);
+        a.data[lbase[b] + (int64_t)e * a.se] = make_float2(x[m].x * a.scale, x[m].y * a.scale);
     }
   }
 }
@@ -610,12 +664,28 @@ static qmt_status launch_mode(const PassArgs& a, unsigned blocks, size_t smem, c
   return QMT_OK;
 }
 
-template <int MODE>
-static qmt_status launch_mode256(const PassArgs& a, unsigned blocks, size_t smem, cudaStream_t s) {
-  QMT_CUDA(cudaFuncSetAttribute(fft256_pass_kernel<MODE>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
-  fft256_pass_kernel<MODE><<<blocks, 256, smem, s>>>(a);
-  QMT_CHECK_LAUNCH("fft256_pass_kernel");
+template <int MODE, int L>
+static qmt_status launch_mode_reg(const PassArgs& a, unsigned blocks, size_t smem, cudaStream_t s) {
+  QMT_CUDA(cudaFuncSetAttribute(fft_reg_pass_kernel<MODE, L>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+  fft_reg_pass_kernel<MODE, L><<<blocks, 256, smem, s>>>(a);
+  QMT_CHECK_LAUNCH("fft_reg_pass_kernel");
   return QMT_OK;
+}
+
+template <int L>
+static qmt_status launch_pass_reg(int mode, PassArgs a, cudaStream_t s) {
+  constexpr int LINES = RegFft<L>::LINES;
+  a.B = LINES;
+  size_t smem = ((size_t)L + (size_t)LINES * RegFft<L>::S_MAX) * sizeof(float2);
+  if (mode == PASS_X_RHS) smem += 16 * (size_t)a.mol.natoms;
+  const unsigned blocks = (unsigned)((a.nlines + LINES - 1) / LINES);
+  if (blocks == 0) return QMT_OK;
+  switch (mode) {
+    case PASS_PLAIN: return launch_mode_reg<PASS_PLAIN, L>(a, blocks, smem, s);
+    case PASS_X_RHS: return launch_mode_reg<PASS_X_RHS, L>(a, blocks, smem, s);
+    case PASS_Z_MUL: return launch_mode_reg<PASS_Z_MUL, L>(a, blocks, smem, s);
+    default: return launch_mode_reg<PASS_X_OUT, L>(a, blocks, smem, s);
+  }
 }
 
 static qmt_status launch_pass(int mode, PassArgs a, cudaStream_t s) {
@@ -624,19 +694,8 @@ static qmt_status launch_pass(int mode, PassArgs a, cudaStream_t s) {
   qmt_status st = twiddles(a.plan.L, &tw);
   if (st) return st;
   a.tw = tw;
-  if (a.plan.L == 256) {   // register kernel for 256-point lines
-    a.B = 16;
-    size_t smem = ((size_t)256 + 16 * F256_S) * sizeof(float2);
-    if (mode == PASS_X_RHS) smem += 16 * (size_t)a.mol.natoms;
-    const unsigned blocks = (unsigned)((a.nlines + 15) / 16);
-    if (blocks == 0) return QMT_OK;
-    switch (mode) {
-      case PASS_PLAIN: return launch_mode256<PASS_PLAIN>(a, blocks, smem, s);
-      case PASS_X_RHS: return launch_mode256<PASS_X_RHS>(a, blocks, smem, s);
-      case PASS_Z_MUL: return launch_mode256<PASS_Z_MUL>(a, blocks, smem, s);
-      default: return launch_mode256<PASS_X_OUT>(a, blocks, smem, s);
-    }
-  }
+  if (a.plan.L == 256) return launch_pass_reg<256>(mode, a, s);   // register kernels
+  if (a.plan.L == 128) return launch_pass_reg<128>(mode, a, s);
   size_t smem = ((size_t)a.plan.L * (1 + 2 * a.B)) * sizeof(float2);
   if (mode == PASS_X_RHS) smem += 16 * (size_t)a.mol.natoms;
   const unsigned blocks = (unsigned)((a.nlines + a.B - 1) / a.B);

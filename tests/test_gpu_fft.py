@@ -28,10 +28,11 @@ def _density(mol, shape, step, centre):
     return qmtools.QMTools.Compute_density(g, mol, precision="fp32")
 
 
-# 256-point lines (one axis each) take the register kernel in every pass mode; other lengths the
-# shared-memory one
+# 256- and 128-point lines (one axis each) take the register kernels in every pass mode; other
+# lengths the shared-memory one
 @pytest.mark.parametrize("shape", [(32, 32, 32), (24, 40, 56), (136, 16, 24), (48, 8, 88),
-                                   (256, 16, 8), (16, 256, 8), (8, 16, 256)])
+                                   (256, 16, 8), (16, 256, 8), (8, 16, 256),
+                                   (128, 16, 8), (16, 128, 8), (8, 16, 128)])
 def test_periodic_matches_numpy(c0, shape):
     sm, mol = c0
     q = _density(mol, shape, 0.35, np.asarray(sm.coords_bohr).mean(axis=0))
@@ -42,7 +43,8 @@ def test_periodic_matches_numpy(c0, shape):
     assert rel_l2(got, ref) < TOL
 
 
-@pytest.mark.parametrize("shape", [(32, 32, 32), (24, 16, 40), (128, 8, 16), (8, 128, 16), (16, 8, 128)])
+@pytest.mark.parametrize("shape", [(32, 32, 32), (24, 16, 40), (128, 8, 16), (8, 128, 16), (16, 8, 128),
+                                   (64, 8, 16), (8, 64, 16), (16, 8, 64)])
 def test_hockney_matches_numpy(c0, shape):
     sm, mol = c0
     q = _density(mol, shape, 0.4, np.asarray(sm.coords_bohr).mean(axis=0))
