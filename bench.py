@@ -21,20 +21,31 @@ device operands) and reads the potential grid back to the host every step.
 Beside the headline step, rank 0 also reports (not part of `value`):
   * `plain_fp32`: the same step with the plain FP32 SIMT density path (the reference's
     precision), and the speed-up of the mixed-precision path over it;
-  * `accuracy`: density rel-L2 / max-abs of the mixed path against this library's FP64
-    density, and the FP64 electron-count error;
+  * `like_for_like`: the same density with the reference's own Poisson route (periodic FFT on
+    the 128^3 grid itself), the step the `--impl reference` arm times;
+  * `c0_route`: the small molecule (8 atoms, N = 58) on 64^3 at 0.2 bohr: FP64 density,
+    analytic GTO potential on the outer shell, 2000 Dirichlet Jacobi sweeps, Hockney FFT on
+    128^3;
+  * `c2_sweep`: the large molecule (60 atoms, N = 588) on 192^3 at 0.12 bohr, the density in
+    every precision, and an FP32 Jacobi solve to a relative FP64 residual of 1e-8;
   * `batched`: 64 molecules of 5-60 atoms (grids = bounding box + 3 bohr per side at
     0.15 bohr) through the continuous-batching engine, against serial plain FP32;
-  * `serving`: a Poisson request stream (atoms log-uniform 3-120) through the engine with
-    p50/p99 latency, against serial plain FP32;
-  * `cpu_baseline`: the FP64 NumPy/SciPy evaluation on a bounded sample, which also checks
-    the mixed result against it (density on the sampled planes, Hartree on the full grid).
+  * `serving`: Poisson request streams at 50, 200 and 800 req/s (atoms log-uniform 3-120)
+    through the engine with p50/p99 latency, against serial plain FP32;
+  * `cpu_baseline`: the FP64 NumPy/SciPy evaluation on a bounded sample;
+  * `accuracy`: the mixed results scored against that FP64 evaluation (C1 density on sampled
+    planes and Hartree on the full grid, every C2 variant on sampled planes).
 
 `--impl reference` times the reference's own implementation of this path.  The reference is
 GPU-only CUDA C driven from Python; its kernels, compiled from its sources into oracle/_ref,
 run here with the reference facade's launch shapes and host steps (density kernel, grid
-total and rescale, periodic cuFFT Poisson route).  Without those builds the FP64 CPU port
-of its algorithm is timed instead.
+total and rescale, periodic cuFFT Poisson route), plus its analytic potential
+(gpu_hartree_GTO) and Jacobi sweeps (gpu_hartree_iteration) on the small molecule's 64^3
+grid.  Without those builds the FP64 CPU port of its algorithm is timed instead.
+
+`--ncu-import CSV` turns an ncu metrics capture of the fused density kernel
+(`--metrics dram__bytes_read.sum,dram__bytes_write.sum --csv`) into
+profiles/density_fused_kernel_c1.traffic.json, which the bench reads for `roofline.traffic`.
 """
 import argparse
 import json
@@ -222,10 +233,12 @@ def cpu_baseline_c1(sm, basis, qmtools, check=None):
 
     Density: 4 z-planes (4*128^2 points) of the 128^3 grid through the oracle (chunked Phi,
     BLAS Phi@P, row-dot), extrapolated per point.  Hartree: one scipy.fft rfftn/irfftn
-    Hockney convolution on the full 256^3 padded grid with all host cores.  With `check`
-    (host copies of the mixed-precision results) the FP64 results also score them: density
-    on the sampled planes, and the FP64 Hockney potential of the same density on the full
-    grid.
+    Hockney convolution on the full 256^3 padded grid with all host cores.
+
+    With `check` (host copies of device results) the same FP64 evaluation scores them; the
+    scores are returned separately (accuracy, not timing): the C1 mixed density on the sampled
+    planes and its Hockney potential on the full grid, and each C2 precision variant on its
+    sampled planes.  Returns (baseline, accuracy or None).
     """
     import scipy.fft
     from oracle import density as od
@@ -254,19 +267,48 @@ def cpu_baseline_c1(sm, basis, qmtools, check=None):
            "sample": f"density on {nzs} z-planes ({nzs * nx * ny} pts, FP64 NumPy, extrapolated per point) + "
                      f"one full {M}^3 scipy.fft Hockney convolution (workers={cores})",
            "density_s_per_pt": t_dens, "fft_s": t_fft}
-    if check is not None:
-        ref = np.asarray(q, dtype=np.float64).ravel()
-        got = check["q_raw"].reshape(nz, ny, nx)[z0:z0 + nzs].ravel().astype(np.float64)
-        vref = op.hockney_poisson(check["q"], (nx, ny, nz), h, (ox, oy, oz), mol.coords, mol.types, 0.2, 6)
-        vref = np.asarray(vref, dtype=np.float64).ravel()
-        vgot = check["v"].astype(np.float64).ravel()
-        out["check_vs_fp64"] = {
-            "density_rel_l2": float(np.linalg.norm(got - ref) / np.linalg.norm(ref)),
-            "density_max_abs": float(np.abs(got - ref).max()),
-            "density_points": int(ref.size),
-            "hartree_rel_l2": float(np.linalg.norm(vgot - vref) / np.linalg.norm(vref)),
-            "hartree_max_abs_volt": float(np.abs(vgot - vref).max())}
-    return out
+    if check is None:
+        return out, None
+    acc = {"reference": "FP64 oracle (NumPy restatement of the reference algorithm) on the same inputs"}
+    c1 = check["c1"]
+    ref = np.asarray(q, dtype=np.float64).ravel()
+    got = c1["q_raw"].reshape(nz, ny, nx)[z0:z0 + nzs].ravel().astype(np.float64)
+    vref = op.hockney_poisson(c1["q"], (nx, ny, nz), h, (ox, oy, oz), mol.coords, mol.types, 0.2, 6)
+    vref = np.asarray(vref, dtype=np.float64).ravel()
+    vgot = c1["v"].astype(np.float64).ravel()
+    acc["c1_mixed"] = {
+        "precision": c1["precision"],
+        "density_rel_l2": float(np.linalg.norm(got - ref) / np.linalg.norm(ref)),
+        "density_max_abs": float(np.abs(got - ref).max()),
+        "density_points": int(ref.size), "density_sample": f"z-planes {z0}..{z0 + nzs - 1} of {nz}",
+        "hartree_rel_l2": float(np.linalg.norm(vgot - vref) / np.linalg.norm(vref)),
+        "hartree_max_abs_volt": float(np.abs(vgot - vref).max()),
+        "hartree_reference": "FP64 Hockney convolution (scipy) of the same density grid",
+        "grid_electrons_fp64_path": c1["sum_fp64"], "grid_electrons_mixed": c1["sum_mixed"],
+        "electron_count_2_trace_ps_fp64": c1["two_trace_ps"],
+        "electron_count_error_mixed": abs(c1["sum_mixed"] - c1["two_trace_ps"]),
+        "electron_count_error_fp64_path": abs(c1["sum_fp64"] - c1["two_trace_ps"])}
+    if "c2" in check:
+        c2 = check["c2"]
+        m2 = c2["sm"].molecule(basis, qmtools.Molecule)
+        gx, gy, gz, gh, gox, goy, goz = c2["geom"]
+        refs = {z: np.asarray(od.density_qube_unscaled((gx, gy, gz), np.float32(gh), (gox, goy, goz), m2.coords,
+                                                       m2.ALMOs, basis.alphas, basis.coeffs, m2.dm,
+                                                       zslab=(z, z + 1)), dtype=np.float64).ravel()
+                for z in c2["planes"]}
+        r = np.concatenate([refs[z] for z in c2["planes"]])
+        var = {}
+        for prec, d in c2["variants"].items():
+            gv = np.concatenate([d["planes"][z].astype(np.float64) for z in c2["planes"]])
+            var[prec] = {"density_rel_l2": float(np.linalg.norm(gv - r) / np.linalg.norm(r)),
+                         "density_max_abs": float(np.abs(gv - r).max()),
+                         "grid_electrons": d["sum"],
+                         "electron_count_error": abs(d["sum"] - c2["two_trace_ps"])}
+        acc["c2_variants"] = {"sample": f"z-planes {list(c2['planes'])} of {gz} ({r.size} pts)",
+                              "electron_count_2_trace_ps_fp64": c2["two_trace_ps"], "variants": var}
+        m2.release()
+    mol.release()
+    return out, acc
 
 
 def _requests(mols, basis, qmtools, serving, arrivals=None):
@@ -291,7 +333,7 @@ def _engine_run(serving, reqs, slots, precision, realtime):
 
 
 def batched_and_serving(basis, qmtools, precision):
-    """C3-like batch and C4-like request stream through the continuous-batching engine."""
+    """C3-like batch and C4-like request streams through the continuous-batching engine."""
     from qmtools import serving
     from qmtools import synthetic as syn
     res = {}
@@ -305,21 +347,162 @@ def batched_and_serving(basis, qmtools, precision):
                       "speedup_vs_serial_plain_fp32": t_fp32 / t_mix,
                       "timing": "host wall clock around the whole batch (set-up, H2D, density, Hockney FFT, D2H); "
                                 "slots grown to the largest requests beforehand"}
-    rate, count = 200.0, 32
-    stream = syn.serving_stream(rate, count)
-    arr = [t for t, _ in stream]
-    mols = [m for _, m in stream]
+    count = 32
+    rates = (50.0, 200.0, 800.0)
+    # the atom counts depend only on the seed, so every rate serves the same molecules
+    mols = [m for _, m in syn.serving_stream(rates[0], count)]
     pts = sum(int(np.prod(m.grid_shape)) for m in mols)
-    reqs = _requests(mols, basis, qmtools, serving, arr)
-    t_mix = _engine_run(serving, reqs, 8, precision, True)
-    lat = serving.latency_stats(reqs)
     t_fp32 = _engine_run(serving, _requests(mols, basis, qmtools, serving), 1, "fp32", False)
-    res["serving"] = {"requests": count, "rate_req_s": rate, "atoms": "log-uniform 3-120", "grid_pts": pts,
-                      "p50_ms": lat["p50_ms"], "p99_ms": lat["p99_ms"], "mean_ms": lat["mean_ms"],
-                      "value": pts / t_mix, "unit": UNIT, "makespan_s": t_mix, "slots": 8,
-                      "serial_plain_fp32": {"value": pts / t_fp32, "wall_s": t_fp32},
-                      "speedup_vs_serial_plain_fp32": t_fp32 / t_mix}
+    streams = {}
+    for rate in rates:
+        stream = syn.serving_stream(rate, count)
+        arr = [t for t, _ in stream]
+        reqs = _requests([m for _, m in stream], basis, qmtools, serving, arr)
+        t_mix = _engine_run(serving, reqs, 8, precision, True)
+        lat = serving.latency_stats(reqs)
+        streams[f"{int(rate)}_req_s"] = {
+            "rate_req_s": rate, "p50_ms": lat["p50_ms"], "p99_ms": lat["p99_ms"], "mean_ms": lat["mean_ms"],
+            "value": pts / t_mix, "unit": UNIT, "makespan_s": t_mix, "arrival_span_s": arr[-1],
+            "speedup_vs_serial_plain_fp32": t_fp32 / t_mix}
+    res["serving"] = {"requests": count, "atoms": "log-uniform 3-120", "grid_pts": pts, "slots": 8,
+                      "serial_plain_fp32": {"value": pts / t_fp32, "wall_s": t_fp32}, "streams": streams}
     return res
+
+
+def _events_ms(fn, reps=1):
+    """Mean duration of fn() over `reps` calls on the current stream, CUDA events."""
+    import torch
+    st = torch.cuda.current_stream()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record(st)
+    for _ in range(reps):
+        fn()
+    e1.record(st)
+    e1.synchronize()
+    return e0.elapsed_time(e1) / reps
+
+
+def c0_route(basis, qmtools, N):
+    """The small-molecule configuration end to end on the device: FP64 density on 64^3 at 0.2 bohr,
+    the analytic GTO potential on the grid's outer shell, 2000 Dirichlet Jacobi sweeps (FP32,
+    FP64 residual) and the Hockney FFT solve on 128^3; each stage timed with CUDA events."""
+    import ctypes as C
+    import torch
+    from qmtools import synthetic as syn
+    sm = syn.config_molecule("c0")
+    mol = sm.molecule(basis, qmtools.Molecule)
+    g = sm.grid(qmtools.Grid)
+    nx, ny, nz, h, ox, oy, oz = g._geom()
+    n = nx * ny * nz
+    st = C.c_void_p(torch.cuda.current_stream().cuda_stream)
+    q = torch.empty(n, device="cuda")
+    seed = torch.zeros(n, device="cuda")
+    rho = torch.empty(n, device="cuda")
+    v = torch.zeros(n, device="cuda")
+    t = torch.empty(n, device="cuda")
+    vfft = torch.empty(n, device="cuda")
+    qs = C.c_double()
+    sw, dl = C.c_int(), C.c_double()
+    vp = lambda x: C.c_void_p(x.data_ptr())
+
+    def density():
+        N.call("qmt_density", mol.handle, nx, ny, nz, h, ox, oy, oz, 1, N.PREC["fp64"], 1, vp(q), None, st)
+
+    def boundary():
+        N.call("qmt_hartree_gto_boundary", mol.handle, nx, ny, nz, h, ox, oy, oz, vp(v), st)
+
+    def jacobi():
+        v.zero_()
+        boundary()
+        seed.zero_()
+        N.call("qmt_density_seed", mol.handle, nx, ny, nz, h, ox, oy, oz, vp(seed), st)
+        torch.sub(seed, q, out=rho)
+        rho.mul_(1.0 / float(h) ** 3)
+        N.call("qmt_jacobi_dirichlet", nx, ny, nz, h, vp(rho), vp(v), vp(t), 2000, 100, 0.0, C.byref(sw),
+               C.byref(dl), st)
+
+    def fft():
+        N.call("qmt_fft_poisson", mol.handle, nx, ny, nz, h, ox, oy, oz, 0.2, 6.0, 1, vp(q), vp(vfft), st)
+
+    for f in (density, boundary, jacobi, fft):
+        f()
+    torch.cuda.synchronize()
+    ms = {"density_fp64": _events_ms(density, 3), "gto_boundary": _events_ms(boundary, 3),
+          "jacobi_2000_sweeps_incl_boundary": _events_ms(jacobi, 1), "fft_hockney_128": _events_ms(fft, 5)}
+    tot = ms["density_fp64"] + ms["jacobi_2000_sweeps_incl_boundary"] + ms["fft_hockney_128"]
+    shell = n - (nx - 2) * (ny - 2) * (nz - 2)
+    res = {"workload": f"C0: 8 atoms C2H6, N=58, 64^3 @ 0.2 bohr; FP64 density, GTO boundary ({shell} shell pts "
+                       "at voxel centres), 2000 Dirichlet Jacobi sweeps FP32/FP64 residual, Hockney FFT 128^3",
+           "ms": ms, "total_ms": tot, "value": n / (tot / 1e3), "unit": UNIT,
+           "jacobi_sweeps": sw.value, "jacobi_fp64_residual": dl.value}
+    mol.release()
+    return res
+
+
+def c2_sweep(basis, qmtools, N, planes=(48, 144)):
+    """The large molecule (60 atoms, N = 588) on 192^3 at 0.12 bohr: the density in every
+    precision (raw electrons per voxel, CUDA-event time per call), host copies of sampled
+    z-planes for scoring against the FP64 oracle, and an FP32 Dirichlet Jacobi solve run until
+    the FP64 residual sum |V_k - V_k-1| falls below 1e-8 of sum |V| (capped)."""
+    import ctypes as C
+    import torch
+    from qmtools import synthetic as syn
+    sm = syn.config_molecule("c2")
+    mol = sm.molecule(basis, qmtools.Molecule)
+    g = sm.grid(qmtools.Grid)
+    nx, ny, nz, h, ox, oy, oz = g._geom()
+    n = nx * ny * nz
+    st = C.c_void_p(torch.cuda.current_stream().cuda_stream)
+    q = torch.empty(n, device="cuda")
+    vp = lambda x: C.c_void_p(x.data_ptr())
+    tr = C.c_double()
+    N.call("qmt_mol_trace_ps", mol.handle, C.byref(tr), st)
+    out = {"workload": f"C2: 60 atoms C20H28N6O6, N={int(mol.norbs)}, 192^3 @ 0.12 bohr", "variants": {}}
+    check = {"sm": sm, "geom": (nx, ny, nz, h, ox, oy, oz), "planes": planes, "variants": {},
+             "two_trace_ps": 2.0 * tr.value}
+    for prec in ("fp64", "fp32", "tf32", "tf32x3", "bf16", "bf16x3", "fp16x3"):
+        s = C.c_double()
+
+        def dens():
+            N.call("qmt_density", mol.handle, nx, ny, nz, h, ox, oy, oz, 1, N.PREC[prec], 0, vp(q), None, st)
+
+        dens()
+        ms = _events_ms(dens, 1 if prec == "fp64" else 3)
+        N.call("qmt_density", mol.handle, nx, ny, nz, h, ox, oy, oz, 1, N.PREC[prec], 0, vp(q), C.byref(s), st)
+        qz = q.view(nz, ny, nx)
+        check["variants"][prec] = {"planes": {z: qz[z].cpu().numpy().ravel().copy() for z in planes},
+                                   "sum": s.value}
+        out["variants"][prec] = {"ms": ms, "value": n / (ms / 1e3), "unit": UNIT, "grid_electrons": s.value}
+    # Jacobi to a relative residual of 1e-8: charge = seed - fp16x3 density, boundary = GTO potential
+    rho = torch.zeros(n, device="cuda")
+    v = torch.zeros(n, device="cuda")
+    t = torch.empty(n, device="cuda")
+    N.call("qmt_density_seed", mol.handle, nx, ny, nz, h, ox, oy, oz, vp(rho), st)
+    rho.sub_(q).mul_(1.0 / float(h) ** 3)
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record()
+    N.call("qmt_hartree_gto_boundary", mol.handle, nx, ny, nz, h, ox, oy, oz, vp(v), st)
+    e1.record()
+    sweeps, rel, chunk, cap = 0, float("inf"), 5000, 100000
+    jac_ms = 0.0
+    sw, dl = C.c_int(), C.c_double()
+    while sweeps < cap:
+        ms = _events_ms(lambda: N.call("qmt_jacobi_dirichlet", nx, ny, nz, h, vp(rho), vp(v), vp(t), chunk, 100,
+                                       0.0, C.byref(sw), C.byref(dl), st))
+        jac_ms += ms
+        sweeps += sw.value
+        norm = float(v.double().abs().sum())
+        rel = dl.value / norm
+        if rel <= 1e-8:
+            break
+    out["jacobi_to_1e-8"] = {"sweeps": sweeps, "fp64_residual_sum_abs_dV": dl.value, "relative_residual": rel,
+                             "converged": rel <= 1e-8, "cap_sweeps": cap, "ms": jac_ms,
+                             "us_per_sweep": 1e3 * jac_ms / max(sweeps, 1),
+                             "gto_boundary_ms": e0.elapsed_time(e1),
+                             "residual": "FP64 sum |V_k - V_k-1| over the grid at the last sweep of a "
+                                         f"{chunk}-sweep launch, relative to sum |V_k|"}
+    mol.release()
+    return out, check
 
 
 def run_ours(args, world, rank, local, pg):
@@ -350,26 +533,33 @@ def run_ours(args, world, rank, local, pg):
     sh = C.c_void_p(stream.cuda_stream)
     qsum = C.c_double()
     handle = mol.handle
+    lib = N.load()
 
-    def step():
-        N.call("qmt_density", handle, nx, ny, nz, h, ox, oy, oz, 1, prec, 1, C.c_void_p(q.data_ptr()),
+    def density(p=prec):
+        N.call("qmt_density", handle, nx, ny, nz, h, ox, oy, oz, 1, p, 1, C.c_void_p(q.data_ptr()),
                C.byref(qsum), sh)
-        N.call("qmt_fft_poisson", handle, nx, ny, nz, h, ox, oy, oz, 0.2, 6.0, 1, C.c_void_p(q.data_ptr()),
+
+    def poisson(padded=1):
+        N.call("qmt_fft_poisson", handle, nx, ny, nz, h, ox, oy, oz, 0.2, 6.0, padded, C.c_void_p(q.data_ptr()),
                C.c_void_p(vout.data_ptr()), sh)
 
-    def timed(fn, k, with_density_events=False):
+    def step():
+        density()
+        poisson()
+
+    def timed(fn, k, split=None):
+        """Mean ms per step over k steps, CUDA events on the launching stream around each step, the
+        L2 flushed before each; with `split` (density, rest) the density part is timed as well."""
         tot = 0.0
         dens = 0.0
         ev = [torch.cuda.Event(enable_timing=True) for _ in range(3)]
         for _ in range(k):
             flush.fill_(1.0)
             ev[0].record(stream)
-            if with_density_events:
-                N.call("qmt_density", handle, nx, ny, nz, h, ox, oy, oz, 1, prec, 1, C.c_void_p(q.data_ptr()),
-                       C.byref(qsum), sh)
+            if split is not None:
+                split[0]()
                 ev[1].record(stream)
-                N.call("qmt_fft_poisson", handle, nx, ny, nz, h, ox, oy, oz, 0.2, 6.0, 1,
-                       C.c_void_p(q.data_ptr()), C.c_void_p(vout.data_ptr()), sh)
+                split[1]()
             else:
                 fn()
                 ev[1].record(stream)
@@ -383,9 +573,11 @@ def run_ours(args, world, rank, local, pg):
         step()
     torch.cuda.synchronize()
     barrier(pg)
+    l0 = lib.qmt_launch_count()
     with clock_sampler(local) as clk:
-        ms, dens_ms = timed(step, args.steps, with_density_events=True)
+        ms, dens_ms = timed(step, args.steps, split=(density, poisson))
     torch.cuda.synchronize()
+    launches = lib.qmt_launch_count() - l0
     barrier(pg)
     ms = max_over_ranks(pg, ms)
 
@@ -394,10 +586,11 @@ def run_ours(args, world, rank, local, pg):
     dm_h = torch.from_numpy(np.ascontiguousarray(mol.dm, dtype=np.float32)).pin_memory()
     v_h = torch.empty(npts, dtype=torch.float32).pin_memory()
 
-    def e2e_step():
+    def e2e_step(padded=1):
         N.call("qmt_mol_set_coords", handle, C.c_void_p(coords_h.data_ptr()), sh)
         N.call("qmt_mol_set_dm", handle, C.c_void_p(dm_h.data_ptr()), sh)
-        step()
+        density()
+        poisson(padded)
         v_h.copy_(vout, non_blocking=True)
 
     for _ in range(max(1, args.warmup)):
@@ -407,7 +600,6 @@ def run_ours(args, world, rank, local, pg):
     e2e_ms, _ = timed(e2e_step, args.steps)
     e2e_ms = max_over_ranks(pg, e2e_ms)
 
-    launches = kernel_launches_per_step(args.precision)
     out = {
         "metric": METRIC, "value": world * npts / (ms / 1000.0), "unit": UNIT, "n_gpus": world,
         "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms, "higher_is_better": True,
@@ -420,7 +612,9 @@ def run_ours(args, world, rank, local, pg):
         "e2e": {"value": world * npts / (e2e_ms / 1000.0), "unit": UNIT,
                 "h2d_bytes_per_step": int(coords_h.numel() * 4 + dm_h.numel() * 4),
                 "d2h_bytes_per_step": int(v_h.numel() * 4)},
-        "gpu_launches": launches,
+        "gpu_launches": int(launches),
+        "gpu_launches_per_step": launches / args.steps,
+        "gpu_launches_counted": "qmt_launch_count() difference around the timed steps (this library's kernels)",
         "clocks": clk.summary(),
     }
     # roofline of the dominant kernel: the density contraction, algorithmic flops npts(2N^2+2N)
@@ -428,11 +622,14 @@ def run_ours(args, world, rank, local, pg):
     flops = npts * (2.0 * nb * nb + 2.0 * nb)
     peak_tf, hbm, kind = peaks()
     achieved = flops / (dens_ms / 1000.0) / 1e12
+    traffic = profiled_traffic() if (args.precision == "fp16x3" and not args.grid) else None
     out["roofline"] = {"bound": "tensor", "kernel": "qmt_density (basis + tcgen05 contraction + row-dot)",
                        "achieved": achieved, "peak": peak_tf, "unit": "TFLOP/s", "frac": achieved / peak_tf,
                        "peak_source": f"bf16_tflops burst, {kind}", "density_ms": dens_ms,
-                       "traffic": profiled_traffic() if (args.precision == "fp16x3" and not args.grid) else None,
-                       "traffic_unit": "DRAM bytes per launch (ncu, dram__bytes_read.sum + dram__bytes_write.sum)"}
+                       "algorithmic_flop_per_launch": flops,
+                       "traffic": traffic["bytes_per_launch"] if traffic else None,
+                       "traffic_unit": "DRAM bytes per launch (ncu, dram__bytes_read.sum + dram__bytes_write.sum)",
+                       "traffic_source": traffic["source"] if traffic else None}
     # the basis evaluation's exponentials, counted separately (npts x primitives of all shells,
     # before screening): what bounds the SIMT half of the kernel
     almos = np.asarray(mol.ALMOs).reshape(-1, 4)
@@ -444,41 +641,51 @@ def run_ours(args, world, rank, local, pg):
     check = None
     if world == 1 and not args.quick:
         # plain FP32 SIMT density (the reference's precision) on the same step
-        p32 = N.PREC["fp32"]
-
         def step32():
-            N.call("qmt_density", handle, nx, ny, nz, h, ox, oy, oz, 1, p32, 1, C.c_void_p(q.data_ptr()),
-                   C.byref(qsum), sh)
-            N.call("qmt_fft_poisson", handle, nx, ny, nz, h, ox, oy, oz, 0.2, 6.0, 1, C.c_void_p(q.data_ptr()),
-                   C.c_void_p(vout.data_ptr()), sh)
+            density(N.PREC["fp32"])
+            poisson()
 
         step32()
         ms32, _ = timed(step32, 5)
         out["plain_fp32"] = {"value": npts / (ms32 / 1000.0), "unit": UNIT, "ms_per_step": ms32,
                              "speedup_of_mixed": ms32 / ms}
-        # accuracy of the mixed path against this library's FP64 density (raw electrons/voxel)
-        q64 = torch.empty_like(q)
+
+        # the reference's own Poisson route (periodic, on the 128^3 grid itself): the step the
+        # reference arm times
+        def step_periodic():
+            density()
+            poisson(0)
+
+        step_periodic()
+        msp, _ = timed(step_periodic, args.steps)
+        e2e_step(0)
+        e2e_p, _ = timed(lambda: e2e_step(0), args.steps)
+        out["like_for_like"] = {
+            "workload": WORKLOAD.replace("density + Hockney FFT Poisson on 256^3",
+                                         "density + periodic FFT Poisson on 128^3 (the reference's solve)"),
+            "value": npts / (msp / 1e3), "unit": UNIT, "ms_per_step": msp,
+            "e2e": {"value": npts / (e2e_p / 1e3), "unit": UNIT}}
+        # device results scored against the FP64 oracle in the CPU leg
         s64, smx = C.c_double(), C.c_double()
-        N.call("qmt_density", handle, nx, ny, nz, h, ox, oy, oz, 1, N.PREC["fp64"], 0, C.c_void_p(q64.data_ptr()),
+        N.call("qmt_density", handle, nx, ny, nz, h, ox, oy, oz, 1, N.PREC["fp64"], 0, C.c_void_p(q.data_ptr()),
                C.byref(s64), sh)
         N.call("qmt_density", handle, nx, ny, nz, h, ox, oy, oz, 1, prec, 0, C.c_void_p(q.data_ptr()),
                C.byref(smx), sh)
         tr = C.c_double()
         N.call("qmt_mol_trace_ps", handle, C.byref(tr), sh)
-        d = (q.double() - q64.double())
-        out["accuracy"] = {"density_rel_l2_vs_fp64": float(d.norm() / q64.double().norm()),
-                           "density_max_abs_vs_fp64": float(d.abs().max()),
-                           "grid_electrons_fp64": s64.value, "grid_electrons_mixed": smx.value,
-                           "electron_count_trace_ps_fp64": 2.0 * tr.value,
-                           "reference": "this library's FP64 density path (checked against the FP64 oracle by the tests)"}
         q_raw = q.cpu().numpy()
         step()
         torch.cuda.synchronize()
-        check = {"q_raw": q_raw, "q": q.cpu().numpy(), "v": vout.cpu().numpy()}
+        check = {"c1": {"precision": args.precision, "q_raw": q_raw, "q": q.cpu().numpy(), "v": vout.cpu().numpy(),
+                        "sum_fp64": s64.value, "sum_mixed": smx.value, "two_trace_ps": 2.0 * tr.value}}
         out.update(batched_and_serving(basis, qmtools, args.precision))
+        out["c0_route"] = c0_route(basis, qmtools, N)
+        out["c2_sweep"], check["c2"] = c2_sweep(basis, qmtools, N)
         out["kernels"] = other_kernels(basis, qmtools, N, hbm, ms - dens_ms, {"n3": npts, "M": 2 * nx})
     if rank == 0 and not args.no_cpu_baseline:
-        out["cpu_baseline"] = cpu_baseline_c1(sm, basis, qmtools, check)
+        out["cpu_baseline"], acc = cpu_baseline_c1(sm, basis, qmtools, check)
+        if acc is not None:
+            out["accuracy"] = acc
     return out
 
 
@@ -553,35 +760,118 @@ def other_kernels(basis, qmtools, N, hbm_peak, fft_ms, nfft):
         ms = e0.elapsed_time(e1)
         out["gto_boundary_c1"] = {"ms": ms, "boundary_points": nb, "points_per_s": nb / (ms / 1e3),
                                   "precision": "FP64 McMurchie-Davidson"}
+        mol.release()
+        # the analytic potential on every corner of the small molecule's 64^3 grid: the
+        # reference arm times its gpu_hartree_GTO on the same grid
+        sm = syn.config_molecule("c0")
+        mol = sm.molecule(basis, qmtools.Molecule)
+        g = sm.grid(qmtools.Grid)
+        nx, ny, nz, h, ox, oy, oz = g._geom()
+        v = torch.zeros(nx * ny * nz, device="cuda")
+        call = lambda: N.call("qmt_hartree_gto", mol.handle, nx, ny, nz, h, ox, oy, oz, C.c_void_p(v.data_ptr()), s)
+        call()
+        ms = _events_ms(call, 3)
+        out["gto_full_grid_c0_64"] = {"ms": ms, "points": nx * ny * nz, "points_per_s": nx * ny * nz / (ms / 1e3),
+                                      "precision": "FP64 McMurchie-Davidson", "points_at": "voxel corners"}
+        mol.release()
     return out
+
+
+TRAFFIC_JSON = ROOT / "profiles" / "density_fused_kernel_c1.traffic.json"
 
 
 def profiled_traffic():
     """DRAM bytes (read + write) per launch of the fused density kernel at the bench size, from
-    the one-pass ncu capture summarised in profiles/density_fused_kernel_c1.md."""
-    import re
-    f = ROOT / "profiles" / "density_fused_kernel_c1.md"
-    if not f.exists():
+    the machine-written summary of an ncu metrics capture (`--ncu-import`), or None."""
+    if not TRAFFIC_JSON.exists():
         return None
-    txt = f.read_text().split("## DRAM traffic at the bench size", 1)[-1]
-    rd = re.search(r"dram__bytes_read\.sum \| ([\d,]+) B", txt)
-    wr = re.search(r"dram__bytes_write\.sum \| ([\d,]+) B", txt)
-    if not (rd and wr):
-        return None
-    return int(rd.group(1).replace(",", "")) + int(wr.group(1).replace(",", ""))
+    d = json.loads(TRAFFIC_JSON.read_text())
+    return {"bytes_per_launch": d["bytes_per_launch"],
+            "source": f"{TRAFFIC_JSON.name}: {d['launches']} launch(es) of {d['kernel']}, {d['command']}"}
 
 
-def kernel_launches_per_step(prec):
-    """Launches of this library's kernels per timed step (density + Hockney FFT)."""
-    dens = 3        # density kernel (fused tensor-core or SIMT), partial-sum reduction, rescale
-    fft = 5         # x forward with the RHS, y forward, z forward x G x z inverse, y inverse, x inverse
-    return dens + fft
+def ncu_import(csv_path, command):
+    """Writes TRAFFIC_JSON from an ncu `--csv` metrics capture of the fused density kernel
+    (one row per launch and metric: ID, Kernel Name, Metric Name, Metric Unit, Metric Value)."""
+    import csv
+    rows = list(csv.DictReader(l for l in Path(csv_path).read_text().splitlines() if l.startswith('"')))
+    scale = {"byte": 1, "Kbyte": 1e3, "Mbyte": 1e6, "Gbyte": 1e9, "KB": 1e3, "MB": 1e6, "GB": 1e9}
+    per = {}
+    for r in rows:
+        if "density_fused_kernel" not in r["Kernel Name"]:
+            continue
+        if r["Metric Name"] not in ("dram__bytes_read.sum", "dram__bytes_write.sum"):
+            continue
+        v = float(r["Metric Value"].replace(",", "")) * scale.get(r["Metric Unit"], 1)
+        per.setdefault(r["ID"], {})[r["Metric Name"]] = v
+    launches = [d for d in per.values() if len(d) == 2]
+    if not launches:
+        raise SystemExit("no density_fused_kernel launch with both DRAM metrics in " + str(csv_path))
+    rd = float(np.mean([d["dram__bytes_read.sum"] for d in launches]))
+    wr = float(np.mean([d["dram__bytes_write.sum"] for d in launches]))
+    out = {"kernel": "density_fused_kernel", "launches": len(launches), "dram_bytes_read": rd,
+           "dram_bytes_write": wr, "bytes_per_launch": rd + wr, "command": command}
+    TRAFFIC_JSON.write_text(json.dumps(out, indent=1) + "\n")
+    print(json.dumps(out))
 
 
 def _ref_libs():
     ref = ROOT / "oracle" / "_ref"
     paths = [ref / "utils.so", ref / "c1_bench" / "density_s1.so", ref / "c1_bench" / "fft.so"]
     return paths if all(p.exists() for p in paths) else None
+
+
+def reference_hartree_kernels():
+    """The reference's analytic potential (gpu_hartree_GTO) and Jacobi sweeps
+    (gpu_hartree_iteration, 1000 pairs = 2000 sweeps launched back to back as its facade loop
+    issues them) on the small molecule's 64^3 grid, CUDA-event timed; the bench's own arm reports
+    qmt_hartree_gto and qmt_jacobi on the same grid (kernels.gto_full_grid_c0_64,
+    kernels.jacobi)."""
+    import ctypes as C
+    import torch
+    import qmtools
+    from qmtools import synthetic as syn
+    so_g = ROOT / "oracle" / "_ref" / "c0_64" / "hartree_gto.so"
+    so_j = ROOT / "oracle" / "_ref" / "c0_64" / "hartree_iter.so"
+    if not (so_g.exists() and so_j.exists()):
+        return None
+    lg, lj = C.CDLL(str(so_g)), C.CDLL(str(so_j))
+    basis = qmtools.BasisSet(qmtools.BASIS_CCPVDZ)
+    sm = syn.config_molecule("c0")
+    mol = sm.molecule(basis, qmtools.Molecule)
+    g = sm.grid(qmtools.Grid)
+    gx, gy, gz = g.GPUblocks
+    n = int(g.npts)
+    dev = "cuda"
+    t = lambda a, dt: torch.from_numpy(np.ascontiguousarray(a, dtype=dt).ravel()).to(dev)
+    types, coords = t(mol.types, np.int32), t(mol.coords, np.float32)
+    alphas, coeffs = t(basis.alphas, np.float32), t(basis.coeffs, np.float32)
+    almos, dm = t(mol.ALMOs, np.int16), t(mol.dm, np.float32)
+    v = torch.zeros(n, device=dev)
+    vp = lambda x: C.c_void_p(x.data_ptr())
+    gto = lambda: lg.ref_hartree_gto(gx, gy, gz, vp(types), vp(coords), vp(alphas), vp(coeffs), vp(almos), vp(dm),
+                                     vp(v))
+    assert gto() == 0
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record()
+    assert gto() == 0
+    e1.record()
+    torch.cuda.synchronize()
+    ms_g = e0.elapsed_time(e1)
+    rho = torch.rand(n, device=dev)
+    a, b = torch.zeros(n, device=dev), torch.zeros(n, device=dev)
+    assert lj.ref_hartree_iteration_pairs(gx, gy, gz, vp(rho), vp(a), vp(b), 10) == 0
+    e0.record()
+    assert lj.ref_hartree_iteration_pairs(gx, gy, gz, vp(rho), vp(a), vp(b), 1000) == 0
+    e1.record()
+    torch.cuda.synchronize()
+    ms_j = e0.elapsed_time(e1)
+    mol.release()
+    return {"gto_full_grid_c0_64": {"ms": ms_g, "points": n, "points_per_s": n / (ms_g / 1e3),
+                                    "kernel": "gpu_hartree_GTO (kernel_hartree.cu:288-869), FP32, voxel corners"},
+            "jacobi_c0_64^3_2000_sweeps": {"ms": ms_j, "us_per_sweep": 1e3 * ms_j / 2000,
+                                           "kernel": "gpu_hartree_iteration (kernel_hartree.cu:85-171), "
+                                                     "2 launches per pair, no host synchronisation"}}
 
 
 def run_reference_gpu(args, world, rank, local, paths):
@@ -647,14 +937,16 @@ def run_reference_gpu(args, world, rank, local, paths):
                 break
         return float(np.mean(ts)), len(ts)
 
-    for _ in range(min(args.warmup, 3)):
+    nwarm = min(args.warmup, 3)   # a reference step takes seconds
+    for _ in range(nwarm):
         step()
     ms, nsteps = timed(args.steps, False, 60.0)
     e2e_ms, _ = timed(max(1, args.steps // 2), True, 30.0)
     ms *= 1000.0
     e2e_ms *= 1000.0
     v_ = n / (ms / 1000.0)
-    return {"metric": METRIC, "value": v_, "unit": UNIT, "n_gpus": world, "steps": nsteps, "warmup": args.warmup,
+    hk = reference_hartree_kernels()
+    return {"metric": METRIC, "value": v_, "unit": UNIT, "n_gpus": world, "steps": nsteps, "warmup": nwarm,
             "ms_per_step": ms, "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "fp32",
             "data": "synthetic", "impl": "reference",
             "config": {"workload": WORKLOAD.replace("density + Hockney FFT Poisson on 256^3",
@@ -664,7 +956,8 @@ def run_reference_gpu(args, world, rank, local, paths):
                              "sample": "the full step on the GPU: the reference's kernels compiled from its sources "
                                        "for sm_100a (oracle/_ref/c1_bench), no host cores used"},
             "e2e": {"value": n / (e2e_ms / 1000.0), "unit": UNIT,
-                    "h2d_bytes_per_step": int(4 * (coords_h.numel() + dm_h.numel())), "d2h_bytes_per_step": 4 * n}}
+                    "h2d_bytes_per_step": int(4 * (coords_h.numel() + dm_h.numel())), "d2h_bytes_per_step": 4 * n},
+            "hartree_kernels": hk}
 
 
 def run_reference(args, world, rank, local, pg):
@@ -712,7 +1005,13 @@ def main():
     ap.add_argument("--quick", action="store_true", help="headline step only (no plain-FP32, batch, serving)")
     ap.add_argument("--grid", type=int, default=0, help="cube edge of a smaller grid for the same molecule")
     ap.add_argument("--only", default="", choices=["", "jacobi"], help="run one kernel family alone (profiling)")
+    ap.add_argument("--ncu-import", default="", help="ncu --csv metrics capture of the fused density kernel "
+                                                     "to summarise into profiles/ (no GPU needed)")
+    ap.add_argument("--ncu-command", default="", help="the command line of that capture (recorded beside it)")
     args = ap.parse_args()
+    if args.ncu_import:
+        ncu_import(args.ncu_import, args.ncu_command)
+        return
     args.warmup = max(args.warmup, 3)
     world, rank, local, pg = dist_setup()
     if args.only == "jacobi":

@@ -60,6 +60,14 @@ const char* qmt_last_error(void);
 int qmt_abi_version(void);
 /* Selects the device for this host thread and checks it is sm_100. */
 qmt_status qmt_init(int device);
+/* Number of kernel launches this library has made in the process so far (new; no reference
+ * counterpart): read it before and after a region to count the region's launches. */
+uint64_t qmt_launch_count(void);
+/* Limit, in nanoseconds, of every bounded wait inside the kernels (grid barriers of the Jacobi
+ * solve, pipeline barriers of the tensor-core density kernels); 0 restores the default of 2 s.
+ * A wait that runs out makes the kernel return early with an error flag that the host reads
+ * (QMT_CUDA_ERR), leaving the context usable.  Process-wide; new, for tests of those paths. */
+qmt_status qmt_set_wait_limit_ns(uint64_t ns);
 
 /* ---- molecule (BasisSet + Molecule device upload) ------------------------------------ */
 /* Replaces the uploads of BasisSet.__init__ (qmtools/qmtools.py:97-103) and
@@ -104,8 +112,7 @@ qmt_status qmt_density(qmt_mol* mol, int nx, int ny, int nz, float step,
 
 /* Selects the tensor-core density implementation (new; process-wide): 0 = automatic (fused
  * when the contraction is fp16/bf16 and N <= 320, staged otherwise), 1 = staged (basis values
- * through HBM), 2 = fused (basis values stay in shared memory), 3 = fused over the upper
- * triangle of P only (half the tensor work, about 2x the FP32 accumulation error). */
+ * through HBM), 2 = fused (basis values stay in shared memory). */
 qmt_status qmt_set_density_path(int mode);
 
 /* ---- analytic GTO potential --------------------------------------------------------- */
@@ -165,7 +172,8 @@ qmt_status qmt_grid_total(const float* q_dev, int64_t n, double* out, void* stre
  * address; make that first call before any stream capture begins.  All calls share the
  * array; every slot a call reads it writes first, so nothing must be cleared, but calls
  * whose work overlaps on the GPU (other streams, other host threads) race on it: order them.
- * Synchronous like qmt_grid_total. */
+ * The looked-up address is kept for the life of the process; a cudaDeviceReset in between is
+ * not supported.  Synchronous like qmt_grid_total. */
 qmt_status qmt_grid_total_noalloc(const float* q_dev, int64_t n, double* out, void* stream);
 /* QMTools.Compute_qscale / gpu_rescale (qmtools/qmtools.py:2808-2813, kernel_utils.cu:54-65). */
 qmt_status qmt_grid_scale(float* q_dev, int64_t n, float factor, void* stream);

@@ -49,6 +49,9 @@ def case_inputs(name, basis=None):
         d = GOLDEN / "molecule_29766_0"
         mol = qmtools.Molecule(str(d / "GEOM-B3LYP.xyz"), str(d / "D-CCSD.npy"), basis)
         return mol, qmtools.Grid.DensityGrid(mol, 0.35, 1.0)
+    if name == "c0_64":
+        sm = syn.config_molecule("c0")
+        return sm.molecule(basis, qmtools.Molecule), sm.grid(qmtools.Grid)
     if name == "c1_bench":
         sm = syn.config_molecule("c1")
         return sm.molecule(basis, qmtools.Molecule), sm.grid(qmtools.Grid)
@@ -63,6 +66,7 @@ CASES = {
     "c1_24": {"density": [1], "hartree_gto": True},
     "sample": {"density": [1], "hartree_gto": False},
     "c1_bench": {"density": [1], "fft": True},
+    "c0_64": {"hartree_gto": True, "hartree_iter": True},   # timing only (bench), no fixture
 }
 VNE_PARAMS = {"adsorb": 0.05, "diff": 0.02}
 NN_SEED = 4242          # seeded pseudo-field and parameters of the automaton cases

@@ -93,6 +93,7 @@ struct TcParams {
   double outscale;
   const double* gsc;   // device {max, 2^g, 2^-g} of the split density matrix
   int* err;
+  uint64_t wait_ns;    // limit of every bounded wait (a test shortens it)
 };
 
 constexpr int MAX_STAGES = 8;
@@ -221,7 +222,7 @@ __global__ void __launch_bounds__(192, 1)
           for (int kc = 0; kc < p.kchunks; ++kc, ++it) {
             const int s = it % p.stages;
             const uint32_t ph = (it / p.stages) & 1u;
-            if (!mbar_wait(&empty_bar[s], ph ^ 1u, &abort_flag)) {
+            if (!mbar_wait(&empty_bar[s], ph ^ 1u, &abort_flag, p.wait_ns)) {
               ok = false;
               break;
             }
@@ -239,7 +240,7 @@ __global__ void __launch_bounds__(192, 1)
       }
       if (!ok) {  // drain copies still in flight before the CTA exits
         for (int s = 0; s < p.stages; ++s)
-          if (last_par[s] >= 0) mbar_wait(&full_bar[s], (uint32_t)last_par[s], &abort_flag, 100000000ull);
+          if (last_par[s] >= 0) mbar_wait_drain(&full_bar[s], (uint32_t)last_par[s], 100000000ull);
       }
     }
   } else if (warp == 1) {
@@ -250,7 +251,7 @@ __global__ void __launch_bounds__(192, 1)
       for (int t = blockIdx.x; t < p.ntiles && ok; t += gridDim.x) {
         for (int pn = 0; pn < p.npanels && ok; ++pn, ++acc_it) {
           const uint32_t buf = acc_it & 1u, aph = (acc_it >> 1) & 1u;
-          if (!mbar_wait(&tempty[buf], aph ^ 1u, &abort_flag)) {
+          if (!mbar_wait(&tempty[buf], aph ^ 1u, &abort_flag, p.wait_ns)) {
             ok = false;
             break;
           }
@@ -259,7 +260,7 @@ __global__ void __launch_bounds__(192, 1)
           for (int kc = 0; kc < p.kchunks; ++kc, ++it) {
             const int s = it % p.stages;
             const uint32_t ph = (it / p.stages) & 1u;
-            if (!mbar_wait(&full_bar[s], ph, &abort_flag)) {
+            if (!mbar_wait(&full_bar[s], ph, &abort_flag, p.wait_ns)) {
               ok = false;
               break;
             }
@@ -292,7 +293,7 @@ __global__ void __launch_bounds__(192, 1)
       }
       // every MMA issued by this thread has completed once drain_bar flips
       tc_commit(&drain_bar);
-      mbar_wait(&drain_bar, 0u, &abort_flag, 500000000ull);
+      mbar_wait_drain(&drain_bar, 0u, 500000000ull);
     }
   } else {
     // epilogue: warps 2..5 -> TMEM lane quadrants 2,3,0,1
@@ -306,7 +307,10 @@ __global__ void __launch_bounds__(192, 1)
       const int64_t grow = (int64_t)t * 128 + row;
       for (int pn = 0; pn < p.npanels; ++pn, ++acc_it) {
         const uint32_t buf = acc_it & 1u, aph = (acc_it >> 1) & 1u;
-        if (!mbar_wait(&tfull[buf], aph, &abort_flag)) {
+        // the four epilogue warps leave together: one of them giving up while the others go on
+        // would leave those waiting at the next named barrier
+        const bool got = mbar_wait(&tfull[buf], aph, &abort_flag, p.wait_ns);
+        if (barrier_any(1, 128, !got)) {
           ok = false;
           break;
         }
@@ -406,21 +410,18 @@ __host__ __device__ inline void split_host(double x, int fmt, void* hi, void* lo
 
 // Scaled, split density matrix on the device: element (r, c), r, c < n, at r * K + c holds
 // P_rc 2^(g - s_r - s_c) split into hi + lo (inv_s = 2^-s, exact powers of two, so this equals
-// ldexp of the same exponents); `tri` keeps c <= r and halves the diagonal.  The pieces must be
-// cleared beforehand (padding stays zero).
+// ldexp of the same exponents).  The pieces must be cleared beforehand (padding stays zero).
 // Element (r, c) goes to r * K + c (row-major), or, with blk_rows > 0, to the K-step blocks of
 // the fused path: block c / 16 holds blk_rows rows of 32 bytes (the 16 columns of one K-step),
 // each row's two 16-byte units exchanged when bit 2 of the row is set -- the 32-byte swizzled
 // K-major image that the MMA reads from shared memory, so that a stage is one contiguous copy.
 __global__ void split_P_kernel(const double* __restrict__ P, int np, int n, int K, const double* __restrict__ inv_s,
-                               const double* __restrict__ gsc, int tri, int fmt, int blk_rows, uint8_t* hi, uint8_t* lo) {
+                               const double* __restrict__ gsc, int fmt, int blk_rows, uint8_t* hi, uint8_t* lo) {
   const int64_t tot = (int64_t)n * n;
   const double two_g = gsc[1];
   for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < tot; i += (int64_t)gridDim.x * blockDim.x) {
     const int r = (int)(i / n), c = (int)(i % n);
-    if (tri && c > r) continue;
-    double v = P[(size_t)c * np + r] * two_g * inv_s[r] * inv_s[c];
-    if (tri && c == r) v *= 0.5;
+    const double v = P[(size_t)c * np + r] * two_g * inv_s[r] * inv_s[c];
     const int e = c & 15, pe = ((((e >> 3) ^ (r >> 2)) & 1) << 3) | (e & 7);   // swizzled position in the row
     const size_t idx = blk_rows > 0 ? ((size_t)(c >> 4) * blk_rows + r) * 16 + pe : (size_t)r * K + c;
     split_host(v, fmt, hi, lo, idx);
@@ -497,14 +498,14 @@ static qmt_status split_exponent(qmt_mol* m, cudaStream_t s) {
   return QMT_OK;
 }
 
-static qmt_status launch_split(qmt_mol* m, int K, int tri, int fmt, int blk_rows, void* hi, void* lo,
+static qmt_status launch_split(qmt_mol* m, int K, int fmt, int blk_rows, void* hi, void* lo,
                                size_t piece_bytes, cudaStream_t s) {
   QMT_CUDA(cudaMemsetAsync(hi, 0, piece_bytes, s));
   QMT_CUDA(cudaMemsetAsync(lo, 0, piece_bytes, s));
   const int64_t tot = (int64_t)m->norbs * m->norbs;
   const int blocks = (int)std::min<int64_t>((tot + 255) / 256, (int64_t)sm_count() * 8);
   split_P_kernel<<<std::max(blocks, 1), 256, 0, s>>>(m->d_P64.as<double>(), m->npad, m->norbs, K,
-                                                     m->d_split_scale.as<double>(), m->d_gscale.as<double>(), tri, fmt, blk_rows,
+                                                     m->d_split_scale.as<double>(), m->d_gscale.as<double>(), fmt, blk_rows,
                                                      reinterpret_cast<uint8_t*>(hi), reinterpret_cast<uint8_t*>(lo));
   QMT_CHECK_LAUNCH("split_P_kernel");
   return QMT_OK;
@@ -513,11 +514,10 @@ static qmt_status launch_split(qmt_mol* m, int K, int tri, int fmt, int blk_rows
 // ---------------------------------------------------------------------------------------
 // Fused path (kind::f16 formats, K <= 320): Phi' never leaves shared memory.
 //
-//   rho = sum_k Phi_k (Phi P)_k over the full symmetric P (default), or, in the triangular
-//   variant, rho = 2 sum_k Phi_k (Phi U)_k with U = triu(P, 1) + diag(P)/2: only the upper
-//   triangle is streamed and multiplied (the K-step covering rows j in [j0, j0+16) touches
-//   output columns k >= j0), half the work, but the partial sums of Phi U are larger than
-//   those of Phi P, so the FP32 tensor-core accumulation loses about a factor 2 in accuracy.
+//   rho = sum_k Phi_k (Phi P)_k over the full symmetric P.  (Streaming only the upper triangle,
+//   rho = 2 sum_k Phi_k (Phi U)_k with U = triu(P, 1) + diag(P)/2, halves the tensor work but
+//   doubles the FP32 accumulation error, and measured 4% slower: the K-step loop is not bound
+//   by tensor work.)
 //
 // CTA layout (one per SM, persistent over 128-row tiles), 10 warps:
 //   warp 0     producer of U: one bulk copy per stage and piece of a K-step block that HBM
@@ -541,7 +541,6 @@ struct FusedParams {
   int kpad, ksteps, nsplit, stages;
   int n16;                 // functions rounded up to 16: K of the MMAs and N (output columns); the
                            // K-steps beyond it only hold zero padding and are skipped
-  int tri;                 // 1: upper-triangular U (half the work); 0: full symmetric P
   int nchunks;             // ceil(n16 / 64) column chunks of A
   int u_rows;              // rows of one K-step block of U in HBM (kpad + 64)
   const uint8_t* u_hi;     // U pieces in K-step blocks (split_P_kernel with blk_rows = u_rows)
@@ -561,8 +560,8 @@ struct FusedParams {
   double* partials;
   double outscale;
   const double* gsc;       // device {max, 2^g, 2^-g} of the split density matrix
-  double g_mul;            // 2 (triangular U) or 1
   int* err;
+  uint64_t wait_ns;        // limit of every bounded wait (a test shortens it)
 };
 
 // Byte offset of element (row, j) in the 128-byte swizzled K-major A tile (64-column chunks of
@@ -1098,13 +1097,12 @@ __device__ __forceinline__ void fused_produce_u(const FusedParams* pp, uint8_t* 
     for (int ks = 0; ks < p.ksteps; ++ks, ++it) {
       const int s = it % p.stages;
       const uint32_t ph = (it / p.stages) & 1u;
-      if (!mbar_wait(&empty_bar[s], ph ^ 1u, abort_flag)) {
+      if (!mbar_wait(&empty_bar[s], ph ^ 1u, abort_flag, p.wait_ns)) {
         ok = false;
         break;
       }
-      const int r0 = p.tri ? ks * 16 : 0;   // first output column touched by this K-step
-      const uint32_t bytes = (uint32_t)(p.n16 - r0) * 32u;
-      const size_t src = ((size_t)ks * p.u_rows + r0) * 32u;
+      const uint32_t bytes = (uint32_t)p.n16 * 32u;
+      const size_t src = (size_t)ks * p.u_rows * 32u;
       uint8_t* st = stages + (size_t)s * p.stage_bytes;
       mbar_expect_tx(&full_bar[s], bytes * (uint32_t)p.nsplit);
       bulk_load(st, p.u_hi + src, bytes, &full_bar[s]);
@@ -1115,7 +1113,7 @@ __device__ __forceinline__ void fused_produce_u(const FusedParams* pp, uint8_t* 
   }
   if (!ok)
     for (int s = 0; s < p.stages; ++s)
-      if ((issued >> s) & 1u) mbar_wait(&full_bar[s], (par >> s) & 1u, abort_flag, 100000000ull);
+      if ((issued >> s) & 1u) mbar_wait_drain(&full_bar[s], (par >> s) & 1u, 100000000ull);
 }
 
 // MMA issuer: per tile, per K-step (after its column chunk of A is complete and its U stage has
@@ -1133,7 +1131,7 @@ __device__ __forceinline__ void fused_issue_mma(const FusedParams* pp, uint32_t 
     for (int ks = 0; ks < p.ksteps; ++ks, ++it) {
       // columns 64c .. 64c+63 of A are complete once every item writing them arrived
       if ((ks & 3) == 0 && p.chunk_need[ks >> 2] > 0) {
-        if (!mbar_wait(&chunk_bar[ks >> 2], tile_it & 1u, abort_flag)) {
+        if (!mbar_wait(&chunk_bar[ks >> 2], tile_it & 1u, abort_flag, p.wait_ns)) {
           ok = false;
           break;
         }
@@ -1141,21 +1139,20 @@ __device__ __forceinline__ void fused_issue_mma(const FusedParams* pp, uint32_t 
       }
       const int s = it % p.stages;
       const uint32_t ph = (it / p.stages) & 1u;
-      if (!mbar_wait(&full_bar[s], ph, abort_flag)) {
+      if (!mbar_wait(&full_bar[s], ph, abort_flag, p.wait_ns)) {
         ok = false;
         break;
       }
       tc_fence_after();
       const int j0 = ks * 16;
-      const int r0 = p.tri ? j0 : 0;
       // A K-step: 32 bytes inside a 128-byte swizzled chunk
       const uint32_t aoff = (uint32_t)((j0 >> 6) * 16384 + ((j0 & 63) >> 4) * 32);
       const uint64_t ahi = sw128_kmajor_desc(abase + aoff), alo = sw128_kmajor_desc(lbase + aoff);
       const uint32_t bst = smem_u32(stages + (size_t)s * p.stage_bytes);
-      for (int c0 = r0; c0 < p.n16; c0 += 256) {
+      for (int c0 = 0; c0 < p.n16; c0 += 256) {
         const int n = min(256, p.n16 - c0);
         const uint32_t idesc = make_idesc(p.fmt, 128, (uint32_t)n);
-        const uint32_t boff = (uint32_t)(c0 - r0) * 32u;
+        const uint32_t boff = (uint32_t)c0 * 32u;
         const uint32_t d = tmem + (uint32_t)c0;
         mma_f16(d, ahi, sw32_kmajor_desc(bst + boff), idesc, ks > 0 ? 1u : 0u);
         if (two) {
@@ -1168,7 +1165,7 @@ __device__ __forceinline__ void fused_issue_mma(const FusedParams* pp, uint32_t 
     if (ok) tc_commit(t_full);
   }
   tc_commit(drain_bar);
-  mbar_wait(drain_bar, 0u, abort_flag, 500000000ull);
+  mbar_wait_drain(drain_bar, 0u, 500000000ull);
 }
 
 template <int FMT>
@@ -1275,7 +1272,10 @@ __global__ void __launch_bounds__(FUSED_THREADS, 1)
         }
       }
       // ---- epilogue -----------------------------------------------------------------------
-      if (!mbar_wait(&t_full, tile_it & 1u, &abort_flag)) break;
+      // the compute warps leave together: one of them giving up while the others go on would
+      // leave those waiting at the next named barrier
+      const bool got = mbar_wait(&t_full, tile_it & 1u, &abort_flag, p.wait_ns);
+      if (barrier_any(1, FUSED_NCT, !got)) break;
       tc_fence_after();
       double acc[2] = {0.0, 0.0};
       const uint32_t trow = tmem + ((uint32_t)(q * 32) << 16);
@@ -1324,7 +1324,7 @@ __global__ void __launch_bounds__(FUSED_THREADS, 1)
         }
         int64_t vox, ix, iy, iz;
         if (tile_voxel(p.pm, t, ct, vox, ix, iy, iz)) {
-          const float qv = (float)(r * (p.g_mul * p.gsc[2]) * p.outscale);
+          const float qv = (float)(r * p.gsc[2] * p.outscale);
           p.qube[vox] = qv;
           mysum = qv;
         }
@@ -1443,10 +1443,9 @@ static qmt_status ensure_mol_tables(qmt_mol* m, const std::vector<float>& fs, in
 // U_jn for j <= n, i.e. Ptilde_jn for j < n and Ptilde_nn / 2 on the diagonal.  Both variants are
 // stored as K-step blocks of kpad + 64 rows x 16 columns in the 32-byte swizzled image of a stage
 // (split_P_kernel), read by one contiguous copy per stage and piece.
-static int g_fused_tri = 0;   // upper-triangular variant of the fused path (off by default)
 
 static qmt_status ensure_fused_operands(qmt_mol* m, int prec, const TcShape& sh, cudaStream_t s) {
-  const int key = prec * 2 + g_fused_tri;
+  const int key = prec;
   if (m->fused_prec == key) return QMT_OK;
   const int K = sh.kpad;
   qmt_status st;
@@ -1454,7 +1453,7 @@ static qmt_status ensure_fused_operands(qmt_mol* m, int prec, const TcShape& sh,
   const int rows = K + 64;
   const size_t piece = (size_t)rows * K * 2;
   if ((st = m->d_fused_B.reserve(2 * piece))) return st;
-  if ((st = launch_split(m, K, g_fused_tri, sh.fmt, K + 64, m->d_fused_B.ptr, m->d_fused_B.as<uint8_t>() + piece,
+  if ((st = launch_split(m, K, sh.fmt, K + 64, m->d_fused_B.ptr, m->d_fused_B.as<uint8_t>() + piece,
                          piece, s)))
     return st;
   m->fused_prec = key;
@@ -1471,7 +1470,7 @@ static int fused_tab_bytes(const qmt_mol* m) {
 // and of one U piece slot in a stage.
 static int fused_n16(const qmt_mol* m) { return (m->norbs + 15) / 16 * 16; }
 static uint32_t fused_a_bytes(int kpad) { return 128u * (uint32_t)kpad * 2u; }
-static uint32_t fused_b_slot(int kpad, int n16) { return (uint32_t)(g_fused_tri ? kpad : n16) * 32u; }
+static uint32_t fused_b_slot(int n16) { return (uint32_t)n16 * 32u; }
 
 // U pipeline stages that fit beside A and the tables (below 2: the fused path does not fit).
 template <int FMT>
@@ -1481,7 +1480,7 @@ static int fused_stages(const TcShape& sh, int n16, int tab_bytes) {
   cudaDeviceGetAttribute(&maxsm, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev);
   cudaFuncAttributes fa;
   if (cudaFuncGetAttributes(&fa, density_fused_kernel<FMT>) != cudaSuccess) return 0;
-  const long a_bytes = fused_a_bytes(sh.kpad), stage_bytes = (long)sh.nsplit * fused_b_slot(sh.kpad, n16);
+  const long a_bytes = fused_a_bytes(sh.kpad), stage_bytes = (long)sh.nsplit * fused_b_slot(n16);
   const long avail = (long)maxsm - (long)fa.sharedSizeBytes - 1024 - sh.nsplit * a_bytes - tab_bytes;
   return (int)std::max<long>(0, std::min<long>(MAX_STAGES, avail / stage_bytes));
 }
@@ -1502,7 +1501,6 @@ static qmt_status run_fused(qmt_mol* m, const TcShape& sh, const PointMap& pm, i
   p.u_hi = B;
   p.u_lo = B + piece;
   p.ksteps = n16 / 16;
-  p.tri = g_fused_tri;
   p.nchunks = (n16 + 63) / 64;
   if (p.nchunks > MAX_FUSED_CHUNKS) return fail(QMT_BAD_ARG, "fused density path supports kpad <= 320");
   for (int a = 0; a < m->natoms; ++a) {
@@ -1514,7 +1512,7 @@ static qmt_status run_fused(qmt_mol* m, const TcShape& sh, const PointMap& pm, i
   }
   p.nsplit = sh.nsplit;
   p.a_bytes = fused_a_bytes(K);
-  p.b_slot = fused_b_slot(K, n16);
+  p.b_slot = fused_b_slot(n16);
   p.stage_bytes = p.nsplit * p.b_slot;
   p.fmt = (uint32_t)sh.fmt;
   p.tab = m->d_fused_tab.as<int4>();
@@ -1527,7 +1525,7 @@ static qmt_status run_fused(qmt_mol* m, const TcShape& sh, const PointMap& pm, i
   p.partials = m->d_partials.as<double>();
   p.outscale = outscale;
   p.gsc = m->d_gscale.as<double>();
-  p.g_mul = g_fused_tri ? 2.0 : 1.0;
+  p.wait_ns = wait_limit_ns();
   p.err = reinterpret_cast<int*>(m->d_scalars.as<double>() + 8);
   auto kern = density_fused_kernel<FMT>;
   const int stages = fused_stages<FMT>(sh, n16, p.tab_bytes);
@@ -1549,7 +1547,7 @@ static qmt_status ensure_tc_operands(qmt_mol* m, int prec, const TcShape& sh, cu
   if ((st = ensure_basis_operands(m, K, s)) || (st = split_exponent(m, s))) return st;
   const size_t piece = (size_t)sh.nrows_b * K * sh.esize;
   if ((st = m->d_tc_P.reserve(2 * piece))) return st;
-  if ((st = launch_split(m, K, 0, sh.fmt, 0, m->d_tc_P.ptr, m->d_tc_P.as<uint8_t>() + piece, piece, s))) return st;
+  if ((st = launch_split(m, K, sh.fmt, 0, m->d_tc_P.ptr, m->d_tc_P.as<uint8_t>() + piece, piece, s))) return st;
   m->tc_prec = prec;
   return QMT_OK;
 }
@@ -1597,6 +1595,7 @@ static qmt_status run_tc(qmt_mol* m, const TcShape& sh, const PointMap& pm, int6
   p.outscale = outscale;
   p.gsc = m->d_gscale.as<double>();
   p.err = reinterpret_cast<int*>(m->d_scalars.as<double>() + 8);
+  p.wait_ns = wait_limit_ns();
 
   int maxsm = 0, dev = 0;
   cudaGetDevice(&dev);
@@ -1707,9 +1706,8 @@ qmt_status density_tc(qmt_mol* mol, int nx, int ny, int nz, float step, float ox
 }  // namespace qmt
 
 extern "C" qmt_status qmt_set_density_path(int mode) {
-  if (mode < 0 || mode > 3)
-    return qmt::fail(QMT_BAD_ARG, "density path must be 0 (auto), 1 (staged), 2 (fused) or 3 (fused, triangular)");
-  qmt::g_density_path = mode == 3 ? 2 : mode;
-  qmt::g_fused_tri = mode == 3 ? 1 : 0;
+  if (mode < 0 || mode > 2)
+    return qmt::fail(QMT_BAD_ARG, "density path must be 0 (auto), 1 (staged) or 2 (fused)");
+  qmt::g_density_path = mode;
   return QMT_OK;
 }

@@ -426,6 +426,7 @@ qmt_status qmt_vne_pseudo(qmt_mol* mol, int nx, int ny, int nz, float step, floa
                                                      res_dev, out_dev, part);
     vne_pseudo_kernel<<<(unsigned)nblk, 256, 0, s>>>(mol->view(), nx, ny, nz, step, ox, oy, oz, ads, dif,
                                                      out_dev, res_dev, part);
+    note_launches(1);   // the first of the two ping-pong launches
     QMT_CHECK_LAUNCH("vne_pseudo_kernel");
     if ((st = reduce_partials(part, nblk, res, 1, 0, s))) return st;
     double h = 0;

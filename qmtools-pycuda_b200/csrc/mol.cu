@@ -4,6 +4,7 @@
 #include <cuda_fp16.h>
 
 #include <algorithm>
+#include <atomic>
 #include <cstring>
 #include <mutex>
 
@@ -46,6 +47,13 @@ void DevBuf::release() {
   ptr = nullptr;
   bytes = 0;
 }
+
+static std::atomic<uint64_t> g_launches{0};
+void note_launches(uint64_t n) { g_launches.fetch_add(n, std::memory_order_relaxed); }
+
+constexpr uint64_t kDefaultWaitNs = 2000000000ull;   // 2 s
+static std::atomic<uint64_t> g_wait_ns{kDefaultWaitNs};
+uint64_t wait_limit_ns() { return g_wait_ns.load(std::memory_order_relaxed); }
 
 int sm_count() {
   static int n = 0;
@@ -267,6 +275,14 @@ extern "C" {
 const char* qmt_last_error(void) { return g_last_error.c_str(); }
 
 int qmt_abi_version(void) { return 1; }
+
+uint64_t qmt_launch_count(void) { return g_launches.load(std::memory_order_relaxed); }
+
+qmt_status qmt_set_wait_limit_ns(uint64_t ns) {
+  if (ns > 60000000000ull) return fail(QMT_BAD_ARG, "wait limit above 60 s");
+  g_wait_ns.store(ns ? ns : kDefaultWaitNs, std::memory_order_relaxed);
+  return QMT_OK;
+}
 
 qmt_status qmt_init(int device) {
   int n = 0;

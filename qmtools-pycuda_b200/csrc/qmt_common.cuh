@@ -24,11 +24,19 @@ qmt_status cuda_fail(cudaError_t e, const char* what);
     if (e_ != cudaSuccess) return ::qmt::cuda_fail(e_, #call);      \
   } while (0)
 
+// Every kernel launch of the library is followed by this check, which also counts it
+// (qmt_launch_count); a call site that launches twice before one check adds the extra launch
+// with note_launches.
 #define QMT_CHECK_LAUNCH(what)                                      \
   do {                                                              \
+    ::qmt::note_launches(1);                                        \
     cudaError_t e_ = cudaGetLastError();                            \
     if (e_ != cudaSuccess) return ::qmt::cuda_fail(e_, what);       \
   } while (0)
+
+void note_launches(uint64_t n);
+// Limit of the kernels' bounded waits on barriers (ns); qmt_set_wait_limit_ns changes it.
+uint64_t wait_limit_ns();
 
 inline cudaStream_t as_stream(void* s) { return reinterpret_cast<cudaStream_t>(s); }
 

@@ -43,6 +43,19 @@ __device__ __forceinline__ bool mbar_try_wait(uint64_t* bar, uint32_t parity) {
   return ok != 0;
 }
 
+// Non-blocking probe of the same phase.
+__device__ __forceinline__ bool mbar_test_wait(uint64_t* bar, uint32_t parity) {
+  uint32_t ok;
+  asm volatile(
+      "{\n\t.reg .pred p;\n\t"
+      "mbarrier.test_wait.parity.shared::cta.b64 p, [%1], %2;\n\t"
+      "selp.u32 %0, 1, 0, p;\n\t}\n"
+      : "=r"(ok)
+      : "r"(smem_u32(bar)), "r"(parity)
+      : "memory");
+  return ok != 0;
+}
+
 __device__ __forceinline__ uint64_t globaltimer_ns() {
   uint64_t t;
   asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
@@ -51,8 +64,20 @@ __device__ __forceinline__ uint64_t globaltimer_ns() {
 
 // Bounded wait for the phase of `parity` to complete: gives up after `limit_ns` of wall
 // time (or as soon as another role raised `abort_flag`), raises the flag and returns false.
+// Limits below 100 us (tests of the give-up paths) poll without blocking and read the clock on
+// every poll, so that the limit, not the length of a blocking try_wait, decides.
 __device__ __forceinline__ bool mbar_wait(uint64_t* bar, uint32_t parity, volatile int* abort_flag,
                                           uint64_t limit_ns = 2000000000ull) {
+  if (limit_ns < 100000ull) {
+    const uint64_t t0 = globaltimer_ns();
+    for (;;) {
+      if (mbar_test_wait(bar, parity)) return true;
+      if (*abort_flag) return false;
+      if (globaltimer_ns() - t0 > limit_ns) break;
+    }
+    *abort_flag = 1;
+    return false;
+  }
   if (mbar_try_wait(bar, parity)) return true;
   const uint64_t t0 = globaltimer_ns();
   for (uint32_t i = 1;; ++i) {
@@ -65,6 +90,36 @@ __device__ __forceinline__ bool mbar_wait(uint64_t* bar, uint32_t parity, volati
   }
   *abort_flag = 1;
   return false;
+}
+
+// Bounded wait used after an abort, for work this thread itself started (copies in flight, MMAs
+// not yet complete): it ignores the abort flag and gives up only after `limit_ns`, so that the
+// CTA does not free shared or tensor memory that is still being written.
+__device__ __forceinline__ bool mbar_wait_drain(uint64_t* bar, uint32_t parity, uint64_t limit_ns) {
+  if (mbar_try_wait(bar, parity)) return true;
+  const uint64_t t0 = globaltimer_ns();
+  for (uint32_t i = 1;; ++i) {
+    if (mbar_try_wait(bar, parity)) return true;
+    if ((i & 63u) == 0u) {
+      if (globaltimer_ns() - t0 > limit_ns) return false;
+      __nanosleep(64);
+    }
+  }
+}
+
+// True on every thread of the named barrier `id` (`nthreads` threads) when `pred` is true on any
+// of them: the group takes one decision even when its members' waits ended differently.
+__device__ __forceinline__ bool barrier_any(int id, int nthreads, bool pred) {
+  uint32_t r;
+  asm volatile(
+      "{\n\t.reg .pred p, q;\n\t"
+      "setp.ne.u32 p, %1, 0;\n\t"
+      "bar.red.or.pred q, %2, %3, p;\n\t"
+      "selp.u32 %0, 1, 0, q;\n\t}\n"
+      : "=r"(r)
+      : "r"((uint32_t)pred), "r"(id), "r"(nthreads)
+      : "memory");
+  return r != 0;
 }
 
 __device__ __forceinline__ void tma_load_2d(void* dst, const CUtensorMap* map, uint64_t* bar, int x, int y) {

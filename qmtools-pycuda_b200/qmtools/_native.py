@@ -25,7 +25,7 @@ _i64 = C.c_int64
 _pd = C.POINTER(C.c_double)
 _pi = C.POINTER(C.c_int)
 
-# name -> argtypes (every function returns int status, except the two noted)
+# name -> argtypes (every function returns an int status, except those in OTHER)
 SIGNATURES = {
     "qmt_init": [_i],
     "qmt_mol_create": [_i, _vp, _vp, _i, _vp, _i, _vp, _vp, _vp, _vp, C.POINTER(_vp)],
@@ -36,6 +36,7 @@ SIGNATURES = {
     "qmt_mol_trace_ps": [_vp, _pd, _vp],
     "qmt_density": [_vp, _i, _i, _i, _f, _f, _f, _f, _i, _i, _i, _vp, _pd, _vp],
     "qmt_set_density_path": [_i],
+    "qmt_set_wait_limit_ns": [C.c_uint64],
     "qmt_hartree_gto": [_vp, _i, _i, _i, _f, _f, _f, _f, _vp, _vp],
     "qmt_hartree_gto_points": [_vp, _i, _vp, _vp, _vp],
     "qmt_hartree_gto_boundary": [_vp, _i, _i, _i, _f, _f, _f, _f, _vp, _vp],
@@ -53,7 +54,8 @@ SIGNATURES = {
     "qmt_vne_pseudo": [_vp, _i, _i, _i, _f, _f, _f, _f, _f, _f, _d, _i, _vp, _vp, _pi, _vp],
     "qmt_nn_singleshot": [_i, _i, _i, _d, _vp, _vp, _vp, _i, _i, _vp],
 }
-OTHER = {"qmt_last_error": ([], C.c_char_p), "qmt_abi_version": ([], C.c_int)}
+OTHER = {"qmt_last_error": ([], C.c_char_p), "qmt_abi_version": ([], C.c_int),
+         "qmt_launch_count": ([], C.c_uint64)}
 
 
 class NativeUnavailable(RuntimeError):

@@ -478,6 +478,47 @@ class QMTools:
             vgrid._download()
         return vgrid
 
+    ### Jacobi relaxation in physical units with the analytic boundary (new facade method).
+    def Compute_hartree_dirichlet(qgrid, molecule, max_sweeps=2000, tolerance=0.0, check_every=100,
+                                  copyBack=True):
+        """Total electrostatic potential (a.u.) at voxel centres by Jacobi relaxation of
+        lap V = -4 pi rho, rho = (nuclear seed charges - electrons per voxel) / h^3, with the
+        outer shell held at the analytic GTO potential of the molecule (electrons and nuclei).
+
+        The reference's Compute_hartree_iter (qmtools/qmtools.py:2497-2573) relaxes the same
+        charge grid in its own units (no 4 pi) with a zero outer shell; this variant fixes the
+        boundary from gpu_hartree_GTO's potential (kernel_hartree.cu:288-869), so the interior
+        converges to the free-space potential.  The FP64 residual sum |V - T| of the last check
+        is returned as `.delta`, the sweeps done as `.sweeps`.  tolerance 0 runs max_sweeps."""
+        import ctypes as C
+        torch = _torch()
+        nx, ny, nz, h, ox, oy, oz = qgrid._geom()
+        seed = QMTools.Compute_qseed(qgrid, molecule, copyBack=False)
+        rho = _new_like(qgrid, 1)
+        torch.sub(seed.field(0), qgrid.field(0), out=rho.field(0))
+        rho.field(0).mul_(1.0 / float(h) ** 3)
+        vgrid = _new_like(qgrid, 1)
+        tgrid = _new_like(qgrid, 1)
+        N.call("qmt_hartree_gto_boundary", molecule.handle, nx, ny, nz, h, ox, oy, oz,
+               C.c_void_p(vgrid.field(0).data_ptr()), N.stream_handle())
+        sw = C.c_int()
+        dl = C.c_double()
+        st = N.load().qmt_jacobi_dirichlet(nx, ny, nz, h, C.c_void_p(rho.field(0).data_ptr()),
+                                           C.c_void_p(vgrid.field(0).data_ptr()),
+                                           C.c_void_p(tgrid.field(0).data_ptr()), int(max_sweeps),
+                                           int(check_every), float(tolerance), C.byref(sw), C.byref(dl),
+                                           N.stream_handle())
+        if st == N.NOT_CONVERGED:
+            warnings.warn(f"Jacobi not converged after {sw.value} sweeps (delta {dl.value:.3e})")
+        else:
+            N.check(st, "qmt_jacobi_dirichlet")
+        vgrid.sweeps = sw.value
+        vgrid.delta = dl.value
+        vgrid.rho = rho
+        if copyBack:
+            vgrid._download()
+        return vgrid
+
     ### FFT Poisson solve (qmtools/qmtools.py:2578-2639); returns (NX,NY,NZ) volts, C-order.
     def Compute_hartree_fft(qgrid, molecule, sigma=0.2, cutoff=6, padded=False):
         import ctypes as C

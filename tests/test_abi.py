@@ -41,3 +41,13 @@ def test_bad_arguments_rejected_without_device():
     assert lib.qmt_density(None, 8, 8, 8, 0.1, 0, 0, 0, 1, 1, 1, None, None, None) == N.BAD_ARG
     assert lib.qmt_jacobi(8, 8, 8, 0.1, None, None, None, 10, 1, 0.0, None, None, None) == N.BAD_ARG
     assert b"Jacobi" in lib.qmt_last_error()
+
+
+def test_wait_limit_and_launch_count_without_device():
+    """The wait limit is checked and set without a device; the launch counter starts at zero
+    in a process that has launched nothing (this suite launches nothing)."""
+    lib = N.load()
+    assert lib.qmt_set_wait_limit_ns(61 * 10 ** 9) == N.BAD_ARG
+    assert lib.qmt_set_wait_limit_ns(1000) == N.OK
+    assert lib.qmt_set_wait_limit_ns(0) == N.OK
+    assert lib.qmt_launch_count() == 0
