@@ -115,6 +115,31 @@ qmt_status qmt_density(qmt_mol* mol, int nx, int ny, int nz, float step,
  * through HBM), 2 = fused (basis values stay in shared memory). */
 qmt_status qmt_set_density_path(int mode);
 
+/* ---- batches of molecules (new; no reference counterpart) ---------------------------- */
+/* The reference evaluates one molecule per Compute_density call (qmtools/qmtools.py:2381-2430).
+ * A batch evaluates the densities of many molecules together: the molecules whose contraction
+ * takes the fused path share one persistent launch over all their tiles; the others (N > 320 or
+ * tf32) get the staged path, one molecule after another; then each grid is summed and, with
+ * rescale, scaled to its nuclear charge.  Inputs: shapes[3 i + (0,1,2)] = nx, ny, nz and
+ * geoms[4 i + (0,1,2,3)] = step, ox, oy, oz (bohr) of molecule i; qube_devs[i] its grid (device,
+ * nx ny nz floats, x-fastest); paths[i] 0 = automatic, 1 = staged, 2 = fused (NULL: automatic).
+ * qmt_batch_create builds every operand (it synchronises `stream`); qmt_batch_density then
+ * allocates nothing and is fully asynchronous, so a CUDA graph can capture it.  With refresh != 0
+ * it first re-derives each molecule's split density matrix on the device from the matrix last
+ * uploaded with qmt_mol_set_dm, so a captured graph follows new uploads.  The molecules must not
+ * be used by other calls while a batch call on them is in flight, and must outlive the batch. */
+typedef struct qmt_batch qmt_batch;
+qmt_status qmt_batch_create(int nmol, qmt_mol* const* mols, const int32_t* shapes, const float* geoms,
+                            int subgrid, int precision, const int32_t* paths, float* const* qube_devs,
+                            void* stream, qmt_batch** out);
+qmt_status qmt_batch_density(qmt_batch* batch, int rescale, int refresh, void* stream);
+/* FP64 grid sums before rescaling, sums[nmol] (host); synchronous; reports and clears the kernels'
+ * barrier-timeout flags (QMT_CUDA_ERR). */
+qmt_status qmt_batch_sums(qmt_batch* batch, double* sums, void* stream);
+/* Molecules of the batch on the shared fused launch (-1 for NULL). */
+int qmt_batch_fused_count(const qmt_batch* batch);
+qmt_status qmt_batch_destroy(qmt_batch* batch);
+
 /* ---- analytic GTO potential --------------------------------------------------------- */
 /* QMTools.Compute_hartree (qmtools/qmtools.py:2436-2489) with gpu_hartree_GTO
  * (kernel_hartree.cu:288-869): V(C) = -2 sum_pq P_pq (phi_p phi_q | 1/|r-C|) + sum_A Z_A/|C-R_A|
@@ -130,6 +155,11 @@ qmt_status qmt_hartree_gto_points(qmt_mol* mol, int npts, const float* pts_dev,
  * Dirichlet boundary of qmt_jacobi_dirichlet.  New entry point. */
 qmt_status qmt_hartree_gto_boundary(qmt_mol* mol, int nx, int ny, int nz, float step,
                                     float ox, float oy, float oz, float* v_dev, void* stream);
+/* Arithmetic of the three analytic-potential entry points above (new; process-wide):
+ * QMT_PREC_FP32 (default) evaluates each pair term in FP32 -- the asymptotic Boys functions
+ * where p |P - C|^2 >= 30, a table otherwise -- and accumulates in FP64, with the nuclear term
+ * in FP64; QMT_PREC_FP64 keeps every operation in FP64 (the checker of the FP32 kernel). */
+qmt_status qmt_set_gto_precision(int precision);
 
 /* ---- Jacobi relaxation ---------------------------------------------------------------- */
 /* QMTools.Compute_hartree_iter (qmtools/qmtools.py:2497-2573) with gpu_hartree_iteration
@@ -147,6 +177,12 @@ qmt_status qmt_jacobi(int nx, int ny, int nz, float step, const float* rho_dev,
 qmt_status qmt_jacobi_dirichlet(int nx, int ny, int nz, float step, const float* rho_dev,
                                 float* v_dev, float* t_dev, int max_sweeps, int check_every,
                                 double tol, int* sweeps_out, double* delta_out, void* stream);
+/* Selects the Jacobi implementation of the two calls above (new; process-wide): 0 = automatic
+ * (one 16-CTA thread-block cluster holding the field in shared memory when nx % 4 == 0,
+ * nx * ny <= 4096 and nz <= 64, else a persistent kernel with a grid barrier between sweeps),
+ * 1 = always the grid-barrier kernel, 2 = always the cluster kernel (QMT_BAD_ARG where it does
+ * not apply).  Both give identical grids; the residual sums may differ in the last bits. */
+qmt_status qmt_set_jacobi_path(int mode);
 
 /* ---- FFT Poisson ---------------------------------------------------------------------- */
 /* QMTools.Compute_hartree_fft (qmtools/qmtools.py:2578-2639) with gpu_add_nuclear_charge
@@ -158,6 +194,14 @@ qmt_status qmt_jacobi_dirichlet(int nx, int ny, int nz, float step, const float*
 qmt_status qmt_fft_poisson(qmt_mol* mol, int nx, int ny, int nz, float step,
                            float ox, float oy, float oz, float sigma, float cutoff,
                            int padded, const float* q_dev, float* out_dev, void* stream);
+/* The free-space solve of qmt_fft_poisson(padded = 1) with explicit padded lengths mx >= 2 nx,
+ * my >= 2 ny, mz >= 2 nz (lengths whose prime factors are at most 127); new, for callers that
+ * pick the transform lengths (the batch autotuner).  The potential does not depend on them
+ * beyond FP32 rounding. */
+qmt_status qmt_fft_poisson_padded(qmt_mol* mol, int nx, int ny, int nz, float step,
+                                  float ox, float oy, float oz, float sigma, float cutoff,
+                                  int mx, int my, int mz, const float* q_dev, float* out_dev,
+                                  void* stream);
 
 /* ---- grid utilities and nuclear fields ----------------------------------------------- */
 /* QMTools.Compute_qtot / gpu_total (qmtools/qmtools.py:2796-2803, kernel_utils.cu:68-98),

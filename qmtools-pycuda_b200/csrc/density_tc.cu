@@ -534,35 +534,64 @@ static qmt_status launch_split(qmt_mol* m, int K, int fmt, int blk_rows, void* h
 // ---------------------------------------------------------------------------------------
 constexpr int MAX_FUSED_CHUNKS = 5;   // fused path: kpad <= 320
 
-struct FusedParams {
-  MolView mol;
+// One molecule of a fused launch.  A launch covers the tiles of one or more molecules; global tile
+// t belongs to the molecule with tile0 <= t < tile0 + ntiles.
+struct FusedMol {
   PointMap pm;
-  int64_t ntiles;
-  int kpad, ksteps, nsplit, stages;
+  int64_t tile0, ntiles;
+  int natoms, norbs;
   int n16;                 // functions rounded up to 16: K of the MMAs and N (output columns); the
                            // K-steps beyond it only hold zero padding and are skipped
-  int nchunks;             // ceil(n16 / 64) column chunks of A
+  int ksteps, nchunks;     // n16 / 16 K-steps; ceil(n16 / 64) column chunks of A
   int u_rows;              // rows of one K-step block of U in HBM (kpad + 64)
   const uint8_t* u_hi;     // U pieces in K-step blocks (split_P_kernel with blk_rows = u_rows)
   const uint8_t* u_lo;
   int chunk_need[MAX_FUSED_CHUNKS];  // production items (atom halves) writing each chunk
-  uint32_t a_bytes;        // one A piece: 128 rows x kpad x 2 B
-  uint32_t b_slot;         // one U piece slot in a stage: n16 (triangular: kpad) rows x 32 B
-  uint32_t stage_bytes;
-  uint32_t fmt;
   const int4* tab;         // molecule tables (ensure_mol_tables)
   int tab_words;           // 16-byte words of tab
   int off_prim;            // byte offsets inside the staged tables: primitive pairs,
   int off_ashell;          //   first shell of each atom,
   int off_coords;          //   nuclear coordinates (float x, y, z)
-  int tab_bytes;           // shared-memory bytes of the staged tables
+  const float* coords;
   float* qube;
-  double* partials;
+  double* partials;        // per tile of this molecule
   double outscale;
   const double* gsc;       // device {max, 2^g, 2^-g} of the split density matrix
+};
+
+struct FusedParams {
+  FusedMol one;            // the molecule of a single-molecule launch (nmol == 1)
+  const FusedMol* mols;    // device array of nmol molecules (nmol > 1)
+  int nmol;
+  int64_t ntiles;          // tiles of all molecules
+  int nsplit, stages;
+  uint32_t a_bytes;        // one A piece: 128 rows x (largest kpad) x 2 B
+  uint32_t b_slot;         // one U piece slot in a stage: (largest n16) rows x 32 B
+  uint32_t stage_bytes;
+  uint32_t fmt;
   int* err;
   uint64_t wait_ns;        // limit of every bounded wait (a test shortens it)
 };
+
+// Arrival count of a column-chunk barrier: each tile pre-arrives CHUNK_COUNT - need, the
+// production items the rest, so that molecules with different atom counts share the barriers.
+constexpr uint32_t CHUNK_COUNT = 1024;
+
+// The molecule of global tile t (binary search over the launch's molecules).
+__device__ __forceinline__ const FusedMol& fused_mol(const FusedParams& p, int64_t t, int& m) {
+  if (p.nmol == 1) {
+    m = 0;
+    return p.one;
+  }
+  int lo = 0, hi = p.nmol - 1;
+  while (lo < hi) {
+    const int mid = (lo + hi + 1) >> 1;
+    if (__ldg(&p.mols[mid].tile0) <= t) lo = mid;
+    else hi = mid - 1;
+  }
+  m = lo;
+  return p.mols[lo];
+}
 
 // Byte offset of element (row, j) in the 128-byte swizzled K-major A tile (64-column chunks of
 // 8-row atoms of 1024 B, 16-byte unit u of a row at u ^ (row & 7)).  Row r + 64 of a column sits
@@ -1094,19 +1123,21 @@ __device__ __forceinline__ void fused_produce_u(const FusedParams* pp, uint8_t* 
   uint32_t it = 0, issued = 0, par = 0;   // bit s: stage s has a copy in flight / its phase parity
   bool ok = true;
   for (int64_t t = blockIdx.x; t < p.ntiles && ok; t += gridDim.x) {
-    for (int ks = 0; ks < p.ksteps; ++ks, ++it) {
+    int m;
+    const FusedMol& M = fused_mol(p, t, m);
+    for (int ks = 0; ks < M.ksteps; ++ks, ++it) {
       const int s = it % p.stages;
       const uint32_t ph = (it / p.stages) & 1u;
       if (!mbar_wait(&empty_bar[s], ph ^ 1u, abort_flag, p.wait_ns)) {
         ok = false;
         break;
       }
-      const uint32_t bytes = (uint32_t)p.n16 * 32u;
-      const size_t src = (size_t)ks * p.u_rows * 32u;
+      const uint32_t bytes = (uint32_t)M.n16 * 32u;
+      const size_t src = (size_t)ks * M.u_rows * 32u;
       uint8_t* st = stages + (size_t)s * p.stage_bytes;
       mbar_expect_tx(&full_bar[s], bytes * (uint32_t)p.nsplit);
-      bulk_load(st, p.u_hi + src, bytes, &full_bar[s]);
-      if (two) bulk_load(st + p.b_slot, p.u_lo + src, bytes, &full_bar[s]);
+      bulk_load(st, M.u_hi + src, bytes, &full_bar[s]);
+      if (two) bulk_load(st + p.b_slot, M.u_lo + src, bytes, &full_bar[s]);
       issued |= 1u << s;
       par = (par & ~(1u << s)) | (ph << s);
     }
@@ -1125,16 +1156,20 @@ __device__ __forceinline__ void fused_issue_mma(const FusedParams* pp, uint32_t 
                                              volatile int* abort_flag) {
   const FusedParams& p = *pp;
   const bool two = p.nsplit == 2;
-  uint32_t it = 0, tile_it = 0;
+  uint32_t it = 0, cpar = 0;   // bit c: phase parity of chunk barrier c
   bool ok = true;
-  for (int64_t t = blockIdx.x; t < p.ntiles && ok; t += gridDim.x, ++tile_it) {
-    for (int ks = 0; ks < p.ksteps; ++ks, ++it) {
+  for (int64_t t = blockIdx.x; t < p.ntiles && ok; t += gridDim.x) {
+    int m;
+    const FusedMol& M = fused_mol(p, t, m);
+    for (int ks = 0; ks < M.ksteps; ++ks, ++it) {
       // columns 64c .. 64c+63 of A are complete once every item writing them arrived
-      if ((ks & 3) == 0 && p.chunk_need[ks >> 2] > 0) {
-        if (!mbar_wait(&chunk_bar[ks >> 2], tile_it & 1u, abort_flag, p.wait_ns)) {
+      const int c = ks >> 2;
+      if ((ks & 3) == 0 && M.chunk_need[c] > 0) {
+        if (!mbar_wait(&chunk_bar[c], (cpar >> c) & 1u, abort_flag, p.wait_ns)) {
           ok = false;
           break;
         }
+        cpar ^= 1u << c;
         tc_fence_after();
       }
       const int s = it % p.stages;
@@ -1149,8 +1184,8 @@ __device__ __forceinline__ void fused_issue_mma(const FusedParams* pp, uint32_t 
       const uint32_t aoff = (uint32_t)((j0 >> 6) * 16384 + ((j0 & 63) >> 4) * 32);
       const uint64_t ahi = sw128_kmajor_desc(abase + aoff), alo = sw128_kmajor_desc(lbase + aoff);
       const uint32_t bst = smem_u32(stages + (size_t)s * p.stage_bytes);
-      for (int c0 = 0; c0 < p.n16; c0 += 256) {
-        const int n = min(256, p.n16 - c0);
+      for (int c0 = 0; c0 < M.n16; c0 += 256) {
+        const int n = min(256, M.n16 - c0);
         const uint32_t idesc = make_idesc(p.fmt, 128, (uint32_t)n);
         const uint32_t boff = (uint32_t)c0 * 32u;
         const uint32_t d = tmem + (uint32_t)c0;
@@ -1187,7 +1222,6 @@ __global__ void __launch_bounds__(FUSED_THREADS, 1)
   uint8_t* stages = smem + p.nsplit * p.a_bytes;
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
   const bool two = p.nsplit == 2;
-  const MolView& mol = p.mol;
 
   if (threadIdx.x == 0) {
     abort_flag = 0;
@@ -1195,21 +1229,18 @@ __global__ void __launch_bounds__(FUSED_THREADS, 1)
       mbar_init(&full_bar[s], 1);
       mbar_init(&empty_bar[s], 1);
     }
-    for (int c = 0; c < p.nchunks; ++c)
-      if (p.chunk_need[c] > 0) mbar_init(&chunk_bar[c], (uint32_t)p.chunk_need[c]);
+    for (int c = 0; c < MAX_FUSED_CHUNKS; ++c) mbar_init(&chunk_bar[c], CHUNK_COUNT);
     mbar_init(&t_full, 1);
     mbar_init(&drain_bar, 1);
     fence_mbar_init();
   }
-  // zero A once: padding columns and rows never written later stay zero
+  // zero A once: padding rows are rewritten with zeros by every tile, padding columns when a
+  // CTA moves to another molecule
   for (uint32_t i = threadIdx.x; i < p.nsplit * p.a_bytes / 16; i += blockDim.x)
     reinterpret_cast<uint4*>(smem)[i] = make_uint4(0, 0, 0, 0);
-  // molecule tables in shared memory: the production loop reads them in dependent chains
+  // molecule tables in shared memory (loaded per molecule): the production loop reads them in
+  // dependent chains
   uint8_t* tabs = stages + (size_t)p.stages * p.stage_bytes;
-  // shell records, primitive pairs and per-atom words (first shell | layout << 24)
-  for (int i = threadIdx.x; i < p.tab_words; i += blockDim.x) reinterpret_cast<int4*>(tabs)[i] = __ldg(p.tab + i);
-  for (int i = threadIdx.x; i < 3 * mol.natoms; i += blockDim.x)
-    reinterpret_cast<float*>(tabs + p.off_coords)[i] = __ldg(mol.coords + i);
   asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
   if (warp == 1) {
     tmem_alloc(&tmem_slot, 512);
@@ -1229,25 +1260,52 @@ __global__ void __launch_bounds__(FUSED_THREADS, 1)
   } else {
     const int ct = threadIdx.x - 64;           // compute thread 0 .. FUSED_NCT-1
     const int4* sh_s = reinterpret_cast<const int4*>(tabs);
-    const float2* pr_s = reinterpret_cast<const float2*>(tabs + p.off_prim);
-    const int* ash_s = reinterpret_cast<const int*>(tabs + p.off_ashell);
-    const float* crd_s = reinterpret_cast<const float*>(tabs + p.off_coords);
     const int cw = ct >> 5;                    // compute warp 0 .. FUSED_NCW-1
     const int q = warp & 3;                    // TMEM lane quadrant of this warp
     const int hh = cw >> 2;                    // epilogue column-chunk class 0 .. FUSED_NCW/4-1
     const int row = q * 32 + lane;
     uint32_t tile_it = 0;
+    int cur_m = -1;
+    const float2* pr_s = nullptr;
+    const int* ash_s = nullptr;
+    const float* crd_s = nullptr;
     for (int64_t t = blockIdx.x; t < p.ntiles; t += gridDim.x, ++tile_it) {
+      int m;
+      const FusedMol& M = fused_mol(p, t, m);
+      const int64_t lt = t - M.tile0;          // tile within the molecule
+      if (m != cur_m) {
+        // another molecule: its tables into shared memory and its padding columns of A cleared
+        // (the previous tile's epilogue, the last reader of both, ended with a named barrier)
+        for (int i = ct; i < M.tab_words; i += FUSED_NCT) reinterpret_cast<int4*>(tabs)[i] = __ldg(M.tab + i);
+        for (int i = ct; i < 3 * M.natoms; i += FUSED_NCT)
+          reinterpret_cast<float*>(tabs + M.off_coords)[i] = __ldg(M.coords + i);
+        const int npadc = M.n16 - M.norbs;
+        for (int i = ct; i < 128 * npadc; i += FUSED_NCT) {
+          const uint32_t off = a_offset(i / npadc, M.norbs + i % npadc);
+          *reinterpret_cast<uint16_t*>(A_hi + off) = 0;
+          if (two) *reinterpret_cast<uint16_t*>(A_lo + off) = 0;
+        }
+        asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+        pr_s = reinterpret_cast<const float2*>(tabs + M.off_prim);
+        ash_s = reinterpret_cast<const int*>(tabs + M.off_ashell);
+        crd_s = reinterpret_cast<const float*>(tabs + M.off_coords);
+        cur_m = m;
+      }
       // ---- Phi' for the tile into A -------------------------------------------------------
       if (ct < 128) {
         double x, y, z;
         int64_t vox;
-        if (!tile_point<double>(p.pm, t, ct, x, y, z, vox)) x = y = z = 1e30;
+        if (!tile_point<double>(M.pm, lt, ct, x, y, z, vox)) x = y = z = 1e30;
         pos[ct][0] = x;
         pos[ct][1] = y;
         pos[ct][2] = z;
       }
-      if (ct == 0) item_ctr = 0;
+      if (ct == 0) {
+        item_ctr = 0;
+        // the arrivals that this molecule's production does not make
+        for (int c = 0; c < M.nchunks; ++c)
+          if (M.chunk_need[c] > 0) mbar_arrive_count(&chunk_bar[c], CHUNK_COUNT - (uint32_t)M.chunk_need[c]);
+      }
       named_barrier(1, FUSED_NCT);
       // work item = (atom, half of the rows), taken in atom order from a shared counter so that
       // column chunks complete roughly in order and the warps stay balanced; two rows per thread
@@ -1256,7 +1314,7 @@ __global__ void __launch_bounds__(FUSED_THREADS, 1)
         int itm = 0;
         if (lane == 0) itm = atomicAdd(&item_ctr, 1);
         itm = __shfl_sync(0xffffffffu, itm, 0);
-        if (itm >= 2 * mol.natoms) break;
+        if (itm >= 2 * M.natoms) break;
         const int a = itm >> 1;
         const int s0 = ash_s[a] & 0xffffff;
         if ((ash_s[a + 1] & 0xffffff) <= s0) continue;
@@ -1279,7 +1337,7 @@ __global__ void __launch_bounds__(FUSED_THREADS, 1)
       tc_fence_after();
       double acc[2] = {0.0, 0.0};
       const uint32_t trow = tmem + ((uint32_t)(q * 32) << 16);
-      for (int c = hh; c * 16 < p.n16; c += FUSED_NCW / 4) {
+      for (int c = hh; c * 16 < M.n16; c += FUSED_NCW / 4) {
         const int col = c * 16;
         // the TMEM load of T' is in flight while the row's Phi' units are read from shared memory
         uint32_t tv[16];
@@ -1315,17 +1373,17 @@ __global__ void __launch_bounds__(FUSED_THREADS, 1)
       rho_part[hh][row] = acc[0] + acc[1];
       named_barrier(1, FUSED_NCT);
       double mysum = 0.0;
-      if (ct < p.pm.vpt) {
+      if (ct < M.pm.vpt) {
         double r = 0.0;
-        for (int sub = 0; sub < p.pm.s3; ++sub) {
-          const int rr = ct * p.pm.s3 + sub;
+        for (int sub = 0; sub < M.pm.s3; ++sub) {
+          const int rr = ct * M.pm.s3 + sub;
 #pragma unroll
           for (int h3 = 0; h3 < FUSED_NCW / 4; ++h3) r += rho_part[h3][rr];
         }
         int64_t vox, ix, iy, iz;
-        if (tile_voxel(p.pm, t, ct, vox, ix, iy, iz)) {
-          const float qv = (float)(r * p.gsc[2] * p.outscale);
-          p.qube[vox] = qv;
+        if (tile_voxel(M.pm, lt, ct, vox, ix, iy, iz)) {
+          const float qv = (float)(r * M.gsc[2] * M.outscale);
+          M.qube[vox] = qv;
           mysum = qv;
         }
       }
@@ -1335,7 +1393,7 @@ __global__ void __launch_bounds__(FUSED_THREADS, 1)
       if (ct == 0) {
         double tot = 0;
         for (int w = 0; w < FUSED_NCW; ++w) tot += red[w];
-        p.partials[t] = tot;
+        M.partials[lt] = tot;
       }
       named_barrier(1, FUSED_NCT);
     }
@@ -1439,10 +1497,9 @@ static qmt_status ensure_mol_tables(qmt_mol* m, const std::vector<float>& fs, in
   return QMT_OK;
 }
 
-// Upper-triangular scaled density matrix for the fused path: row n (output column) holds
-// U_jn for j <= n, i.e. Ptilde_jn for j < n and Ptilde_nn / 2 on the diagonal.  Both variants are
-// stored as K-step blocks of kpad + 64 rows x 16 columns in the 32-byte swizzled image of a stage
-// (split_P_kernel), read by one contiguous copy per stage and piece.
+// Scaled density matrix of the fused path, stored as K-step blocks of kpad + 64 rows x 16 columns
+// in the 32-byte swizzled image of a stage (split_P_kernel), read by one contiguous copy per
+// stage and piece.
 
 static qmt_status ensure_fused_operands(qmt_mol* m, int prec, const TcShape& sh, cudaStream_t s) {
   const int key = prec;
@@ -1485,58 +1542,81 @@ static int fused_stages(const TcShape& sh, int n16, int tab_bytes) {
   return (int)std::max<long>(0, std::min<long>(MAX_STAGES, avail / stage_bytes));
 }
 
-template <int FMT>
-static qmt_status run_fused(qmt_mol* m, const TcShape& sh, const PointMap& pm, int64_t ntiles, float* qube,
-                            double outscale, cudaStream_t s) {
+// The descriptor of one molecule in a fused launch, its tiles starting at global tile `tile0`.
+static qmt_status fused_mol_desc(qmt_mol* m, const TcShape& sh, const PointMap& pm, int64_t tile0, int64_t ntiles,
+                                 float* qube, double outscale, FusedMol& d, int& tab_bytes) {
   const int K = sh.kpad, n16 = fused_n16(m);
   const size_t piece = (size_t)(K + 64) * K * 2;
   const uint8_t* B = m->d_fused_B.as<uint8_t>();
-  FusedParams p{};
-  p.mol = m->view();
-  p.pm = pm;
-  p.ntiles = ntiles;
-  p.kpad = K;
-  p.n16 = n16;
-  p.u_rows = K + 64;
-  p.u_hi = B;
-  p.u_lo = B + piece;
-  p.ksteps = n16 / 16;
-  p.nchunks = (n16 + 63) / 64;
-  if (p.nchunks > MAX_FUSED_CHUNKS) return fail(QMT_BAD_ARG, "fused density path supports kpad <= 320");
+  d = FusedMol{};
+  d.pm = pm;
+  d.tile0 = tile0;
+  d.ntiles = ntiles;
+  d.natoms = m->natoms;
+  d.norbs = m->norbs;
+  d.n16 = n16;
+  d.ksteps = n16 / 16;
+  d.nchunks = (n16 + 63) / 64;
+  d.u_rows = K + 64;
+  d.u_hi = B;
+  d.u_lo = B + piece;
+  if (d.nchunks > MAX_FUSED_CHUNKS) return fail(QMT_BAD_ARG, "fused density path supports kpad <= 320");
+  if (2 * m->natoms >= (int)CHUNK_COUNT) return fail(QMT_BAD_ARG, "too many atoms for the fused density path");
   for (int a = 0; a < m->natoms; ++a) {
     const int sa = m->atom_shell[a], sb = m->atom_shell[a + 1];
     if (sb <= sa) continue;
     const Shell& last = m->shells[sb - 1];
     const int cfirst = m->shells[sa].func >> 6, clast = (last.func + 2 * last.L) >> 6;
-    for (int c = cfirst; c <= clast; ++c) p.chunk_need[c] += 2;   // two row halves per atom
+    for (int c = cfirst; c <= clast; ++c) d.chunk_need[c] += 2;   // two row halves per atom
   }
-  p.nsplit = sh.nsplit;
-  p.a_bytes = fused_a_bytes(K);
-  p.b_slot = fused_b_slot(n16);
+  d.tab = m->d_fused_tab.as<int4>();
+  d.off_prim = (int)m->shells.size() * 16;
+  d.off_ashell = (int)(m->shells.size() + (m->alpha.size() + 1) / 2) * 16;
+  d.tab_words = d.off_ashell / 16 + (m->natoms + 1 + 3) / 4;
+  d.off_coords = d.tab_words * 16;
+  d.coords = m->d_coords.as<float>();
+  tab_bytes = d.off_coords + (3 * m->natoms + 3) / 4 * 16;
+  d.qube = qube;
+  d.partials = m->d_partials.as<double>();
+  d.outscale = outscale;
+  d.gsc = m->d_gscale.as<double>();
+  return QMT_OK;
+}
+
+// One persistent launch over every tile of the molecules in `p` (p.one, or the device array
+// p.mols); shared memory is sized for the largest operand, stage and table of the set.
+template <int FMT>
+static qmt_status launch_fused(FusedParams& p, const TcShape& sh_max, int n16_max, int tab_bytes_max, cudaStream_t s) {
+  p.nsplit = sh_max.nsplit;
+  p.a_bytes = fused_a_bytes(sh_max.kpad);
+  p.b_slot = fused_b_slot(n16_max);
   p.stage_bytes = p.nsplit * p.b_slot;
-  p.fmt = (uint32_t)sh.fmt;
-  p.tab = m->d_fused_tab.as<int4>();
-  p.off_prim = (int)m->shells.size() * 16;
-  p.off_ashell = (int)(m->shells.size() + (m->alpha.size() + 1) / 2) * 16;
-  p.tab_words = p.off_ashell / 16 + (m->natoms + 1 + 3) / 4;
-  p.off_coords = p.tab_words * 16;
-  p.tab_bytes = p.off_coords + (3 * m->natoms + 3) / 4 * 16;
-  p.qube = qube;
-  p.partials = m->d_partials.as<double>();
-  p.outscale = outscale;
-  p.gsc = m->d_gscale.as<double>();
+  p.fmt = (uint32_t)sh_max.fmt;
   p.wait_ns = wait_limit_ns();
-  p.err = reinterpret_cast<int*>(m->d_scalars.as<double>() + 8);
   auto kern = density_fused_kernel<FMT>;
-  const int stages = fused_stages<FMT>(sh, n16, p.tab_bytes);
+  const int stages = fused_stages<FMT>(sh_max, n16_max, tab_bytes_max);
   if (stages < 2) return fail(QMT_BAD_ARG, "fused density tile does not fit in shared memory");
   p.stages = stages;
-  const size_t dyn = (size_t)p.nsplit * p.a_bytes + (size_t)stages * p.stage_bytes + p.tab_bytes + 1024;
+  const size_t dyn = (size_t)p.nsplit * p.a_bytes + (size_t)stages * p.stage_bytes + tab_bytes_max + 1024;
   QMT_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)dyn));
-  const int grid = (int)std::min<int64_t>(ntiles, sm_count());
+  const int grid = (int)std::min<int64_t>(p.ntiles, sm_count());
+  if (grid <= 0) return QMT_OK;
   kern<<<grid, FUSED_THREADS, dyn, s>>>(p);
   QMT_CHECK_LAUNCH("density_fused_kernel");
   return QMT_OK;
+}
+
+template <int FMT>
+static qmt_status run_fused(qmt_mol* m, const TcShape& sh, const PointMap& pm, int64_t ntiles, float* qube,
+                            double outscale, cudaStream_t s) {
+  FusedParams p{};
+  int tab_bytes = 0;
+  qmt_status st = fused_mol_desc(m, sh, pm, 0, ntiles, qube, outscale, p.one, tab_bytes);
+  if (st) return st;
+  p.nmol = 1;
+  p.ntiles = ntiles;
+  p.err = reinterpret_cast<int*>(m->d_scalars.as<double>() + 8);
+  return launch_fused<FMT>(p, sh, p.one.n16, tab_bytes, s);
 }
 
 // Builds the scaled, split density matrix and the Phi column scales for `prec`.
@@ -1552,24 +1632,31 @@ static qmt_status ensure_tc_operands(qmt_mol* m, int prec, const TcShape& sh, cu
   return QMT_OK;
 }
 
+// Staged path.  Basis values go through `phi_hi` / `phi_lo` (the molecule's own buffers, or a
+// batch's shared ones) in chunks of tiles of at most `stage_bytes` in all.
 template <int FMT>
 static qmt_status run_tc(qmt_mol* m, const TcShape& sh, const PointMap& pm, int64_t ntiles, int prec,
-                         float* qube, double outscale, cudaStream_t s) {
+                         float* qube, double outscale, cudaStream_t s, DevBuf* phi_hi = nullptr,
+                         DevBuf* phi_lo = nullptr, size_t stage_bytes = (size_t)2 << 30) {
   qmt_status st;
+  if (!phi_hi) {
+    phi_hi = &m->d_Phi_hi;
+    phi_lo = &m->d_Phi_lo;
+  }
   const size_t tile_bytes = (size_t)128 * sh.kpad * sh.esize;
   const int nsm = sm_count();
-  // staging chunk: bounded to ~2 GiB, a multiple of the SM count when larger than one wave
-  int64_t chunk = std::max<int64_t>(1, ((size_t)2 << 30) / (tile_bytes * sh.nsplit));
+  // staging chunk: bounded by stage_bytes, a multiple of the SM count when larger than one wave
+  int64_t chunk = std::max<int64_t>(1, stage_bytes / (tile_bytes * sh.nsplit));
   if (chunk > nsm) chunk = chunk / nsm * nsm;
   chunk = std::min<int64_t>(chunk, ntiles);
-  if ((st = m->d_Phi_hi.reserve(chunk * tile_bytes))) return st;
-  if (sh.nsplit == 2 && (st = m->d_Phi_lo.reserve(chunk * tile_bytes))) return st;
-  void* lo_ptr = sh.nsplit == 2 ? m->d_Phi_lo.ptr : m->d_Phi_hi.ptr;
+  if ((st = phi_hi->reserve(chunk * tile_bytes))) return st;
+  if (sh.nsplit == 2 && (st = phi_lo->reserve(chunk * tile_bytes))) return st;
+  void* lo_ptr = sh.nsplit == 2 ? phi_lo->ptr : phi_hi->ptr;
 
   CUtensorMap tA_hi, tA_lo, tB_hi, tB_lo;
   const uint8_t* Pb = m->d_tc_P.as<uint8_t>();
   const size_t piece = (size_t)sh.nrows_b * sh.kpad * sh.esize;
-  if ((st = make_map(&tA_hi, m->d_Phi_hi.ptr, sh.esize, sh.kpad, (uint64_t)chunk * 128, sh.ke, 128)) ||
+  if ((st = make_map(&tA_hi, phi_hi->ptr, sh.esize, sh.kpad, (uint64_t)chunk * 128, sh.ke, 128)) ||
       (st = make_map(&tA_lo, lo_ptr, sh.esize, sh.kpad, (uint64_t)chunk * 128, sh.ke, 128)) ||
       (st = make_map(&tB_hi, Pb, sh.esize, sh.kpad, sh.nrows_b, sh.ke, sh.pw)) ||
       (st = make_map(&tB_lo, Pb + piece, sh.esize, sh.kpad, sh.nrows_b, sh.ke, sh.pw)))
@@ -1588,7 +1675,7 @@ static qmt_status run_tc(qmt_mol* m, const TcShape& sh, const PointMap& pm, int6
   p.stage_bytes = sh.nsplit * (p.a_bytes + p.b_bytes);
   p.tx_bytes = p.stage_bytes;
   p.idesc = make_idesc((uint32_t)sh.fmt, 128, (uint32_t)sh.pw);
-  p.phi_hi = m->d_Phi_hi.ptr;
+  p.phi_hi = phi_hi->ptr;
   p.phi_lo = lo_ptr;
   p.qube = qube;
   p.partials = m->d_partials.as<double>();
@@ -1625,7 +1712,7 @@ static qmt_status run_tc(qmt_mol* m, const TcShape& sh, const PointMap& pm, int6
   sp.off_ashell = lay.off_ashell;
   sp.off_coords = lay.words * 16;
   sp.tab_bytes = sp.off_coords + (3 * m->natoms + 3) / 4 * 16;
-  sp.out_hi = m->d_Phi_hi.ptr;
+  sp.out_hi = phi_hi->ptr;
   sp.out_lo = lo_ptr;
   sp.two = sh.nsplit == 2;
   const int buf_bytes = 128 * STAGE_LD * 4;
@@ -1656,6 +1743,15 @@ static qmt_status run_tc(qmt_mol* m, const TcShape& sh, const PointMap& pm, int6
 
 static int g_density_path = 0;   // 0 auto, 1 staged, 2 fused
 
+// The fused path takes fp16/bf16 contractions of up to 320 functions whose tile, stages and tables
+// fit in shared memory.
+static bool fused_fits(const qmt_mol* mol, const TcShape& sh) {
+  if (sh.fmt == FMT_TF32 || sh.kpad > 320 || 2 * mol->natoms >= (int)CHUNK_COUNT) return false;
+  const int tb = fused_tab_bytes(mol);
+  const int n16 = fused_n16(mol);
+  return (sh.fmt == FMT_F16 ? fused_stages<FMT_F16>(sh, n16, tb) : fused_stages<FMT_BF16>(sh, n16, tb)) >= 2;
+}
+
 qmt_status density_tc(qmt_mol* mol, int nx, int ny, int nz, float step, float ox, float oy, float oz,
                       int subgrid, int precision, int rescale, float* qube, double* sum_out,
                       cudaStream_t s) {
@@ -1666,12 +1762,7 @@ qmt_status density_tc(qmt_mol* mol, int nx, int ny, int nz, float step, float ox
   if ((st = make_point_map(nx, ny, nz, step, ox, oy, oz, subgrid, 128, pm, ntiles))) return st;
   if ((st = mol->d_partials.reserve(ntiles * sizeof(double)))) return st;
   const double outscale = 2.0 * (double)step * step * step / pm.s3;
-  bool fusable = sh.fmt != FMT_TF32 && sh.kpad <= 320;
-  if (fusable) {
-    const int tb = fused_tab_bytes(mol);
-    const int n16 = fused_n16(mol);
-    fusable = (sh.fmt == FMT_F16 ? fused_stages<FMT_F16>(sh, n16, tb) : fused_stages<FMT_BF16>(sh, n16, tb)) >= 2;
-  }
+  const bool fusable = fused_fits(mol, sh);
   const bool fused = g_density_path == 2 ? fusable : (g_density_path == 1 ? false : fusable);
   if (g_density_path == 2 && !fusable)
     return fail(QMT_BAD_ARG, "fused density path needs fp16/bf16, N <= 320 and molecule tables that fit in shared memory");
@@ -1703,7 +1794,221 @@ qmt_status density_tc(qmt_mol* mol, int nx, int ny, int nz, float step, float ox
   return QMT_OK;
 }
 
+// ---- batches ---------------------------------------------------------------------------------
+// Staged-path molecules of a batch run one after another on one stream and share one basis-value
+// buffer of this size (both pieces), instead of each holding its own.
+constexpr size_t BATCH_STAGE_BYTES = (size_t)1 << 30;
+
+struct BatchItem {
+  qmt_mol* mol;
+  TcShape sh;
+  PointMap pm;
+  int64_t ntiles;
+  float* qube;
+  double outscale;
+  bool fused;
+};
+
 }  // namespace qmt
+
+struct qmt_batch {
+  int precision = 0, fmt = 0;
+  std::vector<qmt::BatchItem> items;
+  std::vector<qmt::FusedMol> fdesc;   // fused molecules, tiles numbered across them
+  qmt::TcShape sh_max{};
+  int n16_max = 0, tab_bytes_max = 0;
+  int64_t fused_tiles = 0;
+  qmt::DevBuf d_fdesc, d_err;
+  qmt::DevBuf phi_hi, phi_lo;         // staged-path basis values, shared by the batch's molecules
+};
+
+namespace qmt {
+
+// Re-derives (refresh) or checks the molecule's contraction operands for its path.
+static qmt_status batch_operands(const BatchItem& it, int prec, bool refresh, cudaStream_t s) {
+  if (refresh) {
+    it.mol->fused_prec = -1;
+    it.mol->tc_prec = -1;
+  }
+  return it.fused ? ensure_fused_operands(it.mol, prec, it.sh, s) : ensure_tc_operands(it.mol, prec, it.sh, s);
+}
+
+template <int FMT>
+static qmt_status batch_run(qmt_batch* b, int rescale, bool refresh, cudaStream_t s) {
+  qmt_status st;
+  for (const BatchItem& it : b->items)
+    if ((st = batch_operands(it, b->precision, refresh, s))) return st;
+  if (!b->fdesc.empty() && FMT != FMT_TF32) {
+    FusedParams p{};
+    p.nmol = (int)b->fdesc.size();
+    if (p.nmol == 1) p.one = b->fdesc[0];
+    p.mols = b->d_fdesc.as<FusedMol>();
+    p.ntiles = b->fused_tiles;
+    p.err = b->d_err.as<int>();
+    if ((st = launch_fused<FMT == FMT_TF32 ? FMT_F16 : FMT>(p, b->sh_max, b->n16_max, b->tab_bytes_max, s))) return st;
+  }
+  for (const BatchItem& it : b->items)
+    if (!it.fused && (st = run_tc<FMT>(it.mol, it.sh, it.pm, it.ntiles, b->precision, it.qube, it.outscale, s,
+                                       &b->phi_hi, &b->phi_lo, BATCH_STAGE_BYTES)))
+      return st;
+  for (const BatchItem& it : b->items)
+    if ((st = finish_density(it.mol, it.pm.nvox, it.ntiles, rescale, it.qube, nullptr, s))) return st;
+  return QMT_OK;
+}
+
+}  // namespace qmt
+
+using namespace qmt;
+
+extern "C" {
+
+qmt_status qmt_batch_create(int nmol, qmt_mol* const* mols, const int32_t* shapes, const float* geoms,
+                            int subgrid, int precision, const int32_t* paths, float* const* qube_devs,
+                            void* stream, qmt_batch** out) {
+  if (!out || nmol <= 0 || !mols || !shapes || !geoms || !qube_devs)
+    return fail(QMT_BAD_ARG, "bad batch arguments");
+  *out = nullptr;
+  if (precision < QMT_PREC_TF32 || precision > QMT_PREC_FP16X3)
+    return fail(QMT_BAD_ARG, "batches take the tensor-core precisions");
+  cudaStream_t s = as_stream(stream);
+  auto* b = new qmt_batch();
+  b->precision = precision;
+  qmt_status st = QMT_OK;
+  for (int i = 0; i < nmol && !st; ++i) {
+    qmt_mol* m = mols[i];
+    if (!m || !qube_devs[i]) {
+      st = fail(QMT_BAD_ARG, "null molecule or grid in a batch");
+      break;
+    }
+    BatchItem it{};
+    it.mol = m;
+    it.qube = qube_devs[i];
+    it.sh = tc_shape(precision, m->norbs);
+    const float step = geoms[4 * i];
+    if ((st = make_point_map(shapes[3 * i], shapes[3 * i + 1], shapes[3 * i + 2], step, geoms[4 * i + 1],
+                             geoms[4 * i + 2], geoms[4 * i + 3], subgrid, 128, it.pm, it.ntiles)))
+      break;
+    it.outscale = 2.0 * (double)step * step * step / it.pm.s3;
+    const int path = paths ? paths[i] : 0;
+    if (path < 0 || path > 2) {
+      st = fail(QMT_BAD_ARG, "batch path must be 0 (automatic), 1 (staged) or 2 (fused)");
+      break;
+    }
+    const bool fits = fused_fits(m, it.sh);
+    if (path == 2 && !fits) {
+      st = fail(QMT_BAD_ARG, "fused density path requested for a molecule it does not take");
+      break;
+    }
+    it.fused = path == 2 || (path == 0 && fits);
+    if ((st = m->d_partials.reserve(it.ntiles * sizeof(double))) || (st = m->d_scalars.reserve(64 * sizeof(double))))
+      break;
+    if ((st = batch_operands(it, precision, false, s))) break;
+    b->items.push_back(it);
+  }
+  b->fmt = tc_shape(precision, 1).fmt;
+  // fused molecules: one launch sized for the largest of them; drop the largest to the staged path
+  // until the shared-memory plan of the set fits
+  for (;;) {
+    if (st) break;
+    b->fdesc.clear();
+    b->sh_max = TcShape{};
+    b->n16_max = b->tab_bytes_max = 0;
+    b->fused_tiles = 0;
+    int largest = -1;
+    for (size_t i = 0; i < b->items.size(); ++i) {
+      BatchItem& it = b->items[i];
+      if (!it.fused) continue;
+      FusedMol d;
+      int tb = 0;
+      if ((st = fused_mol_desc(it.mol, it.sh, it.pm, b->fused_tiles, it.ntiles, it.qube, it.outscale, d, tb))) break;
+      b->fused_tiles += it.ntiles;
+      b->fdesc.push_back(d);
+      if (it.sh.kpad > b->sh_max.kpad) b->sh_max = it.sh;
+      b->n16_max = std::max(b->n16_max, d.n16);
+      b->tab_bytes_max = std::max(b->tab_bytes_max, tb);
+      if (largest < 0 || it.sh.kpad + tb / 1024 > b->items[largest].sh.kpad + fused_tab_bytes(b->items[largest].mol) / 1024)
+        largest = (int)i;
+    }
+    if (st || b->fdesc.empty()) break;
+    const int stg = b->fmt == FMT_F16 ? fused_stages<FMT_F16>(b->sh_max, b->n16_max, b->tab_bytes_max)
+                                      : fused_stages<FMT_BF16>(b->sh_max, b->n16_max, b->tab_bytes_max);
+    if (stg >= 2) break;
+    b->items[largest].fused = false;
+    if ((st = batch_operands(b->items[largest], precision, false, s))) break;
+  }
+  if (!st && !b->fdesc.empty()) {
+    const size_t bytes = b->fdesc.size() * sizeof(FusedMol);
+    st = b->d_fdesc.reserve(bytes);
+    if (!st) st = b->d_err.reserve(256);
+    if (!st) {
+      const cudaError_t e1 = cudaMemcpyAsync(b->d_fdesc.ptr, b->fdesc.data(), bytes, cudaMemcpyHostToDevice, s);
+      const cudaError_t e2 = cudaMemsetAsync(b->d_err.ptr, 0, 256, s);
+      const cudaError_t e3 = cudaStreamSynchronize(s);
+      if (e1 != cudaSuccess || e2 != cudaSuccess || e3 != cudaSuccess)
+        st = cuda_fail(e1 != cudaSuccess ? e1 : (e2 != cudaSuccess ? e2 : e3), "batch descriptors");
+    }
+  }
+  if (st) {
+    delete b;
+    return st;
+  }
+  *out = b;
+  return QMT_OK;
+}
+
+qmt_status qmt_batch_density(qmt_batch* b, int rescale, int refresh, void* stream) {
+  if (!b) return fail(QMT_BAD_ARG, "null batch");
+  cudaStream_t s = as_stream(stream);
+  if (b->fmt == FMT_TF32) return batch_run<FMT_TF32>(b, rescale, refresh != 0, s);
+  if (b->fmt == FMT_F16) return batch_run<FMT_F16>(b, rescale, refresh != 0, s);
+  return batch_run<FMT_BF16>(b, rescale, refresh != 0, s);
+}
+
+qmt_status qmt_batch_sums(qmt_batch* b, double* sums, void* stream) {
+  if (!b || !sums) return fail(QMT_BAD_ARG, "null argument");
+  cudaStream_t s = as_stream(stream);
+  std::vector<int> errs(b->items.size() + 1, 0);
+  for (size_t i = 0; i < b->items.size(); ++i) {
+    qmt_mol* m = b->items[i].mol;
+    QMT_CUDA(cudaMemcpyAsync(sums + i, m->d_scalars.as<double>(), sizeof(double), cudaMemcpyDeviceToHost, s));
+    QMT_CUDA(cudaMemcpyAsync(&errs[i], m->d_scalars.as<double>() + 8, sizeof(int), cudaMemcpyDeviceToHost, s));
+  }
+  if (b->d_err.ptr)
+    QMT_CUDA(cudaMemcpyAsync(&errs.back(), b->d_err.ptr, sizeof(int), cudaMemcpyDeviceToHost, s));
+  QMT_CUDA(cudaStreamSynchronize(s));
+  bool bad = false;
+  for (size_t i = 0; i < b->items.size(); ++i)
+    if (errs[i]) {
+      bad = true;
+      QMT_CUDA(cudaMemsetAsync(b->items[i].mol->d_scalars.as<double>() + 8, 0, sizeof(int), s));
+    }
+  if (errs.back()) {
+    bad = true;
+    QMT_CUDA(cudaMemsetAsync(b->d_err.ptr, 0, sizeof(int), s));
+  }
+  if (bad) return fail(QMT_CUDA_ERR, "tensor-core density kernel gave up waiting on a barrier");
+  for (size_t i = 0; i < b->items.size(); ++i)
+    if (!std::isfinite(sums[i])) return fail(QMT_NAN, "non-finite density sum");
+  return QMT_OK;
+}
+
+int qmt_batch_fused_count(const qmt_batch* b) {
+  if (!b) return -1;
+  return (int)b->fdesc.size();
+}
+
+qmt_status qmt_batch_destroy(qmt_batch* b) {
+  if (!b) return QMT_OK;
+  cudaDeviceSynchronize();
+  b->d_fdesc.release();
+  b->d_err.release();
+  b->phi_hi.release();
+  b->phi_lo.release();
+  delete b;
+  return QMT_OK;
+}
+
+}  // extern "C"
 
 extern "C" qmt_status qmt_set_density_path(int mode) {
   if (mode < 0 || mode > 2)

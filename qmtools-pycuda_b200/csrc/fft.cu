@@ -607,6 +607,8 @@ struct GreenEntry {
   uint64_t used;        // last use, for least-recently-used eviction
   size_t bytes;
   cudaEvent_t ready;    // recorded after the build, on the stream that built it
+  bool built;           // `ready` seen complete: later solves need no wait (and, inside a CUDA-graph
+                        // capture, make no event call)
 };
 
 // Device-side caches shared by all calls: twiddle tables per (length, device), transformed
@@ -734,9 +736,13 @@ static qmt_status green_hat(int Mx, int My, int Mz, float h_ang, const Plan1D& p
   std::lock_guard<std::mutex> lock(c.green_mu);
   auto it = c.green.find(key);
   if (it != c.green.end()) {
-    it->second.used = ++c.clock;
-    QMT_CUDA(cudaStreamWaitEvent(s, it->second.ready, 0));   // built on another stream, maybe
-    *out = it->second.buf->as<float>();
+    GreenEntry& e = it->second;
+    e.used = ++c.clock;
+    if (!e.built) {
+      if (cudaEventQuery(e.ready) == cudaSuccess) e.built = true;
+      else QMT_CUDA(cudaStreamWaitEvent(s, e.ready, 0));   // still being built on another stream, maybe
+    }
+    *out = e.buf->as<float>();
     return QMT_OK;
   }
   const int64_t M = (int64_t)Mx * My * Mz;
@@ -788,11 +794,15 @@ static qmt_status green_hat(int Mx, int My, int Mz, float h_ang, const Plan1D& p
     c.green_bytes -= lru->second.bytes;
     c.green.erase(lru);
   }
-  c.green[key] = GreenEntry{gb, ++c.clock, nbytes, ready};
+  c.green[key] = GreenEntry{gb, ++c.clock, nbytes, ready, false};
   c.green_bytes += nbytes;
   *out = gb->as<float>();
   return QMT_OK;
 }
+
+static qmt_status fft_poisson(qmt_mol* mol, int nx, int ny, int nz, float step, float ox, float oy, float oz,
+                              float sigma, float cutoff, int padded, int Mx, int My, int Mz, const float* q_dev,
+                              float* out_dev, cudaStream_t s);
 
 }  // namespace qmt
 
@@ -801,13 +811,31 @@ using namespace qmt;
 extern "C" qmt_status qmt_fft_poisson(qmt_mol* mol, int nx, int ny, int nz, float step, float ox, float oy,
                                       float oz, float sigma, float cutoff, int padded, const float* q_dev,
                                       float* out_dev, void* stream) {
-  if (!mol || !q_dev || !out_dev || nx < 2 || ny < 2 || nz < 2 || !(step > 0.f) || !(sigma > 0.f) || cutoff < 0)
-    return fail(QMT_BAD_ARG, "bad FFT Poisson arguments");
-  if (mol->natoms > 4096) return fail(QMT_BAD_ARG, "too many atoms");
-  cudaStream_t s = as_stream(stream);
+  if (nx < 2 || ny < 2 || nz < 2) return fail(QMT_BAD_ARG, "bad FFT Poisson arguments");
   const int Mx = padded ? nice_at_least(2 * nx) : nx;
   const int My = padded ? nice_at_least(2 * ny) : ny;
   const int Mz = padded ? nice_at_least(2 * nz) : nz;
+  return fft_poisson(mol, nx, ny, nz, step, ox, oy, oz, sigma, cutoff, padded ? 1 : 0, Mx, My, Mz, q_dev, out_dev,
+                     as_stream(stream));
+}
+
+extern "C" qmt_status qmt_fft_poisson_padded(qmt_mol* mol, int nx, int ny, int nz, float step, float ox, float oy,
+                                             float oz, float sigma, float cutoff, int mx, int my, int mz,
+                                             const float* q_dev, float* out_dev, void* stream) {
+  if (nx < 2 || ny < 2 || nz < 2 || mx < 2 * nx || my < 2 * ny || mz < 2 * nz)
+    return fail(QMT_BAD_ARG, "padded FFT lengths must be at least twice the grid");
+  return fft_poisson(mol, nx, ny, nz, step, ox, oy, oz, sigma, cutoff, 1, mx, my, mz, q_dev, out_dev,
+                     as_stream(stream));
+}
+
+namespace qmt {
+
+static qmt_status fft_poisson(qmt_mol* mol, int nx, int ny, int nz, float step, float ox, float oy, float oz,
+                              float sigma, float cutoff, int padded, int Mx, int My, int Mz, const float* q_dev,
+                              float* out_dev, cudaStream_t s) {
+  if (!mol || !q_dev || !out_dev || nx < 2 || ny < 2 || nz < 2 || !(step > 0.f) || !(sigma > 0.f) || cutoff < 0)
+    return fail(QMT_BAD_ARG, "bad FFT Poisson arguments");
+  if (mol->natoms > 4096) return fail(QMT_BAD_ARG, "too many atoms");
   Plan1D px, py, pz;
   qmt_status st;
   if ((st = plan_of(Mx, px)) || (st = plan_of(My, py)) || (st = plan_of(Mz, pz))) return st;
@@ -861,3 +889,5 @@ extern "C" qmt_status qmt_fft_poisson(qmt_mol* mol, int nx, int ny, int nz, floa
   a.lload = Mx; a.lstore = nx; a.inv = 1; a.scale = (float)(1.0 / (double)M);
   return launch_pass(PASS_X_OUT, a, s);
 }
+
+}  // namespace qmt

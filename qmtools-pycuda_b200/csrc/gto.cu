@@ -8,8 +8,18 @@
 // with D_tuv already contracted with the density matrix (host, FP64).  The potential at a
 // point C is then
 //     V(C) = -sum_pairs (2 pi / p) sum_tuv D_tuv R_tuv(p, P - C) + sum_A Z_A / |C - R_A|,
-// with R_tuv from Boys functions F_0..F_L (table + Taylor, downward recursion).  All device
-// arithmetic is FP64.
+// with R_tuv from Boys functions F_0..F_L (table + Taylor, downward recursion).
+//
+// Two kernels evaluate it.  gto32_kernel (the default) works in FP32 and accumulates in FP64:
+// where T = p |P - C|^2 >= 30 (99.5% of the point-pair terms on the boundary of the medium
+// molecule's grid) the Boys functions take their asymptotic form
+//     (-2p)^n F_n(T) = sqrt(pi) / (2 sqrt(p)) * (-1)^n (2n-1)!! / r^(2n+1)
+// (relative error below e^-T T^(L-1/2) < 2e-9 for L <= 4), so a term costs one reciprocal square
+// root and the Hermite recursion; nearer terms use an FP32 table with Taylor terms and downward
+// recursion.  Point and pair centres are held relative to the molecule's centroid, the density
+// matrix and prefactor are folded into the FP32 Hermite coefficients, pair terms are summed in
+// FP32 in groups of four and the groups in FP64, and the nuclear term is FP64.  gto_kernel keeps
+// every operation in FP64 (qmt_set_gto_precision selects it).
 #include <algorithm>
 #include <cstdio>
 #include <string>
@@ -262,6 +272,173 @@ __global__ void __launch_bounds__(GTO_THREADS) gto_kernel(const GPair* __restric
   out[o] = (float)V;
 }
 
+// ---- FP32 kernel with FP64 accumulation -----------------------------------------------------
+constexpr int BOYS32_NT = 301;   // T = 0, 0.1, ..., 30 (the far-field form takes over at 30)
+constexpr int BOYS32_NM = 10;    // m = 0..9: F_L and five Taylor terms for L <= 4
+constexpr float T_FAR = 30.0f;
+
+struct GPair32 {
+  float px, py, pz;   // centre relative to the molecule's centroid (bohr)
+  float p;            // exponent sum
+  float fscale;       // sqrt(pi) / (2 sqrt(p)): far-field factor
+  int L;
+  int doff;           // offset of the pref * D_tuv coefficients
+  int pad;
+};
+
+// R_tuv (t+u+v <= L) from h_j = (-2p)^j F_j, j = 0..L, dotted with D.
+template <int L>
+__device__ __forceinline__ float hermite_dot32(const float* __restrict__ D, float X, float Y, float Z,
+                                               const float (&h)[L + 1]) {
+  constexpr int NC = ncoef(L);
+  constexpr HermTable H = make_herm_table();
+  float cur[NC], nxt[NC];
+  cur[0] = h[L];
+#pragma unroll
+  for (int j = L - 1; j >= 0; --j) {
+    nxt[0] = h[j];
+    const int n = ncoef(L - j);
+#pragma unroll
+    for (int k = 1; k < NC; ++k) {
+      if (k < n) {
+        const HermIdx e = H.e[k];
+        const float c = e.dir == 0 ? X : (e.dir == 1 ? Y : Z);
+        float r = c * cur[e.p1];
+        if (e.mult > 0) r = fmaf((float)e.mult, cur[e.p2], r);
+        nxt[k] = r;
+      }
+    }
+#pragma unroll
+    for (int k = 0; k < NC; ++k) cur[k] = nxt[k];
+  }
+  float acc = 0.f;
+#pragma unroll
+  for (int k = 0; k < NC; ++k) acc = fmaf(D[k], cur[k], acc);
+  return acc;
+}
+
+template <int L>
+__device__ __forceinline__ float pair_term32(const GPair32& g, const float* __restrict__ D, float cx, float cy,
+                                             float cz, const float* __restrict__ tab) {
+  const float X = g.px - cx, Y = g.py - cy, Z = g.pz - cz;
+  const float r2 = fmaf(X, X, fmaf(Y, Y, Z * Z));
+  const float T = g.p * r2;
+  float h[L + 1];
+  if (!(T < T_FAR)) {   // (a non-finite T takes this branch too: the table below is never indexed by it)
+    // asymptotic Boys functions: h_j = (-1)^j (2j-1)!! r^-(2j+1), the factor sqrt(pi)/(2 sqrt p)
+    // applied to the sum; one Newton step makes the reciprocal square root correctly rounded
+    float ri = rsqrtf(r2);
+    ri = ri * fmaf(-0.5f * r2 * ri, ri, 1.5f);
+    const float ri2 = ri * ri;
+    h[0] = ri;
+#pragma unroll
+    for (int j = 0; j < L; ++j) h[j + 1] = -(float)(2 * j + 1) * h[j] * ri2;
+    return g.fscale * hermite_dot32<L>(D, X, Y, Z, h);
+  }
+  // F_L by a five-term Taylor expansion about the nearest tabulated T, then downward recursion
+  const int i = (int)fmaf(T, 10.0f, 0.5f);
+  const float d = T - 0.1f * (float)i;
+  const float* row = tab + i * BOYS32_NM + L;
+  float f = row[5];
+#pragma unroll
+  for (int k = 4; k >= 0; --k) f = fmaf(f, -d / (float)(k + 1), row[k]);
+  float F[L + 1];
+  F[L] = f;
+  const float et = expf(-T);
+#pragma unroll
+  for (int m = L - 1; m >= 0; --m) F[m] = fmaf(2.0f * T, F[m + 1], et) / (float)(2 * m + 1);
+  const float m2p = -2.0f * g.p;
+  float pw = 1.0f;
+#pragma unroll
+  for (int j = 0; j <= L; ++j) {
+    h[j] = pw * F[j];
+    pw *= m2p;
+  }
+  return hermite_dot32<L>(D, X, Y, Z, h);
+}
+
+constexpr int GTO32_THREADS = 128;
+constexpr int GTO32_CHUNK = 128;
+
+// The terms of `nc` pairs of one angular momentum L (all in shared memory) at the thread's point,
+// summed in FP32 in groups of four, the groups in FP64.  One L per loop (no dispatch per pair),
+// unrolled so that consecutive pairs' independent dependency chains overlap.
+template <int L>
+__device__ __forceinline__ void chunk_terms(const GPair32* sp, const float* sd, const int* soff, int nc, float x,
+                                            float y, float z, const float* __restrict__ tab, double& V) {
+  float acc = 0.f;
+#pragma unroll 4
+  for (int k = 0; k < nc; ++k) {
+    acc += pair_term32<L>(sp[k], sd + soff[k], x, y, z, tab);
+    if ((k & 3) == 3) {
+      V += (double)acc;
+      acc = 0.f;
+    }
+  }
+  V += (double)acc;
+}
+
+// Pairs are sorted by L; lstart[L] .. lstart[L + 1] are those of angular momentum L.
+struct PairRanges {
+  int lstart[6];
+};
+
+__global__ void __launch_bounds__(GTO32_THREADS) gto32_kernel(const GPair32* __restrict__ pairs, PairRanges pr,
+                                                              const float* __restrict__ dco,
+                                                              const float* __restrict__ tab, MolView mol,
+                                                              const float* __restrict__ nuc32, double rx, double ry,
+                                                              double rz, GtoPoints gp,
+                                                              float* __restrict__ out) {
+  __shared__ GPair32 sp[GTO32_CHUNK];
+  __shared__ float sd[GTO32_CHUNK * 35];
+  __shared__ int soff[GTO32_CHUNK];
+  const int64_t i = blockIdx.x * (int64_t)GTO32_THREADS + threadIdx.x;
+  double cx = 0, cy = 0, cz = 0;
+  int64_t o = -1;
+  const bool valid = i < gp.npts && gto_point(gp, i, cx, cy, cz, o);
+  // the point relative to the centroid, rounded once: every term (and the nuclear sum) sees the
+  // same point
+  const float x = (float)(cx - rx), y = (float)(cy - ry), z = (float)(cz - rz);
+  double V = 0.0;
+#pragma unroll 1
+  for (int L = 0; L <= 4; ++L) {
+    const int p0 = pr.lstart[L], p1 = pr.lstart[L + 1];
+    for (int c0 = p0; c0 < p1; c0 += GTO32_CHUNK) {
+      const int nc = min(GTO32_CHUNK, p1 - c0);
+      __syncthreads();   // the previous chunk's readers are done
+      const int dbase = pairs[c0].doff;
+      if (threadIdx.x < nc) {
+        const GPair32 g = pairs[c0 + threadIdx.x];
+        sp[threadIdx.x] = g;
+        soff[threadIdx.x] = g.doff - dbase;   // coefficients of a chunk are contiguous
+      }
+      const int dn = nc * ncoef(L);
+      for (int k = threadIdx.x; k < dn; k += GTO32_THREADS) sd[k] = dco[dbase + k];
+      __syncthreads();
+      if (valid) {
+        switch (L) {
+          case 0: chunk_terms<0>(sp, sd, soff, nc, x, y, z, tab, V); break;
+          case 1: chunk_terms<1>(sp, sd, soff, nc, x, y, z, tab, V); break;
+          case 2: chunk_terms<2>(sp, sd, soff, nc, x, y, z, tab, V); break;
+          case 3: chunk_terms<3>(sp, sd, soff, nc, x, y, z, tab, V); break;
+          default: chunk_terms<4>(sp, sd, soff, nc, x, y, z, tab, V); break;
+        }
+      }
+    }
+  }
+  if (!valid) return;
+  // nuclear term in FP64 from the same FP32 centroid-relative coordinates as the electrons: a
+  // nucleus and the pairs centred on it (the bulk of its electrons) carry the same rounding, so
+  // the near-cancellation of the two at a distance is not disturbed by a relative shift
+  for (int a = 0; a < mol.natoms; ++a) {
+    const double dx = (double)x - (double)nuc32[3 * a], dy = (double)y - (double)nuc32[3 * a + 1],
+                 dz = (double)z - (double)nuc32[3 * a + 2];
+    const double r = sqrt(dx * dx + dy * dy + dz * dz);
+    if (r > 1e-8) V += mol.types[a] / r;
+  }
+  out[o] = (float)V;
+}
+
 // ---- host: Boys table ------------------------------------------------------------------------
 static qmt_status boys_table(const double** out) {
   static thread_local DevBuf tab;  // one copy per host thread (per device in practice)
@@ -288,6 +465,34 @@ static qmt_status boys_table(const double** out) {
   *out = tab.as<double>();
   return QMT_OK;
 }
+
+static qmt_status boys_table32(const float** out) {
+  static thread_local DevBuf tab;
+  static thread_local bool ready = false;
+  if (!ready) {
+    std::vector<float> h((size_t)BOYS32_NT * BOYS32_NM);
+    for (int i = 0; i < BOYS32_NT; ++i) {
+      const double T = i * 0.1;
+      for (int m = 0; m < BOYS32_NM; ++m) {
+        double term = 1.0 / (2 * m + 1), acc = term;
+        for (int k = 1; k < 400; ++k) {
+          term *= 2 * T / (2 * m + 2 * k + 1);
+          acc += term;
+          if (term < 1e-18 * acc) break;
+        }
+        h[(size_t)i * BOYS32_NM + m] = (float)(std::exp(-T) * acc);
+      }
+    }
+    qmt_status st = tab.reserve(h.size() * sizeof(float));
+    if (st) return st;
+    QMT_CUDA(cudaMemcpy(tab.ptr, h.data(), h.size() * sizeof(float), cudaMemcpyHostToDevice));
+    ready = true;
+  }
+  *out = tab.as<float>();
+  return QMT_OK;
+}
+
+static int g_gto_prec = QMT_PREC_FP32;   // FP32 with FP64 accumulation, or FP64 throughout
 
 // ---- host: pair table --------------------------------------------------------------------------
 static void hermite_e_host(int la, int lb, double a, double b, double xa, double xb, double E[3][3][5]) {
@@ -400,9 +605,9 @@ static qmt_status build_pairs(qmt_mol* m, cudaStream_t s) {
           auto it = index.find(key);
           if (it == index.end()) {
             Acc g{};
-            g.px = (a * Ax + b * Bx) / p;
-            g.py = (a * Ay + b * By) / p;
-            g.pz = (a * Az + b * Bz) / p;
+            g.px = A.atom == B.atom ? Ax : (a * Ax + b * Bx) / p;   // on-site pairs sit on the nucleus
+            g.py = A.atom == B.atom ? Ay : (a * Ay + b * By) / p;
+            g.pz = A.atom == B.atom ? Az : (a * Az + b * Bz) / p;
             g.p = p;
             g.pref = pref;
             g.L = L;
@@ -448,19 +653,68 @@ static qmt_status build_pairs(qmt_mol* m, cudaStream_t s) {
   QMT_CUDA(cudaMemcpyAsync(m->d_pairs.ptr, pairs.data(), pb, cudaMemcpyHostToDevice, s));
   QMT_CUDA(cudaMemcpyAsync(m->d_pairs.as<uint8_t>() + ((pb + 255) / 256) * 256, dco.data(), db,
                            cudaMemcpyHostToDevice, s));
+  // FP32 copy: centres relative to the centroid, pref * D_tuv as the coefficients; then the
+  // nuclei, relative to the same point and rounded the same way
+  double ref[3] = {0, 0, 0};
+  for (int a = 0; a < m->natoms; ++a)
+    for (int d = 0; d < 3; ++d) ref[d] += m->coords[3 * a + d] / m->natoms;
+  std::vector<GPair32> p32(pairs.size());
+  std::vector<float> d32(dco.size());
+  for (size_t k = 0; k < pairs.size(); ++k) {
+    const GPair& g = pairs[k];
+    GPair32& q = p32[k];
+    q.px = (float)(g.px - ref[0]);
+    q.py = (float)(g.py - ref[1]);
+    q.pz = (float)(g.pz - ref[2]);
+    q.p = (float)g.p;
+    q.fscale = (float)(0.88622692545275801365 / std::sqrt(g.p));
+    q.L = g.L;
+    q.doff = g.doff;
+    q.pad = 0;
+    for (int c = 0; c < ncoef(g.L); ++c) d32[g.doff + c] = (float)(g.pref * dco[g.doff + c]);
+  }
+  for (int a = 0; a < m->natoms; ++a)
+    for (int d = 0; d < 3; ++d) d32.push_back((float)((double)m->coords[3 * a + d] - ref[d]));
+  const size_t pb32 = p32.size() * sizeof(GPair32), db32 = d32.size() * sizeof(float);
+  if ((st = m->d_pairs32.reserve(pb32 + db32 + 256))) return st;
+  QMT_CUDA(cudaMemcpyAsync(m->d_pairs32.ptr, p32.data(), pb32, cudaMemcpyHostToDevice, s));
+  QMT_CUDA(cudaMemcpyAsync(m->d_pairs32.as<uint8_t>() + ((pb32 + 255) / 256) * 256, d32.data(), db32,
+                           cudaMemcpyHostToDevice, s));
+  m->gto32_nuc_off = dco.size();
+  // pairs are sorted by L: the start of each L's range (an empty table counts as one L = 0 pair)
+  for (int L = 0; L <= 5; ++L) {
+    int k = 0;
+    while (k < (int)p32.size() && p32[k].L < L) ++k;
+    m->gto_lstart[L] = k;
+  }
   QMT_CUDA(cudaStreamSynchronize(s));
   m->gto_npairs = (int)pairs.size();
   m->gto_doff_bytes = ((pb + 255) / 256) * 256;
+  m->gto32_doff_bytes = ((pb32 + 255) / 256) * 256;
+  for (int d = 0; d < 3; ++d) m->gto_ref[d] = ref[d];
   m->gto_ready = true;
   return QMT_OK;
 }
 
 static qmt_status run_gto(qmt_mol* m, const GtoPoints& gp, float* out, cudaStream_t s) {
   qmt_status st;
-  const double* tab = nullptr;
-  if ((st = boys_table(&tab))) return st;
   if ((st = build_pairs(m, s))) return st;
   if (gp.npts <= 0) return QMT_OK;
+  if (g_gto_prec == QMT_PREC_FP32) {
+    const float* tab32 = nullptr;
+    if ((st = boys_table32(&tab32))) return st;
+    const GPair32* p32 = m->d_pairs32.as<GPair32>();
+    const float* d32 = reinterpret_cast<const float*>(m->d_pairs32.as<uint8_t>() + m->gto32_doff_bytes);
+    const int64_t blocks = (gp.npts + GTO32_THREADS - 1) / GTO32_THREADS;
+    PairRanges pr;
+    for (int L = 0; L <= 5; ++L) pr.lstart[L] = m->gto_lstart[L];
+    gto32_kernel<<<(unsigned)blocks, GTO32_THREADS, 0, s>>>(p32, pr, d32, tab32, m->view(), d32 + m->gto32_nuc_off,
+                                                            m->gto_ref[0], m->gto_ref[1], m->gto_ref[2], gp, out);
+    QMT_CHECK_LAUNCH("gto32_kernel");
+    return QMT_OK;
+  }
+  const double* tab = nullptr;
+  if ((st = boys_table(&tab))) return st;
   const GPair* pairs = m->d_pairs.as<GPair>();
   const double* dco = reinterpret_cast<const double*>(m->d_pairs.as<uint8_t>() + m->gto_doff_bytes);
   const int64_t blocks = (gp.npts + GTO_THREADS - 1) / GTO_THREADS;
@@ -486,6 +740,13 @@ qmt_status qmt_hartree_gto_points(qmt_mol* mol, int npts, const float* pts_dev, 
   if (!mol || npts < 0 || (npts > 0 && (!pts_dev || !v_dev))) return fail(QMT_BAD_ARG, "bad GTO arguments");
   GtoPoints gp{2, 0, 0, 0, 0, 0, 0, 0, pts_dev, npts};
   return run_gto(mol, gp, v_dev, as_stream(stream));
+}
+
+qmt_status qmt_set_gto_precision(int precision) {
+  if (precision != QMT_PREC_FP32 && precision != QMT_PREC_FP64)
+    return fail(QMT_BAD_ARG, "analytic potential precision must be QMT_PREC_FP32 or QMT_PREC_FP64");
+  g_gto_prec = precision;
+  return QMT_OK;
 }
 
 qmt_status qmt_hartree_gto_boundary(qmt_mol* mol, int nx, int ny, int nz, float step, float ox, float oy,

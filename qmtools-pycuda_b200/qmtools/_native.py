@@ -36,13 +36,20 @@ SIGNATURES = {
     "qmt_mol_trace_ps": [_vp, _pd, _vp],
     "qmt_density": [_vp, _i, _i, _i, _f, _f, _f, _f, _i, _i, _i, _vp, _pd, _vp],
     "qmt_set_density_path": [_i],
+    "qmt_batch_create": [_i, _vp, _vp, _vp, _i, _i, _vp, _vp, _vp, C.POINTER(_vp)],
+    "qmt_batch_density": [_vp, _i, _i, _vp],
+    "qmt_batch_sums": [_vp, _pd, _vp],
+    "qmt_batch_destroy": [_vp],
     "qmt_set_wait_limit_ns": [C.c_uint64],
     "qmt_hartree_gto": [_vp, _i, _i, _i, _f, _f, _f, _f, _vp, _vp],
     "qmt_hartree_gto_points": [_vp, _i, _vp, _vp, _vp],
     "qmt_hartree_gto_boundary": [_vp, _i, _i, _i, _f, _f, _f, _f, _vp, _vp],
+    "qmt_set_gto_precision": [_i],
     "qmt_jacobi": [_i, _i, _i, _f, _vp, _vp, _vp, _i, _i, _d, _pi, _pd, _vp],
     "qmt_jacobi_dirichlet": [_i, _i, _i, _f, _vp, _vp, _vp, _i, _i, _d, _pi, _pd, _vp],
+    "qmt_set_jacobi_path": [_i],
     "qmt_fft_poisson": [_vp, _i, _i, _i, _f, _f, _f, _f, _f, _f, _i, _vp, _vp, _vp],
+    "qmt_fft_poisson_padded": [_vp, _i, _i, _i, _f, _f, _f, _f, _f, _f, _i, _i, _i, _vp, _vp, _vp],
     "qmt_grid_total": [_vp, _i64, _pd, _vp],
     "qmt_grid_total_noalloc": [_vp, _i64, _pd, _vp],
     "qmt_grid_scale": [_vp, _i64, _f, _vp],
@@ -55,7 +62,7 @@ SIGNATURES = {
     "qmt_nn_singleshot": [_i, _i, _i, _d, _vp, _vp, _vp, _i, _i, _vp],
 }
 OTHER = {"qmt_last_error": ([], C.c_char_p), "qmt_abi_version": ([], C.c_int),
-         "qmt_launch_count": ([], C.c_uint64)}
+         "qmt_launch_count": ([], C.c_uint64), "qmt_batch_fused_count": ([_vp], C.c_int)}
 
 
 class NativeUnavailable(RuntimeError):

@@ -104,3 +104,31 @@ def test_batch_and_stream_generators():
     st = syn.serving_stream(200.0, 5)
     t = [x for x, _ in st]
     assert all(t[i] < t[i + 1] for i in range(4))
+
+
+def test_fft_candidates_are_nice_and_long_enough():
+    from qmtools.autotune import fft_candidates
+    for n in (24, 40, 64, 68, 136, 160):
+        c = fft_candidates(n)
+        assert c and all(m >= 2 * n for m in c)
+        for m in c:
+            k = m
+            for r in (2, 3, 5, 7):
+                while k % r == 0:
+                    k //= r
+            assert k == 1
+
+
+def test_tuner_without_measuring_uses_defaults(tmp_path):
+    """With measuring off the tuner returns the defaults without touching the GPU or the cache."""
+    import types
+    from qmtools.autotune import PATH_FUSED, PATH_STAGED, Tuner
+    t = Tuner(path=tmp_path / "none.json", measure=False)
+    t._device_key = lambda: "cpu-test"
+    small = types.SimpleNamespace(norbs=100)
+    big = types.SimpleNamespace(norbs=400)
+    assert t.density_path(small, 4096, "fp16x3") == PATH_FUSED
+    assert t.density_path(big, 4096, "fp16x3") == PATH_STAGED
+    assert t.density_path(small, 4096, "tf32x3") == PATH_STAGED
+    assert t.fft_length(40, small) == 80
+    assert not (tmp_path / "none.json").exists()

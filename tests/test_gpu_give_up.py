@@ -26,7 +26,17 @@ def _jacobi(n, sweeps, rho, v, t):
     return st, so.value
 
 
-def test_jacobi_grid_barrier_gives_up_and_recovers():
+@pytest.fixture
+def grid_barrier_path():
+    """The persistent Jacobi kernel (the one with a software grid barrier between sweeps)."""
+    N.call("qmt_set_jacobi_path", 1)
+    try:
+        yield
+    finally:
+        N.call("qmt_set_jacobi_path", 0)
+
+
+def test_jacobi_grid_barrier_gives_up_and_recovers(grid_barrier_path):
     import torch
     N.ensure_device()
     n = 64
