@@ -173,10 +173,12 @@ def _jacobi_call(name, shape, h, rho, v, t, sweeps, check_every=100, tol=0.0):
 
 @pytest.mark.parametrize("mode", ["qmt_jacobi", "qmt_jacobi_dirichlet"])
 @pytest.mark.parametrize("shape", [(64, 64, 64), (32, 48, 40), (16, 16, 17), (8, 8, 2)])
-def test_jacobi_cluster_kernel_equals_grid_barrier_kernel(mode, shape):
-    """The single-cluster kernel (field in the CTAs' shared memory, cluster barrier per sweep) and
-    the persistent grid-barrier kernel give identical grids; slabs of 4, 3, 2 and 1 planes per CTA
-    (including a ragged last slab) and the x neighbours across warp boundaries (nx = 32, 16, 8)."""
+def test_jacobi_kernels_give_identical_grids(mode, shape):
+    """The persistent grid-barrier kernel, the single-cluster kernel (field in the CTAs' shared
+    memory, cluster barrier per sweep) and the temporal-blocking kernel (four sweeps per grid
+    barrier on haloed tiles) give identical grids: slabs of 4, 3, 2 and 1 planes per CTA (a ragged
+    last slab), x neighbours across warp boundaries (nx = 32, 16, 8), partial tiles, an interval
+    cut short by the check sweep schedule (302 sweeps, a check every 25 pairs)."""
     import torch
     from qmtools import _native as N
     N.ensure_device()
@@ -185,24 +187,25 @@ def test_jacobi_cluster_kernel_equals_grid_barrier_kernel(mode, shape):
     rho = torch.rand(n, device="cuda", generator=g) - 0.5
     v0 = torch.rand(n, device="cuda", generator=g)
     out = {}
-    for path in (1, 2):
+    for path in (1, 2, 3):
         N.call("qmt_set_jacobi_path", path)
         try:
             v = v0.clone()
             t = torch.zeros_like(v)
-            st, sw, dl = _jacobi_call(mode, shape, 0.2, rho, v, t, 300, check_every=25, tol=-1.0)
+            st, sw, dl = _jacobi_call(mode, shape, 0.2, rho, v, t, 302, check_every=25, tol=-1.0)
         finally:
             N.call("qmt_set_jacobi_path", 0)
-        assert st == N.OK
-        assert sw == 300
+        assert st == N.OK, (path, N.load().qmt_last_error())
+        assert sw == 302
         out[path] = (v.cpu().numpy(), dl)
-    assert np.array_equal(out[1][0], out[2][0])
-    assert abs(out[1][1] - out[2][1]) <= 1e-12 * abs(out[1][1])
+    for path in (2, 3):
+        assert np.array_equal(out[1][0], out[path][0]), path
+        assert abs(out[1][1] - out[path][1]) <= 1e-12 * abs(out[1][1]), path
 
 
-def test_jacobi_cluster_kernel_stops_at_tolerance():
-    """The cluster kernel's FP64 residual stops the solve at the first check below tol, like the
-    grid-barrier kernel."""
+def test_jacobi_kernels_stop_at_tolerance():
+    """The cluster and temporal-blocking kernels' FP64 residual stops the solve at the first check
+    below tol, like the grid-barrier kernel."""
     import torch
     from qmtools import _native as N
     N.ensure_device()
@@ -210,7 +213,7 @@ def test_jacobi_cluster_kernel_stops_at_tolerance():
     rho = torch.zeros(64 ** 3, device="cuda")
     v0 = torch.rand(64 ** 3, device="cuda")
     res = {}
-    for path in (1, 2):
+    for path in (1, 2, 3):
         N.call("qmt_set_jacobi_path", path)
         try:
             v = v0.clone()
@@ -221,5 +224,6 @@ def test_jacobi_cluster_kernel_stops_at_tolerance():
             N.call("qmt_set_jacobi_path", 0)
         assert st == N.OK and dl <= 50.0 and sw % 20 == 0
         res[path] = (sw, v.cpu().numpy())
-    assert res[1][0] == res[2][0]
-    assert np.array_equal(res[1][1], res[2][1])
+    for path in (2, 3):
+        assert res[1][0] == res[path][0]
+        assert np.array_equal(res[1][1], res[path][1])
