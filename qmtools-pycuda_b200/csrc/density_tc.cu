@@ -543,6 +543,7 @@ struct FusedMol {
   int n16;                 // functions rounded up to 16: K of the MMAs and N (output columns); the
                            // K-steps beyond it only hold zero padding and are skipped
   int ksteps, nchunks;     // n16 / 16 K-steps; ceil(n16 / 64) column chunks of A
+  int tail0;               // n16 & ~63: first column of A's 32-byte swizzled tail blocks
   int u_rows;              // rows of one K-step block of U in HBM (kpad + 64)
   const uint8_t* u_hi;     // U pieces in K-step blocks (split_P_kernel with blk_rows = u_rows)
   const uint8_t* u_lo;
@@ -565,7 +566,7 @@ struct FusedParams {
   int nmol;
   int64_t ntiles;          // tiles of all molecules
   int nsplit, stages;
-  uint32_t a_bytes;        // one A piece: 128 rows x (largest kpad) x 2 B
+  uint32_t a_bytes;        // one A piece: 128 rows x (largest n16) x 2 B
   uint32_t b_slot;         // one U piece slot in a stage: (largest n16) rows x 32 B
   uint32_t stage_bytes;
   uint32_t fmt;
@@ -593,16 +594,22 @@ __device__ __forceinline__ const FusedMol& fused_mol(const FusedParams& p, int64
   return p.mols[lo];
 }
 
-// Byte offset of element (row, j) in the 128-byte swizzled K-major A tile (64-column chunks of
-// 8-row atoms of 1024 B, 16-byte unit u of a row at u ^ (row & 7)).  Row r + 64 of a column sits
-// 8192 B after row r.  (Holding the padding of the last chunk in 32-byte swizzled 16-column
-// blocks instead saves 8 KB of shared memory but the extra branch in this store path slowed
-// production by more than the third U stage it made room for gained.)
-__device__ __forceinline__ uint32_t a_offset(int row, int j) {
-  const int kc = j >> 6, e = j & 63;
-  const int u = (e >> 3) ^ (row & 7);
-  return (uint32_t)(kc * 16384 + (row >> 3) * 1024 + (row & 7) * 128 + u * 16 + (e & 7) * 2);
+// Byte offset of element (row, j) in the K-major A tile of a molecule with n16 columns: columns
+// below tail0 = n16 & ~63 in 128-byte swizzled 64-column chunks (8-row atoms of 1024 B, 16-byte
+// unit u of a row at u ^ (row & 7)); the last n16 - tail0 columns in 32-byte swizzled 16-column
+// blocks (rows of 32 B, the two 16-byte units exchanged when bit 2 of the row is set), so the tile
+// holds exactly n16 columns.  Row r + 64 of a column sits a_row64 bytes after row r.
+__device__ __forceinline__ uint32_t a_offset(int row, int j, int tail0) {
+  if (j < tail0) {
+    const int kc = j >> 6, e = j & 63;
+    const int u = (e >> 3) ^ (row & 7);
+    return (uint32_t)(kc * 16384 + (row >> 3) * 1024 + (row & 7) * 128 + u * 16 + (e & 7) * 2);
+  }
+  const int e = j & 15;
+  return (uint32_t)(tail0 * 256 + ((j - tail0) >> 4) * 4096 + row * 32 + ((((e >> 3) ^ (row >> 2)) & 1) << 4) +
+                    (e & 7) * 2);
 }
+__device__ __forceinline__ uint32_t a_row64(int j, int tail0) { return j < tail0 ? 8192u : 2048u; }
 
 __device__ __forceinline__ uint64_t sw32_kmajor_desc(uint32_t saddr) {
   uint64_t d = 0;
@@ -782,6 +789,7 @@ struct SwizzledRowsOut {
   uint8_t* lo;
   int r0;
   bool two;
+  int tail0;
   template <int NF>
   __device__ __forceinline__ void put(int j0, int nf, const float (&v0)[NF], const float (&v1)[NF]) const {
     bool skip = false;   // the function was stored with its predecessor
@@ -793,8 +801,8 @@ struct SwizzledRowsOut {
         continue;
       }
       const int j = j0 + k;
-      const uint32_t off = a_offset(r0, j);
-      const uint32_t off1 = off + 8192u;   // row r0 + 64
+      const uint32_t off = a_offset(r0, j, tail0);
+      const uint32_t off1 = off + a_row64(j, tail0);   // row r0 + 64
       // two consecutive functions in the same 16-byte unit: one 4-byte store per piece
       if (k + 1 < nf && (j & 1) == 0) {
         store_pair16<FMT>(hi, lo, off, v0[k], v0[k + 1], two);
@@ -1180,9 +1188,17 @@ __device__ __forceinline__ void fused_issue_mma(const FusedParams* pp, uint32_t 
       }
       tc_fence_after();
       const int j0 = ks * 16;
-      // A K-step: 32 bytes inside a 128-byte swizzled chunk
-      const uint32_t aoff = (uint32_t)((j0 >> 6) * 16384 + ((j0 & 63) >> 4) * 32);
-      const uint64_t ahi = sw128_kmajor_desc(abase + aoff), alo = sw128_kmajor_desc(lbase + aoff);
+      // A K-step: 32 bytes inside a 128-byte swizzled chunk, or one 32-byte swizzled tail block
+      uint64_t ahi, alo;
+      if (j0 < M.tail0) {
+        const uint32_t aoff = (uint32_t)((j0 >> 6) * 16384 + ((j0 & 63) >> 4) * 32);
+        ahi = sw128_kmajor_desc(abase + aoff);
+        alo = sw128_kmajor_desc(lbase + aoff);
+      } else {
+        const uint32_t aoff = (uint32_t)(M.tail0 * 256 + ((j0 - M.tail0) >> 4) * 4096);
+        ahi = sw32_kmajor_desc(abase + aoff);
+        alo = sw32_kmajor_desc(lbase + aoff);
+      }
       const uint32_t bst = smem_u32(stages + (size_t)s * p.stage_bytes);
       for (int c0 = 0; c0 < M.n16; c0 += 256) {
         const int n = min(256, M.n16 - c0);
@@ -1211,9 +1227,18 @@ __global__ void __launch_bounds__(FUSED_THREADS, 1)
   __shared__ __align__(8) uint64_t chunk_bar[MAX_FUSED_CHUNKS], t_full, drain_bar;
   __shared__ int item_ctr;
   __shared__ uint32_t tmem_slot;
-  __shared__ double pos[128][3];
-  __shared__ double rho_part[FUSED_NCW / 4][128];
-  __shared__ double red[FUSED_NCW];
+  // tile positions (production) and the epilogue's partial sums share their storage: every reader
+  // of the one is past a barrier of all compute warps before the other is written
+  __shared__ union {
+    double pos[128][3];
+    struct {
+      double rho_part[FUSED_NCW / 4][128];
+      double red[FUSED_NCW];
+    } e;
+  } ps;
+  double(*pos)[3] = ps.pos;
+  double(*rho_part)[128] = ps.e.rho_part;
+  double* red = ps.e.red;
   __shared__ volatile int abort_flag;
 
   uint8_t* smem = reinterpret_cast<uint8_t*>((reinterpret_cast<uintptr_t>(smem_dyn) + 1023) & ~uintptr_t(1023));
@@ -1281,7 +1306,7 @@ __global__ void __launch_bounds__(FUSED_THREADS, 1)
           reinterpret_cast<float*>(tabs + M.off_coords)[i] = __ldg(M.coords + i);
         const int npadc = M.n16 - M.norbs;
         for (int i = ct; i < 128 * npadc; i += FUSED_NCT) {
-          const uint32_t off = a_offset(i / npadc, M.norbs + i % npadc);
+          const uint32_t off = a_offset(i / npadc, M.norbs + i % npadc, M.tail0);
           *reinterpret_cast<uint16_t*>(A_hi + off) = 0;
           if (two) *reinterpret_cast<uint16_t*>(A_lo + off) = 0;
         }
@@ -1319,7 +1344,7 @@ __global__ void __launch_bounds__(FUSED_THREADS, 1)
         const int s0 = ash_s[a] & 0xffffff;
         if ((ash_s[a + 1] & 0xffffff) <= s0) continue;
         const int flast = atom_rows(sh_s, pr_s, ash_s, crd_s, a, pos, (itm & 1) * 32 + lane,
-                                    SwizzledRowsOut<FMT>{A_hi, A_lo, (itm & 1) * 32 + lane, two});
+                                    SwizzledRowsOut<FMT>{A_hi, A_lo, (itm & 1) * 32 + lane, two, M.tail0});
         // publish: generic-proxy writes of A become visible to the tensor core, then one arrival
         // per column chunk this atom wrote
         asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
@@ -1344,9 +1369,17 @@ __global__ void __launch_bounds__(FUSED_THREADS, 1)
         tmem_ld16_issue(trow + (uint32_t)col, tv);
         float ph[16];
         // the row's two 16-byte units of columns col .. col + 15 (layout of a_offset)
-        const int u0 = (col & 63) >> 3;
-        const uint32_t rbase = (uint32_t)((col >> 6) * 16384 + (row >> 3) * 1024 + (row & 7) * 128);
-        const uint32_t uo[2] = {(uint32_t)((u0 ^ (row & 7)) * 16), (uint32_t)(((u0 + 1) ^ (row & 7)) * 16)};
+        uint32_t rbase, uo[2];
+        if (col < M.tail0) {
+          const int u0 = (col & 63) >> 3;
+          rbase = (uint32_t)((col >> 6) * 16384 + (row >> 3) * 1024 + (row & 7) * 128);
+          uo[0] = (uint32_t)((u0 ^ (row & 7)) * 16);
+          uo[1] = (uint32_t)(((u0 + 1) ^ (row & 7)) * 16);
+        } else {
+          rbase = (uint32_t)(M.tail0 * 256 + ((col - M.tail0) >> 4) * 4096 + row * 32);
+          uo[0] = (uint32_t)(((row >> 2) & 1) << 4);
+          uo[1] = 16u - uo[0];
+        }
         const uint8_t* rb = A_hi + rbase;
 #pragma unroll
         for (int u = 0; u < 2; ++u) unpack8<FMT>(*reinterpret_cast<const uint4*>(rb + uo[u]), ph + 8 * u);
@@ -1523,10 +1556,10 @@ static int fused_tab_bytes(const qmt_mol* m) {
   return words * 16 + (m->natoms + 1 + 3) / 4 * 16 + (3 * m->natoms + 3) / 4 * 16;
 }
 
-// Functions rounded up to 16 (K-steps of the fused MMAs), bytes of one A piece (kpad columns)
+// Functions rounded up to 16 (K-steps of the fused MMAs), bytes of one A piece (n16 columns)
 // and of one U piece slot in a stage.
 static int fused_n16(const qmt_mol* m) { return (m->norbs + 15) / 16 * 16; }
-static uint32_t fused_a_bytes(int kpad) { return 128u * (uint32_t)kpad * 2u; }
+static uint32_t fused_a_bytes(int n16) { return 128u * (uint32_t)n16 * 2u; }
 static uint32_t fused_b_slot(int n16) { return (uint32_t)n16 * 32u; }
 
 // U pipeline stages that fit beside A and the tables (below 2: the fused path does not fit).
@@ -1537,7 +1570,7 @@ static int fused_stages(const TcShape& sh, int n16, int tab_bytes) {
   cudaDeviceGetAttribute(&maxsm, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev);
   cudaFuncAttributes fa;
   if (cudaFuncGetAttributes(&fa, density_fused_kernel<FMT>) != cudaSuccess) return 0;
-  const long a_bytes = fused_a_bytes(sh.kpad), stage_bytes = (long)sh.nsplit * fused_b_slot(n16);
+  const long a_bytes = fused_a_bytes(n16), stage_bytes = (long)sh.nsplit * fused_b_slot(n16);
   const long avail = (long)maxsm - (long)fa.sharedSizeBytes - 1024 - sh.nsplit * a_bytes - tab_bytes;
   return (int)std::max<long>(0, std::min<long>(MAX_STAGES, avail / stage_bytes));
 }
@@ -1557,6 +1590,7 @@ static qmt_status fused_mol_desc(qmt_mol* m, const TcShape& sh, const PointMap& 
   d.n16 = n16;
   d.ksteps = n16 / 16;
   d.nchunks = (n16 + 63) / 64;
+  d.tail0 = n16 & ~63;
   d.u_rows = K + 64;
   d.u_hi = B;
   d.u_lo = B + piece;
@@ -1588,7 +1622,7 @@ static qmt_status fused_mol_desc(qmt_mol* m, const TcShape& sh, const PointMap& 
 template <int FMT>
 static qmt_status launch_fused(FusedParams& p, const TcShape& sh_max, int n16_max, int tab_bytes_max, cudaStream_t s) {
   p.nsplit = sh_max.nsplit;
-  p.a_bytes = fused_a_bytes(sh_max.kpad);
+  p.a_bytes = fused_a_bytes(n16_max);
   p.b_slot = fused_b_slot(n16_max);
   p.stage_bytes = p.nsplit * p.b_slot;
   p.fmt = (uint32_t)sh_max.fmt;
