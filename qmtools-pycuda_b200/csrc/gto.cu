@@ -288,7 +288,7 @@ struct GPair32 {
 
 // R_tuv (t+u+v <= L) from h_j = (-2p)^j F_j, j = 0..L, dotted with D.
 template <int L>
-__device__ __forceinline__ float hermite_dot32(const float* __restrict__ D, float X, float Y, float Z,
+__device__ __forceinline__ float hermite_dot32(const float (&D)[ncoef(L)], float X, float Y, float Z,
                                                const float (&h)[L + 1]) {
   constexpr int NC = ncoef(L);
   constexpr HermTable H = make_herm_table();
@@ -318,7 +318,7 @@ __device__ __forceinline__ float hermite_dot32(const float* __restrict__ D, floa
 }
 
 template <int L>
-__device__ __forceinline__ float pair_term32(const GPair32& g, const float* __restrict__ D, float cx, float cy,
+__device__ __forceinline__ float pair_term32(const GPair32& g, const float (&D)[ncoef(L)], float cx, float cy,
                                              float cz, const float* __restrict__ tab) {
   const float X = g.px - cx, Y = g.py - cy, Z = g.pz - cz;
   const float r2 = fmaf(X, X, fmaf(Y, Y, Z * Z));
@@ -358,24 +358,42 @@ __device__ __forceinline__ float pair_term32(const GPair32& g, const float* __re
 }
 
 constexpr int GTO32_THREADS = 128;
+constexpr int GTO32_PPT = 2;                          // points per thread
+constexpr int GTO32_POINTS = GTO32_THREADS * GTO32_PPT;
 constexpr int GTO32_CHUNK = 128;
 
-// The terms of `nc` pairs of one angular momentum L (all in shared memory) at the thread's point,
-// summed in FP32 in groups of four, the groups in FP64.  One L per loop (no dispatch per pair),
-// unrolled so that consecutive pairs' independent dependency chains overlap.
+// The terms of `nc` pairs of one angular momentum L (all in shared memory) at the thread's two
+// points, summed in FP32 in groups of four, the groups in FP64.  One L per loop (no dispatch per
+// pair); a pair's header and coefficients are read once into registers for both points, whose
+// independent dependency chains overlap.
 template <int L>
-__device__ __forceinline__ void chunk_terms(const GPair32* sp, const float* sd, const int* soff, int nc, float x,
-                                            float y, float z, const float* __restrict__ tab, double& V) {
-  float acc = 0.f;
-#pragma unroll 4
+__device__ __forceinline__ void chunk_terms(const GPair32* sp, const float* sd, const int* soff, int nc,
+                                            const float (&x)[GTO32_PPT], const float (&y)[GTO32_PPT],
+                                            const float (&z)[GTO32_PPT], const float* __restrict__ tab,
+                                            double (&V)[GTO32_PPT]) {
+  constexpr int NC = ncoef(L);
+  float acc[GTO32_PPT];
+#pragma unroll
+  for (int q = 0; q < GTO32_PPT; ++q) acc[q] = 0.f;
+#pragma unroll 2
   for (int k = 0; k < nc; ++k) {
-    acc += pair_term32<L>(sp[k], sd + soff[k], x, y, z, tab);
+    const GPair32 g = sp[k];
+    float D[NC];
+    const float* d = sd + soff[k];
+#pragma unroll
+    for (int c = 0; c < NC; ++c) D[c] = d[c];
+#pragma unroll
+    for (int q = 0; q < GTO32_PPT; ++q) acc[q] += pair_term32<L>(g, D, x[q], y[q], z[q], tab);
     if ((k & 3) == 3) {
-      V += (double)acc;
-      acc = 0.f;
+#pragma unroll
+      for (int q = 0; q < GTO32_PPT; ++q) {
+        V[q] += (double)acc[q];
+        acc[q] = 0.f;
+      }
     }
   }
-  V += (double)acc;
+#pragma unroll
+  for (int q = 0; q < GTO32_PPT; ++q) V[q] += (double)acc[q];
 }
 
 // Pairs are sorted by L; lstart[L] .. lstart[L + 1] are those of angular momentum L.
@@ -383,6 +401,7 @@ struct PairRanges {
   int lstart[6];
 };
 
+// Points base + threadIdx.x + q * GTO32_THREADS (q < GTO32_PPT) of each block.
 __global__ void __launch_bounds__(GTO32_THREADS) gto32_kernel(const GPair32* __restrict__ pairs, PairRanges pr,
                                                               const float* __restrict__ dco,
                                                               const float* __restrict__ tab, MolView mol,
@@ -392,14 +411,29 @@ __global__ void __launch_bounds__(GTO32_THREADS) gto32_kernel(const GPair32* __r
   __shared__ GPair32 sp[GTO32_CHUNK];
   __shared__ float sd[GTO32_CHUNK * 35];
   __shared__ int soff[GTO32_CHUNK];
-  const int64_t i = blockIdx.x * (int64_t)GTO32_THREADS + threadIdx.x;
-  double cx = 0, cy = 0, cz = 0;
-  int64_t o = -1;
-  const bool valid = i < gp.npts && gto_point(gp, i, cx, cy, cz, o);
-  // the point relative to the centroid, rounded once: every term (and the nuclear sum) sees the
-  // same point
-  const float x = (float)(cx - rx), y = (float)(cy - ry), z = (float)(cz - rz);
-  double V = 0.0;
+  float x[GTO32_PPT], y[GTO32_PPT], z[GTO32_PPT];
+  int64_t o[GTO32_PPT];
+  bool valid[GTO32_PPT];
+  double V[GTO32_PPT];
+#pragma unroll
+  for (int q = 0; q < GTO32_PPT; ++q) {
+    const int64_t i = blockIdx.x * (int64_t)GTO32_POINTS + q * GTO32_THREADS + threadIdx.x;
+    double cx = 0, cy = 0, cz = 0;
+    o[q] = -1;
+    valid[q] = i < gp.npts && gto_point(gp, i, cx, cy, cz, o[q]);
+    if (!valid[q] && q > 0) {   // a stand-in point: the arithmetic stays finite, nothing is written
+      x[q] = x[0];
+      y[q] = y[0];
+      z[q] = z[0];
+    } else {
+      // the point relative to the centroid, rounded once: every term (and the nuclear sum) sees
+      // the same point
+      x[q] = (float)(cx - rx);
+      y[q] = (float)(cy - ry);
+      z[q] = (float)(cz - rz);
+    }
+    V[q] = 0.0;
+  }
 #pragma unroll 1
   for (int L = 0; L <= 4; ++L) {
     const int p0 = pr.lstart[L], p1 = pr.lstart[L + 1];
@@ -415,7 +449,7 @@ __global__ void __launch_bounds__(GTO32_THREADS) gto32_kernel(const GPair32* __r
       const int dn = nc * ncoef(L);
       for (int k = threadIdx.x; k < dn; k += GTO32_THREADS) sd[k] = dco[dbase + k];
       __syncthreads();
-      if (valid) {
+      if (valid[0]) {
         switch (L) {
           case 0: chunk_terms<0>(sp, sd, soff, nc, x, y, z, tab, V); break;
           case 1: chunk_terms<1>(sp, sd, soff, nc, x, y, z, tab, V); break;
@@ -426,17 +460,21 @@ __global__ void __launch_bounds__(GTO32_THREADS) gto32_kernel(const GPair32* __r
       }
     }
   }
-  if (!valid) return;
   // nuclear term in FP64 from the same FP32 centroid-relative coordinates as the electrons: a
   // nucleus and the pairs centred on it (the bulk of its electrons) carry the same rounding, so
   // the near-cancellation of the two at a distance is not disturbed by a relative shift
-  for (int a = 0; a < mol.natoms; ++a) {
-    const double dx = (double)x - (double)nuc32[3 * a], dy = (double)y - (double)nuc32[3 * a + 1],
-                 dz = (double)z - (double)nuc32[3 * a + 2];
-    const double r = sqrt(dx * dx + dy * dy + dz * dz);
-    if (r > 1e-8) V += mol.types[a] / r;
+#pragma unroll
+  for (int q = 0; q < GTO32_PPT; ++q) {
+    if (!valid[q]) continue;
+    double v = V[q];
+    for (int a = 0; a < mol.natoms; ++a) {
+      const double dx = (double)x[q] - (double)nuc32[3 * a], dy = (double)y[q] - (double)nuc32[3 * a + 1],
+                   dz = (double)z[q] - (double)nuc32[3 * a + 2];
+      const double r = sqrt(dx * dx + dy * dy + dz * dz);
+      if (r > 1e-8) v += mol.types[a] / r;
+    }
+    out[o[q]] = (float)v;
   }
-  out[o] = (float)V;
 }
 
 // ---- host: Boys table ------------------------------------------------------------------------
@@ -705,7 +743,7 @@ static qmt_status run_gto(qmt_mol* m, const GtoPoints& gp, float* out, cudaStrea
     if ((st = boys_table32(&tab32))) return st;
     const GPair32* p32 = m->d_pairs32.as<GPair32>();
     const float* d32 = reinterpret_cast<const float*>(m->d_pairs32.as<uint8_t>() + m->gto32_doff_bytes);
-    const int64_t blocks = (gp.npts + GTO32_THREADS - 1) / GTO32_THREADS;
+    const int64_t blocks = (gp.npts + GTO32_POINTS - 1) / GTO32_POINTS;
     PairRanges pr;
     for (int L = 0; L <= 5; ++L) pr.lstart[L] = m->gto_lstart[L];
     gto32_kernel<<<(unsigned)blocks, GTO32_THREADS, 0, s>>>(p32, pr, d32, tab32, m->view(), d32 + m->gto32_nuc_off,
