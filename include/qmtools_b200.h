@@ -178,12 +178,11 @@ qmt_status qmt_jacobi_dirichlet(int nx, int ny, int nz, float step, const float*
                                 float* v_dev, float* t_dev, int max_sweeps, int check_every,
                                 double tol, int* sweeps_out, double* delta_out, void* stream);
 /* Selects the Jacobi implementation of the two calls above (new; process-wide): 0 = automatic
- * (temporal blocking when every 32 x 8 x 8 tile of the grid gets its own CTA, e.g. 64^3: four
- * sweeps per grid barrier on tiles with halos in shared memory; else one persistent kernel with
- * a grid barrier between sweeps), 1 = always the grid barrier per sweep, 2 = one 16-CTA
- * thread-block cluster holding the field in shared memory (nx % 4 == 0, nx * ny <= 4096,
- * nz <= 64), 3 = always temporal blocking (QMT_BAD_ARG where a choice does not apply).  All give
- * identical grids; the residual sums may differ in the last bits. */
+ * (the cluster kernel for qmt_jacobi_dirichlet where it applies, else the grid-barrier kernel),
+ * 1 = one persistent kernel with a grid barrier between sweeps, 2 = one 16-CTA thread-block
+ * cluster holding the field in shared memory (nx % 4 == 0, nx * ny <= 4096, nz <= 64;
+ * QMT_BAD_ARG where it does not apply).  Both give identical grids; the residual sums may differ
+ * in the last bits. */
 qmt_status qmt_set_jacobi_path(int mode);
 
 /* ---- FFT Poisson ---------------------------------------------------------------------- */

@@ -1133,19 +1133,24 @@ __device__ __forceinline__ void fused_produce_u(const FusedParams* pp, uint8_t* 
   for (int64_t t = blockIdx.x; t < p.ntiles && ok; t += gridDim.x) {
     int m;
     const FusedMol& M = fused_mol(p, t, m);
-    for (int ks = 0; ks < M.ksteps; ++ks, ++it) {
+    // the molecule's values in registers for the tile: read through a reference, they would be
+    // reloaded after every barrier operation (each an asm statement that clobbers memory)
+    const int ksteps = M.ksteps, u_rows = M.u_rows;
+    const uint32_t bytes = (uint32_t)M.n16 * 32u;
+    const uint8_t* const u_hi = M.u_hi;
+    const uint8_t* const u_lo = M.u_lo;
+    for (int ks = 0; ks < ksteps; ++ks, ++it) {
       const int s = it % p.stages;
       const uint32_t ph = (it / p.stages) & 1u;
       if (!mbar_wait(&empty_bar[s], ph ^ 1u, abort_flag, p.wait_ns)) {
         ok = false;
         break;
       }
-      const uint32_t bytes = (uint32_t)M.n16 * 32u;
-      const size_t src = (size_t)ks * M.u_rows * 32u;
+      const size_t src = (size_t)ks * u_rows * 32u;
       uint8_t* st = stages + (size_t)s * p.stage_bytes;
       mbar_expect_tx(&full_bar[s], bytes * (uint32_t)p.nsplit);
-      bulk_load(st, M.u_hi + src, bytes, &full_bar[s]);
-      if (two) bulk_load(st + p.b_slot, M.u_lo + src, bytes, &full_bar[s]);
+      bulk_load(st, u_hi + src, bytes, &full_bar[s]);
+      if (two) bulk_load(st + p.b_slot, u_lo + src, bytes, &full_bar[s]);
       issued |= 1u << s;
       par = (par & ~(1u << s)) | (ph << s);
     }
@@ -1169,10 +1174,16 @@ __device__ __forceinline__ void fused_issue_mma(const FusedParams* pp, uint32_t 
   for (int64_t t = blockIdx.x; t < p.ntiles && ok; t += gridDim.x) {
     int m;
     const FusedMol& M = fused_mol(p, t, m);
-    for (int ks = 0; ks < M.ksteps; ++ks, ++it) {
+    // the molecule's values in registers for the tile (see the producer)
+    const int ksteps = M.ksteps, n16 = M.n16, tail0 = M.tail0;
+    uint32_t need = 0;
+#pragma unroll
+    for (int c = 0; c < MAX_FUSED_CHUNKS; ++c)
+      if (M.chunk_need[c] > 0) need |= 1u << c;
+    for (int ks = 0; ks < ksteps; ++ks, ++it) {
       // columns 64c .. 64c+63 of A are complete once every item writing them arrived
       const int c = ks >> 2;
-      if ((ks & 3) == 0 && M.chunk_need[c] > 0) {
+      if ((ks & 3) == 0 && ((need >> c) & 1u)) {
         if (!mbar_wait(&chunk_bar[c], (cpar >> c) & 1u, abort_flag, p.wait_ns)) {
           ok = false;
           break;
@@ -1190,18 +1201,18 @@ __device__ __forceinline__ void fused_issue_mma(const FusedParams* pp, uint32_t 
       const int j0 = ks * 16;
       // A K-step: 32 bytes inside a 128-byte swizzled chunk, or one 32-byte swizzled tail block
       uint64_t ahi, alo;
-      if (j0 < M.tail0) {
+      if (j0 < tail0) {
         const uint32_t aoff = (uint32_t)((j0 >> 6) * 16384 + ((j0 & 63) >> 4) * 32);
         ahi = sw128_kmajor_desc(abase + aoff);
         alo = sw128_kmajor_desc(lbase + aoff);
       } else {
-        const uint32_t aoff = (uint32_t)(M.tail0 * 256 + ((j0 - M.tail0) >> 4) * 4096);
+        const uint32_t aoff = (uint32_t)(tail0 * 256 + ((j0 - tail0) >> 4) * 4096);
         ahi = sw32_kmajor_desc(abase + aoff);
         alo = sw32_kmajor_desc(lbase + aoff);
       }
       const uint32_t bst = smem_u32(stages + (size_t)s * p.stage_bytes);
-      for (int c0 = 0; c0 < M.n16; c0 += 256) {
-        const int n = min(256, M.n16 - c0);
+      for (int c0 = 0; c0 < n16; c0 += 256) {
+        const int n = min(256, n16 - c0);
         const uint32_t idesc = make_idesc(p.fmt, 128, (uint32_t)n);
         const uint32_t boff = (uint32_t)c0 * 32u;
         const uint32_t d = tmem + (uint32_t)c0;
@@ -1298,6 +1309,7 @@ __global__ void __launch_bounds__(FUSED_THREADS, 1)
       int m;
       const FusedMol& M = fused_mol(p, t, m);
       const int64_t lt = t - M.tile0;          // tile within the molecule
+      const int natoms = M.natoms, n16 = M.n16, tail0 = M.tail0;   // (in registers, see the producer)
       if (m != cur_m) {
         // another molecule: its tables into shared memory and its padding columns of A cleared
         // (the previous tile's epilogue, the last reader of both, ended with a named barrier)
@@ -1339,12 +1351,12 @@ __global__ void __launch_bounds__(FUSED_THREADS, 1)
         int itm = 0;
         if (lane == 0) itm = atomicAdd(&item_ctr, 1);
         itm = __shfl_sync(0xffffffffu, itm, 0);
-        if (itm >= 2 * M.natoms) break;
+        if (itm >= 2 * natoms) break;
         const int a = itm >> 1;
         const int s0 = ash_s[a] & 0xffffff;
         if ((ash_s[a + 1] & 0xffffff) <= s0) continue;
         const int flast = atom_rows(sh_s, pr_s, ash_s, crd_s, a, pos, (itm & 1) * 32 + lane,
-                                    SwizzledRowsOut<FMT>{A_hi, A_lo, (itm & 1) * 32 + lane, two, M.tail0});
+                                    SwizzledRowsOut<FMT>{A_hi, A_lo, (itm & 1) * 32 + lane, two, tail0});
         // publish: generic-proxy writes of A become visible to the tensor core, then one arrival
         // per column chunk this atom wrote
         asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
@@ -1362,7 +1374,7 @@ __global__ void __launch_bounds__(FUSED_THREADS, 1)
       tc_fence_after();
       double acc[2] = {0.0, 0.0};
       const uint32_t trow = tmem + ((uint32_t)(q * 32) << 16);
-      for (int c = hh; c * 16 < M.n16; c += FUSED_NCW / 4) {
+      for (int c = hh; c * 16 < n16; c += FUSED_NCW / 4) {
         const int col = c * 16;
         // the TMEM load of T' is in flight while the row's Phi' units are read from shared memory
         uint32_t tv[16];
@@ -1370,13 +1382,13 @@ __global__ void __launch_bounds__(FUSED_THREADS, 1)
         float ph[16];
         // the row's two 16-byte units of columns col .. col + 15 (layout of a_offset)
         uint32_t rbase, uo[2];
-        if (col < M.tail0) {
+        if (col < tail0) {
           const int u0 = (col & 63) >> 3;
           rbase = (uint32_t)((col >> 6) * 16384 + (row >> 3) * 1024 + (row & 7) * 128);
           uo[0] = (uint32_t)((u0 ^ (row & 7)) * 16);
           uo[1] = (uint32_t)(((u0 + 1) ^ (row & 7)) * 16);
         } else {
-          rbase = (uint32_t)(M.tail0 * 256 + ((col - M.tail0) >> 4) * 4096 + row * 32);
+          rbase = (uint32_t)(tail0 * 256 + ((col - tail0) >> 4) * 4096 + row * 32);
           uo[0] = (uint32_t)(((row >> 2) & 1) << 4);
           uo[1] = 16u - uo[0];
         }

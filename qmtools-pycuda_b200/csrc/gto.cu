@@ -277,15 +277,6 @@ constexpr int BOYS32_NT = 301;   // T = 0, 0.1, ..., 30 (the far-field form take
 constexpr int BOYS32_NM = 10;    // m = 0..9: F_L and five Taylor terms for L <= 4
 constexpr float T_FAR = 30.0f;
 
-struct GPair32 {
-  float px, py, pz;   // centre relative to the molecule's centroid (bohr)
-  float p;            // exponent sum
-  float fscale;       // sqrt(pi) / (2 sqrt(p)): far-field factor
-  int L;
-  int doff;           // offset of the pref * D_tuv coefficients
-  int pad;
-};
-
 // R_tuv (t+u+v <= L) from h_j = (-2p)^j F_j, j = 0..L, dotted with D.
 template <int L>
 __device__ __forceinline__ float hermite_dot32(const float (&D)[ncoef(L)], float X, float Y, float Z,
@@ -396,58 +387,54 @@ __device__ __forceinline__ void chunk_terms(const GPair32* sp, const float* sd, 
   for (int q = 0; q < GTO32_PPT; ++q) V[q] += (double)acc[q];
 }
 
-// Pairs are sorted by L; lstart[L] .. lstart[L + 1] are those of angular momentum L.
-struct PairRanges {
-  int lstart[6];
-};
+__device__ __forceinline__ void point32(const GtoPoints& gp, const Gto32Tables& t, int64_t i, float& x, float& y,
+                                        float& z, int64_t& o, bool& valid) {
+  double cx = 0, cy = 0, cz = 0;
+  o = -1;
+  valid = i < gp.npts && gto_point(gp, i, cx, cy, cz, o);
+  // the point relative to the centroid, rounded once: every term and the nuclear sum see it
+  x = (float)(cx - t.rx);
+  y = (float)(cy - t.ry);
+  z = (float)(cz - t.rz);
+}
 
-// Points base + threadIdx.x + q * GTO32_THREADS (q < GTO32_PPT) of each block.
-__global__ void __launch_bounds__(GTO32_THREADS) gto32_kernel(const GPair32* __restrict__ pairs, PairRanges pr,
-                                                              const float* __restrict__ dco,
-                                                              const float* __restrict__ tab, MolView mol,
-                                                              const float* __restrict__ nuc32, double rx, double ry,
-                                                              double rz, GtoPoints gp,
-                                                              float* __restrict__ out) {
+// Off-site pairs of slice blockIdx.y at the block's points; FP64 partial sums into
+// part[blockIdx.y * npts + i].
+__global__ void __launch_bounds__(GTO32_THREADS) gto32_pairs_kernel(Gto32Tables t, const float* __restrict__ tab,
+                                                                    GtoPoints gp, double* __restrict__ part) {
   __shared__ GPair32 sp[GTO32_CHUNK];
   __shared__ float sd[GTO32_CHUNK * 35];
   __shared__ int soff[GTO32_CHUNK];
   float x[GTO32_PPT], y[GTO32_PPT], z[GTO32_PPT];
-  int64_t o[GTO32_PPT];
+  int64_t o[GTO32_PPT], idx[GTO32_PPT];
   bool valid[GTO32_PPT];
   double V[GTO32_PPT];
 #pragma unroll
   for (int q = 0; q < GTO32_PPT; ++q) {
-    const int64_t i = blockIdx.x * (int64_t)GTO32_POINTS + q * GTO32_THREADS + threadIdx.x;
-    double cx = 0, cy = 0, cz = 0;
-    o[q] = -1;
-    valid[q] = i < gp.npts && gto_point(gp, i, cx, cy, cz, o[q]);
+    idx[q] = blockIdx.x * (int64_t)GTO32_POINTS + q * GTO32_THREADS + threadIdx.x;
+    point32(gp, t, idx[q], x[q], y[q], z[q], o[q], valid[q]);
     if (!valid[q] && q > 0) {   // a stand-in point: the arithmetic stays finite, nothing is written
       x[q] = x[0];
       y[q] = y[0];
       z[q] = z[0];
-    } else {
-      // the point relative to the centroid, rounded once: every term (and the nuclear sum) sees
-      // the same point
-      x[q] = (float)(cx - rx);
-      y[q] = (float)(cy - ry);
-      z[q] = (float)(cz - rz);
     }
     V[q] = 0.0;
   }
+  const int s0 = t.slice[blockIdx.y], s1 = t.slice[blockIdx.y + 1];
 #pragma unroll 1
   for (int L = 0; L <= 4; ++L) {
-    const int p0 = pr.lstart[L], p1 = pr.lstart[L + 1];
+    const int p0 = max(s0, t.lstart[L]), p1 = min(s1, t.lstart[L + 1]);
     for (int c0 = p0; c0 < p1; c0 += GTO32_CHUNK) {
       const int nc = min(GTO32_CHUNK, p1 - c0);
       __syncthreads();   // the previous chunk's readers are done
-      const int dbase = pairs[c0].doff;
+      const int dbase = t.pairs[c0].doff;
       if (threadIdx.x < nc) {
-        const GPair32 g = pairs[c0 + threadIdx.x];
+        const GPair32 g = t.pairs[c0 + threadIdx.x];
         sp[threadIdx.x] = g;
         soff[threadIdx.x] = g.doff - dbase;   // coefficients of a chunk are contiguous
       }
       const int dn = nc * ncoef(L);
-      for (int k = threadIdx.x; k < dn; k += GTO32_THREADS) sd[k] = dco[dbase + k];
+      for (int k = threadIdx.x; k < dn; k += GTO32_THREADS) sd[k] = t.dco[dbase + k];
       __syncthreads();
       if (valid[0]) {
         switch (L) {
@@ -460,21 +447,93 @@ __global__ void __launch_bounds__(GTO32_THREADS) gto32_kernel(const GPair32* __r
       }
     }
   }
-  // nuclear term in FP64 from the same FP32 centroid-relative coordinates as the electrons: a
-  // nucleus and the pairs centred on it (the bulk of its electrons) carry the same rounding, so
-  // the near-cancellation of the two at a distance is not disturbed by a relative shift
 #pragma unroll
-  for (int q = 0; q < GTO32_PPT; ++q) {
-    if (!valid[q]) continue;
-    double v = V[q];
-    for (int a = 0; a < mol.natoms; ++a) {
-      const double dx = (double)x[q] - (double)nuc32[3 * a], dy = (double)y[q] - (double)nuc32[3 * a + 1],
-                   dz = (double)z[q] - (double)nuc32[3 * a + 2];
-      const double r = sqrt(dx * dx + dy * dy + dz * dz);
-      if (r > 1e-8) v += mol.types[a] / r;
+  for (int q = 0; q < GTO32_PPT; ++q)
+    if (valid[q]) part[blockIdx.y * gp.npts + idx[q]] = V[q];
+}
+
+// FP64 R_tuv (t+u+v <= 4) from h_j, dotted with the 35 moments M.
+__device__ __forceinline__ double hermite_dot64(const double* __restrict__ M, double X, double Y, double Z,
+                                                const double (&h)[5]) {
+  constexpr int NC = ncoef(4);
+  constexpr HermTable H = make_herm_table();
+  double cur[NC], nxt[NC];
+  cur[0] = h[4];
+#pragma unroll
+  for (int j = 3; j >= 0; --j) {
+    nxt[0] = h[j];
+    const int n = ncoef(4 - j);
+#pragma unroll
+    for (int k = 1; k < NC; ++k) {
+      if (k < n) {
+        const HermIdx e = H.e[k];
+        const double c = e.dir == 0 ? X : (e.dir == 1 ? Y : Z);
+        double r = c * cur[e.p1];
+        if (e.mult > 0) r = fma((double)e.mult, cur[e.p2], r);
+        nxt[k] = r;
+      }
     }
-    out[o[q]] = (float)v;
+#pragma unroll
+    for (int k = 0; k < NC; ++k) cur[k] = nxt[k];
   }
+  double acc = 0.0;
+#pragma unroll
+  for (int k = 0; k < NC; ++k) acc = fma(__ldg(M + k), cur[k], acc);
+  return acc;
+}
+
+// Per point: the slices' partial sums in order, then atom by atom the far-field on-site pairs as
+// one FP64 multipole, the near-field on-site pairs in FP32, and the nucleus in FP64.
+__global__ void __launch_bounds__(GTO32_THREADS) gto32_atoms_kernel(Gto32Tables t, const float* __restrict__ tab,
+                                                                    MolView mol, GtoPoints gp,
+                                                                    const double* __restrict__ part,
+                                                                    float* __restrict__ out) {
+  const int64_t i = blockIdx.x * (int64_t)GTO32_THREADS + threadIdx.x;
+  float x, y, z;
+  int64_t o;
+  bool valid;
+  point32(gp, t, i, x, y, z, o, valid);
+  if (!valid) return;
+  double V = 0.0;
+  for (int sl = 0; sl < t.nslice; ++sl) V += part[sl * gp.npts + i];
+  for (int a = 0; a < mol.natoms; ++a) {
+    const float ax = t.nuc[3 * a], ay = t.nuc[3 * a + 1], az = t.nuc[3 * a + 2];
+    // the same FP32 displacement and r^2 as the pair terms (pair_term32), so that the far / near
+    // split below is exactly the one a pair-by-pair evaluation would make
+    const float X = ax - x, Y = ay - y, Z = az - z;
+    const float r2 = fmaf(X, X, fmaf(Y, Y, Z * Z));
+    const int b0 = t.onsite_off[a], b1 = t.onsite_off[a + 1];
+    int lo = b0, hi = b1;   // first pair that is not far (exponents descend, so far ones lead)
+    while (lo < hi) {
+      const int mid = (lo + hi) >> 1;
+      if (!(__ldg(t.onsite_p + mid) * r2 < T_FAR)) lo = mid + 1;
+      else hi = mid;
+    }
+    const double Xd = X, Yd = Y, Zd = Z;
+    const double r2d = Xd * Xd + Yd * Yd + Zd * Zd;
+    if (lo > b0) {
+      const double ri = 1.0 / sqrt(r2d), ri2 = ri * ri;
+      double h[5];
+      h[0] = ri;
+#pragma unroll
+      for (int j = 0; j < 4; ++j) h[j + 1] = -(double)(2 * j + 1) * h[j] * ri2;
+      V += hermite_dot64(t.cum + (size_t)(t.cum_off[a] + (lo - b0)) * 35, Xd, Yd, Zd, h);
+    }
+    for (int k = lo; k < b1; ++k) {
+      const GPair32 g = t.onsite[k];
+      const float* d = t.dco + g.doff;
+      switch (g.L) {
+        case 0: { float D[1]; D[0] = d[0]; V += (double)pair_term32<0>(g, D, x, y, z, tab); break; }
+        case 1: { float D[4]; for (int c = 0; c < 4; ++c) D[c] = d[c]; V += (double)pair_term32<1>(g, D, x, y, z, tab); break; }
+        case 2: { float D[10]; for (int c = 0; c < 10; ++c) D[c] = d[c]; V += (double)pair_term32<2>(g, D, x, y, z, tab); break; }
+        case 3: { float D[20]; for (int c = 0; c < 20; ++c) D[c] = d[c]; V += (double)pair_term32<3>(g, D, x, y, z, tab); break; }
+        default: { float D[35]; for (int c = 0; c < 35; ++c) D[c] = d[c]; V += (double)pair_term32<4>(g, D, x, y, z, tab); break; }
+      }
+    }
+    const double r = sqrt(r2d);
+    if (r > 1e-8) V += mol.types[a] / r;
+  }
+  out[o] = (float)V;
 }
 
 // ---- host: Boys table ------------------------------------------------------------------------
@@ -574,6 +633,7 @@ static qmt_status build_pairs(qmt_mol* m, cudaStream_t s) {
   struct Acc {
     double px, py, pz, p, pref;
     int L;
+    int atom_a, atom_b;
     double D[35];
   };
   std::vector<Acc> acc;
@@ -649,6 +709,8 @@ static qmt_status build_pairs(qmt_mol* m, cudaStream_t s) {
             g.p = p;
             g.pref = pref;
             g.L = L;
+            g.atom_a = ka;
+            g.atom_b = kb;
             for (int q = 0; q < ncoef(L); ++q) g.D[q] = D[q];
             index.emplace(key, (int)acc.size());
             acc.push_back(g);
@@ -691,45 +753,108 @@ static qmt_status build_pairs(qmt_mol* m, cudaStream_t s) {
   QMT_CUDA(cudaMemcpyAsync(m->d_pairs.ptr, pairs.data(), pb, cudaMemcpyHostToDevice, s));
   QMT_CUDA(cudaMemcpyAsync(m->d_pairs.as<uint8_t>() + ((pb + 255) / 256) * 256, dco.data(), db,
                            cudaMemcpyHostToDevice, s));
-  // FP32 copy: centres relative to the centroid, pref * D_tuv as the coefficients; then the
-  // nuclei, relative to the same point and rounded the same way
+  // FP32 tables (Gto32Tables): centres relative to the centroid, pref * D_tuv as the coefficients.
   double ref[3] = {0, 0, 0};
   for (int a = 0; a < m->natoms; ++a)
     for (int d = 0; d < 3; ++d) ref[d] += m->coords[3 * a + d] / m->natoms;
-  std::vector<GPair32> p32(pairs.size());
-  std::vector<float> d32(dco.size());
-  for (size_t k = 0; k < pairs.size(); ++k) {
-    const GPair& g = pairs[k];
-    GPair32& q = p32[k];
+  auto to32 = [&](const Acc& g, std::vector<float>& d32) {
+    GPair32 q;
     q.px = (float)(g.px - ref[0]);
     q.py = (float)(g.py - ref[1]);
     q.pz = (float)(g.pz - ref[2]);
     q.p = (float)g.p;
     q.fscale = (float)(0.88622692545275801365 / std::sqrt(g.p));
     q.L = g.L;
-    q.doff = g.doff;
+    q.doff = (int)d32.size();
     q.pad = 0;
-    for (int c = 0; c < ncoef(g.L); ++c) d32[g.doff + c] = (float)(g.pref * dco[g.doff + c]);
+    for (int c = 0; c < ncoef(g.L); ++c) d32.push_back((float)(g.pref * g.D[c]));
+    return q;
+  };
+  std::vector<GPair32> off32, on32;
+  std::vector<float> d32, onp;
+  std::vector<int> on_off(m->natoms + 1, 0), cum_off(m->natoms + 1, 0);
+  std::vector<double> cum;
+  for (int idx : order)   // off-site pairs, already sorted by L
+    if (acc[idx].atom_a != acc[idx].atom_b) off32.push_back(to32(acc[idx], d32));
+  if (off32.empty()) {    // one zero pair keeps the tables well formed
+    Acc z{};
+    z.p = 1.0;
+    off32.push_back(to32(z, d32));
   }
+  std::vector<std::vector<int>> by_atom(m->natoms);
+  for (size_t i = 0; i < acc.size(); ++i)
+    if (acc[i].atom_a == acc[i].atom_b) by_atom[acc[i].atom_a].push_back((int)i);
+  for (int a = 0; a < m->natoms; ++a) {
+    std::vector<int>& v = by_atom[a];
+    // descending exponent: for every point the far-field pairs (p r^2 >= 30) come first
+    std::stable_sort(v.begin(), v.end(), [&](int x, int y) { return (float)acc[x].p > (float)acc[y].p; });
+    on_off[a] = (int)on32.size();
+    cum_off[a] = (int)(cum.size() / 35);
+    std::vector<double> run(35, 0.0);
+    cum.insert(cum.end(), run.begin(), run.end());
+    for (int idx : v) {
+      const Acc& g = acc[idx];
+      on32.push_back(to32(g, d32));
+      onp.push_back((float)g.p);
+      const double f = 0.88622692545275801365 / std::sqrt(g.p) * g.pref;
+      for (int c = 0; c < ncoef(g.L); ++c) run[c] += f * g.D[c];
+      cum.insert(cum.end(), run.begin(), run.end());
+    }
+  }
+  on_off[m->natoms] = (int)on32.size();
+  cum_off[m->natoms] = (int)(cum.size() / 35);
+  std::vector<float> nuc(3 * m->natoms);
   for (int a = 0; a < m->natoms; ++a)
-    for (int d = 0; d < 3; ++d) d32.push_back((float)((double)m->coords[3 * a + d] - ref[d]));
-  const size_t pb32 = p32.size() * sizeof(GPair32), db32 = d32.size() * sizeof(float);
-  if ((st = m->d_pairs32.reserve(pb32 + db32 + 256))) return st;
-  QMT_CUDA(cudaMemcpyAsync(m->d_pairs32.ptr, p32.data(), pb32, cudaMemcpyHostToDevice, s));
-  QMT_CUDA(cudaMemcpyAsync(m->d_pairs32.as<uint8_t>() + ((pb32 + 255) / 256) * 256, d32.data(), db32,
-                           cudaMemcpyHostToDevice, s));
-  m->gto32_nuc_off = dco.size();
-  // pairs are sorted by L: the start of each L's range (an empty table counts as one L = 0 pair)
-  for (int L = 0; L <= 5; ++L) {
-    int k = 0;
-    while (k < (int)p32.size() && p32[k].L < L) ++k;
-    m->gto_lstart[L] = k;
+    for (int d = 0; d < 3; ++d) nuc[3 * a + d] = (float)((double)m->coords[3 * a + d] - ref[d]);
+  if (on32.empty()) {     // keep the device arrays non-empty
+    on32.push_back(GPair32{});
+    onp.push_back(0.f);
   }
+  // one device buffer: off-site pairs | on-site pairs | cum | floats (dco, on-site p, nuclei) | ints
+  auto al = [](size_t b) { return (b + 255) / 256 * 256; };
+  const size_t b_off = al(off32.size() * sizeof(GPair32)), b_on = al(on32.size() * sizeof(GPair32));
+  const size_t b_cum = al(cum.size() * sizeof(double)), b_d = al(d32.size() * sizeof(float));
+  const size_t b_p = al(onp.size() * sizeof(float)), b_nuc = al(nuc.size() * sizeof(float));
+  const size_t b_i = al((on_off.size() + cum_off.size()) * sizeof(int));
+  if ((st = m->d_pairs32.reserve(b_off + b_on + b_cum + b_d + b_p + b_nuc + b_i))) return st;
+  uint8_t* base = m->d_pairs32.as<uint8_t>();
+  std::vector<int> ints(on_off);
+  ints.insert(ints.end(), cum_off.begin(), cum_off.end());
+  size_t o = 0;
+  auto put = [&](const void* src, size_t bytes, size_t span) -> uint8_t* {
+    uint8_t* dst = base + o;
+    o += span;
+    if (bytes && cudaMemcpyAsync(dst, src, bytes, cudaMemcpyHostToDevice, s) != cudaSuccess) return nullptr;
+    return dst;
+  };
+  Gto32Tables& T = m->gto32;
+  T = Gto32Tables{};
+  T.pairs = reinterpret_cast<const GPair32*>(put(off32.data(), off32.size() * sizeof(GPair32), b_off));
+  T.onsite = reinterpret_cast<const GPair32*>(put(on32.data(), on32.size() * sizeof(GPair32), b_on));
+  T.cum = reinterpret_cast<const double*>(put(cum.data(), cum.size() * sizeof(double), b_cum));
+  T.dco = reinterpret_cast<const float*>(put(d32.data(), d32.size() * sizeof(float), b_d));
+  T.onsite_p = reinterpret_cast<const float*>(put(onp.data(), onp.size() * sizeof(float), b_p));
+  T.nuc = reinterpret_cast<const float*>(put(nuc.data(), nuc.size() * sizeof(float), b_nuc));
+  const int* ip = reinterpret_cast<const int*>(put(ints.data(), ints.size() * sizeof(int), b_i));
+  if (!T.pairs || !T.onsite || !T.cum || !T.dco || !T.onsite_p || !T.nuc || !ip)
+    return fail(QMT_CUDA_ERR, "upload of the analytic-potential tables failed");
+  T.onsite_off = ip;
+  T.cum_off = ip + on_off.size();
+  T.rx = ref[0];
+  T.ry = ref[1];
+  T.rz = ref[2];
+  for (int L = 0; L <= 5; ++L) {   // off-site pairs are sorted by L
+    int k = 0;
+    while (k < (int)off32.size() && off32[k].L < L) ++k;
+    T.lstart[L] = k;
+  }
+  // slices of about equal work (pair terms cost about 12 + 2 ncoef(L) operations)
+  std::vector<double> w(off32.size() + 1, 0.0);
+  for (size_t k = 0; k < off32.size(); ++k) w[k + 1] = w[k] + 12.0 + 2.0 * ncoef(off32[k].L);
+  m->gto32_work = w;
   QMT_CUDA(cudaStreamSynchronize(s));
   m->gto_npairs = (int)pairs.size();
   m->gto_doff_bytes = ((pb + 255) / 256) * 256;
-  m->gto32_doff_bytes = ((pb32 + 255) / 256) * 256;
-  for (int d = 0; d < 3; ++d) m->gto_ref[d] = ref[d];
   m->gto_ready = true;
   return QMT_OK;
 }
@@ -741,14 +866,27 @@ static qmt_status run_gto(qmt_mol* m, const GtoPoints& gp, float* out, cudaStrea
   if (g_gto_prec == QMT_PREC_FP32) {
     const float* tab32 = nullptr;
     if ((st = boys_table32(&tab32))) return st;
-    const GPair32* p32 = m->d_pairs32.as<GPair32>();
-    const float* d32 = reinterpret_cast<const float*>(m->d_pairs32.as<uint8_t>() + m->gto32_doff_bytes);
-    const int64_t blocks = (gp.npts + GTO32_POINTS - 1) / GTO32_POINTS;
-    PairRanges pr;
-    for (int L = 0; L <= 5; ++L) pr.lstart[L] = m->gto_lstart[L];
-    gto32_kernel<<<(unsigned)blocks, GTO32_THREADS, 0, s>>>(p32, pr, d32, tab32, m->view(), d32 + m->gto32_nuc_off,
-                                                            m->gto_ref[0], m->gto_ref[1], m->gto_ref[2], gp, out);
-    QMT_CHECK_LAUNCH("gto32_kernel");
+    // enough CTAs to fill the device: the off-site pairs are split into slices whose FP64 partial
+    // sums the second kernel adds in slice order (deterministic)
+    const int64_t pblocks = (gp.npts + GTO32_POINTS - 1) / GTO32_POINTS;
+    const int64_t want = (int64_t)sm_count() * 12;
+    const int nslice = (int)std::max<int64_t>(1, std::min<int64_t>(16, (want + pblocks - 1) / pblocks));
+    Gto32Tables T = m->gto32;
+    T.nslice = nslice;
+    const std::vector<double>& w = m->gto32_work;
+    const int npairs = (int)w.size() - 1;
+    for (int k = 0, j = 0; k <= nslice; ++k) {   // slice k starts at the first pair past k/nslice of the work
+      const double target = w.back() * k / nslice;
+      while (j < npairs && w[j] < target) ++j;
+      T.slice[k] = k == nslice ? npairs : j;
+    }
+    if ((st = m->d_gto_part.reserve((size_t)nslice * gp.npts * sizeof(double)))) return st;
+    double* part = m->d_gto_part.as<double>();
+    gto32_pairs_kernel<<<dim3((unsigned)pblocks, (unsigned)nslice), GTO32_THREADS, 0, s>>>(T, tab32, gp, part);
+    QMT_CHECK_LAUNCH("gto32_pairs_kernel");
+    const int64_t ablocks = (gp.npts + GTO32_THREADS - 1) / GTO32_THREADS;
+    gto32_atoms_kernel<<<(unsigned)ablocks, GTO32_THREADS, 0, s>>>(T, tab32, m->view(), gp, part, out);
+    QMT_CHECK_LAUNCH("gto32_atoms_kernel");
     return QMT_OK;
   }
   const double* tab = nullptr;

@@ -18,7 +18,8 @@
 // CTA order, so the residual is deterministic, and every CTA takes the same stop decision.
 //
 // Small grids (a plane of at most 4096 points, at most 4 planes per CTA of a 16-CTA cluster:
-// the 64^3 grid of the small-molecule configuration) run as one thread-block cluster instead:
+// the 64^3 grid of the small-molecule configuration) can run as one thread-block cluster instead
+// (the automatic choice for the Dirichlet update):
 // the field lives in the CTAs' shared memory (two buffers of each CTA's z-slab), each thread
 // keeps its column of four-point groups and their charges in registers, neighbours come from
 // registers (z inside the slab), warp shuffles (x), shared memory (y, x across warps) and the
@@ -421,165 +422,7 @@ __global__ void __launch_bounds__(JAC_CLUSTER_THREADS, 1) jacobi_cluster_kernel(
   }
 }
 
-// ---- temporal blocking ---------------------------------------------------------------------------
-// Grids small enough that every 32 x 8 x 8 tile gets its own CTA (the 64^3 grid: 128 tiles): each
-// CTA loads its tile and a halo of TB_H points on every interior side into shared memory (V, a second
-// buffer and Q), runs up to TB_H sweeps there -- the updatable region shrinks by one point per sweep
-// on interior sides, points on the grid's outer shell never need neighbours -- and writes its tile
-// back.  One grid barrier per TB_H sweeps instead of per sweep.  Same jac_point, so the grid is
-// identical to the other kernels'.  Intervals end at every check sweep, so the residual (FP64
-// sum |V' - V| of the check sweep over the owned points, CTA sums added in CTA order) and the stop
-// decision are those of the other kernels.
-constexpr int TB_TX = 32, TB_TY = 8, TB_TZ = 8, TB_H = 4;
-constexpr int TB_RX = TB_TX + 2 * TB_H, TB_RY = TB_TY + 2 * TB_H, TB_RZ = TB_TZ + 2 * TB_H;
-constexpr int TB_REG = TB_RX * TB_RY * TB_RZ;   // 10,240 points
-constexpr int TB_THREADS = 256;
-
-template <bool DIRICHLET>
-__global__ void __launch_bounds__(TB_THREADS, 1) jacobi_tb_kernel(JacobiArgs a) {
-  extern __shared__ float tbs[];
-  float* bufs[2] = {tbs, tbs + TB_REG};
-  float* qs = tbs + 2 * TB_REG;
-  __shared__ double red[TB_THREADS / 32];
-  const int nx = a.nx, ny = a.ny, nz = a.nz;
-  const int lane = threadIdx.x & 31, wy = threadIdx.x >> 5;
-  const int ntx = (nx + TB_TX - 1) / TB_TX, nty = (ny + TB_TY - 1) / TB_TY;
-  const int tile = blockIdx.x;   // one tile per CTA (checked on the host)
-  const int x0 = (tile % ntx) * TB_TX, y0 = ((tile / ntx) % nty) * TB_TY, z0 = (tile / (ntx * nty)) * TB_TZ;
-  const int x1 = min(nx, x0 + TB_TX), y1 = min(ny, y0 + TB_TY), z1 = min(nz, z0 + TB_TZ);
-  // the loaded region, clipped to the grid
-  const int lx = max(0, x0 - TB_H), ly = max(0, y0 - TB_H), lz = max(0, z0 - TB_H);
-  const int hx = min(nx, x1 + TB_H), hy = min(ny, y1 + TB_H), hz = min(nz, z1 + TB_H);
-  const int rx = hx - lx, ry = hy - ly, rz = hz - lz;
-  const int rxy = rx * ry;
-  const int64_t plane = (int64_t)nx * ny;
-  int* flag = a.out + 2;
-  const unsigned nb = gridDim.x;
-  // the source terms of the region, once
-  for (int k = threadIdx.x; k < rxy * rz; k += TB_THREADS) {
-    const int x = k % rx, y = (k / rx) % ry, z = k / rxy;
-    qs[k] = jac_source<DIRICHLET>(__ldg(a.Q + (lz + z) * plane + (int64_t)(ly + y) * nx + (lx + x)), a.h, a.src_scale);
-  }
-  const float* gsrc = a.V;
-  float* gdst = a.T;
-  int sweeps = 0, pairs = 0, status = 0;
-  double delta = INFINITY;
-  bool in_T = false;   // the current grid is in T
-  while (sweeps + 2 <= a.max_sweeps) {
-    // sweeps of this interval: up to TB_H, ending at the next check sweep
-    int n = 0, chk = 0;
-    while (n < TB_H && sweeps + n + 2 <= a.max_sweeps) {
-      const int p = pairs + n / 2 + 1;
-      n += 2;
-      if (p % a.check_every == 0 || sweeps + n + 2 > a.max_sweeps) {
-        chk = 1;
-        break;
-      }
-    }
-    for (int k = threadIdx.x; k < rxy * rz; k += TB_THREADS) {
-      const int x = k % rx, y = (k / rx) % ry, z = k / rxy;
-      bufs[0][k] = __ldcg(gsrc + (lz + z) * plane + (int64_t)(ly + y) * nx + (lx + x));
-    }
-    __syncthreads();
-    double ds = 0.0;
-    for (int j = 1; j <= n; ++j) {
-      const float* src = bufs[(j - 1) & 1];
-      float* dst = bufs[j & 1];
-      // updatable at sweep j: interior sides shrink by j, sides on the grid boundary do not
-      const int ux0 = lx > 0 ? lx + j : 0, ux1 = hx < nx ? hx - j : nx;
-      const int uy0 = ly > 0 ? ly + j : 0, uy1 = hy < ny ? hy - j : ny;
-      const int uz0 = lz > 0 ? lz + j : 0, uz1 = hz < nz ? hz - j : nz;
-      const bool last_chk = chk && j == n;
-      for (int z = uz0; z < uz1; ++z)
-        for (int y = uy0 + wy; y < uy1; y += TB_THREADS / 32)
-          for (int x = ux0 + lane; x < ux1; x += 32) {
-            const int k = (z - lz) * rxy + (y - ly) * rx + (x - lx);
-            const float vc = src[k];
-            const bool edge = x == 0 || x == nx - 1 || y == 0 || y == ny - 1 || z == 0 || z == nz - 1;
-            float o;
-            if (edge) {
-              o = jac_point<DIRICHLET>(0.f, 0.f, 0.f, 0.f, 0.f, 0.f, 0.f, vc, true);
-            } else {
-              o = jac_point<DIRICHLET>(src[k - 1], src[k + 1], src[k + rx], src[k - rx], src[k + rxy], src[k - rxy],
-                                       qs[k], vc, false);
-            }
-            dst[k] = o;
-            if (last_chk && x >= x0 && x < x1 && y >= y0 && y < y1 && z >= z0 && z < z1)
-              ds += fabs((double)o - (double)vc);
-          }
-      __syncthreads();
-    }
-    // the owned tile back to global memory
-    const float* fin = bufs[n & 1];
-    for (int z = z0; z < z1; ++z)
-      for (int y = y0 + wy; y < y1; y += TB_THREADS / 32)
-        for (int x = x0 + lane; x < x1; x += 32)
-          __stcg(gdst + z * plane + (int64_t)y * nx + x, fin[(z - lz) * rxy + (y - ly) * rx + (x - lx)]);
-    sweeps += n;
-    pairs += n / 2;
-    if (chk) {
-      double v = ds;
-      for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
-      if (lane == 0) red[wy] = v;
-      __syncthreads();
-      if (threadIdx.x == 0) {
-        double r = 0.0;
-        for (int w = 0; w < TB_THREADS / 32; ++w) r += red[w];
-        __stcg(a.part + blockIdx.x, r);
-      }
-    }
-    if (!grid_barrier(a.bar, flag, nb, a.wait_ns)) {
-      status = 3;
-      break;
-    }
-    in_T = !in_T;
-    gsrc = in_T ? a.T : a.V;
-    gdst = in_T ? a.V : a.T;
-    if (chk) {
-      if (blockIdx.x == 0 && threadIdx.x == 0) {
-        double r = 0.0;
-        for (unsigned b = 0; b < nb; ++b) r += __ldcg(a.part + b);
-        __stcg(a.res, r);
-      }
-      if (!grid_barrier(a.bar, flag, nb, a.wait_ns)) {
-        status = 3;
-        break;
-      }
-      delta = __ldcg(a.res);
-      if (!isfinite(delta)) {
-        status = 2;
-        break;
-      }
-      if (delta <= a.tol) {
-        status = 1;
-        break;
-      }
-    }
-  }
-  // the result belongs in V: copy the owned tile over when it ended in T
-  if (in_T && status != 3) {
-    for (int z = z0; z < z1; ++z)
-      for (int y = y0 + wy; y < y1; y += TB_THREADS / 32)
-        for (int x = x0 + lane; x < x1; x += 32) {
-          const int64_t g = z * plane + (int64_t)y * nx + x;
-          __stcg(a.V + g, __ldcg(a.T + g));
-        }
-  }
-  if (blockIdx.x == 0 && threadIdx.x == 0) {
-    a.out[0] = sweeps;
-    a.out[1] = status;
-    __stcg(a.res + 1, delta);
-  }
-}
-
-// Tiles of the temporal-blocking kernel for this grid, or 0 if it does not apply (more tiles than
-// CTAs that fit on the device at once).
-static int tb_tiles(int nx, int ny, int nz) {
-  const int nt = ((nx + TB_TX - 1) / TB_TX) * ((ny + TB_TY - 1) / TB_TY) * ((nz + TB_TZ - 1) / TB_TZ);
-  return nt <= sm_count() ? nt : 0;
-}
-
-static int g_jacobi_path = 0;   // 0 automatic, 1 grid barrier per sweep, 2 single cluster, 3 temporal blocking
+static int g_jacobi_path = 0;   // 0 automatic, 1 grid barrier per sweep, 2 single cluster
 
 // Planes per CTA of the cluster kernel for this grid (1, 2 or 4), or 0 if it does not apply.
 static int cluster_planes(int nx, int ny, int nz, const float* rho, const float* v) {
@@ -669,8 +512,7 @@ static qmt_status run_jacobi(int nx, int ny, int nz, float step, const float* rh
 
   // scratch: CTA partial sums, barrier words, residuals, status words (grows, never freed)
   static thread_local DevBuf scratch;
-  // (the temporal-blocking kernel runs one CTA per tile, at most one per SM)
-  const size_t part_bytes = ((size_t)std::max(grid, nsm) * sizeof(double) + 255) / 256 * 256;
+  const size_t part_bytes = ((size_t)grid * sizeof(double) + 255) / 256 * 256;
   qmt_status st = scratch.reserve(part_bytes + 256);
   if (st) return st;
   uint8_t* base = scratch.as<uint8_t>();
@@ -681,24 +523,11 @@ static qmt_status run_jacobi(int nx, int ny, int nz, float step, const float* rh
   QMT_CUDA(cudaMemsetAsync(base + part_bytes, 0, 256, s));
   if (max_sweeps >= 2) {
     bool done = false;
-    const int ntb = (g_jacobi_path == 0 || g_jacobi_path == 3) ? tb_tiles(nx, ny, nz) : 0;
-    if (g_jacobi_path == 3 && !ntb) return fail(QMT_BAD_ARG, "the temporal-blocking Jacobi kernel does not apply to this grid");
-    if (ntb) {
-      auto tk = jacobi_tb_kernel<DIRICHLET>;
-      const size_t smem = 3ull * TB_REG * sizeof(float);
-      QMT_CUDA(cudaFuncSetAttribute(tk, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
-      int fit = 0;
-      QMT_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&fit, tk, TB_THREADS, smem));
-      if (fit >= 1) {
-        void* params[] = {&a};
-        QMT_CUDA(cudaLaunchCooperativeKernel((const void*)tk, dim3(ntb), dim3(TB_THREADS), params, smem, s));
-        note_launches(1);
-        done = true;
-      } else if (g_jacobi_path == 3) {
-        return fail(QMT_CUDA_ERR, "temporal-blocking Jacobi kernel does not fit on an SM");
-      }
-    }
-    const int P = (g_jacobi_path == 2) ? cluster_planes(nx, ny, nz, rho, v) : 0;
+    // the cluster kernel where it applies: for the Dirichlet update (measured 3.8 against 4.2 us per
+    // 64^3 sweep); the reference update's IEEE division makes it issue-bound on its 16 SMs (4.5
+    // against 4.3 us), so automatic selection leaves that one on the grid-barrier kernel
+    const bool want_cluster = g_jacobi_path == 2 || (g_jacobi_path == 0 && DIRICHLET);
+    const int P = want_cluster ? cluster_planes(nx, ny, nz, rho, v) : 0;
     if (!done && P > 0 && (st = try_cluster<DIRICHLET>(a, P, s, &done))) return st;
     if (g_jacobi_path == 2 && !done)
       return fail(QMT_BAD_ARG, "the single-cluster Jacobi kernel does not apply to this grid or device");
@@ -741,10 +570,8 @@ extern "C" qmt_status qmt_jacobi_dirichlet(int nx, int ny, int nz, float step, c
 }
 
 extern "C" qmt_status qmt_set_jacobi_path(int mode) {
-  if (mode < 0 || mode > 3)
-    return fail(QMT_BAD_ARG,
-                "Jacobi path must be 0 (automatic), 1 (grid barrier per sweep), 2 (single cluster) or 3 (temporal "
-                "blocking)");
+  if (mode < 0 || mode > 2)
+    return fail(QMT_BAD_ARG, "Jacobi path must be 0 (automatic), 1 (grid barrier per sweep) or 2 (single cluster)");
   g_jacobi_path = mode;
   return QMT_OK;
 }

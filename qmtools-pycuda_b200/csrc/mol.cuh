@@ -3,6 +3,7 @@
 
 #include <vector>
 
+#include "gto.cuh"
 #include "qmt_common.cuh"
 
 namespace qmt {
@@ -53,17 +54,15 @@ struct qmt_mol {
   qmt::DevBuf d_Phi_hi, d_Phi_lo;
   // scratch
   qmt::DevBuf d_partials, d_scalars, d_work;
-  // analytic potential: primitive-pair table (FP64), and its FP32 copy with centres relative to
-  // gto_ref and the density matrix folded into the Hermite coefficients
+  // analytic potential: primitive-pair table (FP64), and the FP32 kernels' tables (gto.cu)
   bool gto_ready = false;
   int gto_npairs = 0;
   size_t gto_doff_bytes = 0;
   qmt::DevBuf d_pairs;
-  size_t gto32_doff_bytes = 0;
-  size_t gto32_nuc_off = 0;     // float offset of the nuclei (relative to gto_ref) after the coefficients
-  int gto_lstart[6] = {0, 0, 0, 0, 0, 0};   // pairs of angular momentum L: [gto_lstart[L], gto_lstart[L+1])
-  double gto_ref[3] = {0, 0, 0};
-  qmt::DevBuf d_pairs32;
+  qmt::DevBuf d_pairs32;        // storage of gto32 (device pointers into it)
+  qmt::Gto32Tables gto32{};
+  std::vector<double> gto32_work;   // cumulative estimated work of the off-site pairs
+  qmt::DevBuf d_gto_part;       // FP64 partial sums of the off-site pair slices
 
   ~qmt_mol();
   qmt_status upload_coords(const float* c, cudaStream_t s);

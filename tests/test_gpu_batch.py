@@ -26,9 +26,14 @@ def mols(basis):
     return out
 
 
-def _single(mol, g, m_lengths):
+def _single(mol, g, m_lengths, path):
+    """One molecule through the facade, on the density path the batch's tuner chose for it."""
     import torch
-    q = qmtools.QMTools.Compute_density(g, mol, precision="fp16x3", copyBack=False)
+    N.call("qmt_set_density_path", int(path))
+    try:
+        q = qmtools.QMTools.Compute_density(g, mol, precision="fp16x3", copyBack=False)
+    finally:
+        N.call("qmt_set_density_path", 0)
     nx, ny, nz, h, ox, oy, oz = g._geom()
     v = torch.empty(nx * ny * nz, device="cuda")
     mx, my, mz = m_lengths
@@ -37,22 +42,28 @@ def _single(mol, g, m_lengths):
     return q.field(0).cpu().numpy(), v.cpu().numpy().reshape(nx, ny, nz)
 
 
-def test_batch_equals_single_molecule_evaluations(mols, tmp_path):
-    tuner = Tuner(path=tmp_path / "tune.json")
+@pytest.mark.parametrize("measure", [False, True], ids=["default_paths", "tuned_paths"])
+def test_batch_equals_single_molecule_evaluations(mols, tmp_path, measure):
+    """Default paths put the four small molecules on one persistent fused launch; measured paths
+    follow the tuner's choices."""
+    tuner = Tuner(path=tmp_path / "tune.json", measure=measure)
     ev = BatchEvaluator([m for _, m, _ in mols], [g for _, _, g in mols], tuner=tuner)
     try:
-        assert ev.fused_count >= 3                      # the small molecules share one launch
         assert ev.paths[3] == PATH_STAGED               # N > 320
+        assert ev.fused_count == sum(1 for p in ev.paths if p == PATH_FUSED)
+        if not measure:
+            assert ev.fused_count == 4
         for rep in range(2):                            # two graph replays
             ev.run()
             ev.synchronize()
             for i, (sm, mol, g) in enumerate(mols):
-                q1, v1 = _single(mol, g, ev.fft_lengths[i])
+                q1, v1 = _single(mol, g, ev.fft_lengths[i], ev.paths[i])
                 assert np.array_equal(ev.density(i), q1), (rep, i)
                 assert np.array_equal(ev.potential(i), v1), (rep, i)
         sums = ev.sums()
         assert np.all(np.isfinite(sums)) and np.all(sums > 0)
-        assert (tmp_path / "tune.json").exists() and tuner.measured > 0
+        if measure:
+            assert (tmp_path / "tune.json").exists() and tuner.measured > 0
     finally:
         ev.close()
 
@@ -73,7 +84,7 @@ def test_batch_graph_follows_new_density_matrices(mols, tmp_path):
         ev.run()
         ev.synchronize()
         for i, (_, m, g) in enumerate(sel):
-            q1, v1 = _single(m, g, ev.fft_lengths[i])
+            q1, v1 = _single(m, g, ev.fft_lengths[i], ev.paths[i])
             assert np.array_equal(ev.density(i), q1)
             assert np.array_equal(ev.potential(i), v1)
         for (_, m, _), dm in zip(sel, saved):

@@ -174,11 +174,10 @@ def _jacobi_call(name, shape, h, rho, v, t, sweeps, check_every=100, tol=0.0):
 @pytest.mark.parametrize("mode", ["qmt_jacobi", "qmt_jacobi_dirichlet"])
 @pytest.mark.parametrize("shape", [(64, 64, 64), (32, 48, 40), (16, 16, 17), (8, 8, 2)])
 def test_jacobi_kernels_give_identical_grids(mode, shape):
-    """The persistent grid-barrier kernel, the single-cluster kernel (field in the CTAs' shared
-    memory, cluster barrier per sweep) and the temporal-blocking kernel (four sweeps per grid
-    barrier on haloed tiles) give identical grids: slabs of 4, 3, 2 and 1 planes per CTA (a ragged
-    last slab), x neighbours across warp boundaries (nx = 32, 16, 8), partial tiles, an interval
-    cut short by the check sweep schedule (302 sweeps, a check every 25 pairs)."""
+    """The persistent grid-barrier kernel and the single-cluster kernel (field in the CTAs' shared
+    memory, cluster barrier per sweep) give identical grids: slabs of 4, 3, 2 and 1 planes per CTA
+    (a ragged last slab), x neighbours across warp boundaries (nx = 32, 16, 8), 302 sweeps with a
+    check every 25 pairs."""
     import torch
     from qmtools import _native as N
     N.ensure_device()
@@ -187,7 +186,7 @@ def test_jacobi_kernels_give_identical_grids(mode, shape):
     rho = torch.rand(n, device="cuda", generator=g) - 0.5
     v0 = torch.rand(n, device="cuda", generator=g)
     out = {}
-    for path in (1, 2, 3):
+    for path in (1, 2):
         N.call("qmt_set_jacobi_path", path)
         try:
             v = v0.clone()
@@ -198,14 +197,13 @@ def test_jacobi_kernels_give_identical_grids(mode, shape):
         assert st == N.OK, (path, N.load().qmt_last_error())
         assert sw == 302
         out[path] = (v.cpu().numpy(), dl)
-    for path in (2, 3):
-        assert np.array_equal(out[1][0], out[path][0]), path
-        assert abs(out[1][1] - out[path][1]) <= 1e-12 * abs(out[1][1]), path
+    assert np.array_equal(out[1][0], out[2][0])
+    assert abs(out[1][1] - out[2][1]) <= 1e-12 * abs(out[1][1])
 
 
 def test_jacobi_kernels_stop_at_tolerance():
-    """The cluster and temporal-blocking kernels' FP64 residual stops the solve at the first check
-    below tol, like the grid-barrier kernel."""
+    """The cluster kernel's FP64 residual stops the solve at the first check below tol, like the
+    grid-barrier kernel."""
     import torch
     from qmtools import _native as N
     N.ensure_device()
@@ -213,7 +211,7 @@ def test_jacobi_kernels_stop_at_tolerance():
     rho = torch.zeros(64 ** 3, device="cuda")
     v0 = torch.rand(64 ** 3, device="cuda")
     res = {}
-    for path in (1, 2, 3):
+    for path in (1, 2):
         N.call("qmt_set_jacobi_path", path)
         try:
             v = v0.clone()
@@ -224,6 +222,5 @@ def test_jacobi_kernels_stop_at_tolerance():
             N.call("qmt_set_jacobi_path", 0)
         assert st == N.OK and dl <= 50.0 and sw % 20 == 0
         res[path] = (sw, v.cpu().numpy())
-    for path in (2, 3):
-        assert res[1][0] == res[path][0]
-        assert np.array_equal(res[1][1], res[path][1])
+    assert res[1][0] == res[2][0]
+    assert np.array_equal(res[1][1], res[2][1])
