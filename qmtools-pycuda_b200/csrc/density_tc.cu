@@ -578,9 +578,11 @@ struct FusedParams {
 // production items the rest, so that molecules with different atom counts share the barriers.
 constexpr uint32_t CHUNK_COUNT = 1024;
 
-// The molecule of global tile t (binary search over the launch's molecules).
+// The molecule of global tile t: p.one in a single-molecule launch (MULTI false: read from the
+// parameter space), else a binary search over the launch's molecules.
+template <bool MULTI>
 __device__ __forceinline__ const FusedMol& fused_mol(const FusedParams& p, int64_t t, int& m) {
-  if (p.nmol == 1) {
+  if (!MULTI) {
     m = 0;
     return p.one;
   }
@@ -1124,6 +1126,7 @@ constexpr int FUSED_THREADS = 64 + FUSED_NCT;  // + U-producer warp + MMA warp
 // U producer: streams the K-step blocks of U into the stage ring (one bulk copy per stage and
 // piece, already in the 32-byte swizzled layout; stage slots and r0 are multiples of 256 bytes
 // and 16 rows).  On an abort it waits (bounded) for its copies in flight before returning.
+template <bool MULTI>
 __device__ __forceinline__ void fused_produce_u(const FusedParams* pp, uint8_t* stages, uint64_t* full_bar,
                                              uint64_t* empty_bar, volatile int* abort_flag) {
   const FusedParams& p = *pp;
@@ -1132,7 +1135,7 @@ __device__ __forceinline__ void fused_produce_u(const FusedParams* pp, uint8_t* 
   bool ok = true;
   for (int64_t t = blockIdx.x; t < p.ntiles && ok; t += gridDim.x) {
     int m;
-    const FusedMol& M = fused_mol(p, t, m);
+    const FusedMol& M = fused_mol<MULTI>(p, t, m);
     // the molecule's values in registers for the tile: read through a reference, they would be
     // reloaded after every barrier operation (each an asm statement that clobbers memory)
     const int ksteps = M.ksteps, u_rows = M.u_rows;
@@ -1163,6 +1166,7 @@ __device__ __forceinline__ void fused_produce_u(const FusedParams* pp, uint8_t* 
 // MMA issuer: per tile, per K-step (after its column chunk of A is complete and its U stage has
 // landed) the split products T' += A_hi U_hi + A_hi U_lo + A_lo U_hi into TMEM; frees the stage
 // with a commit, and signals t_full after the tile's last K-step.
+template <bool MULTI>
 __device__ __forceinline__ void fused_issue_mma(const FusedParams* pp, uint32_t abase, uint32_t lbase, uint8_t* stages,
                                              uint32_t tmem, uint64_t* full_bar, uint64_t* empty_bar,
                                              uint64_t* chunk_bar, uint64_t* t_full, uint64_t* drain_bar,
@@ -1173,7 +1177,7 @@ __device__ __forceinline__ void fused_issue_mma(const FusedParams* pp, uint32_t 
   bool ok = true;
   for (int64_t t = blockIdx.x; t < p.ntiles && ok; t += gridDim.x) {
     int m;
-    const FusedMol& M = fused_mol(p, t, m);
+    const FusedMol& M = fused_mol<MULTI>(p, t, m);
     // the molecule's values in registers for the tile (see the producer)
     const int ksteps = M.ksteps, n16 = M.n16, tail0 = M.tail0;
     uint32_t need = 0;
@@ -1230,7 +1234,7 @@ __device__ __forceinline__ void fused_issue_mma(const FusedParams* pp, uint32_t 
   mbar_wait_drain(drain_bar, 0u, 500000000ull);
 }
 
-template <int FMT>
+template <int FMT, bool MULTI>
 __global__ void __launch_bounds__(FUSED_THREADS, 1)
     density_fused_kernel(const __grid_constant__ FusedParams p) {
   extern __shared__ uint8_t smem_dyn[];
@@ -1265,7 +1269,10 @@ __global__ void __launch_bounds__(FUSED_THREADS, 1)
       mbar_init(&full_bar[s], 1);
       mbar_init(&empty_bar[s], 1);
     }
-    for (int c = 0; c < MAX_FUSED_CHUNKS; ++c) mbar_init(&chunk_bar[c], CHUNK_COUNT);
+    // a single molecule's barriers count its own production items; a batch's count CHUNK_COUNT,
+    // the difference pre-arrived per tile
+    for (int c = 0; c < MAX_FUSED_CHUNKS; ++c)
+      mbar_init(&chunk_bar[c], MULTI ? CHUNK_COUNT : (uint32_t)max(1, p.one.chunk_need[c]));
     mbar_init(&t_full, 1);
     mbar_init(&drain_bar, 1);
     fence_mbar_init();
@@ -1288,10 +1295,10 @@ __global__ void __launch_bounds__(FUSED_THREADS, 1)
   const uint32_t tmem = tmem_slot;
 
   if (warp == 0) {
-    if (lane == 0) fused_produce_u(&p, stages, full_bar, empty_bar, &abort_flag);
+    if (lane == 0) fused_produce_u<MULTI>(&p, stages, full_bar, empty_bar, &abort_flag);
   } else if (warp == 1) {
     if (lane == 0)
-      fused_issue_mma(&p, smem_u32(A_hi), smem_u32(A_lo), stages, tmem, full_bar, empty_bar, chunk_bar, &t_full,
+      fused_issue_mma<MULTI>(&p, smem_u32(A_hi), smem_u32(A_lo), stages, tmem, full_bar, empty_bar, chunk_bar, &t_full,
                       &drain_bar, &abort_flag);
   } else {
     const int ct = threadIdx.x - 64;           // compute thread 0 .. FUSED_NCT-1
@@ -1302,12 +1309,13 @@ __global__ void __launch_bounds__(FUSED_THREADS, 1)
     const int row = q * 32 + lane;
     uint32_t tile_it = 0;
     int cur_m = -1;
-    const float2* pr_s = nullptr;
-    const int* ash_s = nullptr;
-    const float* crd_s = nullptr;
+    // table pointers, derived from the shared-memory base (a single molecule's never change)
+    const float2* pr_s = reinterpret_cast<const float2*>(tabs + (MULTI ? 0 : p.one.off_prim));
+    const int* ash_s = reinterpret_cast<const int*>(tabs + (MULTI ? 0 : p.one.off_ashell));
+    const float* crd_s = reinterpret_cast<const float*>(tabs + (MULTI ? 0 : p.one.off_coords));
     for (int64_t t = blockIdx.x; t < p.ntiles; t += gridDim.x, ++tile_it) {
       int m;
-      const FusedMol& M = fused_mol(p, t, m);
+      const FusedMol& M = fused_mol<MULTI>(p, t, m);
       const int64_t lt = t - M.tile0;          // tile within the molecule
       const int natoms = M.natoms, n16 = M.n16, tail0 = M.tail0;   // (in registers, see the producer)
       if (m != cur_m) {
@@ -1323,9 +1331,11 @@ __global__ void __launch_bounds__(FUSED_THREADS, 1)
           if (two) *reinterpret_cast<uint16_t*>(A_lo + off) = 0;
         }
         asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
-        pr_s = reinterpret_cast<const float2*>(tabs + M.off_prim);
-        ash_s = reinterpret_cast<const int*>(tabs + M.off_ashell);
-        crd_s = reinterpret_cast<const float*>(tabs + M.off_coords);
+        if (MULTI) {
+          pr_s = reinterpret_cast<const float2*>(tabs + M.off_prim);
+          ash_s = reinterpret_cast<const int*>(tabs + M.off_ashell);
+          crd_s = reinterpret_cast<const float*>(tabs + M.off_coords);
+        }
         cur_m = m;
       }
       // ---- Phi' for the tile into A -------------------------------------------------------
@@ -1340,8 +1350,9 @@ __global__ void __launch_bounds__(FUSED_THREADS, 1)
       if (ct == 0) {
         item_ctr = 0;
         // the arrivals that this molecule's production does not make
-        for (int c = 0; c < M.nchunks; ++c)
-          if (M.chunk_need[c] > 0) mbar_arrive_count(&chunk_bar[c], CHUNK_COUNT - (uint32_t)M.chunk_need[c]);
+        if (MULTI)
+          for (int c = 0; c < M.nchunks; ++c)
+            if (M.chunk_need[c] > 0) mbar_arrive_count(&chunk_bar[c], CHUNK_COUNT - (uint32_t)M.chunk_need[c]);
       }
       named_barrier(1, FUSED_NCT);
       // work item = (atom, half of the rows), taken in atom order from a shared counter so that
@@ -1581,7 +1592,7 @@ static int fused_stages(const TcShape& sh, int n16, int tab_bytes) {
   cudaGetDevice(&dev);
   cudaDeviceGetAttribute(&maxsm, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev);
   cudaFuncAttributes fa;
-  if (cudaFuncGetAttributes(&fa, density_fused_kernel<FMT>) != cudaSuccess) return 0;
+  if (cudaFuncGetAttributes(&fa, density_fused_kernel<FMT, true>) != cudaSuccess) return 0;
   const long a_bytes = fused_a_bytes(n16), stage_bytes = (long)sh.nsplit * fused_b_slot(n16);
   const long avail = (long)maxsm - (long)fa.sharedSizeBytes - 1024 - sh.nsplit * a_bytes - tab_bytes;
   return (int)std::max<long>(0, std::min<long>(MAX_STAGES, avail / stage_bytes));
@@ -1639,7 +1650,7 @@ static qmt_status launch_fused(FusedParams& p, const TcShape& sh_max, int n16_ma
   p.stage_bytes = p.nsplit * p.b_slot;
   p.fmt = (uint32_t)sh_max.fmt;
   p.wait_ns = wait_limit_ns();
-  auto kern = density_fused_kernel<FMT>;
+  auto kern = p.nmol > 1 ? density_fused_kernel<FMT, true> : density_fused_kernel<FMT, false>;
   const int stages = fused_stages<FMT>(sh_max, n16_max, tab_bytes_max);
   if (stages < 2) return fail(QMT_BAD_ARG, "fused density tile does not fit in shared memory");
   p.stages = stages;

@@ -10,16 +10,29 @@
 //     V(C) = -sum_pairs (2 pi / p) sum_tuv D_tuv R_tuv(p, P - C) + sum_A Z_A / |C - R_A|,
 // with R_tuv from Boys functions F_0..F_L (table + Taylor, downward recursion).
 //
-// Two kernels evaluate it.  gto32_kernel (the default) works in FP32 and accumulates in FP64:
-// where T = p |P - C|^2 >= 30 (99.5% of the point-pair terms on the boundary of the medium
-// molecule's grid) the Boys functions take their asymptotic form
-//     (-2p)^n F_n(T) = sqrt(pi) / (2 sqrt(p)) * (-1)^n (2n-1)!! / r^(2n+1)
-// (relative error below e^-T T^(L-1/2) < 2e-9 for L <= 4), so a term costs one reciprocal square
-// root and the Hermite recursion; nearer terms use an FP32 table with Taylor terms and downward
-// recursion.  Point and pair centres are held relative to the molecule's centroid, the density
-// matrix and prefactor are folded into the FP32 Hermite coefficients, pair terms are summed in
-// FP32 in groups of four and the groups in FP64, and the nuclear term is FP64.  gto_kernel keeps
-// every operation in FP64 (qmt_set_gto_precision selects it).
+// Two evaluations.  The default (gto32_pairs_kernel, gto64_pairs_kernel, gto32_atoms_kernel) is
+// mixed precision:
+//  * pairs of two different atoms are ranked by size (their far-field multipoles); the largest,
+//    which together hold 95% of the total (a few percent of the pairs), are evaluated in FP64
+//    throughout from FP64 coefficients and centres (gto64_pairs_kernel): an FP32 term's error
+//    (rounded coefficients and arithmetic) is proportional to its size, and the potential at a
+//    grid boundary is the small difference of large electronic and nuclear parts;
+//  * the rest (gto32_pairs_kernel): where T = p |P - C|^2 >= 30 (99.5% of the point-pair terms on
+//    the boundary of the medium molecule's grid) the Boys functions take their asymptotic form
+//        (-2p)^n F_n(T) = sqrt(pi) / (2 sqrt(p)) * (-1)^n (2n-1)!! / r^(2n+1)
+//    (relative error below e^-T T^(L-1/2) < 2e-9 for L <= 4): one reciprocal square root and the
+//    Hermite recursion in FP32, summed in FP32 in groups of four and the groups in FP64; nearer
+//    terms in FP64 (a function kept out of line, so the FP32 loop keeps its register count);
+//  * both pair lists are cut into slices over several CTAs whose FP64 partial sums are added in
+//    order (deterministic);
+//  * pairs centred on one atom: kept per atom in descending exponent order with cumulative FP64
+//    moments, so that the far-field ones at a point are one FP64 multipole evaluation about the
+//    nucleus (an FP32 1/r common to an atom's electrons and missing from its nucleus would leave
+//    Z_A * 1e-7 / r of error), the near-field ones in FP64 from FP64 coefficients;
+//  * point and pair centres relative to the molecule's centroid (FP32 for the FP32 terms, FP64
+//    for the others), the density matrix and prefactor folded into the Hermite coefficients; the
+//    nuclear term in FP64.
+// gto_kernel keeps every operation in FP64 (qmt_set_gto_precision selects it; the checker).
 #include <algorithm>
 #include <cstdio>
 #include <string>
@@ -273,8 +286,6 @@ __global__ void __launch_bounds__(GTO_THREADS) gto_kernel(const GPair* __restric
 }
 
 // ---- FP32 kernel with FP64 accumulation -----------------------------------------------------
-constexpr int BOYS32_NT = 301;   // T = 0, 0.1, ..., 30 (the far-field form takes over at 30)
-constexpr int BOYS32_NM = 10;    // m = 0..9: F_L and five Taylor terms for L <= 4
 constexpr float T_FAR = 30.0f;
 
 // R_tuv (t+u+v <= L) from h_j = (-2p)^j F_j, j = 0..L, dotted with D.
@@ -308,16 +319,73 @@ __device__ __forceinline__ float hermite_dot32(const float (&D)[ncoef(L)], float
   return acc;
 }
 
+// FP64 R_tuv (t+u+v <= L) from h_j, dotted with the coefficients D (float or double).
+template <int L, typename DT>
+__device__ __forceinline__ double hermite_dot64(const DT (&D)[ncoef(L)], double X, double Y, double Z,
+                                                const double (&h)[L + 1]) {
+  constexpr int NC = ncoef(L);
+  constexpr HermTable H = make_herm_table();
+  double cur[NC], nxt[NC];
+  cur[0] = h[L];
+#pragma unroll
+  for (int j = L - 1; j >= 0; --j) {
+    nxt[0] = h[j];
+    const int n = ncoef(L - j);
+#pragma unroll
+    for (int k = 1; k < NC; ++k) {
+      if (k < n) {
+        const HermIdx e = H.e[k];
+        const double c = e.dir == 0 ? X : (e.dir == 1 ? Y : Z);
+        double r = c * cur[e.p1];
+        if (e.mult > 0) r = fma((double)e.mult, cur[e.p2], r);
+        nxt[k] = r;
+      }
+    }
+#pragma unroll
+    for (int k = 0; k < NC; ++k) cur[k] = nxt[k];
+  }
+  double acc = 0.0;
+#pragma unroll
+  for (int k = 0; k < NC; ++k) acc = fma((double)D[k], cur[k], acc);
+  return acc;
+}
+
+// The near-field term of an FP32 pair (T < 30) in FP64: Boys functions from the FP64 table, FP64
+// recursion, the FP32 coefficients read from `d`.  Not inlined, so the few near terms do not raise
+// the register count of the FP32 loop around them.
 template <int L>
-__device__ __forceinline__ float pair_term32(const GPair32& g, const float (&D)[ncoef(L)], float cx, float cy,
-                                             float cz, const float* __restrict__ tab) {
+__device__ __noinline__ double near_term(float px, float py, float pz, float p, const float* __restrict__ d, float cx,
+                                         float cy, float cz, const double* __restrict__ tab64) {
+  const double Xd = (double)(px - cx), Yd = (double)(py - cy), Zd = (double)(pz - cz);
+  const double pd = p;
+  const double Td = pd * (Xd * Xd + Yd * Yd + Zd * Zd);   // < 30.001: inside the FP64 table
+  double F[L + 1], h[L + 1];
+  boys_fn<L>(Td, tab64, F);
+  double pw = 1.0;
+#pragma unroll
+  for (int j = 0; j <= L; ++j) {
+    h[j] = pw * F[j];
+    pw *= -2.0 * pd;
+  }
+  float D[ncoef(L)];
+#pragma unroll
+  for (int c = 0; c < ncoef(L); ++c) D[c] = d[c];
+  return hermite_dot64<L>(D, Xd, Yd, Zd, h);
+}
+
+// One FP32 pair's term at a point.  Far field (T = p r^2 >= 30): FP32, returned (the caller sums
+// these in FP32 groups).  Near field: the diffuse pairs at short range in FP64 (near_term), added to
+// `vnear`; 0 is returned.  The near / far test is the FP32 one, the same everywhere.
+template <int L>
+__device__ __forceinline__ float pair_term32(const GPair32& g, const float (&D)[ncoef(L)], const float* d, float cx,
+                                             float cy, float cz, const double* __restrict__ tab64, double& vnear) {
   const float X = g.px - cx, Y = g.py - cy, Z = g.pz - cz;
   const float r2 = fmaf(X, X, fmaf(Y, Y, Z * Z));
   const float T = g.p * r2;
-  float h[L + 1];
-  if (!(T < T_FAR)) {   // (a non-finite T takes this branch too: the table below is never indexed by it)
+  if (!(T < T_FAR)) {   // (a non-finite T takes this branch too: the table is never indexed by it)
     // asymptotic Boys functions: h_j = (-1)^j (2j-1)!! r^-(2j+1), the factor sqrt(pi)/(2 sqrt p)
     // applied to the sum; one Newton step makes the reciprocal square root correctly rounded
+    float h[L + 1];
     float ri = rsqrtf(r2);
     ri = ri * fmaf(-0.5f * r2 * ri, ri, 1.5f);
     const float ri2 = ri * ri;
@@ -326,32 +394,43 @@ __device__ __forceinline__ float pair_term32(const GPair32& g, const float (&D)[
     for (int j = 0; j < L; ++j) h[j + 1] = -(float)(2 * j + 1) * h[j] * ri2;
     return g.fscale * hermite_dot32<L>(D, X, Y, Z, h);
   }
-  // F_L by a five-term Taylor expansion about the nearest tabulated T, then downward recursion
-  const int i = (int)fmaf(T, 10.0f, 0.5f);
-  const float d = T - 0.1f * (float)i;
-  const float* row = tab + i * BOYS32_NM + L;
-  float f = row[5];
+  vnear += near_term<L>(g.px, g.py, g.pz, g.p, d, cx, cy, cz, tab64);
+  return 0.f;
+}
+
+// One pair's term at a point in FP64 throughout (FP64 coefficients): the far field from the
+// asymptotic Boys functions, the near field from the FP64 table.
+template <int L>
+__device__ __forceinline__ double pair_term64(double px, double py, double pz, double p, double fscale,
+                                              const double (&D)[ncoef(L)], double cx, double cy, double cz,
+                                              const double* __restrict__ tab64) {
+  const double X = px - cx, Y = py - cy, Z = pz - cz;
+  const double r2 = X * X + Y * Y + Z * Z;
+  const double T = p * r2;
+  double h[L + 1];
+  if (!(T < 30.0)) {
+    const double ri = rsqrt(r2), ri2 = ri * ri;
+    h[0] = fscale * ri;
 #pragma unroll
-  for (int k = 4; k >= 0; --k) f = fmaf(f, -d / (float)(k + 1), row[k]);
-  float F[L + 1];
-  F[L] = f;
-  const float et = expf(-T);
+    for (int j = 0; j < L; ++j) h[j + 1] = -(double)(2 * j + 1) * h[j] * ri2;
+  } else {
+    double F[L + 1];
+    boys_fn<L>(T, tab64, F);
+    double pw = 1.0;
 #pragma unroll
-  for (int m = L - 1; m >= 0; --m) F[m] = fmaf(2.0f * T, F[m + 1], et) / (float)(2 * m + 1);
-  const float m2p = -2.0f * g.p;
-  float pw = 1.0f;
-#pragma unroll
-  for (int j = 0; j <= L; ++j) {
-    h[j] = pw * F[j];
-    pw *= m2p;
+    for (int j = 0; j <= L; ++j) {
+      h[j] = pw * F[j];
+      pw *= -2.0 * p;
+    }
   }
-  return hermite_dot32<L>(D, X, Y, Z, h);
+  return hermite_dot64<L>(D, X, Y, Z, h);
 }
 
 constexpr int GTO32_THREADS = 128;
 constexpr int GTO32_PPT = 2;                          // points per thread
 constexpr int GTO32_POINTS = GTO32_THREADS * GTO32_PPT;
 constexpr int GTO32_CHUNK = 128;
+constexpr int GTO64_CHUNK = 64;
 
 // The terms of `nc` pairs of one angular momentum L (all in shared memory) at the thread's two
 // points, summed in FP32 in groups of four, the groups in FP64.  One L per loop (no dispatch per
@@ -360,7 +439,7 @@ constexpr int GTO32_CHUNK = 128;
 template <int L>
 __device__ __forceinline__ void chunk_terms(const GPair32* sp, const float* sd, const int* soff, int nc,
                                             const float (&x)[GTO32_PPT], const float (&y)[GTO32_PPT],
-                                            const float (&z)[GTO32_PPT], const float* __restrict__ tab,
+                                            const float (&z)[GTO32_PPT], const double* __restrict__ tab64,
                                             double (&V)[GTO32_PPT]) {
   constexpr int NC = ncoef(L);
   float acc[GTO32_PPT];
@@ -374,7 +453,7 @@ __device__ __forceinline__ void chunk_terms(const GPair32* sp, const float* sd, 
 #pragma unroll
     for (int c = 0; c < NC; ++c) D[c] = d[c];
 #pragma unroll
-    for (int q = 0; q < GTO32_PPT; ++q) acc[q] += pair_term32<L>(g, D, x[q], y[q], z[q], tab);
+    for (int q = 0; q < GTO32_PPT; ++q) acc[q] += pair_term32<L>(g, D, d, x[q], y[q], z[q], tab64, V[q]);
     if ((k & 3) == 3) {
 #pragma unroll
       for (int q = 0; q < GTO32_PPT; ++q) {
@@ -387,39 +466,78 @@ __device__ __forceinline__ void chunk_terms(const GPair32* sp, const float* sd, 
   for (int q = 0; q < GTO32_PPT; ++q) V[q] += (double)acc[q];
 }
 
-__device__ __forceinline__ void point32(const GtoPoints& gp, const Gto32Tables& t, int64_t i, float& x, float& y,
-                                        float& z, int64_t& o, bool& valid) {
+// The terms of `nc` FP64 pairs of one angular momentum L (in shared memory) at the thread's points.
+template <int L>
+__device__ __forceinline__ void chunk_terms64(const GPair64* sp, const double* sd, const int* soff, int nc,
+                                              const double (&x)[GTO32_PPT], const double (&y)[GTO32_PPT],
+                                              const double (&z)[GTO32_PPT], const double* __restrict__ tab64,
+                                              double (&V)[GTO32_PPT]) {
+  constexpr int NC = ncoef(L);
+#pragma unroll 1
+  for (int k = 0; k < nc; ++k) {
+    const GPair64 g = sp[k];
+    double D[NC];
+    const double* d = sd + soff[k];
+#pragma unroll
+    for (int c = 0; c < NC; ++c) D[c] = d[c];
+#pragma unroll
+    for (int q = 0; q < GTO32_PPT; ++q) V[q] += pair_term64<L>(g.px, g.py, g.pz, g.p, g.fscale, D, x[q], y[q], z[q], tab64);
+  }
+}
+
+// The point relative to the centroid in FP64 (the FP64 terms and the nuclei) and rounded once to
+// FP32 (the FP32 terms).
+__device__ __forceinline__ void point32(const GtoPoints& gp, const Gto32Tables& t, int64_t i, double& xd,
+                                        double& yd, double& zd, float& x, float& y, float& z, int64_t& o,
+                                        bool& valid) {
   double cx = 0, cy = 0, cz = 0;
   o = -1;
   valid = i < gp.npts && gto_point(gp, i, cx, cy, cz, o);
-  // the point relative to the centroid, rounded once: every term and the nuclear sum see it
-  x = (float)(cx - t.rx);
-  y = (float)(cy - t.ry);
-  z = (float)(cz - t.rz);
+  xd = cx - t.rx;
+  yd = cy - t.ry;
+  zd = cz - t.rz;
+  x = (float)xd;
+  y = (float)yd;
+  z = (float)zd;
 }
 
-// Off-site pairs of slice blockIdx.y at the block's points; FP64 partial sums into
+// The block's points: FP64 and FP32 coordinates relative to the centroid; invalid stand-ins copy
+// the first point (finite arithmetic, nothing written).
+__device__ __forceinline__ void block_points(const GtoPoints& gp, const Gto32Tables& t, double (&xd)[GTO32_PPT],
+                                             double (&yd)[GTO32_PPT], double (&zd)[GTO32_PPT],
+                                             float (&x)[GTO32_PPT], float (&y)[GTO32_PPT], float (&z)[GTO32_PPT],
+                                             int64_t (&idx)[GTO32_PPT], bool (&valid)[GTO32_PPT]) {
+#pragma unroll
+  for (int q = 0; q < GTO32_PPT; ++q) {
+    int64_t o;
+    idx[q] = blockIdx.x * (int64_t)GTO32_POINTS + q * GTO32_THREADS + threadIdx.x;
+    point32(gp, t, idx[q], xd[q], yd[q], zd[q], x[q], y[q], z[q], o, valid[q]);
+    if (!valid[q] && q > 0) {
+      x[q] = x[0];
+      y[q] = y[0];
+      z[q] = z[0];
+      xd[q] = xd[0];
+      yd[q] = yd[0];
+      zd[q] = zd[0];
+    }
+  }
+}
+
+// FP32 off-site pairs of slice blockIdx.y at the block's points; FP64 partial sums into
 // part[blockIdx.y * npts + i].
-__global__ void __launch_bounds__(GTO32_THREADS) gto32_pairs_kernel(Gto32Tables t, const float* __restrict__ tab,
+__global__ void __launch_bounds__(GTO32_THREADS, 8) gto32_pairs_kernel(Gto32Tables t, const double* __restrict__ tab64,
                                                                     GtoPoints gp, double* __restrict__ part) {
   __shared__ GPair32 sp[GTO32_CHUNK];
   __shared__ float sd[GTO32_CHUNK * 35];
   __shared__ int soff[GTO32_CHUNK];
   float x[GTO32_PPT], y[GTO32_PPT], z[GTO32_PPT];
-  int64_t o[GTO32_PPT], idx[GTO32_PPT];
+  double xd[GTO32_PPT], yd[GTO32_PPT], zd[GTO32_PPT];
+  int64_t idx[GTO32_PPT];
   bool valid[GTO32_PPT];
+  block_points(gp, t, xd, yd, zd, x, y, z, idx, valid);
   double V[GTO32_PPT];
 #pragma unroll
-  for (int q = 0; q < GTO32_PPT; ++q) {
-    idx[q] = blockIdx.x * (int64_t)GTO32_POINTS + q * GTO32_THREADS + threadIdx.x;
-    point32(gp, t, idx[q], x[q], y[q], z[q], o[q], valid[q]);
-    if (!valid[q] && q > 0) {   // a stand-in point: the arithmetic stays finite, nothing is written
-      x[q] = x[0];
-      y[q] = y[0];
-      z[q] = z[0];
-    }
-    V[q] = 0.0;
-  }
+  for (int q = 0; q < GTO32_PPT; ++q) V[q] = 0.0;
   const int s0 = t.slice[blockIdx.y], s1 = t.slice[blockIdx.y + 1];
 #pragma unroll 1
   for (int L = 0; L <= 4; ++L) {
@@ -438,11 +556,11 @@ __global__ void __launch_bounds__(GTO32_THREADS) gto32_pairs_kernel(Gto32Tables 
       __syncthreads();
       if (valid[0]) {
         switch (L) {
-          case 0: chunk_terms<0>(sp, sd, soff, nc, x, y, z, tab, V); break;
-          case 1: chunk_terms<1>(sp, sd, soff, nc, x, y, z, tab, V); break;
-          case 2: chunk_terms<2>(sp, sd, soff, nc, x, y, z, tab, V); break;
-          case 3: chunk_terms<3>(sp, sd, soff, nc, x, y, z, tab, V); break;
-          default: chunk_terms<4>(sp, sd, soff, nc, x, y, z, tab, V); break;
+          case 0: chunk_terms<0>(sp, sd, soff, nc, x, y, z, tab64, V); break;
+          case 1: chunk_terms<1>(sp, sd, soff, nc, x, y, z, tab64, V); break;
+          case 2: chunk_terms<2>(sp, sd, soff, nc, x, y, z, tab64, V); break;
+          case 3: chunk_terms<3>(sp, sd, soff, nc, x, y, z, tab64, V); break;
+          default: chunk_terms<4>(sp, sd, soff, nc, x, y, z, tab64, V); break;
         }
       }
     }
@@ -452,8 +570,55 @@ __global__ void __launch_bounds__(GTO32_THREADS) gto32_pairs_kernel(Gto32Tables 
     if (valid[q]) part[blockIdx.y * gp.npts + idx[q]] = V[q];
 }
 
+// FP64 off-site pairs of slice blockIdx.y at the block's points; FP64 partial sums into
+// part[(nslice + blockIdx.y) * npts + i].
+__global__ void __launch_bounds__(GTO32_THREADS) gto64_pairs_kernel(Gto32Tables t, const double* __restrict__ tab64,
+                                                                    GtoPoints gp, double* __restrict__ part) {
+  __shared__ GPair64 sp[GTO64_CHUNK];
+  __shared__ double sd[GTO64_CHUNK * 35];
+  __shared__ int soff[GTO64_CHUNK];
+  float x[GTO32_PPT], y[GTO32_PPT], z[GTO32_PPT];
+  double xd[GTO32_PPT], yd[GTO32_PPT], zd[GTO32_PPT];
+  int64_t idx[GTO32_PPT];
+  bool valid[GTO32_PPT];
+  block_points(gp, t, xd, yd, zd, x, y, z, idx, valid);
+  double V[GTO32_PPT];
+#pragma unroll
+  for (int q = 0; q < GTO32_PPT; ++q) V[q] = 0.0;
+  const int s0 = t.slice64[blockIdx.y], s1 = t.slice64[blockIdx.y + 1];
+#pragma unroll 1
+  for (int L = 0; L <= 4; ++L) {
+    const int p0 = max(s0, t.lstart64[L]), p1 = min(s1, t.lstart64[L + 1]);
+    for (int c0 = p0; c0 < p1; c0 += GTO64_CHUNK) {
+      const int nc = min(GTO64_CHUNK, p1 - c0);
+      __syncthreads();
+      const int dbase = t.pairs64[c0].doff;
+      if (threadIdx.x < nc) {
+        const GPair64 g = t.pairs64[c0 + threadIdx.x];
+        sp[threadIdx.x] = g;
+        soff[threadIdx.x] = g.doff - dbase;
+      }
+      const int dn = nc * ncoef(L);
+      for (int k = threadIdx.x; k < dn; k += GTO32_THREADS) sd[k] = t.dco64[dbase + k];
+      __syncthreads();
+      if (valid[0]) {
+        switch (L) {
+          case 0: chunk_terms64<0>(sp, sd, soff, nc, xd, yd, zd, tab64, V); break;
+          case 1: chunk_terms64<1>(sp, sd, soff, nc, xd, yd, zd, tab64, V); break;
+          case 2: chunk_terms64<2>(sp, sd, soff, nc, xd, yd, zd, tab64, V); break;
+          case 3: chunk_terms64<3>(sp, sd, soff, nc, xd, yd, zd, tab64, V); break;
+          default: chunk_terms64<4>(sp, sd, soff, nc, xd, yd, zd, tab64, V); break;
+        }
+      }
+    }
+  }
+#pragma unroll
+  for (int q = 0; q < GTO32_PPT; ++q)
+    if (valid[q]) part[(t.nslice + blockIdx.y) * gp.npts + idx[q]] = V[q];
+}
+
 // FP64 R_tuv (t+u+v <= 4) from h_j, dotted with the 35 moments M.
-__device__ __forceinline__ double hermite_dot64(const double* __restrict__ M, double X, double Y, double Z,
+__device__ __forceinline__ double moments_dot64(const double* __restrict__ M, double X, double Y, double Z,
                                                 const double (&h)[5]) {
   constexpr int NC = ncoef(4);
   constexpr HermTable H = make_herm_table();
@@ -483,24 +648,25 @@ __device__ __forceinline__ double hermite_dot64(const double* __restrict__ M, do
 }
 
 // Per point: the slices' partial sums in order, then atom by atom the far-field on-site pairs as
-// one FP64 multipole, the near-field on-site pairs in FP32, and the nucleus in FP64.
-__global__ void __launch_bounds__(GTO32_THREADS) gto32_atoms_kernel(Gto32Tables t, const float* __restrict__ tab,
+// one FP64 multipole, the near-field on-site pairs and the nucleus, all in FP64 about the FP64
+// nucleus.
+__global__ void __launch_bounds__(GTO32_THREADS) gto32_atoms_kernel(Gto32Tables t, const double* __restrict__ tab64,
                                                                     MolView mol, GtoPoints gp,
                                                                     const double* __restrict__ part,
                                                                     float* __restrict__ out) {
   const int64_t i = blockIdx.x * (int64_t)GTO32_THREADS + threadIdx.x;
   float x, y, z;
+  double xd, yd, zd;
   int64_t o;
   bool valid;
-  point32(gp, t, i, x, y, z, o, valid);
+  point32(gp, t, i, xd, yd, zd, x, y, z, o, valid);
   if (!valid) return;
   double V = 0.0;
-  for (int sl = 0; sl < t.nslice; ++sl) V += part[sl * gp.npts + i];
+  for (int sl = 0; sl < t.nslice + t.nslice64; ++sl) V += part[sl * gp.npts + i];
   for (int a = 0; a < mol.natoms; ++a) {
-    const float ax = t.nuc[3 * a], ay = t.nuc[3 * a + 1], az = t.nuc[3 * a + 2];
-    // the same FP32 displacement and r^2 as the pair terms (pair_term32), so that the far / near
-    // split below is exactly the one a pair-by-pair evaluation would make
-    const float X = ax - x, Y = ay - y, Z = az - z;
+    // far / near split of the atom's pairs by the FP32 test p r^2 >= 30 (any consistent split is
+    // exact up to the asymptotic form's error)
+    const float X = t.nuc[3 * a] - x, Y = t.nuc[3 * a + 1] - y, Z = t.nuc[3 * a + 2] - z;
     const float r2 = fmaf(X, X, fmaf(Y, Y, Z * Z));
     const int b0 = t.onsite_off[a], b1 = t.onsite_off[a + 1];
     int lo = b0, hi = b1;   // first pair that is not far (exponents descend, so far ones lead)
@@ -509,25 +675,28 @@ __global__ void __launch_bounds__(GTO32_THREADS) gto32_atoms_kernel(Gto32Tables 
       if (!(__ldg(t.onsite_p + mid) * r2 < T_FAR)) lo = mid + 1;
       else hi = mid;
     }
-    const double Xd = X, Yd = Y, Zd = Z;
+    const double ax = t.nuc64[3 * a], ay = t.nuc64[3 * a + 1], az = t.nuc64[3 * a + 2];
+    const double Xd = ax - xd, Yd = ay - yd, Zd = az - zd;
     const double r2d = Xd * Xd + Yd * Yd + Zd * Zd;
     if (lo > b0) {
-      const double ri = 1.0 / sqrt(r2d), ri2 = ri * ri;
+      const double ri = rsqrt(r2d), ri2 = ri * ri;
       double h[5];
       h[0] = ri;
 #pragma unroll
       for (int j = 0; j < 4; ++j) h[j + 1] = -(double)(2 * j + 1) * h[j] * ri2;
-      V += hermite_dot64(t.cum + (size_t)(t.cum_off[a] + (lo - b0)) * 35, Xd, Yd, Zd, h);
+      V += moments_dot64(t.cum + (size_t)(t.cum_off[a] + (lo - b0)) * 35, Xd, Yd, Zd, h);
     }
     for (int k = lo; k < b1; ++k) {
       const GPair32 g = t.onsite[k];
-      const float* d = t.dco + g.doff;
+      const double* d = t.dco_on + g.pad;   // p, sqrt(pi) / (2 sqrt(p)), pref * D_tuv
+      const double pk = d[0], fs = d[1];
+      d += 2;
       switch (g.L) {
-        case 0: { float D[1]; D[0] = d[0]; V += (double)pair_term32<0>(g, D, x, y, z, tab); break; }
-        case 1: { float D[4]; for (int c = 0; c < 4; ++c) D[c] = d[c]; V += (double)pair_term32<1>(g, D, x, y, z, tab); break; }
-        case 2: { float D[10]; for (int c = 0; c < 10; ++c) D[c] = d[c]; V += (double)pair_term32<2>(g, D, x, y, z, tab); break; }
-        case 3: { float D[20]; for (int c = 0; c < 20; ++c) D[c] = d[c]; V += (double)pair_term32<3>(g, D, x, y, z, tab); break; }
-        default: { float D[35]; for (int c = 0; c < 35; ++c) D[c] = d[c]; V += (double)pair_term32<4>(g, D, x, y, z, tab); break; }
+        case 0: { double D[1]; D[0] = d[0]; V += pair_term64<0>(ax, ay, az, pk, fs, D, xd, yd, zd, tab64); break; }
+        case 1: { double D[4]; for (int c = 0; c < 4; ++c) D[c] = d[c]; V += pair_term64<1>(ax, ay, az, pk, fs, D, xd, yd, zd, tab64); break; }
+        case 2: { double D[10]; for (int c = 0; c < 10; ++c) D[c] = d[c]; V += pair_term64<2>(ax, ay, az, pk, fs, D, xd, yd, zd, tab64); break; }
+        case 3: { double D[20]; for (int c = 0; c < 20; ++c) D[c] = d[c]; V += pair_term64<3>(ax, ay, az, pk, fs, D, xd, yd, zd, tab64); break; }
+        default: { double D[35]; for (int c = 0; c < 35; ++c) D[c] = d[c]; V += pair_term64<4>(ax, ay, az, pk, fs, D, xd, yd, zd, tab64); break; }
       }
     }
     const double r = sqrt(r2d);
@@ -563,33 +732,10 @@ static qmt_status boys_table(const double** out) {
   return QMT_OK;
 }
 
-static qmt_status boys_table32(const float** out) {
-  static thread_local DevBuf tab;
-  static thread_local bool ready = false;
-  if (!ready) {
-    std::vector<float> h((size_t)BOYS32_NT * BOYS32_NM);
-    for (int i = 0; i < BOYS32_NT; ++i) {
-      const double T = i * 0.1;
-      for (int m = 0; m < BOYS32_NM; ++m) {
-        double term = 1.0 / (2 * m + 1), acc = term;
-        for (int k = 1; k < 400; ++k) {
-          term *= 2 * T / (2 * m + 2 * k + 1);
-          acc += term;
-          if (term < 1e-18 * acc) break;
-        }
-        h[(size_t)i * BOYS32_NM + m] = (float)(std::exp(-T) * acc);
-      }
-    }
-    qmt_status st = tab.reserve(h.size() * sizeof(float));
-    if (st) return st;
-    QMT_CUDA(cudaMemcpy(tab.ptr, h.data(), h.size() * sizeof(float), cudaMemcpyHostToDevice));
-    ready = true;
-  }
-  *out = tab.as<float>();
-  return QMT_OK;
-}
-
 static int g_gto_prec = QMT_PREC_FP32;   // FP32 with FP64 accumulation, or FP64 throughout
+// Share of the off-site pairs' total size (far-field multipoles) left to FP32 terms; the largest
+// pairs, holding the rest, take FP64 terms.
+constexpr double kFp32Share = 0.05;
 
 // ---- host: pair table --------------------------------------------------------------------------
 static void hermite_e_host(int la, int lb, double a, double b, double xa, double xb, double E[3][3][5]) {
@@ -770,16 +916,65 @@ static qmt_status build_pairs(qmt_mol* m, cudaStream_t s) {
     for (int c = 0; c < ncoef(g.L); ++c) d32.push_back((float)(g.pref * g.D[c]));
     return q;
   };
+  auto to64 = [&](const Acc& g, std::vector<double>& d64) {
+    GPair64 q;
+    q.px = g.px - ref[0];
+    q.py = g.py - ref[1];
+    q.pz = g.pz - ref[2];
+    q.p = g.p;
+    q.fscale = 0.88622692545275801365 / std::sqrt(g.p);
+    q.L = g.L;
+    q.doff = (int)d64.size();
+    for (int c = 0; c < ncoef(g.L); ++c) d64.push_back(g.pref * g.D[c]);
+    return q;
+  };
   std::vector<GPair32> off32, on32;
+  std::vector<GPair64> off64;
   std::vector<float> d32, onp;
+  std::vector<double> d64, don;
   std::vector<int> on_off(m->natoms + 1, 0), cum_off(m->natoms + 1, 0);
   std::vector<double> cum;
-  for (int idx : order)   // off-site pairs, already sorted by L
-    if (acc[idx].atom_a != acc[idx].atom_b) off32.push_back(to32(acc[idx], d32));
+  // The off-site pairs that carry most of the charge are evaluated in FP64: the error of an FP32
+  // term (its rounded coefficients and arithmetic) is proportional to its size, and a few percent
+  // of the pairs hold nearly all of it.  Size of a pair at a distance: its far-field multipoles,
+  // order n weighted 10^-n.
+  std::vector<int> offs;
+  for (int idx : order)
+    if (acc[idx].atom_a != acc[idx].atom_b) offs.push_back(idx);
+  std::vector<double> size(acc.size(), 0.0);
+  double total = 0.0;
+  for (int idx : offs) {
+    const Acc& g = acc[idx];
+    double w = 0.0;
+    for (int c = 0, n = 0; n <= g.L; ++n) {
+      double sn = 0.0;
+      for (; c < ncoef(n); ++c) sn += std::fabs(g.D[c]);
+      w += sn * std::pow(0.1, n);
+    }
+    size[idx] = w * std::fabs(g.pref) / std::sqrt(g.p);
+    total += size[idx];
+  }
+  std::vector<int> by_size(offs);
+  std::stable_sort(by_size.begin(), by_size.end(), [&](int x, int y) { return size[x] > size[y]; });
+  std::vector<char> heavy(acc.size(), 0);
+  double rest = total;
+  for (int idx : by_size) {
+    if (rest <= kFp32Share * total) break;
+    heavy[idx] = 1;
+    rest -= size[idx];
+  }
+  for (int idx : offs)    // both lists keep the order by L
+    if (heavy[idx]) off64.push_back(to64(acc[idx], d64));
+    else off32.push_back(to32(acc[idx], d32));
   if (off32.empty()) {    // one zero pair keeps the tables well formed
     Acc z{};
     z.p = 1.0;
     off32.push_back(to32(z, d32));
+  }
+  if (off64.empty()) {
+    Acc z{};
+    z.p = 1.0;
+    off64.push_back(to64(z, d64));
   }
   std::vector<std::vector<int>> by_atom(m->natoms);
   for (size_t i = 0; i < acc.size(); ++i)
@@ -794,7 +989,12 @@ static qmt_status build_pairs(qmt_mol* m, cudaStream_t s) {
     cum.insert(cum.end(), run.begin(), run.end());
     for (int idx : v) {
       const Acc& g = acc[idx];
-      on32.push_back(to32(g, d32));
+      GPair32 q = to32(g, d32);
+      q.pad = (int)don.size();   // the FP64 record: p, sqrt(pi) / (2 sqrt(p)), pref * D_tuv
+      don.push_back(g.p);
+      don.push_back(0.88622692545275801365 / std::sqrt(g.p));
+      for (int c = 0; c < ncoef(g.L); ++c) don.push_back(g.pref * g.D[c]);
+      on32.push_back(q);
       onp.push_back((float)g.p);
       const double f = 0.88622692545275801365 / std::sqrt(g.p) * g.pref;
       for (int c = 0; c < ncoef(g.L); ++c) run[c] += f * g.D[c];
@@ -804,19 +1004,28 @@ static qmt_status build_pairs(qmt_mol* m, cudaStream_t s) {
   on_off[m->natoms] = (int)on32.size();
   cum_off[m->natoms] = (int)(cum.size() / 35);
   std::vector<float> nuc(3 * m->natoms);
+  std::vector<double> nuc64(3 * m->natoms);
   for (int a = 0; a < m->natoms; ++a)
-    for (int d = 0; d < 3; ++d) nuc[3 * a + d] = (float)((double)m->coords[3 * a + d] - ref[d]);
+    for (int d = 0; d < 3; ++d) {
+      nuc64[3 * a + d] = (double)m->coords[3 * a + d] - ref[d];
+      nuc[3 * a + d] = (float)nuc64[3 * a + d];
+    }
   if (on32.empty()) {     // keep the device arrays non-empty
     on32.push_back(GPair32{});
     onp.push_back(0.f);
+    don.push_back(0.0);
   }
-  // one device buffer: off-site pairs | on-site pairs | cum | floats (dco, on-site p, nuclei) | ints
+  // one device buffer: off-site pairs (FP32, FP64) | on-site pairs | doubles (cum, FP64
+  // coefficients, on-site records, nuclei) | floats (dco, on-site p, nuclei) | ints
   auto al = [](size_t b) { return (b + 255) / 256 * 256; };
   const size_t b_off = al(off32.size() * sizeof(GPair32)), b_on = al(on32.size() * sizeof(GPair32));
+  const size_t b_o64 = al(off64.size() * sizeof(GPair64)), b_d64 = al(d64.size() * sizeof(double));
+  const size_t b_don = al(don.size() * sizeof(double)), b_n64 = al(nuc64.size() * sizeof(double));
   const size_t b_cum = al(cum.size() * sizeof(double)), b_d = al(d32.size() * sizeof(float));
   const size_t b_p = al(onp.size() * sizeof(float)), b_nuc = al(nuc.size() * sizeof(float));
   const size_t b_i = al((on_off.size() + cum_off.size()) * sizeof(int));
-  if ((st = m->d_pairs32.reserve(b_off + b_on + b_cum + b_d + b_p + b_nuc + b_i))) return st;
+  if ((st = m->d_pairs32.reserve(b_off + b_o64 + b_on + b_cum + b_d64 + b_don + b_n64 + b_d + b_p + b_nuc + b_i)))
+    return st;
   uint8_t* base = m->d_pairs32.as<uint8_t>();
   std::vector<int> ints(on_off);
   ints.insert(ints.end(), cum_off.begin(), cum_off.end());
@@ -830,13 +1039,18 @@ static qmt_status build_pairs(qmt_mol* m, cudaStream_t s) {
   Gto32Tables& T = m->gto32;
   T = Gto32Tables{};
   T.pairs = reinterpret_cast<const GPair32*>(put(off32.data(), off32.size() * sizeof(GPair32), b_off));
+  T.pairs64 = reinterpret_cast<const GPair64*>(put(off64.data(), off64.size() * sizeof(GPair64), b_o64));
   T.onsite = reinterpret_cast<const GPair32*>(put(on32.data(), on32.size() * sizeof(GPair32), b_on));
   T.cum = reinterpret_cast<const double*>(put(cum.data(), cum.size() * sizeof(double), b_cum));
+  T.dco64 = reinterpret_cast<const double*>(put(d64.data(), d64.size() * sizeof(double), b_d64));
+  T.dco_on = reinterpret_cast<const double*>(put(don.data(), don.size() * sizeof(double), b_don));
+  T.nuc64 = reinterpret_cast<const double*>(put(nuc64.data(), nuc64.size() * sizeof(double), b_n64));
   T.dco = reinterpret_cast<const float*>(put(d32.data(), d32.size() * sizeof(float), b_d));
   T.onsite_p = reinterpret_cast<const float*>(put(onp.data(), onp.size() * sizeof(float), b_p));
   T.nuc = reinterpret_cast<const float*>(put(nuc.data(), nuc.size() * sizeof(float), b_nuc));
   const int* ip = reinterpret_cast<const int*>(put(ints.data(), ints.size() * sizeof(int), b_i));
-  if (!T.pairs || !T.onsite || !T.cum || !T.dco || !T.onsite_p || !T.nuc || !ip)
+  if (!T.pairs || !T.pairs64 || !T.onsite || !T.cum || !T.dco64 || !T.dco_on || !T.nuc64 || !T.dco || !T.onsite_p ||
+      !T.nuc || !ip)
     return fail(QMT_CUDA_ERR, "upload of the analytic-potential tables failed");
   T.onsite_off = ip;
   T.cum_off = ip + on_off.size();
@@ -847,11 +1061,18 @@ static qmt_status build_pairs(qmt_mol* m, cudaStream_t s) {
     int k = 0;
     while (k < (int)off32.size() && off32[k].L < L) ++k;
     T.lstart[L] = k;
+    k = 0;
+    while (k < (int)off64.size() && off64[k].L < L) ++k;
+    T.lstart64[L] = k;
   }
-  // slices of about equal work (pair terms cost about 12 + 2 ncoef(L) operations)
-  std::vector<double> w(off32.size() + 1, 0.0);
-  for (size_t k = 0; k < off32.size(); ++k) w[k + 1] = w[k] + 12.0 + 2.0 * ncoef(off32[k].L);
-  m->gto32_work = w;
+  // cumulative estimated work for the slices (a term costs about 12 + 2 ncoef(L) operations)
+  auto work = [](const auto& v) {
+    std::vector<double> w(v.size() + 1, 0.0);
+    for (size_t k = 0; k < v.size(); ++k) w[k + 1] = w[k] + 12.0 + 2.0 * ncoef(v[k].L);
+    return w;
+  };
+  m->gto32_work = work(off32);
+  m->gto64_work = work(off64);
   QMT_CUDA(cudaStreamSynchronize(s));
   m->gto_npairs = (int)pairs.size();
   m->gto_doff_bytes = ((pb + 255) / 256) * 256;
@@ -864,28 +1085,34 @@ static qmt_status run_gto(qmt_mol* m, const GtoPoints& gp, float* out, cudaStrea
   if ((st = build_pairs(m, s))) return st;
   if (gp.npts <= 0) return QMT_OK;
   if (g_gto_prec == QMT_PREC_FP32) {
-    const float* tab32 = nullptr;
-    if ((st = boys_table32(&tab32))) return st;
-    // enough CTAs to fill the device: the off-site pairs are split into slices whose FP64 partial
-    // sums the second kernel adds in slice order (deterministic)
+    const double* tab64 = nullptr;
+    if ((st = boys_table(&tab64))) return st;
+    // enough CTAs to fill the device: each list of off-site pairs is split into slices whose FP64
+    // partial sums the last kernel adds in slice order (deterministic)
     const int64_t pblocks = (gp.npts + GTO32_POINTS - 1) / GTO32_POINTS;
     const int64_t want = (int64_t)sm_count() * 12;
     const int nslice = (int)std::max<int64_t>(1, std::min<int64_t>(16, (want + pblocks - 1) / pblocks));
     Gto32Tables T = m->gto32;
+    auto cut = [](const std::vector<double>& w, int n, int* slice) {
+      const int np = (int)w.size() - 1;
+      for (int k = 0, j = 0; k <= n; ++k) {   // slice k starts at the first pair past k/n of the work
+        const double target = w.back() * k / n;
+        while (j < np && w[j] < target) ++j;
+        slice[k] = k == n ? np : j;
+      }
+    };
     T.nslice = nslice;
-    const std::vector<double>& w = m->gto32_work;
-    const int npairs = (int)w.size() - 1;
-    for (int k = 0, j = 0; k <= nslice; ++k) {   // slice k starts at the first pair past k/nslice of the work
-      const double target = w.back() * k / nslice;
-      while (j < npairs && w[j] < target) ++j;
-      T.slice[k] = k == nslice ? npairs : j;
-    }
-    if ((st = m->d_gto_part.reserve((size_t)nslice * gp.npts * sizeof(double)))) return st;
+    T.nslice64 = nslice;
+    cut(m->gto32_work, T.nslice, T.slice);
+    cut(m->gto64_work, T.nslice64, T.slice64);
+    if ((st = m->d_gto_part.reserve((size_t)(T.nslice + T.nslice64) * gp.npts * sizeof(double)))) return st;
     double* part = m->d_gto_part.as<double>();
-    gto32_pairs_kernel<<<dim3((unsigned)pblocks, (unsigned)nslice), GTO32_THREADS, 0, s>>>(T, tab32, gp, part);
+    gto32_pairs_kernel<<<dim3((unsigned)pblocks, (unsigned)T.nslice), GTO32_THREADS, 0, s>>>(T, tab64, gp, part);
     QMT_CHECK_LAUNCH("gto32_pairs_kernel");
+    gto64_pairs_kernel<<<dim3((unsigned)pblocks, (unsigned)T.nslice64), GTO32_THREADS, 0, s>>>(T, tab64, gp, part);
+    QMT_CHECK_LAUNCH("gto64_pairs_kernel");
     const int64_t ablocks = (gp.npts + GTO32_THREADS - 1) / GTO32_THREADS;
-    gto32_atoms_kernel<<<(unsigned)ablocks, GTO32_THREADS, 0, s>>>(T, tab32, m->view(), gp, part, out);
+    gto32_atoms_kernel<<<(unsigned)ablocks, GTO32_THREADS, 0, s>>>(T, tab64, m->view(), gp, part, out);
     QMT_CHECK_LAUNCH("gto32_atoms_kernel");
     return QMT_OK;
   }

@@ -61,7 +61,8 @@ struct qmt_mol {
   qmt::DevBuf d_pairs;
   qmt::DevBuf d_pairs32;        // storage of gto32 (device pointers into it)
   qmt::Gto32Tables gto32{};
-  std::vector<double> gto32_work;   // cumulative estimated work of the off-site pairs
+  std::vector<double> gto32_work;   // cumulative estimated work of the FP32 off-site pairs
+  std::vector<double> gto64_work;   // and of the FP64 ones
   qmt::DevBuf d_gto_part;       // FP64 partial sums of the off-site pair slices
 
   ~qmt_mol();
