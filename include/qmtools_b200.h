@@ -111,8 +111,12 @@ qmt_status qmt_density(qmt_mol* mol, int nx, int ny, int nz, float step,
                        int rescale, float* qube_dev, double* sum_out, void* stream);
 
 /* Selects the tensor-core density implementation (new; process-wide): 0 = automatic (fused
- * when the contraction is fp16/bf16 and N <= 320, staged otherwise), 1 = staged (basis values
- * through HBM), 2 = fused (basis values stay in shared memory). */
+ * when the contraction is fp16/bf16 and N <= 320, staged otherwise; fused with the factored
+ * density matrix when it has one), 1 = staged (basis values through HBM), 2 = fused (basis values
+ * stay in shared memory), 3 = fused with the factored density matrix: P = L L^T from a pivoted
+ * Cholesky factorisation (FP64, on the host, once per matrix) and rho = sum_k (Phi L)_k^2, which
+ * needs rank(P) columns instead of N -- for a positive semi-definite P whose rank is at most N/2
+ * (an SCF density matrix has the rank of its occupied orbitals); QMT_BAD_ARG otherwise. */
 qmt_status qmt_set_density_path(int mode);
 
 /* ---- batches of molecules (new; no reference counterpart) ---------------------------- */

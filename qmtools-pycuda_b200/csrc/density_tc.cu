@@ -475,6 +475,7 @@ static qmt_status ensure_basis_operands(qmt_mol* m, int K, cudaStream_t s) {
   }
   qmt_status st = m->d_split_scale.reserve(K * sizeof(double));
   if (st) return st;
+  m->split_inv = inv;
   // pageable uploads return once the data is staged, so `inv` may go
   QMT_CUDA(cudaMemcpyAsync(m->d_split_scale.ptr, inv.data(), K * sizeof(double), cudaMemcpyHostToDevice, s));
   if ((st = ensure_mol_tables(m, fs, K, s))) return st;
@@ -540,8 +541,10 @@ struct FusedMol {
   PointMap pm;
   int64_t tile0, ntiles;
   int natoms, norbs;
-  int n16;                 // functions rounded up to 16: K of the MMAs and N (output columns); the
-                           // K-steps beyond it only hold zero padding and are skipped
+  int n16;                 // functions rounded up to 16: K of the MMAs; the K-steps beyond it
+                           // only hold zero padding and are skipped
+  int nb;                  // N of the MMAs (rows of a K-step block of B): n16 for the density
+                           // matrix, the rank rounded up to 16 for its factor
   int ksteps, nchunks;     // n16 / 16 K-steps; ceil(n16 / 64) column chunks of A
   int tail0;               // n16 & ~63: first column of A's 32-byte swizzled tail blocks
   int u_rows;              // rows of one K-step block of U in HBM (kpad + 64)
@@ -573,6 +576,19 @@ struct FusedParams {
   int* err;
   uint64_t wait_ns;        // limit of every bounded wait (a test shortens it)
 };
+
+// Factored path: a stage holds the factor's hi rows followed by its lo rows, so one MMA of
+// N = 2 nb gives [A_hi B_hi | A_hi B_lo] and, with two pieces, one more [A_lo B_hi | A_lo B_lo].
+// The first kind of the K-steps of the nchunks column chunks goes to fact_nacc(nchunks, nb, two)
+// TMEM accumulators of 2 nb columns (chunk c to accumulator c * na / nchunks), the second kind to
+// one more, and the epilogue adds them.  The accumulators' FP32 additions round with a bias
+// toward zero, which the squares of T would double into rho; few additions of large terms per
+// accumulator keep it small.  Two different accumulators alternate, so no MMA waits on the one
+// before it.
+__host__ __device__ __forceinline__ int fact_nacc(int nchunks, int nb, bool two) {
+  const int fit = 512 / (two ? 2 * nb : nb) - (two ? 1 : 0);
+  return nchunks < fit ? nchunks : fit;
+}
 
 // Arrival count of a column-chunk barrier: each tile pre-arrives CHUNK_COUNT - need, the
 // production items the rest, so that molecules with different atom counts share the barriers.
@@ -1139,7 +1155,7 @@ __device__ __forceinline__ void fused_produce_u(const FusedParams* pp, uint8_t* 
     // the molecule's values in registers for the tile: read through a reference, they would be
     // reloaded after every barrier operation (each an asm statement that clobbers memory)
     const int ksteps = M.ksteps, u_rows = M.u_rows;
-    const uint32_t bytes = (uint32_t)M.n16 * 32u;
+    const uint32_t bytes = (uint32_t)M.nb * 32u;
     const uint8_t* const u_hi = M.u_hi;
     const uint8_t* const u_lo = M.u_lo;
     for (int ks = 0; ks < ksteps; ++ks, ++it) {
@@ -1179,7 +1195,7 @@ __device__ __forceinline__ void fused_issue_mma(const FusedParams* pp, uint32_t 
     int m;
     const FusedMol& M = fused_mol<MULTI>(p, t, m);
     // the molecule's values in registers for the tile (see the producer)
-    const int ksteps = M.ksteps, n16 = M.n16, tail0 = M.tail0;
+    const int ksteps = M.ksteps, nb = M.nb, tail0 = M.tail0;
     uint32_t need = 0;
 #pragma unroll
     for (int c = 0; c < MAX_FUSED_CHUNKS; ++c)
@@ -1215,8 +1231,8 @@ __device__ __forceinline__ void fused_issue_mma(const FusedParams* pp, uint32_t 
         alo = sw32_kmajor_desc(lbase + aoff);
       }
       const uint32_t bst = smem_u32(stages + (size_t)s * p.stage_bytes);
-      for (int c0 = 0; c0 < n16; c0 += 256) {
-        const int n = min(256, n16 - c0);
+      for (int c0 = 0; c0 < nb; c0 += 256) {
+        const int n = min(256, nb - c0);
         const uint32_t idesc = make_idesc(p.fmt, 128, (uint32_t)n);
         const uint32_t boff = (uint32_t)c0 * 32u;
         const uint32_t d = tmem + (uint32_t)c0;
@@ -1234,7 +1250,115 @@ __device__ __forceinline__ void fused_issue_mma(const FusedParams* pp, uint32_t 
   mbar_wait_drain(drain_bar, 0u, 500000000ull);
 }
 
-template <int FMT, bool MULTI>
+// Factored path (single molecule): a stage is one column chunk of the factor, its K-steps each
+// [hi rows | lo rows] (nb rows of 32 bytes apiece), one contiguous copy from HBM (ensure_factor's
+// layout).
+__device__ __forceinline__ uint32_t fact_chunk_ksteps(int c, int ksteps) { return (uint32_t)min(4, ksteps - 4 * c); }
+
+__device__ __forceinline__ void fact_produce(const FusedParams& p, uint8_t* stages, uint64_t* full_bar,
+                                             uint64_t* empty_bar, volatile int* abort_flag) {
+  const FusedMol& M = p.one;
+  const int ksteps = M.ksteps, nchunks = M.nchunks;
+  const uint32_t kbytes = (uint32_t)p.nsplit * (uint32_t)M.nb * 32u;   // one K-step of the factor
+  const uint8_t* const src0 = M.u_hi;
+  int s = 0;
+  uint32_t ph = 0, issued = 0, par = 0;
+  bool ok = true;
+  for (int64_t t = blockIdx.x; t < p.ntiles && ok; t += gridDim.x) {
+    for (int c = 0; c < nchunks; ++c) {
+      if (!mbar_wait(&empty_bar[s], ph ^ 1u, abort_flag, p.wait_ns)) {
+        ok = false;
+        break;
+      }
+      const uint32_t bytes = fact_chunk_ksteps(c, ksteps) * kbytes;
+      mbar_expect_tx(&full_bar[s], bytes);
+      bulk_load(stages + (size_t)s * p.stage_bytes, src0 + (size_t)c * 4 * kbytes, bytes, &full_bar[s]);
+      issued |= 1u << s;
+      par = (par & ~(1u << s)) | (ph << s);
+      if (++s == p.stages) {
+        s = 0;
+        ph ^= 1u;
+      }
+    }
+  }
+  if (!ok)
+    for (int q = 0; q < p.stages; ++q)
+      if ((issued >> q) & 1u) mbar_wait_drain(&full_bar[q], (par >> q) & 1u, 100000000ull);
+}
+
+// Per chunk: wait for its columns of A and its stage, then per K-step one MMA of N = 2 nb
+// [A_hi B_hi | A_hi B_lo] into the chunk's accumulator and, with two pieces, [A_lo B_hi | A_lo B_lo]
+// into the last (fact_nacc); the stage is freed by one commit per chunk.
+__device__ __forceinline__ void fact_issue(const FusedParams& p, uint32_t abase, uint32_t lbase, uint8_t* stages,
+                                           uint32_t tmem, uint64_t* full_bar, uint64_t* empty_bar, uint64_t* chunk_bar,
+                                           uint64_t* t_full, uint64_t* drain_bar, volatile int* abort_flag) {
+  const FusedMol& M = p.one;
+  const bool two = p.nsplit == 2;
+  const int ksteps = M.ksteps, nb = M.nb, tail0 = M.tail0, nchunks = M.nchunks;
+  const int nfull = two ? 2 * nb : nb;
+  const int na = fact_nacc(nchunks, nb, two);
+  const uint32_t idesc = make_idesc(p.fmt, 128, (uint32_t)nfull);
+  const uint32_t kbytes = (uint32_t)nfull * 32u;
+  const uint32_t dsmall = tmem + (uint32_t)(na * nfull);
+  uint32_t dmain[MAX_FUSED_CHUNKS], firstmask = 0, need = 0;
+#pragma unroll
+  for (int c = 0; c < MAX_FUSED_CHUNKS; ++c) {
+    const int a = c < nchunks ? c * na / nchunks : 0;
+    dmain[c] = tmem + (uint32_t)(a * nfull);
+    if (c < nchunks && (c == 0 || (c - 1) * na / nchunks != a)) firstmask |= 1u << c;
+    if (M.chunk_need[c] > 0) need |= 1u << c;
+  }
+  int s = 0;
+  uint32_t ph = 0, cpar = 0;
+  bool ok = true;
+  for (int64_t t = blockIdx.x; t < p.ntiles && ok; t += gridDim.x) {
+#pragma unroll 1
+    for (int c = 0; c < nchunks; ++c) {
+      if ((need >> c) & 1u) {
+        if (!mbar_wait(&chunk_bar[c], (cpar >> c) & 1u, abort_flag, p.wait_ns)) {
+          ok = false;
+          break;
+        }
+        cpar ^= 1u << c;
+      }
+      if (!mbar_wait(&full_bar[s], ph, abort_flag, p.wait_ns)) {
+        ok = false;
+        break;
+      }
+      tc_fence_after();
+      const uint32_t bst = smem_u32(stages + (size_t)s * p.stage_bytes);
+      const uint32_t kc = fact_chunk_ksteps(c, ksteps);
+      const uint32_t dm = dmain[c];
+      const bool first = (firstmask >> c) & 1u;
+      for (uint32_t kk = 0; kk < kc; ++kk) {
+        const int j0 = (4 * c + (int)kk) * 16;
+        uint64_t ahi, alo;
+        if (j0 < tail0) {
+          const uint32_t aoff = (uint32_t)(c * 16384 + kk * 32);
+          ahi = sw128_kmajor_desc(abase + aoff);
+          alo = sw128_kmajor_desc(lbase + aoff);
+        } else {
+          const uint32_t aoff = (uint32_t)(tail0 * 256 + ((j0 - tail0) >> 4) * 4096);
+          ahi = sw32_kmajor_desc(abase + aoff);
+          alo = sw32_kmajor_desc(lbase + aoff);
+        }
+        const uint64_t bd = sw32_kmajor_desc(bst + kk * kbytes);
+        mma_f16(dm, ahi, bd, idesc, (first && kk == 0) ? 0u : 1u);
+        if (two) mma_f16(dsmall, alo, bd, idesc, (c == 0 && kk == 0) ? 0u : 1u);
+      }
+      tc_commit(&empty_bar[s]);
+      if (++s == p.stages) {
+        s = 0;
+        ph ^= 1u;
+      }
+    }
+    if (ok) tc_commit(t_full);
+  }
+  tc_commit(drain_bar);
+  mbar_wait_drain(drain_bar, 0u, 500000000ull);
+}
+
+template <int FMT, bool MULTI, bool FACT>
 __global__ void __launch_bounds__(FUSED_THREADS, 1)
     density_fused_kernel(const __grid_constant__ FusedParams p) {
   extern __shared__ uint8_t smem_dyn[];
@@ -1295,9 +1419,15 @@ __global__ void __launch_bounds__(FUSED_THREADS, 1)
   const uint32_t tmem = tmem_slot;
 
   if (warp == 0) {
-    if (lane == 0) fused_produce_u<MULTI>(&p, stages, full_bar, empty_bar, &abort_flag);
+    if (lane == 0) {
+      if (FACT) fact_produce(p, stages, full_bar, empty_bar, &abort_flag);
+      else fused_produce_u<MULTI>(&p, stages, full_bar, empty_bar, &abort_flag);
+    }
   } else if (warp == 1) {
-    if (lane == 0)
+    if (lane == 0 && FACT)
+      fact_issue(p, smem_u32(A_hi), smem_u32(A_lo), stages, tmem, full_bar, empty_bar, chunk_bar, &t_full, &drain_bar,
+                 &abort_flag);
+    else if (lane == 0)
       fused_issue_mma<MULTI>(&p, smem_u32(A_hi), smem_u32(A_lo), stages, tmem, full_bar, empty_bar, chunk_bar, &t_full,
                       &drain_bar, &abort_flag);
   } else {
@@ -1385,45 +1515,79 @@ __global__ void __launch_bounds__(FUSED_THREADS, 1)
       tc_fence_after();
       double acc[2] = {0.0, 0.0};
       const uint32_t trow = tmem + ((uint32_t)(q * 32) << 16);
-      for (int c = hh; c * 16 < n16; c += FUSED_NCW / 4) {
-        const int col = c * 16;
-        // the TMEM load of T' is in flight while the row's Phi' units are read from shared memory
-        uint32_t tv[16];
-        tmem_ld16_issue(trow + (uint32_t)col, tv);
-        float ph[16];
-        // the row's two 16-byte units of columns col .. col + 15 (layout of a_offset)
-        uint32_t rbase, uo[2];
-        if (col < tail0) {
-          const int u0 = (col & 63) >> 3;
-          rbase = (uint32_t)((col >> 6) * 16384 + (row >> 3) * 1024 + (row & 7) * 128);
-          uo[0] = (uint32_t)((u0 ^ (row & 7)) * 16);
-          uo[1] = (uint32_t)(((u0 + 1) ^ (row & 7)) * 16);
-        } else {
-          rbase = (uint32_t)(tail0 * 256 + ((col - tail0) >> 4) * 4096 + row * 32);
-          uo[0] = (uint32_t)(((row >> 2) & 1) << 4);
-          uo[1] = 16u - uo[0];
-        }
-        const uint8_t* rb = A_hi + rbase;
+      if (FACT) {
+        // T = the accumulators' sum (FP32, rounded), rho = sum_k 2^-2h_k T_ik^2 over this warp's
+        // column chunks (FP64: the terms are all positive); M.gsc holds the scales 2^-2h_k
+        // (each accumulator: nb columns of A_x B_hi, then with two pieces nb of A_x B_lo)
+        const int nb = M.nb, nfull = two ? 2 * nb : nb;
+        const int ngrp = (fact_nacc(M.nchunks, nb, two) + (two ? 1 : 0)) * (two ? 2 : 1);
+        for (int c = hh; c * 16 < nb; c += FUSED_NCW / 4) {
+          float tsum[16];
 #pragma unroll
-        for (int u = 0; u < 2; ++u) unpack8<FMT>(*reinterpret_cast<const uint4*>(rb + uo[u]), ph + 8 * u);
-        if (two) {
-          const uint8_t* rl = A_lo + rbase;
+          for (int k = 0; k < 16; ++k) tsum[k] = 0.f;
+          for (int gi = 0; gi < ngrp; gi += 2) {   // column group gi: accumulator gi / 2, half gi % 2
+            uint32_t t0[16], t1[16];
+            const uint32_t c0 = (uint32_t)((two ? (gi >> 1) * nfull + (gi & 1) * nb : gi * nb) + c * 16);
+            const uint32_t c1 = (uint32_t)((two ? ((gi + 1) >> 1) * nfull + ((gi + 1) & 1) * nb : (gi + 1) * nb) + c * 16);
+            tmem_ld16_issue(trow + c0, t0);
+            if (gi + 1 < ngrp) tmem_ld16_issue(trow + c1, t1);
+            tmem_ld16_wait(t0);
+            if (gi + 1 < ngrp) {
+              tmem_ld16_wait(t1);
 #pragma unroll
-          for (int u = 0; u < 2; ++u) {
-            float lo8[8];
-            unpack8<FMT>(*reinterpret_cast<const uint4*>(rl + uo[u]), lo8);
+              for (int k = 0; k < 16; ++k) tsum[k] += __uint_as_float(t0[k]) + __uint_as_float(t1[k]);
+            } else {
 #pragma unroll
-            for (int e = 0; e < 8; ++e) ph[8 * u + e] += lo8[e];
+              for (int k = 0; k < 16; ++k) tsum[k] += __uint_as_float(t0[k]);
+            }
+          }
+#pragma unroll
+          for (int k = 0; k < 16; ++k) {
+            const double v = (double)tsum[k];
+            acc[k & 1] = fma(__ldg(M.gsc + c * 16 + k) * v, v, acc[k & 1]);
           }
         }
-        tmem_ld16_wait(tv);
-        // eight products per FP32 partial, partials summed in FP64 (the FP32 partials add
-        // ~3e-8 relative error; converting every product to FP64 ties up the conversion pipe)
-        float a32[2] = {0.f, 0.f};
+      } else {
+        for (int c = hh; c * 16 < n16; c += FUSED_NCW / 4) {
+          const int col = c * 16;
+          // the TMEM load of T' is in flight while the row's Phi' units are read from shared memory
+          uint32_t tv[16];
+          tmem_ld16_issue(trow + (uint32_t)col, tv);
+          float ph[16];
+          // the row's two 16-byte units of columns col .. col + 15 (layout of a_offset)
+          uint32_t rbase, uo[2];
+          if (col < tail0) {
+            const int u0 = (col & 63) >> 3;
+            rbase = (uint32_t)((col >> 6) * 16384 + (row >> 3) * 1024 + (row & 7) * 128);
+            uo[0] = (uint32_t)((u0 ^ (row & 7)) * 16);
+            uo[1] = (uint32_t)(((u0 + 1) ^ (row & 7)) * 16);
+          } else {
+            rbase = (uint32_t)(tail0 * 256 + ((col - tail0) >> 4) * 4096 + row * 32);
+            uo[0] = (uint32_t)(((row >> 2) & 1) << 4);
+            uo[1] = 16u - uo[0];
+          }
+          const uint8_t* rb = A_hi + rbase;
 #pragma unroll
-        for (int k = 0; k < 16; ++k) a32[k & 1] = fmaf(ph[k], __uint_as_float(tv[k]), a32[k & 1]);
-        acc[0] += (double)a32[0];
-        acc[1] += (double)a32[1];
+          for (int u = 0; u < 2; ++u) unpack8<FMT>(*reinterpret_cast<const uint4*>(rb + uo[u]), ph + 8 * u);
+          if (two) {
+            const uint8_t* rl = A_lo + rbase;
+#pragma unroll
+            for (int u = 0; u < 2; ++u) {
+              float lo8[8];
+              unpack8<FMT>(*reinterpret_cast<const uint4*>(rl + uo[u]), lo8);
+#pragma unroll
+              for (int e = 0; e < 8; ++e) ph[8 * u + e] += lo8[e];
+            }
+          }
+          tmem_ld16_wait(tv);
+          // eight products per FP32 partial, partials summed in FP64 (the FP32 partials add
+          // ~3e-8 relative error; converting every product to FP64 ties up the conversion pipe)
+          float a32[2] = {0.f, 0.f};
+#pragma unroll
+          for (int k = 0; k < 16; ++k) a32[k & 1] = fmaf(ph[k], __uint_as_float(tv[k]), a32[k & 1]);
+          acc[0] += (double)a32[0];
+          acc[1] += (double)a32[1];
+        }
       }
       tc_fence_before();
       rho_part[hh][row] = acc[0] + acc[1];
@@ -1438,7 +1602,7 @@ __global__ void __launch_bounds__(FUSED_THREADS, 1)
         }
         int64_t vox, ix, iy, iz;
         if (tile_voxel(M.pm, lt, ct, vox, ix, iy, iz)) {
-          const float qv = (float)(r * M.gsc[2] * M.outscale);
+          const float qv = (float)(r * (FACT ? 1.0 : M.gsc[2]) * M.outscale);
           M.qube[vox] = qv;
           mysum = qv;
         }
@@ -1573,6 +1737,96 @@ static qmt_status ensure_fused_operands(qmt_mol* m, int prec, const TcShape& sh,
   return QMT_OK;
 }
 
+// ---- factored density matrix -----------------------------------------------------------------
+// A density matrix of rank r (r = occupied orbitals for an SCF density, P = 2 C_occ C_occ^T) is
+// P = L L^T with L n x r, and then rho_i = sum_jk Phi_ij P_jk Phi_ik = sum_k (Phi L)_ik^2: the
+// contraction needs N = r columns instead of n.  L comes from a pivoted Cholesky factorisation in
+// FP64 (largest remaining diagonal first), stopped once every remaining diagonal element is at
+// most kFactorTol of the largest one; the factor is used when the matrix it leaves out is at most
+// kFactorResid of max |P| (float32 input rounding is ~6e-8) and the rank is at most half of n.
+// A matrix that is not positive semi-definite, or of high rank, takes the unfactored path.
+constexpr double kFactorTol = 1e-7;
+constexpr double kFactorResid = 2e-7;
+constexpr int kFactorMaxRank = 64;    // N = 2 x 64 per MMA and three main accumulators (fact_nacc)
+
+// The scaled factor W_jk = L_jk 2^(h_k - s_j) (so Phi' W = 2^h_k (Phi L)_k, each column scaled
+// to a maximum near 2^14) split into hi + lo pieces, as the fused kernel streams it: K-step block
+// j / 16 holds the r16 hi rows, then (two pieces) the r16 lo rows, one row per factor column k of
+// 32 bytes (functions j .. j + 15 of that column, the two 16-byte units exchanged when bit 2 of the
+// row is set), so that one MMA of N = 2 r16 takes both and four consecutive blocks are one
+// stage.  The column scales 2^-2h_k of the squares go to d_fact_scale.  Sets fact_rank = 0 when
+// the matrix is not factored.
+static qmt_status ensure_factor(qmt_mol* m, int prec, const TcShape& sh, cudaStream_t s) {
+  if (m->fact_prec == prec) return QMT_OK;
+  qmt_status st;
+  if ((st = ensure_basis_operands(m, sh.kpad, s))) return st;
+  const int n = m->norbs, np = m->npad, n16 = (n + 15) / 16 * 16;
+  const std::vector<double>& P = m->host_P64();
+  double dmax = 0.0, pmax = 0.0;
+  for (int j = 0; j < n; ++j) dmax = std::max(dmax, P[(size_t)j * np + j]);
+  for (int j = 0; j < n; ++j)
+    for (int k = 0; k < n; ++k) pmax = std::max(pmax, std::fabs(P[(size_t)j * np + k]));
+  m->fact_prec = prec;
+  m->fact_rank = 0;
+  const int rmax = std::min(kFactorMaxRank, n16 / 2);
+  std::vector<double> L;            // column k at L[k * n .. k * n + n)
+  std::vector<double> d(n);
+  for (int j = 0; j < n; ++j) d[j] = P[(size_t)j * np + j];
+  int r = 0;
+  for (;;) {
+    int jp = 0;
+    for (int j = 1; j < n; ++j)
+      if (d[j] > d[jp]) jp = j;
+    if (!(d[jp] > kFactorTol * dmax)) break;
+    if (r == rmax) return QMT_OK;   // rank too high for the factored path to pay
+    const double piv = std::sqrt(d[jp]);
+    L.resize((size_t)(r + 1) * n);
+    double* col = L.data() + (size_t)r * n;
+    for (int i = 0; i < n; ++i) {
+      double v = P[(size_t)i * np + jp];
+      for (int q = 0; q < r; ++q) v -= L[(size_t)q * n + i] * L[(size_t)q * n + jp];
+      col[i] = v / piv;
+    }
+    col[jp] = piv;
+    for (int i = 0; i < n; ++i) d[i] -= col[i] * col[i];
+    d[jp] = 0.0;
+    ++r;
+  }
+  // what the factor leaves out
+  for (int i = 0; i < n; ++i)
+    for (int j = 0; j <= i; ++j) {
+      double v = P[(size_t)i * np + j];
+      for (int q = 0; q < r; ++q) v -= L[(size_t)q * n + i] * L[(size_t)q * n + j];
+      if (std::fabs(v) > kFactorResid * pmax) return QMT_OK;
+    }
+  const int r16 = std::max(16, (r + 15) / 16 * 16);
+  const size_t kblock = (size_t)sh.nsplit * r16 * 16;   // elements of one K-step block
+  const size_t total = (size_t)(n16 / 16) * kblock * 2;  // bytes
+  std::vector<uint8_t> buf(total, 0), spare(total, 0);
+  uint8_t* lo = sh.nsplit == 2 ? buf.data() + (size_t)r16 * 32 : spare.data();
+  std::vector<double> sc(r16, 0.0);
+  for (int q = 0; q < r; ++q) {
+    double wmax = 0.0;
+    for (int j = 0; j < n; ++j) wmax = std::max(wmax, std::fabs(L[(size_t)q * n + j] * m->split_inv[j]));
+    int h = wmax > 0 ? (int)std::floor(std::log2(16000.0 / wmax)) : 0;
+    h = std::max(-100, std::min(100, h));
+    sc[q] = std::ldexp(1.0, -2 * h);
+    for (int j = 0; j < n; ++j) {
+      const double w = std::ldexp(L[(size_t)q * n + j] * m->split_inv[j], h);
+      const int e = j & 15, pe = ((((e >> 3) ^ (q >> 2)) & 1) << 3) | (e & 7);
+      split_host(w, sh.fmt, buf.data(), lo, (size_t)(j >> 4) * kblock + (size_t)q * 16 + pe);
+    }
+  }
+  if ((st = m->d_fact_B.reserve(total)) || (st = m->d_fact_scale.reserve(r16 * sizeof(double)))) return st;
+  QMT_CUDA(cudaMemcpyAsync(m->d_fact_B.ptr, buf.data(), total, cudaMemcpyHostToDevice, s));
+  QMT_CUDA(cudaMemcpyAsync(m->d_fact_scale.ptr, sc.data(), r16 * sizeof(double), cudaMemcpyHostToDevice, s));
+  // the host buffers go out of scope: the copies must have read them
+  QMT_CUDA(cudaStreamSynchronize(s));
+  m->fact_rank = r;
+  m->fact_r16 = r16;
+  return QMT_OK;
+}
+
 // Shared-memory bytes of the molecule tables staged by the fused kernel.
 static int fused_tab_bytes(const qmt_mol* m) {
   const int words = (int)(m->shells.size() + (m->alpha.size() + 1) / 2);
@@ -1583,27 +1837,33 @@ static int fused_tab_bytes(const qmt_mol* m) {
 // and of one U piece slot in a stage.
 static int fused_n16(const qmt_mol* m) { return (m->norbs + 15) / 16 * 16; }
 static uint32_t fused_a_bytes(int n16) { return 128u * (uint32_t)n16 * 2u; }
-static uint32_t fused_b_slot(int n16) { return (uint32_t)n16 * 32u; }
+static uint32_t fused_b_slot(int nb) { return (uint32_t)nb * 32u; }
 
 // U pipeline stages that fit beside A and the tables (below 2: the fused path does not fit).
+// Bytes of one stage: a K-step of B (nb rows per piece), or four for the factor.
+static long fused_stage_bytes(const TcShape& sh, int nb, bool fact) {
+  return (long)(fact ? 4 : 1) * sh.nsplit * fused_b_slot(nb);
+}
+
 template <int FMT>
-static int fused_stages(const TcShape& sh, int n16, int tab_bytes) {
+static int fused_stages(const TcShape& sh, int n16, int nb, int tab_bytes, bool fact = false) {
   int maxsm = 0, dev = 0;
   cudaGetDevice(&dev);
   cudaDeviceGetAttribute(&maxsm, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev);
   cudaFuncAttributes fa;
-  if (cudaFuncGetAttributes(&fa, density_fused_kernel<FMT, true>) != cudaSuccess) return 0;
-  const long a_bytes = fused_a_bytes(n16), stage_bytes = (long)sh.nsplit * fused_b_slot(n16);
+  if (cudaFuncGetAttributes(&fa, density_fused_kernel<FMT, true, false>) != cudaSuccess) return 0;
+  const long a_bytes = fused_a_bytes(n16), stage_bytes = fused_stage_bytes(sh, nb, fact);
   const long avail = (long)maxsm - (long)fa.sharedSizeBytes - 1024 - sh.nsplit * a_bytes - tab_bytes;
   return (int)std::max<long>(0, std::min<long>(MAX_STAGES, avail / stage_bytes));
 }
 
-// The descriptor of one molecule in a fused launch, its tiles starting at global tile `tile0`.
+// The descriptor of one molecule in a fused launch, its tiles starting at global tile `tile0`; B
+// is the scaled density matrix, or its factor (`fact`, built by ensure_factor).
 static qmt_status fused_mol_desc(qmt_mol* m, const TcShape& sh, const PointMap& pm, int64_t tile0, int64_t ntiles,
-                                 float* qube, double outscale, FusedMol& d, int& tab_bytes) {
+                                 float* qube, double outscale, FusedMol& d, int& tab_bytes, bool fact = false) {
   const int K = sh.kpad, n16 = fused_n16(m);
-  const size_t piece = (size_t)(K + 64) * K * 2;
-  const uint8_t* B = m->d_fused_B.as<uint8_t>();
+  const size_t piece = fact ? 0 : (size_t)(K + 64) * K * 2;   // (the factor's pieces are interleaved)
+  const uint8_t* B = fact ? m->d_fact_B.as<uint8_t>() : m->d_fused_B.as<uint8_t>();
   d = FusedMol{};
   d.pm = pm;
   d.tile0 = tile0;
@@ -1614,7 +1874,8 @@ static qmt_status fused_mol_desc(qmt_mol* m, const TcShape& sh, const PointMap& 
   d.ksteps = n16 / 16;
   d.nchunks = (n16 + 63) / 64;
   d.tail0 = n16 & ~63;
-  d.u_rows = K + 64;
+  d.nb = fact ? m->fact_r16 : n16;
+  d.u_rows = fact ? m->fact_r16 : K + 64;
   d.u_hi = B;
   d.u_lo = B + piece;
   if (d.nchunks > MAX_FUSED_CHUNKS) return fail(QMT_BAD_ARG, "fused density path supports kpad <= 320");
@@ -1636,22 +1897,24 @@ static qmt_status fused_mol_desc(qmt_mol* m, const TcShape& sh, const PointMap& 
   d.qube = qube;
   d.partials = m->d_partials.as<double>();
   d.outscale = outscale;
-  d.gsc = m->d_gscale.as<double>();
+  d.gsc = fact ? m->d_fact_scale.as<double>() : m->d_gscale.as<double>();
   return QMT_OK;
 }
 
 // One persistent launch over every tile of the molecules in `p` (p.one, or the device array
 // p.mols); shared memory is sized for the largest operand, stage and table of the set.
 template <int FMT>
-static qmt_status launch_fused(FusedParams& p, const TcShape& sh_max, int n16_max, int tab_bytes_max, cudaStream_t s) {
+static qmt_status launch_fused(FusedParams& p, const TcShape& sh_max, int n16_max, int nb_max, int tab_bytes_max,
+                               cudaStream_t s, bool fact = false) {
   p.nsplit = sh_max.nsplit;
   p.a_bytes = fused_a_bytes(n16_max);
-  p.b_slot = fused_b_slot(n16_max);
-  p.stage_bytes = p.nsplit * p.b_slot;
+  p.b_slot = fused_b_slot(nb_max);
+  p.stage_bytes = (uint32_t)fused_stage_bytes(sh_max, nb_max, fact);
   p.fmt = (uint32_t)sh_max.fmt;
   p.wait_ns = wait_limit_ns();
-  auto kern = p.nmol > 1 ? density_fused_kernel<FMT, true> : density_fused_kernel<FMT, false>;
-  const int stages = fused_stages<FMT>(sh_max, n16_max, tab_bytes_max);
+  auto kern = fact ? density_fused_kernel<FMT, false, true>
+                   : (p.nmol > 1 ? density_fused_kernel<FMT, true, false> : density_fused_kernel<FMT, false, false>);
+  const int stages = fused_stages<FMT>(sh_max, n16_max, nb_max, tab_bytes_max, fact);
   if (stages < 2) return fail(QMT_BAD_ARG, "fused density tile does not fit in shared memory");
   p.stages = stages;
   const size_t dyn = (size_t)p.nsplit * p.a_bytes + (size_t)stages * p.stage_bytes + tab_bytes_max + 1024;
@@ -1665,15 +1928,15 @@ static qmt_status launch_fused(FusedParams& p, const TcShape& sh_max, int n16_ma
 
 template <int FMT>
 static qmt_status run_fused(qmt_mol* m, const TcShape& sh, const PointMap& pm, int64_t ntiles, float* qube,
-                            double outscale, cudaStream_t s) {
+                            double outscale, cudaStream_t s, bool fact = false) {
   FusedParams p{};
   int tab_bytes = 0;
-  qmt_status st = fused_mol_desc(m, sh, pm, 0, ntiles, qube, outscale, p.one, tab_bytes);
+  qmt_status st = fused_mol_desc(m, sh, pm, 0, ntiles, qube, outscale, p.one, tab_bytes, fact);
   if (st) return st;
   p.nmol = 1;
   p.ntiles = ntiles;
   p.err = reinterpret_cast<int*>(m->d_scalars.as<double>() + 8);
-  return launch_fused<FMT>(p, sh, p.one.n16, tab_bytes, s);
+  return launch_fused<FMT>(p, sh, p.one.n16, p.one.nb, tab_bytes, s, fact);
 }
 
 // Builds the scaled, split density matrix and the Phi column scales for `prec`.
@@ -1798,7 +2061,7 @@ static qmt_status run_tc(qmt_mol* m, const TcShape& sh, const PointMap& pm, int6
   return QMT_OK;
 }
 
-static int g_density_path = 0;   // 0 auto, 1 staged, 2 fused
+static int g_density_path = 0;   // 0 auto, 1 staged, 2 fused, 3 fused with the factored matrix
 
 // The fused path takes fp16/bf16 contractions of up to 320 functions whose tile, stages and tables
 // fit in shared memory.
@@ -1806,7 +2069,7 @@ static bool fused_fits(const qmt_mol* mol, const TcShape& sh) {
   if (sh.fmt == FMT_TF32 || sh.kpad > 320 || 2 * mol->natoms >= (int)CHUNK_COUNT) return false;
   const int tb = fused_tab_bytes(mol);
   const int n16 = fused_n16(mol);
-  return (sh.fmt == FMT_F16 ? fused_stages<FMT_F16>(sh, n16, tb) : fused_stages<FMT_BF16>(sh, n16, tb)) >= 2;
+  return (sh.fmt == FMT_F16 ? fused_stages<FMT_F16>(sh, n16, n16, tb) : fused_stages<FMT_BF16>(sh, n16, n16, tb)) >= 2;
 }
 
 qmt_status density_tc(qmt_mol* mol, int nx, int ny, int nz, float step, float ox, float oy, float oz,
@@ -1820,13 +2083,20 @@ qmt_status density_tc(qmt_mol* mol, int nx, int ny, int nz, float step, float ox
   if ((st = mol->d_partials.reserve(ntiles * sizeof(double)))) return st;
   const double outscale = 2.0 * (double)step * step * step / pm.s3;
   const bool fusable = fused_fits(mol, sh);
-  const bool fused = g_density_path == 2 ? fusable : (g_density_path == 1 ? false : fusable);
-  if (g_density_path == 2 && !fusable)
+  const bool fused = g_density_path >= 2 ? fusable : (g_density_path == 1 ? false : fusable);
+  if (g_density_path >= 2 && !fusable)
     return fail(QMT_BAD_ARG, "fused density path needs fp16/bf16, N <= 320 and molecule tables that fit in shared memory");
+  bool fact = false;
+  if (fused && g_density_path != 2) {   // the factored matrix when there is one (automatic, or asked for)
+    if ((st = ensure_factor(mol, precision, sh, s))) return st;
+    fact = mol->fact_rank > 0;
+    if (g_density_path == 3 && !fact)
+      return fail(QMT_BAD_ARG, "factored density path needs a positive semi-definite density matrix of low rank");
+  }
   if (fused) {
-    if ((st = ensure_fused_operands(mol, precision, sh, s))) return st;
-    if (sh.fmt == FMT_F16) st = run_fused<FMT_F16>(mol, sh, pm, ntiles, qube, outscale, s);
-    else st = run_fused<FMT_BF16>(mol, sh, pm, ntiles, qube, outscale, s);
+    if (!fact && (st = ensure_fused_operands(mol, precision, sh, s))) return st;
+    if (sh.fmt == FMT_F16) st = run_fused<FMT_F16>(mol, sh, pm, ntiles, qube, outscale, s, fact);
+    else st = run_fused<FMT_BF16>(mol, sh, pm, ntiles, qube, outscale, s, fact);
   } else {
     if ((st = ensure_tc_operands(mol, precision, sh, s))) return st;
     if (sh.fmt == FMT_TF32) st = run_tc<FMT_TF32>(mol, sh, pm, ntiles, precision, qube, outscale, s);
@@ -1902,7 +2172,8 @@ static qmt_status batch_run(qmt_batch* b, int rescale, bool refresh, cudaStream_
     p.mols = b->d_fdesc.as<FusedMol>();
     p.ntiles = b->fused_tiles;
     p.err = b->d_err.as<int>();
-    if ((st = launch_fused<FMT == FMT_TF32 ? FMT_F16 : FMT>(p, b->sh_max, b->n16_max, b->tab_bytes_max, s))) return st;
+    if ((st = launch_fused<FMT == FMT_TF32 ? FMT_F16 : FMT>(p, b->sh_max, b->n16_max, b->n16_max, b->tab_bytes_max, s)))
+      return st;
   }
   for (const BatchItem& it : b->items)
     if (!it.fused && (st = run_tc<FMT>(it.mol, it.sh, it.pm, it.ntiles, b->precision, it.qube, it.outscale, s,
@@ -1987,8 +2258,8 @@ qmt_status qmt_batch_create(int nmol, qmt_mol* const* mols, const int32_t* shape
         largest = (int)i;
     }
     if (st || b->fdesc.empty()) break;
-    const int stg = b->fmt == FMT_F16 ? fused_stages<FMT_F16>(b->sh_max, b->n16_max, b->tab_bytes_max)
-                                      : fused_stages<FMT_BF16>(b->sh_max, b->n16_max, b->tab_bytes_max);
+    const int stg = b->fmt == FMT_F16 ? fused_stages<FMT_F16>(b->sh_max, b->n16_max, b->n16_max, b->tab_bytes_max)
+                                      : fused_stages<FMT_BF16>(b->sh_max, b->n16_max, b->n16_max, b->tab_bytes_max);
     if (stg >= 2) break;
     b->items[largest].fused = false;
     if ((st = batch_operands(b->items[largest], precision, false, s))) break;
@@ -2068,8 +2339,8 @@ qmt_status qmt_batch_destroy(qmt_batch* b) {
 }  // extern "C"
 
 extern "C" qmt_status qmt_set_density_path(int mode) {
-  if (mode < 0 || mode > 2)
-    return qmt::fail(QMT_BAD_ARG, "density path must be 0 (auto), 1 (staged) or 2 (fused)");
+  if (mode < 0 || mode > 3)
+    return qmt::fail(QMT_BAD_ARG, "density path must be 0 (auto), 1 (staged), 2 (fused) or 3 (fused, factored)");
   qmt::g_density_path = mode;
   return QMT_OK;
 }

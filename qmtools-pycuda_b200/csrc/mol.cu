@@ -87,7 +87,7 @@ using namespace qmt;
 qmt_mol::~qmt_mol() {
   for (DevBuf* b : {&d_coords, &d_types, &d_shells, &d_alpha, &d_coeff, &d_alpha64, &d_coeff64,
                     &d_P32, &d_P64, &d_Phi_hi, &d_Phi_lo, &d_tc_P, &d_partials,
-                    &d_scalars, &d_pairs, &d_work, &d_atom_shell, &d_fused_B, &d_fused_tab, &d_split_scale,
+                    &d_scalars, &d_pairs, &d_work, &d_atom_shell, &d_fused_B, &d_fact_B, &d_fact_scale, &d_fused_tab, &d_split_scale,
                     &d_dm_raw, &d_gscale, &d_pairs32, &d_gto_part})
     b->release();
 }
@@ -162,6 +162,7 @@ qmt_status qmt_mol::upload_dm(const float* dm, cudaStream_t s) {
   QMT_CHECK_LAUNCH("sym_dm_kernel");
   tc_prec = -1;
   fused_prec = -1;
+  fact_prec = -1;
   gto_ready = false;
   return QMT_OK;
 }
@@ -177,6 +178,7 @@ static qmt_status mol_init(qmt_mol* m, int natoms, const int32_t* types, const f
   m->coeff.clear();
   m->tc_prec = -1;
   m->fused_prec = -1;
+  m->fact_prec = -1;
   m->gto_ready = false;
   m->basis_ops_ready = false;
   m->natoms = natoms;

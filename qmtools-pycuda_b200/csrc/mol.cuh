@@ -45,6 +45,12 @@ struct qmt_mol {
   int fused_prec = -1;          // precision of the fused-path operands below
   qmt::DevBuf d_fused_B;        // scaled density matrix pieces for the fused path (hi then lo)
   qmt::DevBuf d_split_scale;    // 2^-s_j per function for the device split of the density matrix
+  std::vector<double> split_inv; // the same on the host
+  int fact_prec = -1;           // precision of the factored-path operands below (-1: not built)
+  int fact_rank = 0;            // rank of the density-matrix factor P = L L^T (0: not factored)
+  int fact_r16 = 0;             // the rank rounded up to 16 (the MMA N)
+  qmt::DevBuf d_fact_B;         // scaled factor pieces, K-step blocks of fact_r16 rows (hi then lo)
+  qmt::DevBuf d_fact_scale;     // per factor column k, the scale 2^-2h_k of its squares
   qmt::DevBuf d_fused_tab;      // fused path: packed shell records, then (alpha, scaled coefficient) pairs
   qmt::DevBuf d_coords, d_types, d_shells, d_alpha, d_coeff, d_alpha64, d_coeff64;
   qmt::DevBuf d_P32, d_P64;

@@ -55,7 +55,7 @@ def test_density_c0_all_precisions(c0, prec):
     assert abs(out.qsum - ref.sum()) <= max(10 * TOL[prec], 1e-9) * abs(ref.sum())
 
 
-@pytest.mark.parametrize("density_path", [1, 2])
+@pytest.mark.parametrize("density_path", [1, 2, 3])
 @pytest.mark.parametrize("shape", [(13, 7, 5), (33, 17, 9), (8, 4, 4)])
 def test_density_partial_tile_blocks(c0, density_path, shape):
     """Grids that are not a multiple of the 8 x 4 x 4 voxel tiles, through the C ABI (the Grid
@@ -144,9 +144,10 @@ def test_density_deterministic(c1):
     assert a.qsum == b.qsum
 
 
-@pytest.fixture(params=[1, 2], ids=["staged", "fused"])
+@pytest.fixture(params=[1, 2, 3], ids=["staged", "fused", "factored"])
 def density_path(request):
-    """Run a test once through each tensor-core implementation, then restore automatic choice."""
+    """Run a test once through each tensor-core implementation (the factored one takes the synthetic
+    molecules' rank-n_occ density matrices), then restore automatic choice."""
     from qmtools import _native as N
     N.call("qmt_set_density_path", request.param)
     yield request.param
@@ -155,7 +156,7 @@ def density_path(request):
 
 @pytest.mark.parametrize("prec", ["fp16x3", "bf16x3", "bf16"])
 def test_density_paths_agree_with_oracle(c1, density_path, prec):
-    """Staged (HBM) and fused (shared-memory) tensor-core paths, N = 294."""
+    """Staged (HBM), fused (shared-memory) and factored tensor-core paths, N = 294."""
     sm, mol = c1
     g = _small_grid(sm, 24, 0.8)
     ref = _oracle(g, mol)
@@ -205,3 +206,44 @@ def test_set_dm_and_translate_update_the_handle(basis):
     got = qmtools.QMTools.Compute_density(g, mol, precision="fp16x3", rescale=False).qube.ravel()
     assert rel_l2(got, ref) <= TOL["fp16x3"]
     mol.release()
+
+
+def test_factored_path_needs_a_low_rank_psd_matrix(basis):
+    """A density matrix that is not positive semi-definite is not factored: the automatic choice
+    falls back to the unfactored fused path (same grid as asking for it), and asking for the
+    factored path is an error.  The synthetic matrix (rank n_occ) is factored, and its grid matches
+    the unfactored one."""
+    import ctypes as C
+    from qmtools import _native as N
+    sm = syn.config_molecule("c0")
+    mol = sm.molecule(basis, qmtools.Molecule)
+    g = _small_grid(sm, 24, 0.45)
+    try:
+        grids = {}
+        for path in (2, 3, 0):
+            N.call("qmt_set_density_path", path)
+            grids[path] = qmtools.QMTools.Compute_density(g, mol, precision="fp16x3", rescale=False).qube.ravel()
+        assert rel_l2(grids[3], grids[2]) <= 1e-6
+        assert np.array_equal(grids[0], grids[3])
+        rng = np.random.default_rng(11)
+        dm = np.array(mol.dm, dtype=np.float64)
+        dm = dm + 0.05 * rng.standard_normal(dm.shape)
+        mol.set_dm(0.5 * (dm + dm.T))
+        ref = _oracle(g, mol)
+        N.call("qmt_set_density_path", 0)
+        auto = qmtools.QMTools.Compute_density(g, mol, precision="fp16x3", rescale=False).qube.ravel()
+        assert rel_l2(auto, ref) <= TOL["fp16x3"]
+        N.call("qmt_set_density_path", 2)
+        fused = qmtools.QMTools.Compute_density(g, mol, precision="fp16x3", rescale=False).qube.ravel()
+        assert np.array_equal(auto, fused)
+        N.call("qmt_set_density_path", 3)
+        nx, ny, nz, h, ox, oy, oz = g._geom()
+        import torch
+        q = torch.zeros(nx * ny * nz, device="cuda")
+        st = N.load().qmt_density(mol.handle, nx, ny, nz, C.c_float(h), C.c_float(ox), C.c_float(oy), C.c_float(oz),
+                                  1, N.PREC["fp16x3"], 0, C.c_void_p(q.data_ptr()), None, N.stream_handle())
+        assert st == N.BAD_ARG
+        assert b"factored" in N.load().qmt_last_error()
+    finally:
+        N.call("qmt_set_density_path", 0)
+        mol.release()

@@ -59,7 +59,7 @@ def test_jacobi_grid_barrier_gives_up_and_recovers(grid_barrier_path):
     assert torch.equal(v, ref_v)
 
 
-@pytest.mark.parametrize("path", [2, 1], ids=["fused", "staged"])
+@pytest.mark.parametrize("path", [2, 1, 3], ids=["fused", "staged", "factored"])
 def test_density_pipeline_waits_give_up_and_recover(basis, path):
     """Both tensor-core kernels (fused: shared-memory Phi'; staged: TMA-fed) give up on their
     pipeline barriers; the sticky flag is reported by the call that returns the sum, cleared,
