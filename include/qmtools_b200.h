@@ -115,8 +115,11 @@ qmt_status qmt_density(qmt_mol* mol, int nx, int ny, int nz, float step,
  * density matrix when it has one), 1 = staged (basis values through HBM), 2 = fused (basis values
  * stay in shared memory), 3 = fused with the factored density matrix: P = L L^T from a pivoted
  * Cholesky factorisation (FP64, on the host, once per matrix) and rho = sum_k (Phi L)_k^2, which
- * needs rank(P) columns instead of N -- for a positive semi-definite P whose rank is at most N/2
- * (an SCF density matrix has the rank of its occupied orbitals); QMT_BAD_ARG otherwise. */
+ * needs rank(P) columns instead of N -- for a positive semi-definite P of rank at most
+ * min(64, N/2) (an SCF density matrix has the rank of its occupied orbitals); QMT_BAD_ARG when the
+ * factorisation finds P indefinite or of higher rank.  What the factor leaves out is checked on
+ * the device (max |P - L L^T| <= 2e-7 max |P|), which runs the unfactored kernel instead when the
+ * check fails, without a host round trip. */
 qmt_status qmt_set_density_path(int mode);
 
 /* ---- batches of molecules (new; no reference counterpart) ---------------------------- */

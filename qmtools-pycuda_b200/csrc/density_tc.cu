@@ -575,6 +575,8 @@ struct FusedParams {
   uint32_t fmt;
   int* err;
   uint64_t wait_ns;        // limit of every bounded wait (a test shortens it)
+  const int* gate;         // when set, the launch runs only if *gate == gate_want (the device-side
+  int gate_want;           // check of the factored matrix picks one of two launches)
 };
 
 // Factored path: a stage holds the factor's hi rows followed by its lo rows, so one MMA of
@@ -1362,6 +1364,7 @@ template <int FMT, bool MULTI, bool FACT>
 __global__ void __launch_bounds__(FUSED_THREADS, 1)
     density_fused_kernel(const __grid_constant__ FusedParams p) {
   extern __shared__ uint8_t smem_dyn[];
+  if (p.gate && *p.gate != p.gate_want) return;   // the other launch of the pair does the work
   __shared__ __align__(8) uint64_t full_bar[MAX_STAGES], empty_bar[MAX_STAGES];
   __shared__ __align__(8) uint64_t chunk_bar[MAX_FUSED_CHUNKS], t_full, drain_bar;
   __shared__ int item_ctr;
@@ -1745,6 +1748,49 @@ static qmt_status ensure_fused_operands(qmt_mol* m, int prec, const TcShape& sh,
 // most kFactorTol of the largest one; the factor is used when the matrix it leaves out is at most
 // kFactorResid of max |P| (float32 input rounding is ~6e-8) and the rank is at most half of n.
 // A matrix that is not positive semi-definite, or of high rank, takes the unfactored path.
+// Raises *bad when some |P_ij - sum_q L_iq L_jq| (i >= j) exceeds tol; L row i at L[i * ld].
+__global__ void fact_residual_kernel(const double* __restrict__ P, int np, const double* __restrict__ L, int n, int ld,
+                                     int r, double tol, int* bad) {
+  const int64_t tot = (int64_t)n * n;
+  for (int64_t idx = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; idx < tot; idx += (int64_t)gridDim.x * blockDim.x) {
+    const int i = (int)(idx / n), j = (int)(idx - (int64_t)i * n);
+    if (j > i) continue;
+    double v = P[(size_t)i * np + j];
+    const double* li = L + (size_t)i * ld;
+    const double* lj = L + (size_t)j * ld;
+    for (int q = 0; q < r; ++q) v -= li[q] * lj[q];
+    if (fabs(v) > tol) *bad = 1;
+  }
+}
+
+// The factor's stage layout (ensure_factor): element (j, q), j < n16, q < r16, of W = L_jq 2^-s_j
+// 2^h_q (zero outside j < n, q < r) split into hi + lo (fp16 or bf16, as split_host); K-step block j / 16 holds nsplit x r16 rows
+// of 32 bytes (hi rows, then lo rows), the two 16-byte units of a row exchanged when bit 2 of the
+// row is set.
+__global__ void fact_split_kernel(const double* __restrict__ L, int n, int ld, int r, int n16, int r16,
+                                  const double* __restrict__ inv_s, const double* __restrict__ two_h, int fmt,
+                                  int nsplit, uint8_t* __restrict__ out) {
+  const int64_t tot = (int64_t)n16 * r16;
+  for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < tot; i += (int64_t)gridDim.x * blockDim.x) {
+    const int j = (int)(i / r16), q = (int)(i - (int64_t)j * r16);
+    const double w = (j < n && q < r) ? L[(size_t)j * ld + q] * inv_s[j] * two_h[q] : 0.0;
+    const int e = j & 15, pe = ((((e >> 3) ^ (q >> 2)) & 1) << 3) | (e & 7);
+    const size_t idx = (size_t)(j >> 4) * nsplit * r16 * 16 + (size_t)q * 16 + pe;
+    uint16_t hi, lo;
+    if (fmt == FMT_F16) {
+      const __half h = __float2half_rn((float)w);
+      hi = __half_as_ushort(h);
+      lo = __half_as_ushort(__float2half_rn((float)(w - (double)__half2float(h))));
+    } else {
+      const __nv_bfloat16 h = __float2bfloat16_rn((float)w);
+      hi = __bfloat16_as_ushort(h);
+      lo = __bfloat16_as_ushort(__float2bfloat16_rn((float)(w - (double)__bfloat162float(h))));
+    }
+    reinterpret_cast<uint16_t*>(out)[idx] = hi;
+    if (nsplit == 2) reinterpret_cast<uint16_t*>(out)[idx + (size_t)r16 * 16] = lo;
+  }
+}
+
 constexpr double kFactorTol = 1e-7;
 constexpr double kFactorResid = 2e-7;
 constexpr int kFactorMaxRank = 64;    // N = 2 x 64 per MMA and three main accumulators (fact_nacc)
@@ -1769,7 +1815,8 @@ static qmt_status ensure_factor(qmt_mol* m, int prec, const TcShape& sh, cudaStr
   m->fact_prec = prec;
   m->fact_rank = 0;
   const int rmax = std::min(kFactorMaxRank, n16 / 2);
-  std::vector<double> L;            // column k at L[k * n .. k * n + n)
+  // L row by row (row i at Lr[i * rmax]), so that the dot products run over contiguous memory
+  std::vector<double> Lr((size_t)n * rmax, 0.0);
   std::vector<double> d(n);
   for (int j = 0; j < n; ++j) d[j] = P[(size_t)j * np + j];
   int r = 0;
@@ -1779,49 +1826,67 @@ static qmt_status ensure_factor(qmt_mol* m, int prec, const TcShape& sh, cudaStr
       if (d[j] > d[jp]) jp = j;
     if (!(d[jp] > kFactorTol * dmax)) break;
     if (r == rmax) return QMT_OK;   // rank too high for the factored path to pay
-    const double piv = std::sqrt(d[jp]);
-    L.resize((size_t)(r + 1) * n);
-    double* col = L.data() + (size_t)r * n;
+    const double piv = std::sqrt(d[jp]), ipiv = 1.0 / piv;
+    const double* lj = Lr.data() + (size_t)jp * rmax;
     for (int i = 0; i < n; ++i) {
-      double v = P[(size_t)i * np + jp];
-      for (int q = 0; q < r; ++q) v -= L[(size_t)q * n + i] * L[(size_t)q * n + jp];
-      col[i] = v / piv;
+      const double* li = Lr.data() + (size_t)i * rmax;
+      double a0 = 0, a1 = 0, a2 = 0, a3 = 0;
+      int q = 0;
+      for (; q + 4 <= r; q += 4) {
+        a0 += li[q] * lj[q];
+        a1 += li[q + 1] * lj[q + 1];
+        a2 += li[q + 2] * lj[q + 2];
+        a3 += li[q + 3] * lj[q + 3];
+      }
+      for (; q < r; ++q) a0 += li[q] * lj[q];
+      Lr[(size_t)i * rmax + r] = (P[(size_t)i * np + jp] - ((a0 + a1) + (a2 + a3))) * ipiv;
     }
-    col[jp] = piv;
-    for (int i = 0; i < n; ++i) d[i] -= col[i] * col[i];
+    Lr[(size_t)jp * rmax + r] = piv;
+    for (int i = 0; i < n; ++i) d[i] -= Lr[(size_t)i * rmax + r] * Lr[(size_t)i * rmax + r];
     d[jp] = 0.0;
     ++r;
   }
-  // what the factor leaves out
+  // an indefinite matrix leaves clearly negative diagonal elements behind
   for (int i = 0; i < n; ++i)
-    for (int j = 0; j <= i; ++j) {
-      double v = P[(size_t)i * np + j];
-      for (int q = 0; q < r; ++q) v -= L[(size_t)q * n + i] * L[(size_t)q * n + j];
-      if (std::fabs(v) > kFactorResid * pmax) return QMT_OK;
-    }
+    if (d[i] < -10.0 * kFactorTol * dmax) return QMT_OK;
+  // what the factor leaves out, max |P - L L^T|, is checked on the device (n^2 r products) into
+  // the gate flag, without a round trip: the factored launch runs when it is 0, the unfactored
+  // one when it is 1 (density_tc)
+  {
+    const size_t lbytes = (size_t)n * rmax * sizeof(double);
+    if ((st = m->d_fact_L.reserve(lbytes + 16))) return st;
+    int* flag = reinterpret_cast<int*>(m->d_fact_L.as<uint8_t>() + lbytes);
+    QMT_CUDA(cudaMemcpyAsync(m->d_fact_L.ptr, Lr.data(), lbytes, cudaMemcpyHostToDevice, s));
+    QMT_CUDA(cudaMemsetAsync(flag, 0, sizeof(int), s));
+    const int64_t tot = (int64_t)n * n;
+    const int blocks = (int)std::min<int64_t>((tot + 255) / 256, (int64_t)sm_count() * 4);
+    fact_residual_kernel<<<std::max(blocks, 1), 256, 0, s>>>(m->d_P64.as<double>(), np, m->d_fact_L.as<double>(), n,
+                                                             rmax, r, kFactorResid * pmax, flag);
+    QMT_CHECK_LAUNCH("fact_residual_kernel");
+    m->fact_gate = flag;
+  }
+  // column scales on the host (2^-2h_k for the squares, then 2^h_k for the split), the scaled,
+  // split factor in its stage layout on the device
   const int r16 = std::max(16, (r + 15) / 16 * 16);
-  const size_t kblock = (size_t)sh.nsplit * r16 * 16;   // elements of one K-step block
-  const size_t total = (size_t)(n16 / 16) * kblock * 2;  // bytes
-  std::vector<uint8_t> buf(total, 0), spare(total, 0);
-  uint8_t* lo = sh.nsplit == 2 ? buf.data() + (size_t)r16 * 32 : spare.data();
-  std::vector<double> sc(r16, 0.0);
+  std::vector<double> sc(2 * r16, 0.0);
   for (int q = 0; q < r; ++q) {
     double wmax = 0.0;
-    for (int j = 0; j < n; ++j) wmax = std::max(wmax, std::fabs(L[(size_t)q * n + j] * m->split_inv[j]));
+    for (int j = 0; j < n; ++j) wmax = std::max(wmax, std::fabs(Lr[(size_t)j * rmax + q] * m->split_inv[j]));
     int h = wmax > 0 ? (int)std::floor(std::log2(16000.0 / wmax)) : 0;
     h = std::max(-100, std::min(100, h));
     sc[q] = std::ldexp(1.0, -2 * h);
-    for (int j = 0; j < n; ++j) {
-      const double w = std::ldexp(L[(size_t)q * n + j] * m->split_inv[j], h);
-      const int e = j & 15, pe = ((((e >> 3) ^ (q >> 2)) & 1) << 3) | (e & 7);
-      split_host(w, sh.fmt, buf.data(), lo, (size_t)(j >> 4) * kblock + (size_t)q * 16 + pe);
-    }
+    sc[r16 + q] = std::ldexp(1.0, h);
   }
-  if ((st = m->d_fact_B.reserve(total)) || (st = m->d_fact_scale.reserve(r16 * sizeof(double)))) return st;
-  QMT_CUDA(cudaMemcpyAsync(m->d_fact_B.ptr, buf.data(), total, cudaMemcpyHostToDevice, s));
-  QMT_CUDA(cudaMemcpyAsync(m->d_fact_scale.ptr, sc.data(), r16 * sizeof(double), cudaMemcpyHostToDevice, s));
-  // the host buffers go out of scope: the copies must have read them
-  QMT_CUDA(cudaStreamSynchronize(s));
+  const size_t total = (size_t)(n16 / 16) * sh.nsplit * r16 * 32;   // bytes
+  if ((st = m->d_fact_B.reserve(total)) || (st = m->d_fact_scale.reserve(2 * r16 * sizeof(double)))) return st;
+  QMT_CUDA(cudaMemcpyAsync(m->d_fact_scale.ptr, sc.data(), 2 * r16 * sizeof(double), cudaMemcpyHostToDevice, s));
+  const int64_t tot = (int64_t)n16 * r16;
+  const int blocks = (int)std::min<int64_t>((tot + 255) / 256, (int64_t)sm_count() * 4);
+  fact_split_kernel<<<std::max(blocks, 1), 256, 0, s>>>(m->d_fact_L.as<double>(), n, rmax, r, n16, r16,
+                                                         m->d_split_scale.as<double>(),
+                                                         m->d_fact_scale.as<double>() + r16, sh.fmt, sh.nsplit,
+                                                         m->d_fact_B.as<uint8_t>());
+  QMT_CHECK_LAUNCH("fact_split_kernel");
   m->fact_rank = r;
   m->fact_r16 = r16;
   return QMT_OK;
@@ -1928,11 +1993,14 @@ static qmt_status launch_fused(FusedParams& p, const TcShape& sh_max, int n16_ma
 
 template <int FMT>
 static qmt_status run_fused(qmt_mol* m, const TcShape& sh, const PointMap& pm, int64_t ntiles, float* qube,
-                            double outscale, cudaStream_t s, bool fact = false) {
+                            double outscale, cudaStream_t s, bool fact = false, const int* gate = nullptr,
+                            int gate_want = 0) {
   FusedParams p{};
   int tab_bytes = 0;
   qmt_status st = fused_mol_desc(m, sh, pm, 0, ntiles, qube, outscale, p.one, tab_bytes, fact);
   if (st) return st;
+  p.gate = gate;
+  p.gate_want = gate_want;
   p.nmol = 1;
   p.ntiles = ntiles;
   p.err = reinterpret_cast<int*>(m->d_scalars.as<double>() + 8);
@@ -2094,9 +2162,16 @@ qmt_status density_tc(qmt_mol* mol, int nx, int ny, int nz, float step, float ox
       return fail(QMT_BAD_ARG, "factored density path needs a positive semi-definite density matrix of low rank");
   }
   if (fused) {
-    if (!fact && (st = ensure_fused_operands(mol, precision, sh, s))) return st;
-    if (sh.fmt == FMT_F16) st = run_fused<FMT_F16>(mol, sh, pm, ntiles, qube, outscale, s, fact);
-    else st = run_fused<FMT_BF16>(mol, sh, pm, ntiles, qube, outscale, s, fact);
+    // with a factor, the device check of what it leaves out picks the launch (no host round trip)
+    if ((st = ensure_fused_operands(mol, precision, sh, s))) return st;
+    const int* gate = fact ? mol->fact_gate : nullptr;
+    if (sh.fmt == FMT_F16) {
+      if (fact) st = run_fused<FMT_F16>(mol, sh, pm, ntiles, qube, outscale, s, true, gate, 0);
+      if (!st) st = run_fused<FMT_F16>(mol, sh, pm, ntiles, qube, outscale, s, false, gate, 1);
+    } else {
+      if (fact) st = run_fused<FMT_BF16>(mol, sh, pm, ntiles, qube, outscale, s, true, gate, 0);
+      if (!st) st = run_fused<FMT_BF16>(mol, sh, pm, ntiles, qube, outscale, s, false, gate, 1);
+    }
   } else {
     if ((st = ensure_tc_operands(mol, precision, sh, s))) return st;
     if (sh.fmt == FMT_TF32) st = run_tc<FMT_TF32>(mol, sh, pm, ntiles, precision, qube, outscale, s);

@@ -50,6 +50,8 @@ struct qmt_mol {
   int fact_rank = 0;            // rank of the density-matrix factor P = L L^T (0: not factored)
   int fact_r16 = 0;             // the rank rounded up to 16 (the MMA N)
   qmt::DevBuf d_fact_B;         // scaled factor pieces, K-step blocks of fact_r16 rows (hi then lo)
+  qmt::DevBuf d_fact_L;         // the factor (FP64, row by row) and a flag, for the residual check
+  const int* fact_gate = nullptr; // that flag: 0 when the factor reproduces P, 1 when it does not
   qmt::DevBuf d_fact_scale;     // per factor column k, the scale 2^-2h_k of its squares
   qmt::DevBuf d_fused_tab;      // fused path: packed shell records, then (alpha, scaled coefficient) pairs
   qmt::DevBuf d_coords, d_types, d_shells, d_alpha, d_coeff, d_alpha64, d_coeff64;

@@ -209,10 +209,10 @@ def test_set_dm_and_translate_update_the_handle(basis):
 
 
 def test_factored_path_needs_a_low_rank_psd_matrix(basis):
-    """A density matrix that is not positive semi-definite is not factored: the automatic choice
-    falls back to the unfactored fused path (same grid as asking for it), and asking for the
-    factored path is an error.  The synthetic matrix (rank n_occ) is factored, and its grid matches
-    the unfactored one."""
+    """A density matrix that is not positive semi-definite is not factored (the host factorisation
+    finds it indefinite): the automatic choice falls back to the unfactored fused path (same grid
+    as asking for it), and asking for the factored path is an error.  The synthetic matrix (rank
+    n_occ) is factored, and its grid matches the unfactored one."""
     import ctypes as C
     from qmtools import _native as N
     sm = syn.config_molecule("c0")
