@@ -702,10 +702,20 @@ def run_ours(args, world, rank, local, pg):
     peak_tf, hbm, kind = peaks()
     achieved = flops / (dens_ms / 1000.0) / 1e12
     traffic = profiled_traffic() if (args.precision == "fp16x3" and not args.grid) else None
-    out["roofline"] = {"bound": "tensor", "kernel": "qmt_density (basis + tcgen05 contraction + row-dot)",
+    rank = C.c_int()
+    N.call("qmt_density_factor_rank", handle, C.byref(rank), sh)
+    rank = int(rank.value)
+    r16 = max(16, (rank + 15) // 16 * 16)
+    out["roofline"] = {"bound": "tensor",
+                       "kernel": "density_fused_kernel (basis values in shared memory + tcgen05 contraction)",
                        "achieved": achieved, "peak": peak_tf, "unit": "TFLOP/s", "frac": achieved / peak_tf,
                        "peak_source": f"bf16_tflops burst, {kind}", "density_ms": dens_ms,
                        "algorithmic_flop_per_launch": flops,
+                       "algorithmic_flop_definition": "npts (2 N^2 + 2 N): Phi P plus the row-dot",
+                       "contraction": (f"factored density matrix P = L L^T, rank {rank}: rho = sum_k (Phi L)_k^2, "
+                                       f"MMA N = {2 * r16} (hi and lo rows of L) x 2 products, "
+                                       f"{npts * 2.0 * nb * 2 * r16 * 2:.3e} tensor flop per launch"
+                                       if rank else "unfactored: Phi P (N columns) x 3 products, row-dot with Phi"),
                        "traffic": traffic["bytes_per_launch"] if traffic else None,
                        "traffic_unit": "DRAM bytes per launch (ncu, dram__bytes_read.sum + dram__bytes_write.sum)",
                        "traffic_source": traffic["source"] if traffic else None}
@@ -717,6 +727,12 @@ def run_ours(args, world, rank, local, pg):
     nprim = sum(int(np.count_nonzero(co[so:so + 20])) for _, so in shells)
     out["roofline"]["exponentials_per_launch"] = int(npts * nprim)
     out["roofline"]["exponentials_per_s"] = npts * nprim / (dens_ms / 1000.0)
+    # the basis evaluation bounds the factored kernel: exponentials against the SFU rate (16 per
+    # SM and clock, nominal, at the sampled clock)
+    clk = out["clocks"].get("sm_mhz") or 1965.0
+    sfu_peak = 16.0 * 148 * clk * 1e6
+    out["roofline"]["sfu_exp_peak_per_s"] = sfu_peak
+    out["roofline"]["sfu_frac"] = npts * nprim / (dens_ms / 1000.0) / sfu_peak
     check = None
     if world == 1 and not args.quick:
         # plain FP32 SIMT density (the reference's precision) on the same step
@@ -827,24 +843,7 @@ def other_kernels(basis, qmtools, N, hbm_peak, fft_ms, nfft):
                               "achieved_GBps": fbytes / (fft_ms / 1e3) / 1e9,
                               "frac_of_hbm_peak": fbytes / (fft_ms / 1e3) / 1e9 / hbm_peak,
                               "definition": "8 n^3 + 100 H bytes, H = M^2 (M/2+1), M = 2n"}
-        sm = syn.config_molecule("c1")
-        mol = sm.molecule(basis, qmtools.Molecule)
-        g = sm.grid(qmtools.Grid)
-        nx, ny, nz, h, ox, oy, oz = g._geom()
-        v = torch.zeros(nx * ny * nz, device="cuda")
-        call = lambda: N.call("qmt_hartree_gto_boundary", mol.handle, nx, ny, nz, h, ox, oy, oz,
-                              C.c_void_p(v.data_ptr()), s)
-        call()
-        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-        e0.record()
-        call()
-        e1.record()
-        torch.cuda.synchronize()
-        nb = nx * ny * nz - (nx - 2) * (ny - 2) * (nz - 2)
-        ms = e0.elapsed_time(e1)
-        out["gto_boundary_c1"] = {"ms": ms, "boundary_points": nb, "points_per_s": nb / (ms / 1e3),
-                                  "precision": "FP64 McMurchie-Davidson"}
-        mol.release()
+        out["gto_boundary_c1"] = gto_boundary(basis, qmtools, N, s)
         # the analytic potential on every corner of the small molecule's 64^3 grid: the
         # reference arm times its gpu_hartree_GTO on the same grid
         sm = syn.config_molecule("c0")
@@ -859,6 +858,43 @@ def other_kernels(basis, qmtools, N, hbm_peak, fft_ms, nfft):
                                       "precision": "FP64 McMurchie-Davidson", "points_at": "voxel corners"}
         mol.release()
     return out
+
+
+def gto_boundary(basis, qmtools, N, s, reps=3):
+    """The analytic potential on the medium molecule's grid boundary (the Dirichlet boundary of the
+    Jacobi route): the default mixed FP32/FP64 kernels against the FP64 kernel, time and rel-L2."""
+    import ctypes as C
+    import torch
+    from qmtools import synthetic as syn
+    sm = syn.config_molecule("c1")
+    mol = sm.molecule(basis, qmtools.Molecule)
+    g = sm.grid(qmtools.Grid)
+    nx, ny, nz, h, ox, oy, oz = g._geom()
+    nb = nx * ny * nz - (nx - 2) * (ny - 2) * (nz - 2)
+    res = {}
+    for name, prec in (("fp64", N.PREC["fp64"]), ("mixed", N.PREC["fp32"])):
+        v = torch.zeros(nx * ny * nz, device="cuda")
+        N.call("qmt_set_gto_precision", prec)
+        call = lambda: N.call("qmt_hartree_gto_boundary", mol.handle, nx, ny, nz, h, ox, oy, oz,
+                              C.c_void_p(v.data_ptr()), s)
+        call()
+        res[name] = (_events_ms(call, reps), v.double().cpu().numpy())
+    N.call("qmt_set_gto_precision", N.PREC["fp32"])
+    # the reference's work measure: boundary points x primitive pairs of the basis functions
+    # (p >= q) x ~40 flop
+    almos = np.asarray(mol.ALMOs).reshape(-1, 4)
+    co = np.asarray(mol.basisset.coeffs)
+    npf = np.array([int(np.count_nonzero(co[int(r[3]):int(r[3]) + 20])) for r in almos], dtype=np.float64)
+    pairs = 0.5 * (npf.sum() ** 2 + (npf ** 2).sum())
+    flops = nb * pairs * 40.0
+    ms = res["mixed"][0]
+    a, b = res["mixed"][1], res["fp64"][1]
+    mol.release()
+    return {"ms": ms, "ms_fp64_kernel": res["fp64"][0], "boundary_points": nb, "points_per_s": nb / (ms / 1e3),
+            "precision": "mixed: FP32 pair terms, FP64 for the largest pairs, near fields, atoms and sums",
+            "rel_l2_vs_fp64_kernel": float(np.linalg.norm(a - b) / np.linalg.norm(b)),
+            "algorithmic_flop": flops, "flop_definition": "boundary points x sum_{p>=q} nprim_p nprim_q x 40",
+            "achieved_tflops": flops / (ms / 1e3) / 1e12}
 
 
 TRAFFIC_JSON = ROOT / "profiles" / "density_fused_kernel_c1.traffic.json"
@@ -1088,7 +1124,7 @@ def main():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--quick", action="store_true", help="headline step only (no plain-FP32, batch, serving)")
     ap.add_argument("--grid", type=int, default=0, help="cube edge of a smaller grid for the same molecule")
-    ap.add_argument("--only", default="", choices=["", "jacobi"], help="run one kernel family alone (profiling)")
+    ap.add_argument("--only", default="", choices=["", "jacobi", "gto"], help="run one kernel family alone (profiling)")
     ap.add_argument("--ncu-import", default="", help="ncu --csv metrics capture of the fused density kernel "
                                                      "to summarise into profiles/ (no GPU needed)")
     ap.add_argument("--ncu-command", default="", help="the command line of that capture (recorded beside it)")
@@ -1107,6 +1143,19 @@ def main():
         torch.cuda.set_device(local)
         N.ensure_device(None)
         print(json.dumps(other_kernels(None, qmtools, N, peaks()[1], 0.0, None)["jacobi"]))
+        return
+    if args.only == "gto":
+        # the analytic boundary potential alone (FP64 kernel once, then the mixed kernels
+        # 1 + reps times): its profiling case
+        import ctypes as C
+        import torch
+        import qmtools
+        from qmtools import _native as N
+        qmtools.set_verbose(False)
+        torch.cuda.set_device(local)
+        N.ensure_device(None)
+        basis = qmtools.BasisSet(qmtools.BASIS_CCPVDZ)
+        print(json.dumps(gto_boundary(basis, qmtools, N, C.c_void_p(torch.cuda.current_stream().cuda_stream))))
         return
     try:
         if args.impl == "reference":

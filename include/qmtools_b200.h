@@ -122,6 +122,10 @@ qmt_status qmt_density(qmt_mol* mol, int nx, int ny, int nz, float step,
  * check fails, without a host round trip. */
 qmt_status qmt_set_density_path(int mode);
 
+/* Rank of the factor the last density call on `mol` contracted with (new): 0 when it ran the
+ * unfactored kernel.  Synchronises `stream` (the device-side check decides). */
+qmt_status qmt_density_factor_rank(qmt_mol* mol, int* rank_out, void* stream);
+
 /* ---- batches of molecules (new; no reference counterpart) ---------------------------- */
 /* The reference evaluates one molecule per Compute_density call (qmtools/qmtools.py:2381-2430).
  * A batch evaluates the densities of many molecules together: the molecules whose contraction

@@ -2413,6 +2413,18 @@ qmt_status qmt_batch_destroy(qmt_batch* b) {
 
 }  // extern "C"
 
+extern "C" qmt_status qmt_density_factor_rank(qmt_mol* mol, int* rank_out, void* stream) {
+  if (!mol || !rank_out) return qmt::fail(QMT_BAD_ARG, "null argument");
+  *rank_out = 0;
+  if (mol->fact_prec < 0 || mol->fact_rank <= 0 || !mol->fact_gate) return QMT_OK;
+  int gate = 1;
+  cudaStream_t s = qmt::as_stream(stream);
+  QMT_CUDA(cudaMemcpyAsync(&gate, mol->fact_gate, sizeof(int), cudaMemcpyDeviceToHost, s));
+  QMT_CUDA(cudaStreamSynchronize(s));
+  if (gate == 0) *rank_out = mol->fact_rank;
+  return QMT_OK;
+}
+
 extern "C" qmt_status qmt_set_density_path(int mode) {
   if (mode < 0 || mode > 3)
     return qmt::fail(QMT_BAD_ARG, "density path must be 0 (auto), 1 (staged), 2 (fused) or 3 (fused, factored)");

@@ -36,6 +36,7 @@ SIGNATURES = {
     "qmt_mol_trace_ps": [_vp, _pd, _vp],
     "qmt_density": [_vp, _i, _i, _i, _f, _f, _f, _f, _i, _i, _i, _vp, _pd, _vp],
     "qmt_set_density_path": [_i],
+    "qmt_density_factor_rank": [_vp, _pi, _vp],
     "qmt_batch_create": [_i, _vp, _vp, _vp, _i, _i, _vp, _vp, _vp, C.POINTER(_vp)],
     "qmt_batch_density": [_vp, _i, _i, _vp],
     "qmt_batch_sums": [_vp, _pd, _vp],
