@@ -129,11 +129,15 @@ qmt_status qmt_density_factor_rank(qmt_mol* mol, int* rank_out, void* stream);
 /* ---- batches of molecules (new; no reference counterpart) ---------------------------- */
 /* The reference evaluates one molecule per Compute_density call (qmtools/qmtools.py:2381-2430).
  * A batch evaluates the densities of many molecules together: the molecules whose contraction
- * takes the fused path share one persistent launch over all their tiles; the others (N > 320 or
- * tf32) get the staged path, one molecule after another; then each grid is summed and, with
- * rescale, scaled to its nuclear charge.  Inputs: shapes[3 i + (0,1,2)] = nx, ny, nz and
- * geoms[4 i + (0,1,2,3)] = step, ox, oy, oz (bohr) of molecule i; qube_devs[i] its grid (device,
- * nx ny nz floats, x-fastest); paths[i] 0 = automatic, 1 = staged, 2 = fused (NULL: automatic).
+ * takes the fused path share one persistent launch over all their tiles (one for those with a
+ * factored density matrix, one for the others); the rest (N > 320 or tf32) get the staged path,
+ * one molecule after another; then each grid is summed and, with rescale, scaled to its nuclear
+ * charge.  Inputs: shapes[3 i + (0,1,2)] = nx, ny, nz and geoms[4 i + (0,1,2,3)] = step, ox, oy,
+ * oz (bohr) of molecule i; qube_devs[i] its grid (device, nx ny nz floats, x-fastest); paths[i]
+ * 0 = automatic (fused or staged), 1 = staged, 2 = fused, 3 = fused with the factored density
+ * matrix when it has one that passes its check (as qmt_set_density_path mode 3), else fused
+ * (NULL: automatic).  A factored molecule's factor is built at creation: refresh != 0 is refused
+ * for a batch that holds one.
  * qmt_batch_create builds every operand (it synchronises `stream`); qmt_batch_density then
  * allocates nothing and is fully asynchronous, so a CUDA graph can capture it.  With refresh != 0
  * it first re-derives each molecule's split density matrix on the device from the matrix last
@@ -147,8 +151,9 @@ qmt_status qmt_batch_density(qmt_batch* batch, int rescale, int refresh, void* s
 /* FP64 grid sums before rescaling, sums[nmol] (host); synchronous; reports and clears the kernels'
  * barrier-timeout flags (QMT_CUDA_ERR). */
 qmt_status qmt_batch_sums(qmt_batch* batch, double* sums, void* stream);
-/* Molecules of the batch on the shared fused launch (-1 for NULL). */
+/* Molecules of the batch on the fused launches, and of those on the factored one (-1 for NULL). */
 int qmt_batch_fused_count(const qmt_batch* batch);
+int qmt_batch_factored_count(const qmt_batch* batch);
 qmt_status qmt_batch_destroy(qmt_batch* batch);
 
 /* ---- analytic GTO potential --------------------------------------------------------- */

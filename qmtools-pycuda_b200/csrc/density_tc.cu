@@ -1252,21 +1252,22 @@ __device__ __forceinline__ void fused_issue_mma(const FusedParams* pp, uint32_t 
   mbar_wait_drain(drain_bar, 0u, 500000000ull);
 }
 
-// Factored path (single molecule): a stage is one column chunk of the factor, its K-steps each
-// [hi rows | lo rows] (nb rows of 32 bytes apiece), one contiguous copy from HBM (ensure_factor's
-// layout).
+// Factored path: a stage is one column chunk of the factor, its K-steps each [hi rows | lo rows]
+// (nb rows of 32 bytes apiece), one contiguous copy from HBM (ensure_factor's layout).
 __device__ __forceinline__ uint32_t fact_chunk_ksteps(int c, int ksteps) { return (uint32_t)min(4, ksteps - 4 * c); }
 
+template <bool MULTI>
 __device__ __forceinline__ void fact_produce(const FusedParams& p, uint8_t* stages, uint64_t* full_bar,
                                              uint64_t* empty_bar, volatile int* abort_flag) {
-  const FusedMol& M = p.one;
-  const int ksteps = M.ksteps, nchunks = M.nchunks;
-  const uint32_t kbytes = (uint32_t)p.nsplit * (uint32_t)M.nb * 32u;   // one K-step of the factor
-  const uint8_t* const src0 = M.u_hi;
   int s = 0;
   uint32_t ph = 0, issued = 0, par = 0;
   bool ok = true;
   for (int64_t t = blockIdx.x; t < p.ntiles && ok; t += gridDim.x) {
+    int m;
+    const FusedMol& M = fused_mol<MULTI>(p, t, m);
+    const int ksteps = M.ksteps, nchunks = M.nchunks;
+    const uint32_t kbytes = (uint32_t)p.nsplit * (uint32_t)M.nb * 32u;   // one K-step of the factor
+    const uint8_t* const src0 = M.u_hi;
     for (int c = 0; c < nchunks; ++c) {
       if (!mbar_wait(&empty_bar[s], ph ^ 1u, abort_flag, p.wait_ns)) {
         ok = false;
@@ -1291,29 +1292,40 @@ __device__ __forceinline__ void fact_produce(const FusedParams& p, uint8_t* stag
 // Per chunk: wait for its columns of A and its stage, then per K-step one MMA of N = 2 nb
 // [A_hi B_hi | A_hi B_lo] into the chunk's accumulator and, with two pieces, [A_lo B_hi | A_lo B_lo]
 // into the last (fact_nacc); the stage is freed by one commit per chunk.
+template <bool MULTI>
 __device__ __forceinline__ void fact_issue(const FusedParams& p, uint32_t abase, uint32_t lbase, uint8_t* stages,
                                            uint32_t tmem, uint64_t* full_bar, uint64_t* empty_bar, uint64_t* chunk_bar,
                                            uint64_t* t_full, uint64_t* drain_bar, volatile int* abort_flag) {
-  const FusedMol& M = p.one;
   const bool two = p.nsplit == 2;
-  const int ksteps = M.ksteps, nb = M.nb, tail0 = M.tail0, nchunks = M.nchunks;
-  const int nfull = two ? 2 * nb : nb;
-  const int na = fact_nacc(nchunks, nb, two);
-  const uint32_t idesc = make_idesc(p.fmt, 128, (uint32_t)nfull);
-  const uint32_t kbytes = (uint32_t)nfull * 32u;
-  const uint32_t dsmall = tmem + (uint32_t)(na * nfull);
-  uint32_t dmain[MAX_FUSED_CHUNKS], firstmask = 0, need = 0;
-#pragma unroll
-  for (int c = 0; c < MAX_FUSED_CHUNKS; ++c) {
-    const int a = c < nchunks ? c * na / nchunks : 0;
-    dmain[c] = tmem + (uint32_t)(a * nfull);
-    if (c < nchunks && (c == 0 || (c - 1) * na / nchunks != a)) firstmask |= 1u << c;
-    if (M.chunk_need[c] > 0) need |= 1u << c;
-  }
-  int s = 0;
+  int s = 0, cur_m = -1;
   uint32_t ph = 0, cpar = 0;
+  int ksteps = 0, nb = 0, tail0 = 0, nchunks = 0;
+  uint32_t idesc = 0, kbytes = 0, dsmall = 0, firstmask = 0, need = 0;
+  uint32_t dmain[MAX_FUSED_CHUNKS];
   bool ok = true;
   for (int64_t t = blockIdx.x; t < p.ntiles && ok; t += gridDim.x) {
+    int m;
+    const FusedMol& M = fused_mol<MULTI>(p, t, m);
+    if (m != cur_m) {   // the molecule's shape of the contraction (once for a single molecule)
+      ksteps = M.ksteps;
+      nb = M.nb;
+      tail0 = M.tail0;
+      nchunks = M.nchunks;
+      const int nfull = two ? 2 * nb : nb;
+      const int na = fact_nacc(nchunks, nb, two);
+      idesc = make_idesc(p.fmt, 128, (uint32_t)nfull);
+      kbytes = (uint32_t)nfull * 32u;
+      dsmall = tmem + (uint32_t)(na * nfull);
+      firstmask = need = 0;
+#pragma unroll
+      for (int c = 0; c < MAX_FUSED_CHUNKS; ++c) {
+        const int a = c < nchunks ? c * na / nchunks : 0;
+        dmain[c] = tmem + (uint32_t)(a * nfull);
+        if (c < nchunks && (c == 0 || (c - 1) * na / nchunks != a)) firstmask |= 1u << c;
+        if (M.chunk_need[c] > 0) need |= 1u << c;
+      }
+      cur_m = m;
+    }
 #pragma unroll 1
     for (int c = 0; c < nchunks; ++c) {
       if ((need >> c) & 1u) {
@@ -1423,13 +1435,13 @@ __global__ void __launch_bounds__(FUSED_THREADS, 1)
 
   if (warp == 0) {
     if (lane == 0) {
-      if (FACT) fact_produce(p, stages, full_bar, empty_bar, &abort_flag);
+      if (FACT) fact_produce<MULTI>(p, stages, full_bar, empty_bar, &abort_flag);
       else fused_produce_u<MULTI>(&p, stages, full_bar, empty_bar, &abort_flag);
     }
   } else if (warp == 1) {
     if (lane == 0 && FACT)
-      fact_issue(p, smem_u32(A_hi), smem_u32(A_lo), stages, tmem, full_bar, empty_bar, chunk_bar, &t_full, &drain_bar,
-                 &abort_flag);
+      fact_issue<MULTI>(p, smem_u32(A_hi), smem_u32(A_lo), stages, tmem, full_bar, empty_bar, chunk_bar, &t_full,
+                        &drain_bar, &abort_flag);
     else if (lane == 0)
       fused_issue_mma<MULTI>(&p, smem_u32(A_hi), smem_u32(A_lo), stages, tmem, full_bar, empty_bar, chunk_bar, &t_full,
                       &drain_bar, &abort_flag);
@@ -1977,8 +1989,8 @@ static qmt_status launch_fused(FusedParams& p, const TcShape& sh_max, int n16_ma
   p.stage_bytes = (uint32_t)fused_stage_bytes(sh_max, nb_max, fact);
   p.fmt = (uint32_t)sh_max.fmt;
   p.wait_ns = wait_limit_ns();
-  auto kern = fact ? density_fused_kernel<FMT, false, true>
-                   : (p.nmol > 1 ? density_fused_kernel<FMT, true, false> : density_fused_kernel<FMT, false, false>);
+  auto kern = p.nmol > 1 ? (fact ? density_fused_kernel<FMT, true, true> : density_fused_kernel<FMT, true, false>)
+                         : (fact ? density_fused_kernel<FMT, false, true> : density_fused_kernel<FMT, false, false>);
   const int stages = fused_stages<FMT>(sh_max, n16_max, nb_max, tab_bytes_max, fact);
   if (stages < 2) return fail(QMT_BAD_ARG, "fused density tile does not fit in shared memory");
   p.stages = stages;
@@ -2209,25 +2221,37 @@ struct BatchItem {
   float* qube;
   double outscale;
   bool fused;
+  bool fact;   // fused, with the factored density matrix
 };
 
 }  // namespace qmt
 
+// One persistent fused launch of a batch: its molecules' descriptors, tiles numbered across them.
+struct qmt_batch_group {
+  std::vector<qmt::FusedMol> fdesc;
+  qmt::TcShape sh_max{};
+  int n16_max = 0, nb_max = 0, tab_bytes_max = 0;
+  int64_t tiles = 0;
+  qmt::DevBuf d_fdesc;
+};
+
 struct qmt_batch {
   int precision = 0, fmt = 0;
   std::vector<qmt::BatchItem> items;
-  std::vector<qmt::FusedMol> fdesc;   // fused molecules, tiles numbered across them
-  qmt::TcShape sh_max{};
-  int n16_max = 0, tab_bytes_max = 0;
-  int64_t fused_tiles = 0;
-  qmt::DevBuf d_fdesc, d_err;
+  qmt_batch_group fused, fact;        // unfactored and factored fused launches
+  qmt::DevBuf d_err;
   qmt::DevBuf phi_hi, phi_lo;         // staged-path basis values, shared by the batch's molecules
 };
 
 namespace qmt {
 
-// Re-derives (refresh) or checks the molecule's contraction operands for its path.
+// Re-derives (refresh) or checks the molecule's contraction operands for its path (a factored
+// molecule's factor comes from the host matrix at batch creation and is not re-derived).
 static qmt_status batch_operands(const BatchItem& it, int prec, bool refresh, cudaStream_t s) {
+  if (it.fact) {
+    if (refresh) return fail(QMT_BAD_ARG, "a batch with factored molecules cannot re-derive their operands");
+    return QMT_OK;
+  }
   if (refresh) {
     it.mol->fused_prec = -1;
     it.mol->tc_prec = -1;
@@ -2235,20 +2259,57 @@ static qmt_status batch_operands(const BatchItem& it, int prec, bool refresh, cu
   return it.fused ? ensure_fused_operands(it.mol, prec, it.sh, s) : ensure_tc_operands(it.mol, prec, it.sh, s);
 }
 
+// Descriptors of the fused molecules of one kind (factored or not) and the shared-memory plan of
+// their launch; `stages` < 2 when the plan does not fit, `largest` the molecule to move out then.
+static qmt_status batch_group(qmt_batch* b, qmt_batch_group& g, bool fact, int& stages, int& largest) {
+  g.fdesc.clear();
+  g.sh_max = TcShape{};
+  g.n16_max = g.nb_max = g.tab_bytes_max = 0;
+  g.tiles = 0;
+  largest = -1;
+  stages = MAX_STAGES;
+  for (size_t i = 0; i < b->items.size(); ++i) {
+    BatchItem& it = b->items[i];
+    if (!it.fused || it.fact != fact) continue;
+    FusedMol d;
+    int tb = 0;
+    qmt_status st = fused_mol_desc(it.mol, it.sh, it.pm, g.tiles, it.ntiles, it.qube, it.outscale, d, tb, fact);
+    if (st) return st;
+    g.tiles += it.ntiles;
+    g.fdesc.push_back(d);
+    if (it.sh.kpad > g.sh_max.kpad) g.sh_max = it.sh;
+    g.n16_max = std::max(g.n16_max, d.n16);
+    g.nb_max = std::max(g.nb_max, d.nb);
+    g.tab_bytes_max = std::max(g.tab_bytes_max, tb);
+    if (largest < 0 || it.sh.kpad + tb / 1024 > b->items[largest].sh.kpad + fused_tab_bytes(b->items[largest].mol) / 1024)
+      largest = (int)i;
+  }
+  if (!g.fdesc.empty())
+    stages = b->fmt == FMT_F16 ? fused_stages<FMT_F16>(g.sh_max, g.n16_max, g.nb_max, g.tab_bytes_max, fact)
+                               : fused_stages<FMT_BF16>(g.sh_max, g.n16_max, g.nb_max, g.tab_bytes_max, fact);
+  return QMT_OK;
+}
+
+template <int FMT>
+static qmt_status batch_launch(qmt_batch* b, const qmt_batch_group& g, bool fact, cudaStream_t s) {
+  if (g.fdesc.empty()) return QMT_OK;
+  FusedParams p{};
+  p.nmol = (int)g.fdesc.size();
+  if (p.nmol == 1) p.one = g.fdesc[0];
+  p.mols = g.d_fdesc.as<FusedMol>();
+  p.ntiles = g.tiles;
+  p.err = b->d_err.as<int>();
+  return launch_fused<FMT>(p, g.sh_max, g.n16_max, g.nb_max, g.tab_bytes_max, s, fact);
+}
+
 template <int FMT>
 static qmt_status batch_run(qmt_batch* b, int rescale, bool refresh, cudaStream_t s) {
   qmt_status st;
   for (const BatchItem& it : b->items)
     if ((st = batch_operands(it, b->precision, refresh, s))) return st;
-  if (!b->fdesc.empty() && FMT != FMT_TF32) {
-    FusedParams p{};
-    p.nmol = (int)b->fdesc.size();
-    if (p.nmol == 1) p.one = b->fdesc[0];
-    p.mols = b->d_fdesc.as<FusedMol>();
-    p.ntiles = b->fused_tiles;
-    p.err = b->d_err.as<int>();
-    if ((st = launch_fused<FMT == FMT_TF32 ? FMT_F16 : FMT>(p, b->sh_max, b->n16_max, b->n16_max, b->tab_bytes_max, s)))
-      return st;
+  if (FMT != FMT_TF32) {
+    constexpr int F = FMT == FMT_TF32 ? FMT_F16 : FMT;
+    if ((st = batch_launch<F>(b, b->fact, true, s)) || (st = batch_launch<F>(b, b->fused, false, s))) return st;
   }
   for (const BatchItem& it : b->items)
     if (!it.fused && (st = run_tc<FMT>(it.mol, it.sh, it.pm, it.ntiles, b->precision, it.qube, it.outscale, s,
@@ -2293,63 +2354,62 @@ qmt_status qmt_batch_create(int nmol, qmt_mol* const* mols, const int32_t* shape
       break;
     it.outscale = 2.0 * (double)step * step * step / it.pm.s3;
     const int path = paths ? paths[i] : 0;
-    if (path < 0 || path > 2) {
-      st = fail(QMT_BAD_ARG, "batch path must be 0 (automatic), 1 (staged) or 2 (fused)");
+    if (path < 0 || path > 3) {
+      st = fail(QMT_BAD_ARG, "batch path must be 0 (automatic), 1 (staged), 2 (fused) or 3 (fused, factored)");
       break;
     }
     const bool fits = fused_fits(m, it.sh);
-    if (path == 2 && !fits) {
+    if (path >= 2 && !fits) {
       st = fail(QMT_BAD_ARG, "fused density path requested for a molecule it does not take");
       break;
     }
-    it.fused = path == 2 || (path == 0 && fits);
+    it.fused = path >= 2 || (path == 0 && fits);
+    it.fact = false;
+    if (path == 3) {   // factored when the matrix has a factor that passes the device check
+      int gate = 1;
+      if ((st = ensure_factor(m, precision, it.sh, s))) break;
+      if (m->fact_rank > 0) {
+        const cudaError_t e1 = cudaMemcpyAsync(&gate, m->fact_gate, sizeof(int), cudaMemcpyDeviceToHost, s);
+        const cudaError_t e2 = cudaStreamSynchronize(s);
+        if (e1 != cudaSuccess || e2 != cudaSuccess) {
+          st = cuda_fail(e1 != cudaSuccess ? e1 : e2, "factor check");
+          break;
+        }
+      }
+      it.fact = m->fact_rank > 0 && gate == 0;
+    }
     if ((st = m->d_partials.reserve(it.ntiles * sizeof(double))) || (st = m->d_scalars.reserve(64 * sizeof(double))))
       break;
     if ((st = batch_operands(it, precision, false, s))) break;
     b->items.push_back(it);
   }
   b->fmt = tc_shape(precision, 1).fmt;
-  // fused molecules: one launch sized for the largest of them; drop the largest to the staged path
-  // until the shared-memory plan of the set fits
-  for (;;) {
-    if (st) break;
-    b->fdesc.clear();
-    b->sh_max = TcShape{};
-    b->n16_max = b->tab_bytes_max = 0;
-    b->fused_tiles = 0;
-    int largest = -1;
-    for (size_t i = 0; i < b->items.size(); ++i) {
-      BatchItem& it = b->items[i];
-      if (!it.fused) continue;
-      FusedMol d;
-      int tb = 0;
-      if ((st = fused_mol_desc(it.mol, it.sh, it.pm, b->fused_tiles, it.ntiles, it.qube, it.outscale, d, tb))) break;
-      b->fused_tiles += it.ntiles;
-      b->fdesc.push_back(d);
-      if (it.sh.kpad > b->sh_max.kpad) b->sh_max = it.sh;
-      b->n16_max = std::max(b->n16_max, d.n16);
-      b->tab_bytes_max = std::max(b->tab_bytes_max, tb);
-      if (largest < 0 || it.sh.kpad + tb / 1024 > b->items[largest].sh.kpad + fused_tab_bytes(b->items[largest].mol) / 1024)
-        largest = (int)i;
+  // fused molecules of each kind: one launch sized for the largest of them; drop the largest to
+  // the staged path until the shared-memory plan of the set fits
+  for (int kind = 0; kind < 2 && !st; ++kind) {
+    qmt_batch_group& g = kind ? b->fact : b->fused;
+    for (;;) {
+      int stg = 0, largest = -1;
+      if ((st = batch_group(b, g, kind == 1, stg, largest))) break;
+      if (g.fdesc.empty() || stg >= 2) break;
+      b->items[largest].fused = b->items[largest].fact = false;
+      if ((st = batch_operands(b->items[largest], precision, false, s))) break;
     }
-    if (st || b->fdesc.empty()) break;
-    const int stg = b->fmt == FMT_F16 ? fused_stages<FMT_F16>(b->sh_max, b->n16_max, b->n16_max, b->tab_bytes_max)
-                                      : fused_stages<FMT_BF16>(b->sh_max, b->n16_max, b->n16_max, b->tab_bytes_max);
-    if (stg >= 2) break;
-    b->items[largest].fused = false;
-    if ((st = batch_operands(b->items[largest], precision, false, s))) break;
   }
-  if (!st && !b->fdesc.empty()) {
-    const size_t bytes = b->fdesc.size() * sizeof(FusedMol);
-    st = b->d_fdesc.reserve(bytes);
-    if (!st) st = b->d_err.reserve(256);
+  if (!st) st = b->d_err.reserve(256);
+  for (qmt_batch_group* g : {&b->fused, &b->fact}) {
+    if (st || g->fdesc.empty()) continue;
+    const size_t bytes = g->fdesc.size() * sizeof(FusedMol);
+    st = g->d_fdesc.reserve(bytes);
     if (!st) {
-      const cudaError_t e1 = cudaMemcpyAsync(b->d_fdesc.ptr, b->fdesc.data(), bytes, cudaMemcpyHostToDevice, s);
-      const cudaError_t e2 = cudaMemsetAsync(b->d_err.ptr, 0, 256, s);
-      const cudaError_t e3 = cudaStreamSynchronize(s);
-      if (e1 != cudaSuccess || e2 != cudaSuccess || e3 != cudaSuccess)
-        st = cuda_fail(e1 != cudaSuccess ? e1 : (e2 != cudaSuccess ? e2 : e3), "batch descriptors");
+      const cudaError_t e1 = cudaMemcpyAsync(g->d_fdesc.ptr, g->fdesc.data(), bytes, cudaMemcpyHostToDevice, s);
+      if (e1 != cudaSuccess) st = cuda_fail(e1, "batch descriptors");
     }
+  }
+  if (!st) {
+    const cudaError_t e2 = cudaMemsetAsync(b->d_err.ptr, 0, 256, s);
+    const cudaError_t e3 = cudaStreamSynchronize(s);
+    if (e2 != cudaSuccess || e3 != cudaSuccess) st = cuda_fail(e2 != cudaSuccess ? e2 : e3, "batch descriptors");
   }
   if (st) {
     delete b;
@@ -2397,13 +2457,19 @@ qmt_status qmt_batch_sums(qmt_batch* b, double* sums, void* stream) {
 
 int qmt_batch_fused_count(const qmt_batch* b) {
   if (!b) return -1;
-  return (int)b->fdesc.size();
+  return (int)(b->fused.fdesc.size() + b->fact.fdesc.size());
+}
+
+int qmt_batch_factored_count(const qmt_batch* b) {
+  if (!b) return -1;
+  return (int)b->fact.fdesc.size();
 }
 
 qmt_status qmt_batch_destroy(qmt_batch* b) {
   if (!b) return QMT_OK;
   cudaDeviceSynchronize();
-  b->d_fdesc.release();
+  b->fused.d_fdesc.release();
+  b->fact.d_fdesc.release();
   b->d_err.release();
   b->phi_hi.release();
   b->phi_lo.release();

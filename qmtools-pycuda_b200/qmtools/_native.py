@@ -63,7 +63,8 @@ SIGNATURES = {
     "qmt_nn_singleshot": [_i, _i, _i, _d, _vp, _vp, _vp, _i, _i, _vp],
 }
 OTHER = {"qmt_last_error": ([], C.c_char_p), "qmt_abi_version": ([], C.c_int),
-         "qmt_launch_count": ([], C.c_uint64), "qmt_batch_fused_count": ([_vp], C.c_int)}
+         "qmt_launch_count": ([], C.c_uint64), "qmt_batch_fused_count": ([_vp], C.c_int),
+         "qmt_batch_factored_count": ([_vp], C.c_int)}
 
 
 class NativeUnavailable(RuntimeError):

@@ -23,7 +23,7 @@ import numpy as np
 
 from . import _native as N
 
-PATH_STAGED, PATH_FUSED = 1, 2
+PATH_STAGED, PATH_FUSED, PATH_FACTORED = 1, 2, 3
 
 
 def _nice(n):

@@ -6,8 +6,9 @@ reference evaluates one molecule per facade call, qmtools/qmtools.py:2381-2639).
 * keeps every molecule's operands, its density grid and its potential grid on the device (one
   flat buffer each, 256-byte aligned slices);
 * evaluates all densities through `qmt_batch_density`: the molecules whose contraction takes the
-  fused path share one persistent launch over all their tiles, the rest take the staged path;
-  every grid is then scaled to its nuclear charge;
+  fused path share persistent launches over all their tiles (one for those whose density matrix
+  has a low-rank factor, one for the others), the rest take the staged path; every grid is then
+  scaled to its nuclear charge;
 * solves the free-space (Hockney) FFT Poisson problem of every molecule with the padded lengths
   the autotuner picked (`qmtools.autotune`);
 * captures all of it into one CUDA graph after a first eager run (which builds every operand,
@@ -49,8 +50,12 @@ class BatchEvaluator:
         total = int(self.offsets[-1])
         self.q = torch.zeros(total, dtype=torch.float32, device="cuda")
         self.v = torch.zeros(total, dtype=torch.float32, device="cuda") if hartree else None
-        # tuned choices
+        # tuned choices; a fused molecule takes its factored density matrix when it has one (a
+        # batch that re-derives its operands in the graph keeps the unfactored matrices)
+        from .autotune import PATH_FUSED, PATH_FACTORED
         self.paths = [self.tuner.density_path(m, n, precision) for m, n in zip(self.molecules, self.npts)]
+        if not self.refresh:
+            self.paths = [PATH_FACTORED if p == PATH_FUSED else p for p in self.paths]
         self.fft_lengths = []
         if hartree:
             for m, (nx, ny, nz, *_) in zip(self.molecules, geo):
@@ -68,6 +73,7 @@ class BatchEvaluator:
                    paths.ctypes.data, qptrs, C.c_void_p(self.stream.cuda_stream), C.byref(b))
         self.batch = b
         self.fused_count = N.load().qmt_batch_fused_count(b)
+        self.factored_count = N.load().qmt_batch_factored_count(b)
         self.graph = None
         # eager runs: the first builds the Green's functions and twiddle tables, the second finds
         # them built, so that the captured calls make no allocation and no event call

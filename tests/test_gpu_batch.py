@@ -1,6 +1,7 @@
-"""Batched evaluation: one persistent fused launch over many molecules, the staged path for the
-large ones, Hockney solves with tuned padding, all captured in one CUDA graph.  Each molecule's
-result must equal its single-molecule evaluation through the facade."""
+"""Batched evaluation: persistent fused launches over many molecules (the factored density matrices
+on one, the others on another), the staged path for the large ones, Hockney solves with tuned
+padding, all captured in one CUDA graph.  Each molecule's result must equal its single-molecule
+evaluation through the facade."""
 import ctypes as C
 
 import numpy as np
@@ -9,7 +10,7 @@ import pytest
 import qmtools
 from qmtools import _native as N
 from qmtools import synthetic as syn
-from qmtools.autotune import PATH_FUSED, PATH_STAGED, Tuner, fft_candidates
+from qmtools.autotune import PATH_FACTORED, PATH_FUSED, PATH_STAGED, Tuner, fft_candidates
 from qmtools.batch import BatchEvaluator
 
 pytestmark = pytest.mark.gpu
@@ -44,22 +45,37 @@ def _single(mol, g, m_lengths, path):
 
 @pytest.mark.parametrize("measure", [False, True], ids=["default_paths", "tuned_paths"])
 def test_batch_equals_single_molecule_evaluations(mols, tmp_path, measure):
-    """Default paths put the four small molecules on one persistent fused launch; measured paths
-    follow the tuner's choices."""
+    """Default paths put the four small molecules on one persistent fused launch, with their
+    factored density matrices (the synthetic matrices have rank n_occ); measured paths follow the
+    tuner's choices."""
     tuner = Tuner(path=tmp_path / "tune.json", measure=measure)
     ev = BatchEvaluator([m for _, m, _ in mols], [g for _, _, g in mols], tuner=tuner)
     try:
         assert ev.paths[3] == PATH_STAGED               # N > 320
-        assert ev.fused_count == sum(1 for p in ev.paths if p == PATH_FUSED)
+        assert ev.fused_count == sum(1 for p in ev.paths if p in (PATH_FUSED, PATH_FACTORED))
+        assert ev.factored_count == sum(1 for p in ev.paths if p == PATH_FACTORED)
         if not measure:
-            assert ev.fused_count == 4
+            assert ev.fused_count == 4 and ev.factored_count == 4
+        first = None
         for rep in range(2):                            # two graph replays
             ev.run()
             ev.synchronize()
+            grids = [(ev.density(i), ev.potential(i)) for i in range(len(mols))]
+            if first is None:
+                first = grids
             for i, (sm, mol, g) in enumerate(mols):
+                q, v = grids[i]
+                # replays repeat themselves exactly
+                assert np.array_equal(q, first[i][0]) and np.array_equal(v, first[i][1]), (rep, i)
                 q1, v1 = _single(mol, g, ev.fft_lengths[i], ev.paths[i])
-                assert np.array_equal(ev.density(i), q1), (rep, i)
-                assert np.array_equal(ev.potential(i), v1), (rep, i)
+                if ev.paths[i] == PATH_FACTORED and ev.factored_count > 1:
+                    # the factored launch over several molecules is another compilation of the
+                    # same arithmetic (the kernel template for many molecules): equal to rounding
+                    assert np.abs(q - q1).max() <= 4e-7 * np.abs(q1).max(), (rep, i)
+                    assert np.linalg.norm(v - v1) <= 1e-6 * np.linalg.norm(v1), (rep, i)
+                else:
+                    assert np.array_equal(q, q1), (rep, i)
+                    assert np.array_equal(v, v1), (rep, i)
         sums = ev.sums()
         assert np.all(np.isfinite(sums)) and np.all(sums > 0)
         if measure:
@@ -69,11 +85,13 @@ def test_batch_equals_single_molecule_evaluations(mols, tmp_path, measure):
 
 
 def test_batch_graph_follows_new_density_matrices(mols, tmp_path):
-    """With refresh the captured graph re-derives the split density matrices from new uploads."""
+    """With refresh the captured graph re-derives the split density matrices from new uploads (and
+    keeps the unfactored matrices: a factor is built on the host)."""
     sel = [mols[0], mols[2]]
     ev = BatchEvaluator([m for _, m, _ in sel], [g for _, _, g in sel], tuner=Tuner(path=tmp_path / "t.json"),
                         refresh=True)
     try:
+        assert ev.factored_count == 0 and PATH_FACTORED not in ev.paths
         rng = np.random.default_rng(3)
         saved = [np.array(m.dm) for _, m, _ in sel]
         for (_, m, _), dm in zip(sel, saved):
