@@ -702,20 +702,20 @@ def run_ours(args, world, rank, local, pg):
     peak_tf, hbm, kind = peaks()
     achieved = flops / (dens_ms / 1000.0) / 1e12
     traffic = profiled_traffic() if (args.precision == "fp16x3" and not args.grid) else None
-    rank = C.c_int()
-    N.call("qmt_density_factor_rank", handle, C.byref(rank), sh)
-    rank = int(rank.value)
-    r16 = max(16, (rank + 15) // 16 * 16)
+    frank = C.c_int()
+    N.call("qmt_density_factor_rank", handle, C.byref(frank), sh)
+    frank = int(frank.value)
+    r16 = max(16, (frank + 15) // 16 * 16)
     out["roofline"] = {"bound": "tensor",
                        "kernel": "density_fused_kernel (basis values in shared memory + tcgen05 contraction)",
                        "achieved": achieved, "peak": peak_tf, "unit": "TFLOP/s", "frac": achieved / peak_tf,
                        "peak_source": f"bf16_tflops burst, {kind}", "density_ms": dens_ms,
                        "algorithmic_flop_per_launch": flops,
                        "algorithmic_flop_definition": "npts (2 N^2 + 2 N): Phi P plus the row-dot",
-                       "contraction": (f"factored density matrix P = L L^T, rank {rank}: rho = sum_k (Phi L)_k^2, "
+                       "contraction": (f"factored density matrix P = L L^T, rank {frank}: rho = sum_k (Phi L)_k^2, "
                                        f"MMA N = {2 * r16} (hi and lo rows of L) x 2 products, "
                                        f"{npts * 2.0 * nb * 2 * r16 * 2:.3e} tensor flop per launch"
-                                       if rank else "unfactored: Phi P (N columns) x 3 products, row-dot with Phi"),
+                                       if frank else "unfactored: Phi P (N columns) x 3 products, row-dot with Phi"),
                        "traffic": traffic["bytes_per_launch"] if traffic else None,
                        "traffic_unit": "DRAM bytes per launch (ncu, dram__bytes_read.sum + dram__bytes_write.sum)",
                        "traffic_source": traffic["source"] if traffic else None}
