@@ -91,9 +91,13 @@ struct TcParams {
   float* qube;
   double* partials;
   double outscale;
-  const double* gsc;   // device {max, 2^g, 2^-g} of the split density matrix
+  const double* gsc;   // device {max, 2^g, 2^-g} of the split density matrix (factored: the
+                       // column scales 2^-2h_k of the squares)
   int* err;
   uint64_t wait_ns;    // limit of every bounded wait (a test shortens it)
+  int nb;              // factored: rank rounded up to 16 (B holds its hi rows, then its lo rows)
+  const int* gate;     // when set, the launch runs only if *gate == gate_want (device-side check
+  int gate_want;       // of the factor picks the factored or the unfactored launch)
 };
 
 constexpr int MAX_STAGES = 8;
@@ -163,12 +167,18 @@ __device__ __forceinline__ void load_phi16(const TcParams& p, int64_t row, int c
   }
 }
 
-template <int FMT>
+// FACT: B is the factored density matrix (one box of nb hi rows then nb lo rows per K-chunk, one
+// output panel); per K-step one MMA [A_hi B_hi | A_hi B_lo] into the buffer's first accumulator and
+// one [A_lo B_hi | A_lo B_lo] into its second; the epilogue adds the four column groups and sums
+// the squares with the column scales (no re-read of Phi').  TMEM buffers of 2 x N columns, two of
+// them when they fit in 512.
+template <int FMT, bool FACT>
 __global__ void __launch_bounds__(192, 1)
     density_mma_kernel(const __grid_constant__ CUtensorMap tmA_hi, const __grid_constant__ CUtensorMap tmA_lo,
                        const __grid_constant__ CUtensorMap tmB_hi, const __grid_constant__ CUtensorMap tmB_lo,
                        const TcParams p) {
   extern __shared__ uint8_t smem_dyn[];
+  if (p.gate && *p.gate != p.gate_want) return;   // the other launch of the pair does the work
   __shared__ __align__(8) uint64_t full_bar[MAX_STAGES], empty_bar[MAX_STAGES];
   __shared__ __align__(8) uint64_t tfull[2], tempty[2], drain_bar;
   __shared__ uint32_t tmem_slot;
@@ -233,7 +243,7 @@ __global__ void __launch_bounds__(192, 1)
             if (p.nsplit == 2) tma_load_2d(st + p.a_bytes, &tmA_lo, &full_bar[s], x, t * 128);
             uint8_t* bst = st + p.nsplit * p.a_bytes;
             tma_load_2d(bst, &tmB_hi, &full_bar[s], x, pn * p.pw);
-            if (p.nsplit == 2) tma_load_2d(bst + p.b_bytes, &tmB_lo, &full_bar[s], x, pn * p.pw);
+            if (p.nsplit == 2 && !FACT) tma_load_2d(bst + p.b_bytes, &tmB_lo, &full_bar[s], x, pn * p.pw);
             last_par[s] = (int)ph;
           }
         }
@@ -248,15 +258,18 @@ __global__ void __launch_bounds__(192, 1)
       uint32_t it = 0, acc_it = 0;
       bool ok = true;
       const int ksteps = 128 / (p.esize * (p.esize == 4 ? 8 : 16));  // 4 steps of 32 bytes
+      // factored: N = the factor's hi and lo rows, a buffer holds two accumulators of N
+      const uint32_t nfac = (uint32_t)(p.nsplit * p.nb), fbuf = (uint32_t)p.nsplit * nfac;
+      const uint32_t nbuf = FACT ? (fbuf <= 256u ? 2u : 1u) : 2u;
       for (int t = blockIdx.x; t < p.ntiles && ok; t += gridDim.x) {
         for (int pn = 0; pn < p.npanels && ok; ++pn, ++acc_it) {
-          const uint32_t buf = acc_it & 1u, aph = (acc_it >> 1) & 1u;
+          const uint32_t buf = nbuf == 2u ? (acc_it & 1u) : 0u, aph = ((nbuf == 2u ? acc_it >> 1 : acc_it)) & 1u;
           if (!mbar_wait(&tempty[buf], aph ^ 1u, &abort_flag, p.wait_ns)) {
             ok = false;
             break;
           }
           tc_fence_after();
-          const uint32_t d = tmem + buf * 256u;
+          const uint32_t d = tmem + buf * (FACT ? 256u * (2u / nbuf) : 256u);
           for (int kc = 0; kc < p.kchunks; ++kc, ++it) {
             const int s = it % p.stages;
             const uint32_t ph = (it / p.stages) & 1u;
@@ -278,6 +291,9 @@ __global__ void __launch_bounds__(192, 1)
                   mma_tf32(d, sw128_kmajor_desc(a0 + off), sw128_kmajor_desc(b1 + off), p.idesc, 1u);
                   mma_tf32(d, sw128_kmajor_desc(a1 + off), sw128_kmajor_desc(b0 + off), p.idesc, 1u);
                 }
+              } else if (FACT) {
+                mma_f16(d, sw128_kmajor_desc(a0 + off), sw128_kmajor_desc(b0 + off), p.idesc, acc);
+                if (p.nsplit == 2) mma_f16(d + nfac, sw128_kmajor_desc(a1 + off), sw128_kmajor_desc(b0 + off), p.idesc, acc);
               } else {
                 mma_f16(d, sw128_kmajor_desc(a0 + off), sw128_kmajor_desc(b0 + off), p.idesc, acc);
                 if (p.nsplit == 2) {
@@ -302,11 +318,13 @@ __global__ void __launch_bounds__(192, 1)
     const int et = threadIdx.x - 64;
     uint32_t acc_it = 0;
     bool ok = true;
+    const uint32_t nfac = (uint32_t)(p.nsplit * p.nb), fbuf = (uint32_t)p.nsplit * nfac;
+    const uint32_t nbuf = FACT ? (fbuf <= 256u ? 2u : 1u) : 2u;
     for (int t = blockIdx.x; t < p.ntiles && ok; t += gridDim.x) {
       double acc = 0.0;
       const int64_t grow = (int64_t)t * 128 + row;
       for (int pn = 0; pn < p.npanels; ++pn, ++acc_it) {
-        const uint32_t buf = acc_it & 1u, aph = (acc_it >> 1) & 1u;
+        const uint32_t buf = nbuf == 2u ? (acc_it & 1u) : 0u, aph = ((nbuf == 2u ? acc_it >> 1 : acc_it)) & 1u;
         // the four epilogue warps leave together: one of them giving up while the others go on
         // would leave those waiting at the next named barrier
         const bool got = mbar_wait(&tfull[buf], aph, &abort_flag, p.wait_ns);
@@ -315,21 +333,45 @@ __global__ void __launch_bounds__(192, 1)
           break;
         }
         tc_fence_after();
-        for (int c = 0; c < p.pw / 32; ++c) {
-          const int col = pn * p.pw + 32 * c;
-          if (col >= p.kpad) break;
-          float v[32], ph[32];
-          tmem_ld32(tmem + ((uint32_t)(q * 32) << 16) + buf * 256u + 32u * c, v);
-          if constexpr (FMT == FMT_TF32) load_phi32(p, grow, col, ph);
-          else load_phi16<FMT>(p, grow, col, ph);
+        if (FACT) {
+          // T_k = the sum of the column groups (hi x hi, hi x lo, lo x hi, lo x lo), then
+          // rho = sum_k 2^-2h_k T_k^2
+          const uint32_t tb = tmem + ((uint32_t)(q * 32) << 16) + buf * 256u * (2u / nbuf);
+          const int ng = p.nsplit == 2 ? 4 : 1;
+          for (int c = 0; c * 16 < p.nb; ++c) {
+            float tsum[16];
 #pragma unroll
-          for (int k = 0; k < 32; ++k) acc = fma((double)ph[k], (double)v[k], acc);
+            for (int e = 0; e < 16; ++e) tsum[e] = 0.f;
+            for (int gi = 0; gi < ng; ++gi) {
+              uint32_t tv[16];
+              tmem_ld16_issue(tb + (uint32_t)(gi * p.nb + c * 16), tv);
+              tmem_ld16_wait(tv);
+#pragma unroll
+              for (int e = 0; e < 16; ++e) tsum[e] += __uint_as_float(tv[e]);
+            }
+#pragma unroll
+            for (int e = 0; e < 16; ++e) {
+              const double v = (double)tsum[e];
+              acc = fma(__ldg(p.gsc + c * 16 + e) * v, v, acc);
+            }
+          }
+        } else {
+          for (int c = 0; c < p.pw / 32; ++c) {
+            const int col = pn * p.pw + 32 * c;
+            if (col >= p.kpad) break;
+            float v[32], ph[32];
+            tmem_ld32(tmem + ((uint32_t)(q * 32) << 16) + buf * 256u + 32u * c, v);
+            if constexpr (FMT == FMT_TF32) load_phi32(p, grow, col, ph);
+            else load_phi16<FMT>(p, grow, col, ph);
+#pragma unroll
+            for (int k = 0; k < 32; ++k) acc = fma((double)ph[k], (double)v[k], acc);
+          }
         }
         tc_fence_before();
         mbar_arrive(&tempty[buf]);
       }
       if (!ok) break;
-      rho_s[row] = acc * p.gsc[2];
+      rho_s[row] = FACT ? acc : acc * p.gsc[2];
       named_barrier(1, 128);
       double mysum = 0.0;
       if (et < p.pm.vpt) {
@@ -1803,9 +1845,35 @@ __global__ void fact_split_kernel(const double* __restrict__ L, int n, int ld, i
   }
 }
 
+// The factor as the staged path's B operand: row q < r16 holds the hi piece of factor column q,
+// row r16 + q its lo piece (two pieces), each kpad elements of W_jq = L_jq 2^-s_j 2^h_q (zero
+// outside j < n, q < r), row-major; the tensor map gives the 128-byte swizzle.
+__global__ void fact_rows_kernel(const double* __restrict__ L, int n, int ld, int r, int kpad, int r16,
+                                 const double* __restrict__ inv_s, const double* __restrict__ two_h, int fmt,
+                                 int nsplit, uint16_t* __restrict__ out) {
+  const int64_t tot = (int64_t)r16 * kpad;
+  for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < tot; i += (int64_t)gridDim.x * blockDim.x) {
+    const int q = (int)(i / kpad), j = (int)(i - (int64_t)q * kpad);
+    const double w = (j < n && q < r) ? L[(size_t)j * ld + q] * inv_s[j] * two_h[q] : 0.0;
+    uint16_t hi, lo;
+    if (fmt == FMT_F16) {
+      const __half h = __float2half_rn((float)w);
+      hi = __half_as_ushort(h);
+      lo = __half_as_ushort(__float2half_rn((float)(w - (double)__half2float(h))));
+    } else {
+      const __nv_bfloat16 h = __float2bfloat16_rn((float)w);
+      hi = __bfloat16_as_ushort(h);
+      lo = __bfloat16_as_ushort(__float2bfloat16_rn((float)(w - (double)__bfloat162float(h))));
+    }
+    out[(size_t)q * kpad + j] = hi;
+    if (nsplit == 2) out[(size_t)(r16 + q) * kpad + j] = lo;
+  }
+}
+
 constexpr double kFactorTol = 1e-7;
 constexpr double kFactorResid = 2e-7;
-constexpr int kFactorMaxRank = 64;    // N = 2 x 64 per MMA and three main accumulators (fact_nacc)
+constexpr int kFactorMaxRank = 128;   // N = 2 x 128 per MMA of the staged path's factored kernel
+constexpr int kFusedFactorMaxR16 = 64; // the fused factored kernel: N = 2 x 64, three main accumulators
 
 // The scaled factor W_jk = L_jk 2^(h_k - s_j) (so Phi' W = 2^h_k (Phi L)_k, each column scaled
 // to a maximum near 2^14) split into hi + lo pieces, as the fused kernel streams it: K-step block
@@ -1901,6 +1969,25 @@ static qmt_status ensure_factor(qmt_mol* m, int prec, const TcShape& sh, cudaStr
   QMT_CHECK_LAUNCH("fact_split_kernel");
   m->fact_rank = r;
   m->fact_r16 = r16;
+  m->fact_rows_prec = -1;
+  return QMT_OK;
+}
+
+// The factor in the staged path's B layout (fact_rows_kernel), once per factor.
+static qmt_status ensure_factor_rows(qmt_mol* m, int prec, const TcShape& sh, cudaStream_t s) {
+  if (m->fact_rows_prec == prec) return QMT_OK;
+  const int r16 = m->fact_r16, n16 = (m->norbs + 15) / 16 * 16;
+  const int rmax = std::min(kFactorMaxRank, n16 / 2);
+  qmt_status st = m->d_fact_Bs.reserve((size_t)sh.nsplit * r16 * sh.kpad * 2);
+  if (st) return st;
+  const int64_t tot = (int64_t)r16 * sh.kpad;
+  const int blocks = (int)std::min<int64_t>((tot + 255) / 256, (int64_t)sm_count() * 4);
+  fact_rows_kernel<<<std::max(blocks, 1), 256, 0, s>>>(m->d_fact_L.as<double>(), m->norbs, rmax, m->fact_rank,
+                                                        sh.kpad, r16, m->d_split_scale.as<double>(),
+                                                        m->d_fact_scale.as<double>() + r16, sh.fmt, sh.nsplit,
+                                                        m->d_fact_Bs.as<uint16_t>());
+  QMT_CHECK_LAUNCH("fact_rows_kernel");
+  m->fact_rows_prec = prec;
   return QMT_OK;
 }
 
@@ -2037,7 +2124,8 @@ static qmt_status ensure_tc_operands(qmt_mol* m, int prec, const TcShape& sh, cu
 template <int FMT>
 static qmt_status run_tc(qmt_mol* m, const TcShape& sh, const PointMap& pm, int64_t ntiles, int prec,
                          float* qube, double outscale, cudaStream_t s, DevBuf* phi_hi = nullptr,
-                         DevBuf* phi_lo = nullptr, size_t stage_bytes = (size_t)2 << 30) {
+                         DevBuf* phi_lo = nullptr, size_t stage_bytes = (size_t)2 << 30, int fact = 0) {
+  // fact: 0 unfactored; 1 factored only; 2 both launches, gated by the device check of the factor
   qmt_status st;
   if (!phi_hi) {
     phi_hi = &m->d_Phi_hi;
@@ -2053,13 +2141,17 @@ static qmt_status run_tc(qmt_mol* m, const TcShape& sh, const PointMap& pm, int6
   if (sh.nsplit == 2 && (st = phi_lo->reserve(chunk * tile_bytes))) return st;
   void* lo_ptr = sh.nsplit == 2 ? phi_lo->ptr : phi_hi->ptr;
 
-  CUtensorMap tA_hi, tA_lo, tB_hi, tB_lo;
+  CUtensorMap tA_hi, tA_lo, tB_hi, tB_lo, tF;
   const uint8_t* Pb = m->d_tc_P.as<uint8_t>();
   const size_t piece = (size_t)sh.nrows_b * sh.kpad * sh.esize;
   if ((st = make_map(&tA_hi, phi_hi->ptr, sh.esize, sh.kpad, (uint64_t)chunk * 128, sh.ke, 128)) ||
-      (st = make_map(&tA_lo, lo_ptr, sh.esize, sh.kpad, (uint64_t)chunk * 128, sh.ke, 128)) ||
-      (st = make_map(&tB_hi, Pb, sh.esize, sh.kpad, sh.nrows_b, sh.ke, sh.pw)) ||
-      (st = make_map(&tB_lo, Pb + piece, sh.esize, sh.kpad, sh.nrows_b, sh.ke, sh.pw)))
+      (st = make_map(&tA_lo, lo_ptr, sh.esize, sh.kpad, (uint64_t)chunk * 128, sh.ke, 128)))
+    return st;
+  if (fact != 1 && ((st = make_map(&tB_hi, Pb, sh.esize, sh.kpad, sh.nrows_b, sh.ke, sh.pw)) ||
+                    (st = make_map(&tB_lo, Pb + piece, sh.esize, sh.kpad, sh.nrows_b, sh.ke, sh.pw))))
+    return st;
+  const int nfac = sh.nsplit * m->fact_r16;   // the factored launch's N: hi rows, then lo rows
+  if (fact && (st = make_map(&tF, m->d_fact_Bs.ptr, sh.esize, sh.kpad, (uint64_t)nfac, sh.ke, (uint32_t)nfac)))
     return st;
 
   TcParams p{};
@@ -2083,18 +2175,39 @@ static qmt_status run_tc(qmt_mol* m, const TcShape& sh, const PointMap& pm, int6
   p.gsc = m->d_gscale.as<double>();
   p.err = reinterpret_cast<int*>(m->d_scalars.as<double>() + 8);
   p.wait_ns = wait_limit_ns();
+  if (fact == 2) {
+    p.gate = m->fact_gate;
+    p.gate_want = 1;
+  }
+  // the factored launch: one panel of N = nfac (the factor's hi and lo rows in one box)
+  TcParams pf = p;
+  pf.npanels = 1;
+  pf.pw = nfac;
+  pf.b_bytes = (uint32_t)nfac * 128u;
+  pf.stage_bytes = sh.nsplit * pf.a_bytes + pf.b_bytes;
+  pf.tx_bytes = pf.stage_bytes;
+  pf.idesc = make_idesc((uint32_t)sh.fmt, 128, (uint32_t)nfac);
+  pf.gsc = m->d_fact_scale.as<double>();
+  pf.nb = m->fact_r16;
+  pf.gate = fact == 2 ? m->fact_gate : nullptr;
+  pf.gate_want = 0;
 
   int maxsm = 0, dev = 0;
   cudaGetDevice(&dev);
   cudaDeviceGetAttribute(&maxsm, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev);
   const int static_bytes = 4096;
-  int stages = (int)((maxsm - static_bytes - 1024) / p.stage_bytes);
-  stages = std::min(stages, MAX_STAGES);
-  if (stages < 2) return fail(QMT_BAD_ARG, "tensor-core stage does not fit in shared memory");
-  p.stages = stages;
-  const size_t dyn = (size_t)stages * p.stage_bytes + 1024;
-  auto kern = density_mma_kernel<FMT>;
-  QMT_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)dyn));
+  auto plan = [&](TcParams& q) -> size_t {
+    q.stages = std::min((int)((maxsm - static_bytes - 1024) / q.stage_bytes), MAX_STAGES);
+    return (size_t)q.stages * q.stage_bytes + 1024;
+  };
+  const size_t dyn = plan(p), dynf = plan(pf);
+  if ((fact != 1 && p.stages < 2) || (fact && pf.stages < 2))
+    return fail(QMT_BAD_ARG, "tensor-core stage does not fit in shared memory");
+  constexpr int FF = FMT == FMT_TF32 ? FMT_F16 : FMT;   // (the factored kernel takes fp16 / bf16)
+  auto kern = density_mma_kernel<FMT, false>;
+  auto kernf = density_mma_kernel<FF, true>;
+  if (fact != 1) QMT_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)dyn));
+  if (fact) QMT_CUDA(cudaFuncSetAttribute(kernf, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)dynf));
 
   // staging kernel: molecule tables in shared memory unless they would keep two CTAs off an SM
   const MolTabLayout lay = mol_tab_layout(m, sh.kpad);
@@ -2131,11 +2244,17 @@ static qmt_status run_tc(qmt_mol* m, const TcShape& sh, const PointMap& pm, int6
     const int gb = (int)std::min<int64_t>(nt, (int64_t)nsm * stage_ctas);
     skern<<<gb, STAGE_THREADS, sdyn, s>>>(sp);
     QMT_CHECK_LAUNCH("basis_window_kernel");
-    p.tile0 = t0;
-    p.ntiles = nt;
+    p.tile0 = pf.tile0 = t0;
+    p.ntiles = pf.ntiles = nt;
     const int gm = (int)std::min<int64_t>(nt, nsm);
-    kern<<<gm, 192, dyn, s>>>(tA_hi, tA_lo, tB_hi, tB_lo, p);
-    QMT_CHECK_LAUNCH("density_mma_kernel");
+    if (fact) {
+      kernf<<<gm, 192, dynf, s>>>(tA_hi, tA_lo, tF, tF, pf);
+      QMT_CHECK_LAUNCH("density_mma_kernel");
+    }
+    if (fact != 1) {
+      kern<<<gm, 192, dyn, s>>>(tA_hi, tA_lo, tB_hi, tB_lo, p);
+      QMT_CHECK_LAUNCH("density_mma_kernel");
+    }
   }
   (void)prec;
   return QMT_OK;
@@ -2166,10 +2285,12 @@ qmt_status density_tc(qmt_mol* mol, int nx, int ny, int nz, float step, float ox
   const bool fused = g_density_path >= 2 ? fusable : (g_density_path == 1 ? false : fusable);
   if (g_density_path >= 2 && !fusable)
     return fail(QMT_BAD_ARG, "fused density path needs fp16/bf16, N <= 320 and molecule tables that fit in shared memory");
+  // the factored matrix when there is one (automatic, or asked for): fused (rank <= 64) or staged
+  // (rank <= 128, fp16 / bf16)
   bool fact = false;
-  if (fused && g_density_path != 2) {   // the factored matrix when there is one (automatic, or asked for)
+  if (sh.fmt != FMT_TF32 && g_density_path != 1 && g_density_path != 2) {
     if ((st = ensure_factor(mol, precision, sh, s))) return st;
-    fact = mol->fact_rank > 0;
+    fact = mol->fact_rank > 0 && (!fused || mol->fact_r16 <= kFusedFactorMaxR16);
     if (g_density_path == 3 && !fact)
       return fail(QMT_BAD_ARG, "factored density path needs a positive semi-definite density matrix of low rank");
   }
@@ -2186,9 +2307,13 @@ qmt_status density_tc(qmt_mol* mol, int nx, int ny, int nz, float step, float ox
     }
   } else {
     if ((st = ensure_tc_operands(mol, precision, sh, s))) return st;
+    if (fact && (st = ensure_factor_rows(mol, precision, sh, s))) return st;
+    const int fmode = fact ? 2 : 0;   // with a factor, the device check picks the launch
     if (sh.fmt == FMT_TF32) st = run_tc<FMT_TF32>(mol, sh, pm, ntiles, precision, qube, outscale, s);
-    else if (sh.fmt == FMT_F16) st = run_tc<FMT_F16>(mol, sh, pm, ntiles, precision, qube, outscale, s);
-    else st = run_tc<FMT_BF16>(mol, sh, pm, ntiles, precision, qube, outscale, s);
+    else if (sh.fmt == FMT_F16)
+      st = run_tc<FMT_F16>(mol, sh, pm, ntiles, precision, qube, outscale, s, nullptr, nullptr, (size_t)2 << 30, fmode);
+    else
+      st = run_tc<FMT_BF16>(mol, sh, pm, ntiles, precision, qube, outscale, s, nullptr, nullptr, (size_t)2 << 30, fmode);
   }
   if (st) return st;
   st = finish_density(mol, pm.nvox, ntiles, rescale, qube, sum_out, s);
@@ -2376,7 +2501,7 @@ qmt_status qmt_batch_create(int nmol, qmt_mol* const* mols, const int32_t* shape
           break;
         }
       }
-      it.fact = m->fact_rank > 0 && gate == 0;
+      it.fact = m->fact_rank > 0 && gate == 0 && m->fact_r16 <= kFusedFactorMaxR16;
     }
     if ((st = m->d_partials.reserve(it.ntiles * sizeof(double))) || (st = m->d_scalars.reserve(64 * sizeof(double))))
       break;

@@ -87,7 +87,7 @@ using namespace qmt;
 qmt_mol::~qmt_mol() {
   for (DevBuf* b : {&d_coords, &d_types, &d_shells, &d_alpha, &d_coeff, &d_alpha64, &d_coeff64,
                     &d_P32, &d_P64, &d_Phi_hi, &d_Phi_lo, &d_tc_P, &d_partials,
-                    &d_scalars, &d_pairs, &d_work, &d_atom_shell, &d_fused_B, &d_fact_B, &d_fact_scale, &d_fact_L,
+                    &d_scalars, &d_pairs, &d_work, &d_atom_shell, &d_fused_B, &d_fact_B, &d_fact_scale, &d_fact_L, &d_fact_Bs,
                     &d_fused_tab, &d_split_scale,
                     &d_dm_raw, &d_gscale, &d_pairs32, &d_gto_part})
     b->release();

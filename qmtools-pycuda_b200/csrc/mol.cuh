@@ -51,6 +51,8 @@ struct qmt_mol {
   int fact_r16 = 0;             // the rank rounded up to 16 (the MMA N)
   qmt::DevBuf d_fact_B;         // scaled factor pieces, K-step blocks of fact_r16 rows (hi then lo)
   qmt::DevBuf d_fact_L;         // the factor (FP64, row by row) and a flag, for the residual check
+  int fact_rows_prec = -1;      // precision of d_fact_Bs (-1: not built for the current factor)
+  qmt::DevBuf d_fact_Bs;        // the factor as the staged path's B operand (fact_rows_kernel)
   const int* fact_gate = nullptr; // that flag: 0 when the factor reproduces P, 1 when it does not
   qmt::DevBuf d_fact_scale;     // per factor column k, the scale 2^-2h_k of its squares
   qmt::DevBuf d_fused_tab;      // fused path: packed shell records, then (alpha, scaled coefficient) pairs
