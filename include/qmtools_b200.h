@@ -111,13 +111,14 @@ qmt_status qmt_density(qmt_mol* mol, int nx, int ny, int nz, float step,
                        int rescale, float* qube_dev, double* sum_out, void* stream);
 
 /* Selects the tensor-core density implementation (new; process-wide): 0 = automatic (fused
- * when the contraction is fp16/bf16 and N <= 320, staged otherwise; fused with the factored
- * density matrix when it has one), 1 = staged (basis values through HBM), 2 = fused (basis values
- * stay in shared memory), 3 = fused with the factored density matrix: P = L L^T from a pivoted
- * Cholesky factorisation (FP64, on the host, once per matrix) and rho = sum_k (Phi L)_k^2, which
- * needs rank(P) columns instead of N -- for a positive semi-definite P of rank at most
- * min(64, N/2) (an SCF density matrix has the rank of its occupied orbitals); QMT_BAD_ARG when the
- * factorisation finds P indefinite or of higher rank.  What the factor leaves out is checked on
+ * when the contraction is fp16/bf16 and N <= 320, staged otherwise; with the factored density
+ * matrix when it has one), 1 = staged (basis values through HBM), 2 = fused (basis values
+ * stay in shared memory), 3 = the factored density matrix: P = L L^T from a pivoted Cholesky
+ * factorisation (FP64, on the host, once per matrix) and rho = sum_k (Phi L)_k^2, which needs
+ * rank(P) columns instead of N -- for a positive semi-definite P of rank at most min(128, N/2)
+ * (an SCF density matrix has the rank of its occupied orbitals), on the fused path when N <= 320
+ * and the rank <= 64, else on the staged path (fp16 / bf16); QMT_BAD_ARG when the factorisation
+ * finds P indefinite or of higher rank.  What the factor leaves out is checked on
  * the device (max |P - L L^T| <= 2e-7 max |P|), which runs the unfactored kernel instead when the
  * check fails, without a host round trip. */
 qmt_status qmt_set_density_path(int mode);
@@ -134,10 +135,10 @@ qmt_status qmt_density_factor_rank(qmt_mol* mol, int* rank_out, void* stream);
  * one molecule after another; then each grid is summed and, with rescale, scaled to its nuclear
  * charge.  Inputs: shapes[3 i + (0,1,2)] = nx, ny, nz and geoms[4 i + (0,1,2,3)] = step, ox, oy,
  * oz (bohr) of molecule i; qube_devs[i] its grid (device, nx ny nz floats, x-fastest); paths[i]
- * 0 = automatic (fused or staged), 1 = staged, 2 = fused, 3 = fused with the factored density
- * matrix when it has one that passes its check (as qmt_set_density_path mode 3), else fused
- * (NULL: automatic).  A factored molecule's factor is built at creation: refresh != 0 is refused
- * for a batch that holds one.
+ * 0 = automatic (fused or staged), 1 = staged, 2 = fused, 3 = fused or staged with the factored
+ * density matrix when it has one that passes its check (as qmt_set_density_path mode 3), else
+ * unfactored (NULL: automatic).  A factored molecule's factor is built at creation: refresh != 0
+ * is refused for a batch that holds one.
  * qmt_batch_create builds every operand (it synchronises `stream`); qmt_batch_density then
  * allocates nothing and is fully asynchronous, so a CUDA graph can capture it.  With refresh != 0
  * it first re-derives each molecule's split density matrix on the device from the matrix last
@@ -151,7 +152,8 @@ qmt_status qmt_batch_density(qmt_batch* batch, int rescale, int refresh, void* s
 /* FP64 grid sums before rescaling, sums[nmol] (host); synchronous; reports and clears the kernels'
  * barrier-timeout flags (QMT_CUDA_ERR). */
 qmt_status qmt_batch_sums(qmt_batch* batch, double* sums, void* stream);
-/* Molecules of the batch on the fused launches, and of those on the factored one (-1 for NULL). */
+/* Molecules of the batch on the fused launches, and those with a factored density matrix (fused
+ * or staged) (-1 for NULL). */
 int qmt_batch_fused_count(const qmt_batch* batch);
 int qmt_batch_factored_count(const qmt_batch* batch);
 qmt_status qmt_batch_destroy(qmt_batch* batch);

@@ -2282,8 +2282,8 @@ qmt_status density_tc(qmt_mol* mol, int nx, int ny, int nz, float step, float ox
   if ((st = mol->d_partials.reserve(ntiles * sizeof(double)))) return st;
   const double outscale = 2.0 * (double)step * step * step / pm.s3;
   const bool fusable = fused_fits(mol, sh);
-  const bool fused = g_density_path >= 2 ? fusable : (g_density_path == 1 ? false : fusable);
-  if (g_density_path >= 2 && !fusable)
+  const bool fused = g_density_path == 1 ? false : fusable;
+  if (g_density_path == 2 && !fusable)
     return fail(QMT_BAD_ARG, "fused density path needs fp16/bf16, N <= 320 and molecule tables that fit in shared memory");
   // the factored matrix when there is one (automatic, or asked for): fused (rank <= 64) or staged
   // (rank <= 128, fp16 / bf16)
@@ -2375,7 +2375,7 @@ namespace qmt {
 static qmt_status batch_operands(const BatchItem& it, int prec, bool refresh, cudaStream_t s) {
   if (it.fact) {
     if (refresh) return fail(QMT_BAD_ARG, "a batch with factored molecules cannot re-derive their operands");
-    return QMT_OK;
+    return it.fused ? QMT_OK : ensure_factor_rows(it.mol, prec, it.sh, s);
   }
   if (refresh) {
     it.mol->fused_prec = -1;
@@ -2438,7 +2438,7 @@ static qmt_status batch_run(qmt_batch* b, int rescale, bool refresh, cudaStream_
   }
   for (const BatchItem& it : b->items)
     if (!it.fused && (st = run_tc<FMT>(it.mol, it.sh, it.pm, it.ntiles, b->precision, it.qube, it.outscale, s,
-                                       &b->phi_hi, &b->phi_lo, BATCH_STAGE_BYTES)))
+                                       &b->phi_hi, &b->phi_lo, BATCH_STAGE_BYTES, it.fact ? 1 : 0)))
       return st;
   for (const BatchItem& it : b->items)
     if ((st = finish_density(it.mol, it.pm.nvox, it.ntiles, rescale, it.qube, nullptr, s))) return st;
@@ -2484,13 +2484,13 @@ qmt_status qmt_batch_create(int nmol, qmt_mol* const* mols, const int32_t* shape
       break;
     }
     const bool fits = fused_fits(m, it.sh);
-    if (path >= 2 && !fits) {
+    if (path == 2 && !fits) {
       st = fail(QMT_BAD_ARG, "fused density path requested for a molecule it does not take");
       break;
     }
-    it.fused = path >= 2 || (path == 0 && fits);
+    it.fused = path == 2 || ((path == 0 || path == 3) && fits);
     it.fact = false;
-    if (path == 3) {   // factored when the matrix has a factor that passes the device check
+    if (path == 3 && it.sh.fmt != FMT_TF32) {   // factored when the matrix has a factor that passes the check
       int gate = 1;
       if ((st = ensure_factor(m, precision, it.sh, s))) break;
       if (m->fact_rank > 0) {
@@ -2501,7 +2501,7 @@ qmt_status qmt_batch_create(int nmol, qmt_mol* const* mols, const int32_t* shape
           break;
         }
       }
-      it.fact = m->fact_rank > 0 && gate == 0 && m->fact_r16 <= kFusedFactorMaxR16;
+      it.fact = m->fact_rank > 0 && gate == 0 && (!it.fused || m->fact_r16 <= kFusedFactorMaxR16);
     }
     if ((st = m->d_partials.reserve(it.ntiles * sizeof(double))) || (st = m->d_scalars.reserve(64 * sizeof(double))))
       break;
@@ -2517,7 +2517,7 @@ qmt_status qmt_batch_create(int nmol, qmt_mol* const* mols, const int32_t* shape
       int stg = 0, largest = -1;
       if ((st = batch_group(b, g, kind == 1, stg, largest))) break;
       if (g.fdesc.empty() || stg >= 2) break;
-      b->items[largest].fused = b->items[largest].fact = false;
+      b->items[largest].fused = false;   // (a factored molecule stays factored on the staged path)
       if ((st = batch_operands(b->items[largest], precision, false, s))) break;
     }
   }
@@ -2587,7 +2587,9 @@ int qmt_batch_fused_count(const qmt_batch* b) {
 
 int qmt_batch_factored_count(const qmt_batch* b) {
   if (!b) return -1;
-  return (int)b->fact.fdesc.size();
+  int n = 0;
+  for (const BatchItem& it : b->items) n += it.fact ? 1 : 0;
+  return n;
 }
 
 qmt_status qmt_batch_destroy(qmt_batch* b) {

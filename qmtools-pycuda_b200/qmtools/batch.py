@@ -50,12 +50,13 @@ class BatchEvaluator:
         total = int(self.offsets[-1])
         self.q = torch.zeros(total, dtype=torch.float32, device="cuda")
         self.v = torch.zeros(total, dtype=torch.float32, device="cuda") if hartree else None
-        # tuned choices; a fused molecule takes its factored density matrix when it has one (a
-        # batch that re-derives its operands in the graph keeps the unfactored matrices)
-        from .autotune import PATH_FUSED, PATH_FACTORED
+        # tuned choices; every molecule takes its factored density matrix when it has one, on the
+        # fused path when it fits (a batch that re-derives its operands in the graph keeps the
+        # unfactored matrices)
+        from .autotune import PATH_FACTORED
         self.paths = [self.tuner.density_path(m, n, precision) for m, n in zip(self.molecules, self.npts)]
-        if not self.refresh:
-            self.paths = [PATH_FACTORED if p == PATH_FUSED else p for p in self.paths]
+        if not self.refresh and not precision.startswith("tf32"):
+            self.paths = [PATH_FACTORED for _ in self.paths]
         self.fft_lengths = []
         if hartree:
             for m, (nx, ny, nz, *_) in zip(self.molecules, geo):
