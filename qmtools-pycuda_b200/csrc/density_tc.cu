@@ -731,10 +731,37 @@ __device__ __forceinline__ void unpack8(uint4 a, float* out) {
   }
 }
 
+// Primitive exponentials exp(-alpha q), zero at and beyond the cut-off.  FAST producers (the fused
+// kernel with the factored density matrix) take 2^(-beta q), beta = alpha log2(e) formed once per
+// primitive, with a single ex2.approx in place of the longer expf sequence: Phi' about a sixth
+// faster, at a larger error (fp16x3 density against the FP64 path, relative L2: 4.1e-7 -> 5.4e-7
+// on a 24^3 grid at 0.8 bohr around the 30-atom molecule, 4.2e-7 -> 4.5e-7 on its 128^3 grid at
+// 0.15 bohr).  The unfactored contraction sits nearer its 1e-6 budget (9.7e-7 on the coarse grid)
+// and keeps expf.
+constexpr float kLog2e = 1.44269504f;
+constexpr float kExpCut2 = kExpCut * kLog2e;   // the cut-off in the base-2 scale
+
+template <bool FAST>
+__device__ __forceinline__ float exp_scale(float alpha) {
+  if constexpr (FAST) return alpha * kLog2e;
+  else return alpha;
+}
+
+template <bool FAST>
+__device__ __forceinline__ float exp_cut(float x) {   // x = exp_scale<FAST>(alpha) * q
+  if constexpr (FAST) {
+    float r;
+    asm("ex2.approx.ftz.f32 %0, %1;" : "=f"(r) : "f"(-x));
+    return x < kExpCut2 ? r : 0.f;
+  } else {
+    return x < kExpCut ? expf(-x) : 0.f;
+  }
+}
+
 // Contracted radial parts sum_k c_k exp(-alpha_k r^2) (zero beyond the cut-off) of NP primitives
 // (alpha, c) at two points, in primitive order.  When the next shell of the atom has the same
 // exponents (pn != nullptr) its radial parts are formed from the same exponentials.
-template <int NP>
+template <int NP, bool FAST>
 __device__ __forceinline__ void radial_np(const float2* pa, const float2* pn, float q0, float q1, float& r0,
                                           float& r1, float& n0, float& n1) {
   float2 ac[NP];
@@ -743,9 +770,9 @@ __device__ __forceinline__ void radial_np(const float2* pa, const float2* pn, fl
   float e0[NP], e1[NP];
 #pragma unroll
   for (int k = 0; k < NP; ++k) {
-    const float x0 = ac[k].x * q0, x1 = ac[k].x * q1;
-    e0[k] = x0 < kExpCut ? expf(-x0) : 0.f;
-    e1[k] = x1 < kExpCut ? expf(-x1) : 0.f;
+    const float b = exp_scale<FAST>(ac[k].x);
+    e0[k] = exp_cut<FAST>(b * q0);
+    e1[k] = exp_cut<FAST>(b * q1);
   }
   r0 = 0.f;
   r1 = 0.f;
@@ -773,7 +800,7 @@ __device__ __forceinline__ void radial_np(const float2* pa, const float2* pn, fl
 // same order as the generic loop, so the values are identical.
 enum { SHAPE_GENERIC = 0, SHAPE_S3S1P1 = 1, SHAPE_S8S8S1P3P1D1 = 2 };
 
-template <int NP>
+template <int NP, bool FAST>
 __device__ __forceinline__ void exps2(const float2* pa, float q0, float q1, float qmin, float (&e0)[NP],
                                       float (&e1)[NP], float (&c)[NP]) {
   float2 ac[NP];
@@ -785,9 +812,9 @@ __device__ __forceinline__ void exps2(const float2* pa, float q0, float q1, floa
     e0[k] = 0.f;
     e1[k] = 0.f;
     if (ac[k].x * qmin < kExpCut) {   // uniform over the warp: qmin is the item's minimum
-      const float x0 = ac[k].x * q0, x1 = ac[k].x * q1;
-      e0[k] = x0 < kExpCut ? expf(-x0) : 0.f;
-      e1[k] = x1 < kExpCut ? expf(-x1) : 0.f;
+      const float b = exp_scale<FAST>(ac[k].x);
+      e0[k] = exp_cut<FAST>(b * q0);
+      e1[k] = exp_cut<FAST>(b * q1);
     }
   }
 }
@@ -907,8 +934,9 @@ struct WindowRowsOut {
 // in `pos`, 1e30 for rows without a point), handed to `out` shell by shell.  Tables as staged
 // by the kernels: shell records, (alpha, scaled coefficient) pairs in descending alpha order,
 // per-atom words (first shell | layout << 24), float nuclear coordinates.  The whole warp works
-// on the atom (lanes r0 = half * 32 + lane).  Returns the atom's last function.
-template <class Out>
+// on the atom (lanes r0 = half * 32 + lane); FAST selects the exponentials of exp_cut.  Returns
+// the atom's last function.
+template <bool FAST, class Out>
 __device__ __forceinline__ int atom_rows(const int4* sh_s, const float2* pr_s, const int* ash_s, const float* crd_s,
                                          int a, const double (*pos)[3], int r0, const Out& out) {
   const int as0 = ash_s[a];
@@ -937,15 +965,15 @@ __device__ __forceinline__ int atom_rows(const int4* sh_s, const float2* pr_s, c
     if (shape == SHAPE_S3S1P1) {
       {
         float e0[3], e1[3], c[3];
-        exps2<3>(pa, q0, q1, qmin, e0, e1, c);
+        exps2<3, FAST>(pa, q0, q1, qmin, e0, e1, c);
         contract2<3>(c, e0, e1, rA0, rA1);
       }
       float rB0, rB1, rC0, rC1;
       {
         float e0[1], e1[1], c[1];
-        exps2<1>(pa + 3, q0, q1, qmin, e0, e1, c);
+        exps2<1, FAST>(pa + 3, q0, q1, qmin, e0, e1, c);
         contract2<1>(c, e0, e1, rB0, rB1);
-        exps2<1>(pa + 4, q0, q1, qmin, e0, e1, c);
+        exps2<1, FAST>(pa + 4, q0, q1, qmin, e0, e1, c);
         contract2<1>(c, e0, e1, rC0, rC1);
       }
       if (!ok0) rA0 = rB0 = rC0 = 0.f;
@@ -961,7 +989,7 @@ __device__ __forceinline__ int atom_rows(const int4* sh_s, const float2* pr_s, c
       float rB0, rB1;
       {
         float e0[8], e1[8], c[8], d[8];
-        exps2<8>(pa, q0, q1, qmin, e0, e1, c);
+        exps2<8, FAST>(pa, q0, q1, qmin, e0, e1, c);
         contract2<8>(c, e0, e1, rA0, rA1);
 #pragma unroll
         for (int k = 0; k < 8; ++k) d[k] = pa[8 + k].y;   // second s shell: same exponents
@@ -970,19 +998,19 @@ __device__ __forceinline__ int atom_rows(const int4* sh_s, const float2* pr_s, c
       float rC0, rC1, rD0, rD1, rE0, rE1, rF0, rF1;
       {
         float e0[1], e1[1], c[1];
-        exps2<1>(pa + 16, q0, q1, qmin, e0, e1, c);
+        exps2<1, FAST>(pa + 16, q0, q1, qmin, e0, e1, c);
         contract2<1>(c, e0, e1, rC0, rC1);
       }
       {
         float e0[3], e1[3], c[3];
-        exps2<3>(pa + 17, q0, q1, qmin, e0, e1, c);
+        exps2<3, FAST>(pa + 17, q0, q1, qmin, e0, e1, c);
         contract2<3>(c, e0, e1, rD0, rD1);
       }
       {
         float e0[1], e1[1], c[1];
-        exps2<1>(pa + 20, q0, q1, qmin, e0, e1, c);
+        exps2<1, FAST>(pa + 20, q0, q1, qmin, e0, e1, c);
         contract2<1>(c, e0, e1, rE0, rE1);
-        exps2<1>(pa + 21, q0, q1, qmin, e0, e1, c);
+        exps2<1, FAST>(pa + 21, q0, q1, qmin, e0, e1, c);
         contract2<1>(c, e0, e1, rF0, rF1);
       }
       if (!ok0) rA0 = rB0 = rC0 = rD0 = rE0 = rF0 = 0.f;
@@ -1020,22 +1048,22 @@ __device__ __forceinline__ int atom_rows(const int4* sh_s, const float2* pr_s, c
           rad0 = rad1 = 0.f;
           nx0 = nx1 = 0.f;
           break;
-        case 1: radial_np<1>(pa, pn, q0, q1, rad0, rad1, nx0, nx1); break;
-        case 2: radial_np<2>(pa, pn, q0, q1, rad0, rad1, nx0, nx1); break;
-        case 3: radial_np<3>(pa, pn, q0, q1, rad0, rad1, nx0, nx1); break;
-        case 4: radial_np<4>(pa, pn, q0, q1, rad0, rad1, nx0, nx1); break;
-        case 5: radial_np<5>(pa, pn, q0, q1, rad0, rad1, nx0, nx1); break;
-        case 6: radial_np<6>(pa, pn, q0, q1, rad0, rad1, nx0, nx1); break;
-        case 7: radial_np<7>(pa, pn, q0, q1, rad0, rad1, nx0, nx1); break;
-        case 8: radial_np<8>(pa, pn, q0, q1, rad0, rad1, nx0, nx1); break;
+        case 1: radial_np<1, FAST>(pa, pn, q0, q1, rad0, rad1, nx0, nx1); break;
+        case 2: radial_np<2, FAST>(pa, pn, q0, q1, rad0, rad1, nx0, nx1); break;
+        case 3: radial_np<3, FAST>(pa, pn, q0, q1, rad0, rad1, nx0, nx1); break;
+        case 4: radial_np<4, FAST>(pa, pn, q0, q1, rad0, rad1, nx0, nx1); break;
+        case 5: radial_np<5, FAST>(pa, pn, q0, q1, rad0, rad1, nx0, nx1); break;
+        case 6: radial_np<6, FAST>(pa, pn, q0, q1, rad0, rad1, nx0, nx1); break;
+        case 7: radial_np<7, FAST>(pa, pn, q0, q1, rad0, rad1, nx0, nx1); break;
+        case 8: radial_np<8, FAST>(pa, pn, q0, q1, rad0, rad1, nx0, nx1); break;
         default:
           rad0 = 0.f;
           rad1 = 0.f;
           for (int k = 0; k < np_ - sk; ++k) {
             const float2 ac = pa[k];
-            const float a0 = ac.x * q0, a1 = ac.x * q1;
-            rad0 = fmaf(ac.y, a0 < kExpCut ? expf(-a0) : 0.f, rad0);
-            rad1 = fmaf(ac.y, a1 < kExpCut ? expf(-a1) : 0.f, rad1);
+            const float b = exp_scale<FAST>(ac.x);
+            rad0 = fmaf(ac.y, exp_cut<FAST>(b * q0), rad0);
+            rad1 = fmaf(ac.y, exp_cut<FAST>(b * q1), rad1);
           }
       }
     }
@@ -1157,7 +1185,7 @@ __global__ void __launch_bounds__(STAGE_THREADS, 2) basis_window_kernel(const St
         const int a = ar.x + (itm >> 1);
         if ((ash_s[a + 1] & 0xffffff) <= (ash_s[a] & 0xffffff)) continue;
         const int r0 = (itm & 1) * 32 + lane;
-        atom_rows(sh_s, pr_s, ash_s, crd_s, a, pos, r0,
+        atom_rows<false>(sh_s, pr_s, ash_s, crd_s, a, pos, r0,
                   WindowRowsOut{buf + r0 * STAGE_LD, buf + (r0 + 64) * STAGE_LD, c0, pos[r0][0] < 1e29,
                                 pos[r0 + 64][0] < 1e29});
       }
@@ -1423,18 +1451,17 @@ __global__ void __launch_bounds__(FUSED_THREADS, 1)
   __shared__ __align__(8) uint64_t chunk_bar[MAX_FUSED_CHUNKS], t_full, drain_bar;
   __shared__ int item_ctr;
   __shared__ uint32_t tmem_slot;
-  // tile positions (production) and the epilogue's partial sums share their storage: every reader
-  // of the one is past a barrier of all compute warps before the other is written
+  // tile positions (production) and the epilogue's row partials share their storage: every
+  // reader of the one is past a barrier of all compute warps before the other is written
   __shared__ union {
     double pos[128][3];
-    struct {
-      double rho_part[FUSED_NCW / 4][128];
-      double red[FUSED_NCW];
-    } e;
+    double rho_part[FUSED_NCW / 4][128];
   } ps;
   double(*pos)[3] = ps.pos;
-  double(*rho_part)[128] = ps.e.rho_part;
-  double* red = ps.e.red;
+  double(*rho_part)[128] = ps.rho_part;
+  // per-warp sums of the tile (written after the next tile's first epilogue barrier, read by
+  // compute thread 0 before it reaches that barrier: no barrier needed after the read)
+  __shared__ double red[FUSED_NCW];
   __shared__ volatile int abort_flag;
 
   uint8_t* smem = reinterpret_cast<uint8_t*>((reinterpret_cast<uintptr_t>(smem_dyn) + 1023) & ~uintptr_t(1023));
@@ -1553,7 +1580,7 @@ __global__ void __launch_bounds__(FUSED_THREADS, 1)
         const int a = itm >> 1;
         const int s0 = ash_s[a] & 0xffffff;
         if ((ash_s[a + 1] & 0xffffff) <= s0) continue;
-        const int flast = atom_rows(sh_s, pr_s, ash_s, crd_s, a, pos, (itm & 1) * 32 + lane,
+        const int flast = atom_rows<FACT>(sh_s, pr_s, ash_s, crd_s, a, pos, (itm & 1) * 32 + lane,
                                     SwizzledRowsOut<FMT>{A_hi, A_lo, (itm & 1) * 32 + lane, two, tail0});
         // publish: generic-proxy writes of A become visible to the tensor core, then one arrival
         // per column chunk this atom wrote
@@ -1573,8 +1600,8 @@ __global__ void __launch_bounds__(FUSED_THREADS, 1)
       double acc[2] = {0.0, 0.0};
       const uint32_t trow = tmem + ((uint32_t)(q * 32) << 16);
       if (FACT) {
-        // T = the accumulators' sum (FP32, rounded), rho = sum_k 2^-2h_k T_ik^2 over this warp's
-        // column chunks (FP64: the terms are all positive); M.gsc holds the scales 2^-2h_k
+        // T = the accumulators' sum (FP32, rounded), rho = sum_k (2^-h_k T_ik)^2 over this warp's
+        // column chunks; M.gsc holds the column scales (layout of ensure_factor)
         // (each accumulator: nb columns of A_x B_hi, then with two pieces nb of A_x B_lo)
         const int nb = M.nb, nfull = two ? 2 * nb : nb;
         const int ngrp = (fact_nacc(M.nchunks, nb, two) + (two ? 1 : 0)) * (two ? 2 : 1);
@@ -1598,11 +1625,22 @@ __global__ void __launch_bounds__(FUSED_THREADS, 1)
               for (int k = 0; k < 16; ++k) tsum[k] += __uint_as_float(t0[k]);
             }
           }
+          // (2^-h_k T_k)^2 with the FP32 scales after the FP64 ones: eight squares per FP32
+          // partial, the partials summed in FP64, as in the unfactored epilogue
+          const float4* hs = reinterpret_cast<const float4*>(reinterpret_cast<const float*>(M.gsc + 2 * nb) + c * 16);
+          float a32[2] = {0.f, 0.f};
 #pragma unroll
-          for (int k = 0; k < 16; ++k) {
-            const double v = (double)tsum[k];
-            acc[k & 1] = fma(__ldg(M.gsc + c * 16 + k) * v, v, acc[k & 1]);
+          for (int k4 = 0; k4 < 4; ++k4) {
+            const float4 h4 = __ldg(hs + k4);
+            const float hk[4] = {h4.x, h4.y, h4.z, h4.w};
+#pragma unroll
+            for (int e = 0; e < 4; ++e) {
+              const float u = tsum[4 * k4 + e] * hk[e];
+              a32[e & 1] = fmaf(u, u, a32[e & 1]);
+            }
           }
+          acc[0] += (double)a32[0];
+          acc[1] += (double)a32[1];
         }
       } else {
         for (int c = hh; c * 16 < n16; c += FUSED_NCW / 4) {
@@ -1667,12 +1705,11 @@ __global__ void __launch_bounds__(FUSED_THREADS, 1)
       for (int o = 16; o > 0; o >>= 1) mysum += __shfl_xor_sync(0xffffffffu, mysum, o);
       if (lane == 0) red[cw] = mysum;
       named_barrier(1, FUSED_NCT);
-      if (ct == 0) {
+      if (ct == 0) {   // the other warps go on to the next tile meanwhile
         double tot = 0;
         for (int w = 0; w < FUSED_NCW; ++w) tot += red[w];
         M.partials[lt] = tot;
       }
-      named_barrier(1, FUSED_NCT);
     }
   }
 
@@ -1945,10 +1982,12 @@ static qmt_status ensure_factor(qmt_mol* m, int prec, const TcShape& sh, cudaStr
     QMT_CHECK_LAUNCH("fact_residual_kernel");
     m->fact_gate = flag;
   }
-  // column scales on the host (2^-2h_k for the squares, then 2^h_k for the split), the scaled,
-  // split factor in its stage layout on the device
+  // column scales on the host -- 2^-2h_k (FP64, the staged path's squares), 2^h_k (FP64, the
+  // split), then 2^-h_k (FP32, the fused path's squares (2^-h_k T_k)^2: an exact scaling) -- and
+  // the scaled, split factor in its stage layout on the device
   const int r16 = std::max(16, (r + 15) / 16 * 16);
-  std::vector<double> sc(2 * r16, 0.0);
+  std::vector<double> sc(2 * r16 + r16 / 2, 0.0);
+  float* scf = reinterpret_cast<float*>(sc.data() + 2 * r16);
   for (int q = 0; q < r; ++q) {
     double wmax = 0.0;
     for (int j = 0; j < n; ++j) wmax = std::max(wmax, std::fabs(Lr[(size_t)j * rmax + q] * m->split_inv[j]));
@@ -1956,10 +1995,12 @@ static qmt_status ensure_factor(qmt_mol* m, int prec, const TcShape& sh, cudaStr
     h = std::max(-100, std::min(100, h));
     sc[q] = std::ldexp(1.0, -2 * h);
     sc[r16 + q] = std::ldexp(1.0, h);
+    scf[q] = std::ldexp(1.0f, -h);
   }
+  const size_t sc_bytes = sc.size() * sizeof(double);
   const size_t total = (size_t)(n16 / 16) * sh.nsplit * r16 * 32;   // bytes
-  if ((st = m->d_fact_B.reserve(total)) || (st = m->d_fact_scale.reserve(2 * r16 * sizeof(double)))) return st;
-  QMT_CUDA(cudaMemcpyAsync(m->d_fact_scale.ptr, sc.data(), 2 * r16 * sizeof(double), cudaMemcpyHostToDevice, s));
+  if ((st = m->d_fact_B.reserve(total)) || (st = m->d_fact_scale.reserve(sc_bytes))) return st;
+  QMT_CUDA(cudaMemcpyAsync(m->d_fact_scale.ptr, sc.data(), sc_bytes, cudaMemcpyHostToDevice, s));
   const int64_t tot = (int64_t)n16 * r16;
   const int blocks = (int)std::min<int64_t>((tot + 255) / 256, (int64_t)sm_count() * 4);
   fact_split_kernel<<<std::max(blocks, 1), 256, 0, s>>>(m->d_fact_L.as<double>(), n, rmax, r, n16, r16,

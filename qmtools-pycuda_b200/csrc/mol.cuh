@@ -54,7 +54,7 @@ struct qmt_mol {
   int fact_rows_prec = -1;      // precision of d_fact_Bs (-1: not built for the current factor)
   qmt::DevBuf d_fact_Bs;        // the factor as the staged path's B operand (fact_rows_kernel)
   const int* fact_gate = nullptr; // that flag: 0 when the factor reproduces P, 1 when it does not
-  qmt::DevBuf d_fact_scale;     // per factor column k, the scale 2^-2h_k of its squares
+  qmt::DevBuf d_fact_scale;     // per factor column k: 2^-2h_k, 2^h_k (FP64), then 2^-h_k (FP32)
   qmt::DevBuf d_fused_tab;      // fused path: packed shell records, then (alpha, scaled coefficient) pairs
   qmt::DevBuf d_coords, d_types, d_shells, d_alpha, d_coeff, d_alpha64, d_coeff64;
   qmt::DevBuf d_P32, d_P64;
