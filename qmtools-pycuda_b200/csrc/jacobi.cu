@@ -58,23 +58,31 @@ __device__ __forceinline__ uint64_t jac_timer_ns() {
 }
 
 // Sense-counting grid barrier for a cooperative launch (all CTAs co-resident).  Returns false
-// on every CTA once any CTA has waited more than `wait_ns` or raised the flag.
+// on every CTA once any CTA has waited more than `wait_ns` or raised the flag.  Arrivals are
+// acquire-release atomics on bar[0] (the CTA's writes are ordered before its arrival by the CTA
+// barrier); the last arrival resets the count and releases the generation bar[1], which the
+// others read with acquire loads: no full memory fences.
+__device__ __forceinline__ unsigned ld_acquire_gpu(const unsigned* p) {
+  unsigned v;
+  asm volatile("ld.acquire.gpu.global.u32 %0, [%1];" : "=r"(v) : "l"(p) : "memory");
+  return v;
+}
+
 __device__ bool grid_barrier(unsigned* bar, int* flag, unsigned nblocks, uint64_t wait_ns) {
   __shared__ int ok_s;
   __syncthreads();
   if (threadIdx.x == 0 && threadIdx.y == 0) {
-    volatile unsigned* gen = bar + 1;
     volatile int* vflag = flag;
-    const unsigned g = *gen;
-    __threadfence();
+    const unsigned g = ld_acquire_gpu(bar + 1);
     int ok = 1;
-    if (atomicAdd(bar, 1u) == nblocks - 1) {
-      atomicExch(bar, 0u);
-      __threadfence();
-      atomicAdd(bar + 1, 1u);
+    unsigned old;
+    asm volatile("atom.add.acq_rel.gpu.global.u32 %0, [%1], 1;" : "=r"(old) : "l"(bar) : "memory");
+    if (old == nblocks - 1) {
+      asm volatile("st.relaxed.gpu.global.u32 [%0], 0;" ::"l"(bar) : "memory");
+      asm volatile("red.release.gpu.global.add.u32 [%0], 1;" ::"l"(bar + 1) : "memory");
     } else {
       const uint64_t t0 = jac_timer_ns();
-      while (*gen == g) {
+      while (ld_acquire_gpu(bar + 1) == g) {
         if (*vflag) {
           ok = 0;
           break;
@@ -86,16 +94,12 @@ __device__ bool grid_barrier(unsigned* bar, int* flag, unsigned nblocks, uint64_
         }
       }
     }
-    __threadfence();
     ok_s = ok && !*vflag;
   }
   __syncthreads();
   return ok_s != 0;
 }
 
-// Source term of a point: Q / h (reference mode) or 4 pi h^2 rho (Dirichlet mode), the same FP32
-// value every sweep.
-// (explicit roundings: both kernels must give the same bits, whatever the compiler contracts)
 template <bool DIRICHLET>
 __device__ __forceinline__ float jac_source(float q, float h, float src_scale) {
   if constexpr (!DIRICHLET) return q / h;
@@ -127,12 +131,31 @@ __device__ __forceinline__ float jac_point(float xm, float xp, float yp, float y
 
 __device__ __forceinline__ float4 ldcg4(const float* p) { return __ldcg(reinterpret_cast<const float4*>(p)); }
 
+// A thread's work items in a sweep: the grid-stride sequence tid, tid + nthreads, ... over
+// the groups (or points), as grid coordinates of the first item and of the stride, advanced by
+// additions with carries -- no division per item (the stride is below nxq * ny * nz, so each
+// carry needs one subtraction).  Set up once per launch.
+struct JacWalk {
+  int x, y, z;      // first item: x group (vec4) or point
+  int sx, sy, sz;   // the stride
+};
+
+__device__ JacWalk jac_walk(const JacobiArgs& a) {
+  const uint32_t w = a.vec4 ? (uint32_t)(a.nx >> 2) : (uint32_t)a.nx;
+  const uint32_t ny = (uint32_t)a.ny;
+  const uint32_t nthreads = gridDim.x * JAC_THREADS;   // (the grid is a few CTAs per SM)
+  const uint32_t tid = blockIdx.x * JAC_THREADS + threadIdx.y * JX + threadIdx.x;
+  const uint32_t r = tid / w, rs = nthreads / w;
+  return JacWalk{(int)(tid - r * w), (int)(r % ny), (int)(r / ny), (int)(nthreads - rs * w), (int)(rs % ny),
+                 (int)(rs / ny)};
+}
+
 // One sweep src -> dst.  Work items are groups of four consecutive x points (float4 loads of
 // the row, the four neighbouring rows and Q, scalar loads of the two x halo values), spread over
 // all CTAs; every load of a group is independent, so many are in flight per thread.  Returns
 // this thread's FP64 sum |dst - src| when `resid` is set.
 template <bool DIRICHLET>
-__device__ double sweep(const JacobiArgs& a, const float* src, float* dst, bool resid) {
+__device__ double sweep(const JacobiArgs& a, const float* src, float* dst, bool resid, const JacWalk& wk) {
   const int nx = a.nx, ny = a.ny, nz = a.nz;
   const int64_t row = nx, plane = (int64_t)nx * ny;
   const int64_t nthreads = (int64_t)gridDim.x * JAC_THREADS;
@@ -141,10 +164,9 @@ __device__ double sweep(const JacobiArgs& a, const float* src, float* dst, bool 
   if (a.vec4) {
     const int nxq = nx >> 2;
     const int64_t ngroups = (int64_t)nxq * ny * nz;
+    int xq = wk.x, y = wk.y, z = wk.z;
+    const int sx = wk.sx, sy = wk.sy, sz = wk.sz;
     for (int64_t gi = tid; gi < ngroups; gi += nthreads) {
-      const int xq = (int)(gi % nxq);
-      const int64_t r = gi / nxq;
-      const int y = (int)(r % ny), z = (int)(r / ny);
       const int x0 = xq * 4;
       const int64_t b = z * plane + (int64_t)y * row + x0;
       const float4 c = ldcg4(src + b);
@@ -170,13 +192,23 @@ __device__ double sweep(const JacobiArgs& a, const float* src, float* dst, bool 
       if (resid)
         dsum += (fabs((double)o.x - (double)c.x) + fabs((double)o.y - (double)c.y)) +
                 (fabs((double)o.z - (double)c.z) + fabs((double)o.w - (double)c.w));
+      xq += sx;
+      if (xq >= nxq) {
+        xq -= nxq;
+        ++y;
+      }
+      y += sy;
+      if (y >= ny) {
+        y -= ny;
+        ++z;
+      }
+      z += sz;
     }
   } else {
     const int64_t n = plane * nz;
+    int x = wk.x, y = wk.y, z = wk.z;
+    const int sx = wk.sx, sy = wk.sy, sz = wk.sz;
     for (int64_t g = tid; g < n; g += nthreads) {
-      const int x = (int)(g % nx);
-      const int64_t r = g / nx;
-      const int y = (int)(r % ny), z = (int)(r / ny);
       const float vc = __ldcg(src + g);
       const float xm = x > 0 ? __ldcg(src + g - 1) : 0.f;
       const float xp = x + 1 < nx ? __ldcg(src + g + 1) : 0.f;
@@ -189,6 +221,17 @@ __device__ double sweep(const JacobiArgs& a, const float* src, float* dst, bool 
           jac_point<DIRICHLET>(xm, xp, yp, ym, zp, zm, jac_source<DIRICHLET>(__ldg(a.Q + g), a.h, a.src_scale), vc, edge);
       __stcg(dst + g, o);
       if (resid) dsum += fabs((double)o - (double)vc);
+      x += sx;
+      if (x >= nx) {
+        x -= nx;
+        ++y;
+      }
+      y += sy;
+      if (y >= ny) {
+        y -= ny;
+        ++z;
+      }
+      z += sz;
     }
   }
   return dsum;
@@ -202,15 +245,16 @@ __global__ void __launch_bounds__(JAC_THREADS, JAC_BLOCKS_PER_SM) jacobi_persist
   double delta = INFINITY;
   int sweeps = 0, pairs = 0, status = 0;
   const int lin = threadIdx.y * JX + threadIdx.x;
+  const JacWalk wk = jac_walk(a);
   while (sweeps + 2 <= a.max_sweeps) {
     ++pairs;
     const bool check = pairs % a.check_every == 0 || sweeps + 4 > a.max_sweeps;
-    sweep<DIRICHLET>(a, a.V, a.T, false);
+    sweep<DIRICHLET>(a, a.V, a.T, false, wk);
     if (!grid_barrier(a.bar, flag, nb, a.wait_ns)) {
       status = 3;
       break;
     }
-    const double ds = sweep<DIRICHLET>(a, a.T, a.V, check);
+    const double ds = sweep<DIRICHLET>(a, a.T, a.V, check, wk);
     sweeps += 2;
     if (!check) {
       if (!grid_barrier(a.bar, flag, nb, a.wait_ns)) {
