@@ -17,8 +17,9 @@
 //    throughout from FP64 coefficients and centres (gto64_pairs_kernel): an FP32 term's error
 //    (rounded coefficients and arithmetic) is proportional to its size, and the potential at a
 //    grid boundary is the small difference of large electronic and nuclear parts;
-//  * the rest (gto32_pairs_kernel): where T = p |P - C|^2 >= 30 (99.5% of the point-pair terms on
-//    the boundary of the medium molecule's grid) the Boys functions take their asymptotic form
+//  * the rest (gto32_pairs_kernel), less those below 1e-11 of the total size (kFp32Screen): where
+//    T = p |P - C|^2 >= 30 (99.5% of the point-pair terms on the boundary of the medium
+//    molecule's grid) the Boys functions take their asymptotic form
 //        (-2p)^n F_n(T) = sqrt(pi) / (2 sqrt(p)) * (-1)^n (2n-1)!! / r^(2n+1)
 //    (relative error below e^-T T^(L-1/2) < 2e-9 for L <= 4): one reciprocal square root and the
 //    Hermite recursion in FP32, summed in FP32 in groups of four and the groups in FP64; nearer
@@ -736,6 +737,13 @@ static int g_gto_prec = QMT_PREC_FP32;   // FP32 with FP64 accumulation, or FP64
 // Share of the off-site pairs' total size (far-field multipoles) left to FP32 terms; the largest
 // pairs, holding the rest, take FP64 terms.
 constexpr double kFp32Share = 0.05;
+// Off-site pairs whose size is below this fraction of the total are left out of the FP32 terms.
+// On the medium molecule (30 atoms, cc-pVDZ) the FP32 pairs' sizes spread evenly over the decades
+// from 1e-4 to 1e-20 of the total; the half below 1e-11 (together 7e-8 of the total) moves the
+// potential on its grid boundary by 1e-7 of its norm against the FP64 kernel (6e-8 with every
+// pair; 1e-6 with the cut at 1e-10) and took a third of the FP32 kernel's time.  The FP64 kernel
+// keeps every pair.
+constexpr double kFp32Screen = 1e-11;
 
 // ---- host: pair table --------------------------------------------------------------------------
 static void hermite_e_host(int la, int lb, double a, double b, double xa, double xb, double E[3][3][5]) {
@@ -965,7 +973,7 @@ static qmt_status build_pairs(qmt_mol* m, cudaStream_t s) {
   }
   for (int idx : offs)    // both lists keep the order by L
     if (heavy[idx]) off64.push_back(to64(acc[idx], d64));
-    else off32.push_back(to32(acc[idx], d32));
+    else if (size[idx] >= kFp32Screen * total) off32.push_back(to32(acc[idx], d32));
   if (off32.empty()) {    // one zero pair keeps the tables well formed
     Acc z{};
     z.p = 1.0;
