@@ -323,7 +323,7 @@ def _requests(mols, basis, qmtools, serving, arrivals=None):
 def _engine_run(serving, reqs, slots, precision, realtime):
     import torch
     eng = serving.Engine(slots=slots, precision=precision)
-    eng.warm(reqs)                              # steady state: slots grown to the largest requests
+    eng.warm(reqs)                              # steady state: every slot has served every request once
     torch.cuda.synchronize()
     t0 = time.perf_counter()
     eng.run(reqs, realtime=realtime)

@@ -1924,14 +1924,18 @@ static qmt_status ensure_factor(qmt_mol* m, int prec, const TcShape& sh, cudaStr
   qmt_status st;
   if ((st = ensure_basis_operands(m, sh.kpad, s))) return st;
   const int n = m->norbs, np = m->npad, n16 = (n + 15) / 16 * 16;
+  m->fact_prec = prec;
+  m->fact_rank = 0;
+  const int rmax = std::min(kFactorMaxRank, n16 / 2);
+  // a density matrix of N_e electrons whose occupations are at most 2 has rank >= N_e / 2: with
+  // the nuclear charge for N_e (ions of up to 16 charges allowed for) a rank above rmax is known
+  // without the factorisation's host work (tens of milliseconds at a thousand functions)
+  if (0.5 * m->qtot > rmax + 8) return QMT_OK;
   const std::vector<double>& P = m->host_P64();
   double dmax = 0.0, pmax = 0.0;
   for (int j = 0; j < n; ++j) dmax = std::max(dmax, P[(size_t)j * np + j]);
   for (int j = 0; j < n; ++j)
     for (int k = 0; k < n; ++k) pmax = std::max(pmax, std::fabs(P[(size_t)j * np + k]));
-  m->fact_prec = prec;
-  m->fact_rank = 0;
-  const int rmax = std::min(kFactorMaxRank, n16 / 2);
   // L row by row (row i at Lr[i * rmax]), so that the dot products run over contiguous memory
   std::vector<double> Lr((size_t)n * rmax, 0.0);
   std::vector<double> d(n);
