@@ -174,9 +174,11 @@ qmt_status qmt_hartree_gto_points(qmt_mol* mol, int npts, const float* pts_dev,
 qmt_status qmt_hartree_gto_boundary(qmt_mol* mol, int nx, int ny, int nz, float step,
                                     float ox, float oy, float oz, float* v_dev, void* stream);
 /* Arithmetic of the three analytic-potential entry points above (new; process-wide):
- * QMT_PREC_FP32 (default) evaluates each pair term in FP32 -- the asymptotic Boys functions
- * where p |P - C|^2 >= 30, a table otherwise -- and accumulates in FP64, with the nuclear term
- * in FP64; QMT_PREC_FP64 keeps every operation in FP64 (the checker of the FP32 kernel). */
+ * QMT_PREC_FP32 (default) is mixed: the largest off-site primitive pairs (95% of the total size)
+ * and the on-site pairs, the near field and the nuclei in FP64; the other off-site pairs in FP32
+ * (asymptotic Boys functions where p |P - C|^2 >= 30), less those below 1e-11 of the total
+ * size, summed in FP64; QMT_PREC_FP64 keeps every pair and every operation in FP64 (the checker
+ * of the mixed kernels). */
 qmt_status qmt_set_gto_precision(int precision);
 
 /* ---- Jacobi relaxation ---------------------------------------------------------------- */
