@@ -1931,15 +1931,22 @@ static qmt_status ensure_factor(qmt_mol* m, int prec, const TcShape& sh, cudaStr
   // the nuclear charge for N_e (ions of up to 16 charges allowed for) a rank above rmax is known
   // without the factorisation's host work (tens of milliseconds at a thousand functions)
   if (0.5 * m->qtot > rmax + 8) return QMT_OK;
-  const std::vector<double>& P = m->host_P64();
-  double dmax = 0.0, pmax = 0.0;
-  for (int j = 0; j < n; ++j) dmax = std::max(dmax, P[(size_t)j * np + j]);
-  for (int j = 0; j < n; ++j)
-    for (int k = 0; k < n; ++k) pmax = std::max(pmax, std::fabs(P[(size_t)j * np + k]));
-  // L row by row (row i at Lr[i * rmax]), so that the dot products run over contiguous memory
-  std::vector<double> Lr((size_t)n * rmax, 0.0);
-  std::vector<double> d(n);
-  for (int j = 0; j < n; ++j) d[j] = P[(size_t)j * np + j];
+  // P_ij from the lower triangle of the matrix as given (no symmetric host copy is built)
+  const float* dm = m->dm_host.data();
+  auto Pij = [&](int i, int j) -> double { return i >= j ? dm[(size_t)i * n + j] : dm[(size_t)j * n + i]; };
+  // the scale of the device check's tolerance: max |P_jk| <= max_j P_jj for a positive
+  // semi-definite P (for any other matrix the check is only the stricter and falls back to the
+  // unfactored one)
+  double dmax = 0.0;
+  for (int j = 0; j < n; ++j) dmax = std::max(dmax, Pij(j, j));
+  const double pmax = dmax;
+  // L row by row (row i at Lr[i * rmax]), so that the dot products run over contiguous memory;
+  // the host buffers are the handle's, reused (no fresh pages per density-matrix change)
+  std::vector<double>& Lr = m->fact_Lr_host;
+  std::vector<double>& d = m->fact_d_host;
+  Lr.assign((size_t)n * rmax, 0.0);
+  d.assign(n, 0.0);
+  for (int j = 0; j < n; ++j) d[j] = Pij(j, j);
   int r = 0;
   for (;;) {
     int jp = 0;
@@ -1960,7 +1967,7 @@ static qmt_status ensure_factor(qmt_mol* m, int prec, const TcShape& sh, cudaStr
         a3 += li[q + 3] * lj[q + 3];
       }
       for (; q < r; ++q) a0 += li[q] * lj[q];
-      Lr[(size_t)i * rmax + r] = (P[(size_t)i * np + jp] - ((a0 + a1) + (a2 + a3))) * ipiv;
+      Lr[(size_t)i * rmax + r] = (Pij(i, jp) - ((a0 + a1) + (a2 + a3))) * ipiv;
     }
     Lr[(size_t)jp * rmax + r] = piv;
     for (int i = 0; i < n; ++i) d[i] -= Lr[(size_t)i * rmax + r] * Lr[(size_t)i * rmax + r];

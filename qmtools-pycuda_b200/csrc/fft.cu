@@ -615,9 +615,11 @@ struct GreenEntry {
 // Green's functions per (padded shape, step, device) up to GREEN_CACHE_BYTES of octants, and one
 // growing scratch grid per device for building them.  `tw_mu` guards the twiddles and `green_mu`
 // the rest; building a Green's function takes green_mu and then (through its FFT passes) tw_mu,
-// never the other way round.  No host synchronisation: a solve on another stream waits for a
-// cached octant's `ready` event on the device, and a build waits for the previous build's use
-// of the scratch grid (`tmp_done`) the same way.
+// never the other way round.  No host synchronisation in steady state: a solve on another
+// stream waits for a cached octant's `ready` event on the device, and a build waits for the
+// previous build's use of the scratch grid (`tmp_done`) the same way.  (Growing the scratch and
+// evicting an entry past GREEN_CACHE_BYTES free device memory with cudaFree, which does
+// synchronise the device: a workload of many new shapes pays that per new shape.)
 constexpr size_t GREEN_CACHE_BYTES = (size_t)4 << 30;
 struct DevCache {
   std::mutex tw_mu, green_mu;

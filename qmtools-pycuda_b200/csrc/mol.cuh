@@ -48,6 +48,7 @@ struct qmt_mol {
   std::vector<double> split_inv; // the same on the host
   int fact_prec = -1;           // precision of the factored-path operands below (-1: not built)
   int fact_rank = 0;            // rank of the density-matrix factor P = L L^T (0: not factored)
+  std::vector<double> fact_Lr_host, fact_d_host;   // host work buffers of the factorisation
   int fact_r16 = 0;             // the rank rounded up to 16 (the MMA N)
   qmt::DevBuf d_fact_B;         // scaled factor pieces, K-step blocks of fact_r16 rows (hi then lo)
   qmt::DevBuf d_fact_L;         // the factor (FP64, row by row) and a flag, for the residual check
