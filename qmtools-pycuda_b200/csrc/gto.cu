@@ -351,9 +351,30 @@ __device__ __forceinline__ double hermite_dot64(const DT (&D)[ncoef(L)], double 
   return acc;
 }
 
-// The near-field term of an FP32 pair (T < 30) in FP64: Boys functions from the FP64 table, FP64
-// recursion, the FP32 coefficients read from `d`.  Not inlined, so the few near terms do not raise
-// the register count of the FP32 loop around them.
+// F_m(T), m = 0..L <= 4, T < 40: each from its own Taylor step about the nearest table point,
+// F_m(T) = sum_k F_{m+k}(T_i) (-d)^k / k!, |d| <= 0.05, k <= 6 (truncation ~1e-13 relative):
+// no exponential and no division, unlike the downward recursion of boys_fn.
+template <int L>
+__device__ __forceinline__ void boys_taylor(double T, const double* __restrict__ tab, double* F) {
+  const int i = (int)(T * (1.0 / BOYS_DT) + 0.5);
+  const double d = T - i * BOYS_DT;
+  const double* row = tab + (size_t)i * BOYS_NM;
+  double c[7];
+  c[0] = 1.0;
+#pragma unroll
+  for (int k = 1; k < 7; ++k) c[k] = c[k - 1] * (-d * (1.0 / k));
+#pragma unroll
+  for (int m = 0; m <= L; ++m) {
+    double f = 0.0;
+#pragma unroll
+    for (int k = 6; k >= 0; --k) f = fma(row[m + k], c[k], f);
+    F[m] = f;
+  }
+}
+
+// The near-field term of an FP32 pair (T < 30) in FP64: Boys functions from the FP64 table
+// (boys_taylor), FP64 recursion, the FP32 coefficients read from `d`.  Not inlined, so the few
+// near terms do not raise the register count of the FP32 loop around them.
 template <int L>
 __device__ __noinline__ double near_term(float px, float py, float pz, float p, const float* __restrict__ d, float cx,
                                          float cy, float cz, const double* __restrict__ tab64) {
@@ -361,7 +382,7 @@ __device__ __noinline__ double near_term(float px, float py, float pz, float p, 
   const double pd = p;
   const double Td = pd * (Xd * Xd + Yd * Yd + Zd * Zd);   // < 30.001: inside the FP64 table
   double F[L + 1], h[L + 1];
-  boys_fn<L>(Td, tab64, F);
+  boys_taylor<L>(Td, tab64, F);
   double pw = 1.0;
 #pragma unroll
   for (int j = 0; j <= L; ++j) {
