@@ -421,7 +421,7 @@ __device__ __forceinline__ float pair_term32(const GPair32& g, const float (&D)[
 }
 
 // One pair's term at a point in FP64 throughout (FP64 coefficients): the far field from the
-// asymptotic Boys functions, the near field from the FP64 table.
+// asymptotic Boys functions, the near field from the FP64 table (boys_taylor).
 template <int L>
 __device__ __forceinline__ double pair_term64(double px, double py, double pz, double p, double fscale,
                                               const double (&D)[ncoef(L)], double cx, double cy, double cz,
@@ -437,7 +437,7 @@ __device__ __forceinline__ double pair_term64(double px, double py, double pz, d
     for (int j = 0; j < L; ++j) h[j + 1] = -(double)(2 * j + 1) * h[j] * ri2;
   } else {
     double F[L + 1];
-    boys_fn<L>(T, tab64, F);
+    boys_taylor<L>(T, tab64, F);
     double pw = 1.0;
 #pragma unroll
     for (int j = 0; j <= L; ++j) {
