@@ -978,12 +978,21 @@ __device__ __forceinline__ int atom_rows(const int4* sh_s, const float2* pr_s, c
       }
       if (!ok0) rA0 = rB0 = rC0 = 0.f;
       if (!ok1) rA1 = rB1 = rC1 = 0.f;
+      // the atom's five functions stored as one group (pairs across the shells' boundaries)
+      float g0[5], g1[5];
       shell_vals<0>(0, rA0, rA1, x0, y0, z0, x1, y1, z1, s_0, s_1);
-      out.put(f0, 1, s_0, s_1);
+      g0[0] = s_0[0];
+      g1[0] = s_1[0];
       shell_vals<0>(0, rB0, rB1, x0, y0, z0, x1, y1, z1, s_0, s_1);
-      out.put(f0 + 1, 1, s_0, s_1);
+      g0[1] = s_0[0];
+      g1[1] = s_1[0];
       shell_vals<1>(1, rC0, rC1, x0, y0, z0, x1, y1, z1, p_0, p_1);
-      out.put(f0 + 2, 3, p_0, p_1);
+#pragma unroll
+      for (int k = 0; k < 3; ++k) {
+        g0[2 + k] = p_0[k];
+        g1[2 + k] = p_1[k];
+      }
+      out.put(f0, 5, g0, g1);
       flast = f0 + 4;
     } else {
       float rB0, rB1;
@@ -1015,19 +1024,37 @@ __device__ __forceinline__ int atom_rows(const int4* sh_s, const float2* pr_s, c
       }
       if (!ok0) rA0 = rB0 = rC0 = rD0 = rE0 = rF0 = 0.f;
       if (!ok1) rA1 = rB1 = rC1 = rD1 = rE1 = rF1 = 0.f;
+      // the atom's fourteen functions stored as one group (pairs across the shells' boundaries)
+      float g0[14], g1[14];
       shell_vals<0>(0, rA0, rA1, x0, y0, z0, x1, y1, z1, s_0, s_1);
-      out.put(f0, 1, s_0, s_1);
+      g0[0] = s_0[0];
+      g1[0] = s_1[0];
       shell_vals<0>(0, rB0, rB1, x0, y0, z0, x1, y1, z1, s_0, s_1);
-      out.put(f0 + 1, 1, s_0, s_1);
+      g0[1] = s_0[0];
+      g1[1] = s_1[0];
       shell_vals<0>(0, rC0, rC1, x0, y0, z0, x1, y1, z1, s_0, s_1);
-      out.put(f0 + 2, 1, s_0, s_1);
+      g0[2] = s_0[0];
+      g1[2] = s_1[0];
       shell_vals<1>(1, rD0, rD1, x0, y0, z0, x1, y1, z1, p_0, p_1);
-      out.put(f0 + 3, 3, p_0, p_1);
+#pragma unroll
+      for (int k = 0; k < 3; ++k) {
+        g0[3 + k] = p_0[k];
+        g1[3 + k] = p_1[k];
+      }
       shell_vals<1>(1, rE0, rE1, x0, y0, z0, x1, y1, z1, p_0, p_1);
-      out.put(f0 + 6, 3, p_0, p_1);
+#pragma unroll
+      for (int k = 0; k < 3; ++k) {
+        g0[6 + k] = p_0[k];
+        g1[6 + k] = p_1[k];
+      }
       float d_0[5], d_1[5];
       shell_vals<2>(2, rF0, rF1, x0, y0, z0, x1, y1, z1, d_0, d_1);
-      out.put(f0 + 9, 5, d_0, d_1);
+#pragma unroll
+      for (int k = 0; k < 5; ++k) {
+        g0[9 + k] = d_0[k];
+        g1[9 + k] = d_1[k];
+      }
+      out.put(f0, 14, g0, g1);
       flast = f0 + 13;
     }
   }
