@@ -879,8 +879,37 @@ struct SwizzledRowsOut {
   int r0;
   bool two;
   int tail0;
+  // functions K0, K0 + 2, ... of a whole group (nf == NF) inside the swizzled chunks, from an even
+  // column j0 + K0 on: pairs, the last one alone when the count is odd
+  template <int K0, int NF>
+  __device__ __forceinline__ void put_pairs(int j0, const float (&v0)[NF], const float (&v1)[NF]) const {
+#pragma unroll
+    for (int k = K0; k < NF; k += 2) {
+      const uint32_t off = a_offset(r0, j0 + k, 1 << 30);
+      if (k + 1 < NF) {
+        store_pair16<FMT>(hi, lo, off, v0[k], v0[k + 1], two);
+        store_pair16<FMT>(hi, lo, off + 8192u, v1[k], v1[k + 1], two);
+      } else {
+        store_split16<FMT>(hi, lo, off, v0[k], two);
+        store_split16<FMT>(hi, lo, off + 8192u, v1[k], two);
+      }
+    }
+  }
   template <int NF>
   __device__ __forceinline__ void put(int j0, int nf, const float (&v0)[NF], const float (&v1)[NF]) const {
+    if (NF >= 5 && nf == NF && j0 + NF <= tail0) {
+      // a whole atom's group inside the swizzled chunks (uniform over the warp): the pairing is
+      // fixed by the parity of j0, with no per-function test
+      if (j0 & 1) {
+        const uint32_t off = a_offset(r0, j0, 1 << 30);
+        store_split16<FMT>(hi, lo, off, v0[0], two);
+        store_split16<FMT>(hi, lo, off + 8192u, v1[0], two);
+        put_pairs<1>(j0, v0, v1);
+      } else {
+        put_pairs<0>(j0, v0, v1);
+      }
+      return;
+    }
     bool skip = false;   // the function was stored with its predecessor
 #pragma unroll
     for (int k = 0; k < NF; ++k) {
